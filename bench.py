@@ -1,0 +1,369 @@
+"""Benchmark of the H.psi hot path on the 16-atom bcc workload (96^3 grid, 128 bands, FP64).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = one Kohn-Sham H.psi (FD8 kinetic + local potential + GTH
+Kleinman-Bylander nonlocal) over all 128 real Gamma-point bands of the
+2x2x2 bcc supercell (a = 12 bohr, h = 0.125 bohr, 16 atoms), seeded synthetic
+psi ~ U[-0.5, 0.5] (seed 2) and a seeded synthetic local potential.
+
+value  = algorithmic H.psi bytes / device time (GB/s), all ranks, inputs resident in HBM;
+         algorithmic bytes per apply = nb*N*(8 read + 8 write) + 8*N (V) + projector tables.
+e2e    = the same bytes / time of the public-API call with pinned HOST psi in and H.psi out
+         (host->device and device->host copies inside the timed region).
+N > 1  : each rank applies H to its own 128-band slice of a 128*N-band set (band
+         decomposition, no data-path collective): weak scaling.
+--impl reference: the reference's own CPU operators (oracle/_ref, compiled from the
+         reference source) on the host cores, bands split over processes as the
+         reference's state decomposition does; bounded sample per step.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "qumasun-workshop-template_b200")
+ORACLE = os.path.join(ROOT, "oracle")
+
+METRIC = "LOBPCG SCF wall-time to 1e-6 Ha/atom: mixed vs FP64 on B200; HBM GB/s of H·ψ"
+UNIT = "GB/s"
+NX = NY = NZ = 96
+H_GRID = 0.125
+NB = 128
+A_CELL = 6.0
+REPS = 2
+SEED = 2
+GTH = dict(nl=2, r=(0.40, 0.55), h=(5.0, 1.5))
+RCUT = 6.0
+
+
+def positions():
+    pos = []
+    for i in range(REPS):
+        for j in range(REPS):
+            for k in range(REPS):
+                base = np.array([i, j, k], float) * A_CELL
+                pos.append(base)
+                pos.append(base + 0.5 * A_CELL)
+    return np.array(pos)
+
+
+def potential(N):
+    rng = np.random.default_rng(SEED + 1000)
+    return rng.uniform(-1.0, 1.0, size=N)
+
+
+def algorithmic_bytes(nb, N, n_proj_points, wmax, elem=8):
+    return nb * N * 2 * elem + N * elem + n_proj_points * wmax * elem
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,utilization.gpu")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 10:
+                continue
+            try:
+                rows.append(dict(sm=float(parts[1]), smax=float(parts[2]), hw=parts[5], hwt=parts[6], swt=parts[7],
+                                 pcap=parts[8], util=float(parts[9])))
+            except ValueError:
+                continue
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        load = [r for r in rows if r["util"] > 0] or rows
+        reasons = set()
+        for r in load:
+            for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"), ("swt", "sw_thermal_slowdown"),
+                              ("pcap", "sw_power_cap")):
+                if r[key].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median([r["sm"] for r in load])), "sm_max_mhz": max(r["smax"] for r in rows),
+                "reasons": sorted(reasons), "samples": len(load)}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference arm (the reference's own operators, oracle/_ref)
+# ---------------------------------------------------------------------------
+def _ref_worker(args):
+    """Runs in a spawned process: H.psi on `count` bands with the reference's code."""
+    seed, count, reps = args
+    sys.path.insert(0, ORACLE)
+    import oracle as O
+    if O.ref_available():
+        O.ref_set_threads(1)
+    N = NX * NY * NZ
+    grid = (NX, NY, NZ, H_GRID, H_GRID, H_GRID)
+    V = potential(N)
+    rng = np.random.default_rng(seed)
+    psi = rng.uniform(-0.5, 0.5, size=(count, N))
+    sp = [dict(nl=GTH["nl"], r=GTH["r"], h=GTH["h"])] * (2 * REPS ** 3)
+    times = []
+    if O.ref_available():
+        cube = O.gth_cube_tables(positions(), sp, NX, NY, NZ, H_GRID, H_GRID, H_GRID, RCUT)
+        run = lambda: O.ref_hamiltonian(grid, V, cube, psi, count)
+    else:
+        tab = O.gth_tables(positions(), sp, H_GRID, H_GRID, H_GRID, RCUT)
+        run = lambda: O.hamiltonian(grid, V, tab, psi, count)
+    run()  # warm
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t0)
+    return times
+
+
+def cpu_kind():
+    sys.path.insert(0, ORACLE)
+    import oracle as O
+    return "reference" if O.ref_available() else "port"
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    N = NX * NY * NZ
+    bands_per_proc = 1
+    steps, warm = args.steps, args.warmup
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        t0 = time.perf_counter()
+        res = pool.map(_ref_worker, [(SEED + 17 * i, bands_per_proc, warm + steps) for i in range(cores)])
+        wall = time.perf_counter() - t0
+    # per step: every process applies H to its bands once; step time = slowest process
+    per_step = [max(r[warm + s] for r in res) for s in range(steps)]
+    t = float(np.mean(per_step))
+    nb = cores * bands_per_proc
+    sphere_pts = _sphere_points()
+    value = algorithmic_bytes(nb, N, sphere_pts, 4) / t / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+        "warmup": warm, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded psi U[-0.5,0.5], seeded potential, GTH projectors)",
+        "config": {"workload": "H.psi, bcc 2x2x2 supercell (16 atoms), 96^3 grid, FP64 real Gamma",
+                   "bands_per_step": nb, "grid": [NX, NY, NZ]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": cpu_kind(),
+                         "sample": f"{nb} of 128 bands per step, one band per process, {cores} spawned processes "
+                                   f"(state decomposition), 1 BLAS thread each; wall {wall:.1f} s"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def _sphere_points():
+    sys.path.insert(0, ORACLE)
+    import oracle as O
+    sp = [dict(nl=GTH["nl"], r=GTH["r"], h=GTH["h"])] * (2 * REPS ** 3)
+    tab = O.gth_tables(positions(), sp, H_GRID, H_GRID, H_GRID, RCUT)
+    return int(tab[0].sum())
+
+
+def cpu_baseline_sample():
+    """The reference (oracle/_ref) H.psi timed on the host on a bounded band sample."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(1) as pool:
+        t1 = pool.map(_ref_worker, [(SEED, 1, 1)])[0][0]
+    count = int(max(1, min(NB, math.floor(10.0 / max(t1, 1e-3)))))
+    with ctx.Pool(1) as pool:
+        t = pool.map(_ref_worker, [(SEED, count, 1)])[0][0]
+    N = NX * NY * NZ
+    value = algorithmic_bytes(count, N, _sphere_points(), 4) / t / 1e9
+    return {"value": value, "unit": UNIT, "cores": 1, "kind": cpu_kind(),
+            "sample": f"{count} of 128 bands of the same workload, one process, 1 thread, {t:.1f} s"}
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    assert args.warmup >= 3, "at least 3 warm-up steps"
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    sys.path.insert(0, PKG)
+    import qsb
+
+    N = NX * NY * NZ
+    H = qsb.Hamiltonian(NX, NY, NZ, H_GRID, H_GRID, H_GRID)
+    H.set_potential(potential(N))
+    pos = positions()
+    H.set_gth_projectors(pos, [0] * len(pos), [GTH["nl"]], [GTH["r"]], [GTH["h"]], RCUT)
+    n_pts, n_proj = H.projector_info()
+
+    gen = torch.Generator().manual_seed(SEED + 7919 * rank)
+    psi_host = (torch.rand(NB, N, dtype=torch.float64, generator=gen) - 0.5).pin_memory()
+    hpsi_host = torch.empty_like(psi_host).pin_memory()
+    psi = psi_host.cuda()
+    hpsi = torch.empty_like(psi)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        H.apply(psi, hpsi)
+    torch.cuda.synchronize()
+    H.get_timing()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+
+    # ---- device-resident timing -------------------------------------------------
+    H.set_timing(True)
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        H.apply(psi, hpsi)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    H.set_timing(False)
+    ms = e0.elapsed_time(e1) / args.steps
+    proj_ms, sten_ms, applies, launches = H.get_timing()
+    # keep the GPU busy long enough for the clock sampler to see the load
+    t_end = time.time() + 1.0
+    while time.time() < t_end:
+        for _ in range(20):
+            H.apply(psi, hpsi)
+        torch.cuda.synchronize()
+
+    # ---- end to end through the public API with host buffers -------------------
+    e2e_steps = max(3, min(args.steps, 10))
+    for _ in range(2):
+        psi.copy_(psi_host, non_blocking=True)
+        H.apply(psi, hpsi)
+        hpsi_host.copy_(hpsi, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(e2e_steps):
+        psi.copy_(psi_host, non_blocking=True)
+        H.apply(psi, hpsi)
+        hpsi_host.copy_(hpsi, non_blocking=True)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = f0.elapsed_time(f1) / e2e_steps
+    clk = clocks.stop()
+
+    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, e2e_ms = t.tolist()
+
+    alg = algorithmic_bytes(NB, N, n_pts, 4)
+    value = world * alg / (ms * 1e-3) / 1e9
+    e2e_value = world * alg / (e2e_ms * 1e-3) / 1e9
+    peak, peak_kind = load_peaks()
+    # dominant kernel: the fused stencil (FD8 + V + nonlocal expansion); its
+    # algorithmic bytes are psi read + Hpsi write + V + the grid-ordered projector table.
+    sten_avg_s = sten_ms / max(applies, 1) * 1e-3
+    sten_bytes = NB * N * 16 + N * 8 + n_pts * 4 * 8
+    achieved = sten_bytes / sten_avg_s / 1e9
+    traffic = None
+    tr_file = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tr_file):
+        traffic = json.load(open(tr_file)).get("fd8_kernel_bytes_per_launch")
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded psi U[-0.5,0.5], seeded potential, analytic GTH projectors)",
+        "config": {"workload": "H.psi, bcc 2x2x2 supercell (16 atoms, a=12 bohr), 96^3 grid (h=0.125), "
+                               "128 bands per GPU, FP64 real Gamma, FD8 + V + GTH s+p KB nonlocal",
+                   "grid": [NX, NY, NZ], "bands_per_gpu": NB, "atoms": len(pos), "projector_points": n_pts,
+                   "parallelism": f"band decomposition x{world}",
+                   "l2": "inputs larger than L2 (psi 906 MB per GPU)"},
+        "band_grid_points_per_s": world * NB * N / (ms * 1e-3),
+        "breakdown_ms": {"nonlocal_projection": proj_ms / max(applies, 1), "fused_stencil": sten_ms / max(applies, 1)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "fd8_kernel (FD8 + V + fused nonlocal pull)",
+                     "peak_source": f"{peak_kind} hbm_gbs"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": NB * N * 8, "d2h_bytes_per_step": NB * N * 8,
+                "ms_per_step": e2e_ms},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample()
+    if rank == 0:
+        print(json.dumps(line))
+    H.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

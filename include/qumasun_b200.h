@@ -1,0 +1,157 @@
+/*
+ * qumasun_b200.h — C ABI of the B200 (sm_100a) Kohn-Sham H.psi + LOBPCG path.
+ *
+ * Plain pointers and sizes only; every call returns a qsb_status and, on
+ * failure, qsb_last_error() describes it.  All array arguments named *_dev
+ * or documented as "device" are CUDA device pointers; "stream" is a
+ * cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * Layouts are the reference's own, so a caller's buffers pass through unchanged
+ * (source/qumasun_base1.h:457-460, source/soacomplex.h:4):
+ *   - grid index i = ix + nx*(iy + ny*iz), x fastest, periodic in x, y, z;
+ *   - real band bundle:    band b at  psi + b*N                    (N = nx*ny*nz);
+ *   - complex band bundle: band b re at psi + 2*b*N, im at psi + (2*b+1)*N  (SoA).
+ * dtype QSB_F64 means double arrays, QSB_F32 float arrays (same layouts).
+ *
+ * Reference interfaces each entry point replaces are cited as path:line
+ * within the reference project (atsushi-m-ito/QUMASUN-workshop-template).
+ */
+#ifndef QUMASUN_B200_H
+#define QUMASUN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define QSB_API __attribute__((visibility("default")))
+#else
+#define QSB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum qsb_status {
+    QSB_OK = 0,
+    QSB_ERR_INVALID = 1,   /* bad argument (size, pointer, dtype) */
+    QSB_ERR_CUDA = 2,      /* a CUDA runtime/library call failed */
+    QSB_ERR_NOMEM = 3,     /* device allocation failed */
+    QSB_ERR_STATE = 4,     /* call made on an incompletely set-up context */
+    QSB_ERR_SOLVER = 5,    /* small dense eigensolver / Cholesky failed */
+    QSB_ERR_NUMERIC = 6    /* non-finite values detected */
+} qsb_status;
+
+typedef enum qsb_dtype { QSB_F64 = 0, QSB_F32 = 1 } qsb_dtype;
+
+/* Text of the last error raised on the calling thread ("" if none). */
+QSB_API const char* qsb_last_error(void);
+/* Library version string. */
+QSB_API const char* qsb_version(void);
+
+/* ---------------------------------------------------------------------------
+ * FD8 stencils (stateless).
+ * ------------------------------------------------------------------------- */
+
+/* out += coef * Laplacian_8th(p) for nb real bands, periodic boundaries.
+ * Replaces Laplacian8th<T>(grid, out, p, coef, dx, dy, dz)
+ * (source/GridDifference8th.h:177-184; stencil :82-148, halo :19-78), applied
+ * band by band; same accumulate ("+=") semantics. */
+QSB_API qsb_status qsb_laplacian8th(qsb_dtype dtype, int nx, int ny, int nz, int nb,
+                            void* out_dev, const void* p_dev, double coef,
+                            double dx, double dy, double dz, void* stream);
+
+/* out += coef * (Laplacian + 2 i g.grad - |g|^2) src for nb complex SoA bands:
+ * out.re gets Lap_g(re) - D_g(im), out.im gets Lap_g(im) + D_g(re).
+ * Replaces LaplacianKpoint8th_ddm(grid, out, src, coef, dx, dy, dz, gx, gy, gz)
+ * (source/GridDifferenceKpoint8th.h:324-366, stencil :17-120) with
+ * split_dimension 0, including its |g_d| < 1e-8 dispatch; no static buffers. */
+QSB_API qsb_status qsb_laplacian_kpoint8th(qsb_dtype dtype, int nx, int ny, int nz, int nb,
+                                   void* out_dev, const void* src_dev, double coef,
+                                   double dx, double dy, double dz,
+                                   double gx, double gy, double gz, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Hamiltonian context: local potential + nonlocal KB projectors on one grid.
+ * Replaces the state QUMASUN_BASE1 / PseudoPotNonlocal_SvF2_kpoint hold for
+ * mHamiltonianMatrix_ddm (source/qumasun_base1.matrix.h:263-317).
+ * ------------------------------------------------------------------------- */
+typedef struct qsb_ham qsb_ham;
+
+QSB_API qsb_status qsb_ham_create(qsb_ham** ham, int nx, int ny, int nz, double dx, double dy, double dz);
+QSB_API qsb_status qsb_ham_destroy(qsb_ham* ham);
+
+/* V: N doubles (the total local potential Vtot), host (on_device = 0) or
+ * device (on_device = 1) memory.  Copied into the context (FP64 and FP32). */
+QSB_API qsb_status qsb_ham_set_potential(qsb_ham* ham, const double* V, int on_device);
+
+/* Nonlocal Kleinman-Bylander projectors, host arrays, copied into the context.
+ * Replaces PseudoPotNonlocal_SvF2_kpoint::UpdatePosition's products
+ * (source/PseudoPotNonlocal_SvF2_kpoint.h:3315-3406): per atom a point list
+ * and a projector table, like PP_Proj_Ylm_each_atom::projector_RY (:216-236).
+ *   npts[a]    points of atom a (any shape: voxel sphere or the reference's cube blocks)
+ *   widths[a]  projectors of atom a (sum of 2l+1 over channels; 0 allowed)
+ *   coords     3 ints per point, UNFOLDED grid coordinates (may lie outside
+ *              [0,n)); the point acts on grid point (coords mod n) and its Bloch
+ *              phase is exp(i g.(ix*dx, iy*dy, iz*dz)) as in mCreateBlochExp (:3538-3605)
+ *   beta       per atom npts[a] x widths[a] values, column-major (point fastest)
+ *   energy     per atom widths[a] KB energies E_w (projector_energy_RY, :151)
+ * Arrays are concatenated over atoms in atom order. */
+QSB_API qsb_status qsb_ham_set_projectors(qsb_ham* ham, int n_atoms, const int* npts, const int* widths,
+                                  const int* coords, const double* beta, const double* energy);
+
+/* Same, building analytic GTH (Goedecker-Teter-Hutter) projectors with one
+ * radial function per channel (l = 0: 1 projector, l = 1: 3 projectors with
+ * real harmonics x, y, z) on voxel spheres of radius rcut_factor*r_l.
+ *   pos[3a..]    atom positions in bohr (any real value; folded periodically)
+ *   species[a]   index into the species tables
+ *   nl[s]        channels of species s (0, 1 or 2)
+ *   r_l[2s+l], h_l[2s+l]   GTH radius and h^l_11 of channel l of species s */
+QSB_API qsb_status qsb_ham_set_gth_projectors(qsb_ham* ham, int n_atoms, const double* pos, const int* species,
+                                      int n_species, const int* nl, const double* r_l, const double* h_l,
+                                      double rcut_factor);
+
+/* Number of projector points held (sum over atoms), and total projectors. */
+QSB_API qsb_status qsb_ham_projector_info(const qsb_ham* ham, int64_t* total_points, int* total_projectors);
+
+/* hpsi = V psi + V_NL psi - 1/2 Laplacian_8th(psi)   ("=" semantics)
+ * is_complex = 0: nb real bands, Gamma point (g ignored).
+ * is_complex = 1: nb complex SoA bands at Bloch vector g (bohr^-1), with the
+ *                 k-point kinetic operator of LaplacianKpoint8th_ddm and the
+ *                 Bloch-phased projectors of ProjectionPP_bundle.
+ * Replaces mHamiltonianMatrix_ddm (source/qumasun_base1.matrix.h:263-291):
+ * SetZero, mPotentialMatrix_ddm, ProjectionPP_bundle, mKineticMatrixAdd_ddm_kpint. */
+QSB_API qsb_status qsb_ham_apply(qsb_ham* ham, qsb_dtype dtype, int is_complex, int nb,
+                         const void* psi_dev, void* hpsi_dev,
+                         double gx, double gy, double gz, void* stream);
+
+/* hpsi += V_NL psi.  Replaces PseudoPotNonlocal_SvF2_kpoint::ProjectionPP_bundle
+ * (source/PseudoPotNonlocal_SvF2_kpoint.h:4239-4247, CPU :3911-4046, GPU :4053-4236). */
+QSB_API qsb_status qsb_ham_nonlocal_apply(qsb_ham* ham, qsb_dtype dtype, int is_complex, int nb,
+                                  const void* psi_dev, void* hpsi_dev,
+                                  double gx, double gy, double gz, void* stream);
+
+/* <beta_aw | psi_c> * dV for every projector and column into out_host
+ * (double, layout [column][projector], projectors in atom order, columns:
+ * real -> band b; complex -> 2b (re), 2b+1 (im)), the quantity
+ * mInnerNonlocalPsi_v4_bundle computes (source/PseudoPotNonlocal_SvF2_kpoint.h:4463-4576;
+ * index layout there is per atom, here global). */
+QSB_API qsb_status qsb_ham_nonlocal_project(qsb_ham* ham, qsb_dtype dtype, int is_complex, int nb,
+                                    const void* psi_dev, double gx, double gy, double gz,
+                                    double* out_host, void* stream);
+
+/* Per-kernel device timing of qsb_ham_apply, in the spirit of the reference's
+ * StopWatch sectors (source/StopWatch.h:11-60, watch_pp in
+ * source/PseudoPotNonlocal_SvF2_kpoint.h:261-272).  While enabled, every
+ * qsb_ham_apply records CUDA events on its stream around the nonlocal
+ * projection kernels and the fused stencil kernel.  qsb_ham_get_timing
+ * synchronizes those events, returns the summed milliseconds and the number of
+ * applies since the last call, and resets the counters. */
+QSB_API qsb_status qsb_ham_set_timing(qsb_ham* ham, int enable);
+QSB_API qsb_status qsb_ham_get_timing(qsb_ham* ham, double* project_ms, double* stencil_ms, int* applies,
+                                      int* kernel_launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QUMASUN_B200_H */

@@ -1,0 +1,313 @@
+"""Test oracle for the H.psi hot path — TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
+arm may import this module; the product (libqumasun_b200.so and its binding)
+never does.
+
+It wraps two CPU libraries built by oracle/Makefile:
+  * oracle/_build/libqsoracle.so — the C restatement (oracle/qsoracle.c);
+  * oracle/_ref/libqsref.so      — the REFERENCE's own headers compiled from its
+    source tree (oracle/ref_entry.cpp); present only where it was built.
+and restates in numpy the analytic GTH projector tables (the reference has no
+GTH support; the published GTH form is restated, see gth_tables) and the
+seeded synthetic inputs.
+"""
+import ctypes
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_ORACLE = os.path.join(HERE, "_build", "libqsoracle.so")
+LIB_REF = os.path.join(HERE, "_ref", "libqsref.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip)
+
+
+_oracle = None
+_ref = None
+
+
+def oracle_lib():
+    """The C restatement (built on demand with make if missing)."""
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(LIB_ORACLE):
+            import subprocess
+            subprocess.run(["make", "-s", "-C", HERE], check=True)
+        _oracle = ctypes.CDLL(LIB_ORACLE)
+    return _oracle
+
+
+def ref_available():
+    return os.path.exists(LIB_REF)
+
+
+def ref_lib():
+    """The reference's own code (oracle/_ref/libqsref.so)."""
+    global _ref
+    if _ref is None:
+        _ref = ctypes.CDLL(LIB_REF)
+        _ref.qsref_lobpcg_z_work_doubles.restype = ctypes.c_size_t
+    return _ref
+
+
+# --------------------------------------------------------------------------
+# configurations (BASELINE workloads), seeded inputs
+# --------------------------------------------------------------------------
+# GTH parameters used by the bcc cells (Z_ion = 6 element) and the water
+# molecule (O, H); r_l / h_l per channel, channels s (l=0) and p (l=1).
+GTH_BCC = dict(zion=6.0, rloc=0.45, c1=-4.0, c2=0.6, nl=2, r=(0.40, 0.55), h=(5.0, 1.5))
+GTH_O = dict(zion=6.0, rloc=0.247, c1=-16.58, c2=2.40, nl=1, r=(0.222, 0.0), h=(18.27, 0.0))
+GTH_H = dict(zion=1.0, rloc=0.2, c1=-4.18, c2=0.725, nl=0, r=(0.0, 0.0), h=(0.0, 0.0))
+RCUT_FACTOR = 6.0
+
+
+def bcc_positions(a, reps, jitter=0.0, seed=None):
+    """bcc lattice of edge a (bohr) repeated reps^3 times; optional N(0, jitter) displacements."""
+    pos = []
+    for i in range(reps):
+        for j in range(reps):
+            for k in range(reps):
+                base = np.array([i, j, k], dtype=float) * a
+                pos.append(base)
+                pos.append(base + 0.5 * a)
+    pos = np.array(pos)
+    if jitter > 0.0:
+        rng = np.random.default_rng(seed)
+        pos = pos + rng.normal(0.0, jitter, size=pos.shape)
+    return pos
+
+
+def gth_tables(pos, species_params, dx, dy, dz, rcut_factor=RCUT_FACTOR):
+    """Voxel-sphere GTH projector tables in the C ABI's point-list format.
+
+    Restates the GTH separable projector of one radial function per channel
+    (Goedecker-Teter-Hutter PRB 54, 1703 (1996); HGH PRB 58, 3641 (1998)):
+      p_l(r) = sqrt(2) r^l exp(-r^2/(2 r_l^2)) / (r_l^(l+3/2) sqrt(Gamma(l+3/2)))
+    times real harmonics Y00 = 1/sqrt(4 pi), Y1 = sqrt(3/(4 pi)) (x, y, z)/r,
+    zero beyond rcut_factor * r_l, on the points with |r - R| <= max_l rcut.
+    Returns (npts, widths, coords, beta, energy) as numpy arrays.
+    """
+    npts, widths, coords, beta, energy = [], [], [], [], []
+    for R, sp in zip(pos, species_params):
+        nl = sp["nl"]
+        w = (1 if nl >= 1 else 0) + (3 if nl >= 2 else 0)
+        if w == 0:
+            npts.append(0)
+            widths.append(0)
+            continue
+        rl = sp["r"]
+        rmax = max(rcut_factor * rl[l] for l in range(nl))
+        ix = np.arange(math.floor((R[0] - rmax) / dx), math.ceil((R[0] + rmax) / dx) + 1)
+        iy = np.arange(math.floor((R[1] - rmax) / dy), math.ceil((R[1] + rmax) / dy) + 1)
+        iz = np.arange(math.floor((R[2] - rmax) / dz), math.ceil((R[2] + rmax) / dz) + 1)
+        Z, Y, X = np.meshgrid(iz, iy, ix, indexing="ij")
+        X = X.ravel(); Y = Y.ravel(); Z = Z.ravel()
+        x = X * dx - R[0]; y = Y * dy - R[1]; z = Z * dz - R[2]
+        r2 = x * x + y * y + z * z
+        keep = r2 <= rmax * rmax
+        X, Y, Z, x, y, z, r2 = X[keep], Y[keep], Z[keep], x[keep], y[keep], z[keep], r2[keep]
+        r = np.sqrt(r2)
+        cols = []
+        pre0 = math.sqrt(2.0) / (rl[0] ** 1.5 * math.sqrt(math.sqrt(math.pi) / 2.0)) / math.sqrt(4.0 * math.pi)
+        cols.append(np.where(r <= rcut_factor * rl[0], pre0 * np.exp(-r2 / (2.0 * rl[0] ** 2)), 0.0))
+        en = [sp["h"][0]]
+        if nl >= 2:
+            pre1 = (math.sqrt(2.0) / (rl[1] ** 2.5 * math.sqrt(3.0 * math.sqrt(math.pi) / 4.0))
+                    * math.sqrt(3.0 / (4.0 * math.pi)))
+            e1 = np.where(r <= rcut_factor * rl[1], pre1 * np.exp(-r2 / (2.0 * rl[1] ** 2)), 0.0)
+            cols += [e1 * x, e1 * y, e1 * z]
+            en += [sp["h"][1]] * 3
+        npts.append(len(X))
+        widths.append(w)
+        coords.append(np.stack([X, Y, Z], axis=1).astype(np.int32).ravel())
+        beta.append(np.concatenate(cols))
+        energy += en
+    cat = lambda L, dt: np.ascontiguousarray(np.concatenate(L).astype(dt)) if L else np.zeros(0, dt)
+    return (np.array(npts, np.int32), np.array(widths, np.int32), cat(coords, np.int32), cat(beta, np.float64),
+            np.array(energy, np.float64))
+
+
+def gth_cube_tables(pos, species_params, nx, ny, nz, dx, dy, dz, rcut_factor=RCUT_FACTOR):
+    """The same projectors on the reference's CUBE subgrid blocks (GetOverlapPeriodic,
+    source/GridSubgrid.h:690-740), for the reference-side nonlocal.  Returns
+    (cubes[6 per atom], widths, proj (block layout, column-major per atom), energy,
+    point-list form (npts, coords) of the same blocks)."""
+    lib = ref_lib()
+    cubes, widths, proj, energy, npts, coords = [], [], [], [], [], []
+    blocks_buf = np.zeros(9 * 4096, np.int32)
+    gsz = ctypes.c_int(0)
+    for R, sp in zip(pos, species_params):
+        nl = sp["nl"]
+        w = (1 if nl >= 1 else 0) + (3 if nl >= 2 else 0)
+        rl = sp["r"]
+        rmax = max([rcut_factor * rl[l] for l in range(nl)] + [0.0])
+        b = [math.floor((R[0] - rmax) / dx), math.floor((R[1] - rmax) / dy), math.floor((R[2] - rmax) / dz)]
+        e = [math.ceil((R[0] + rmax) / dx) + 1, math.ceil((R[1] + rmax) / dy) + 1, math.ceil((R[2] + rmax) / dz) + 1]
+        cube = np.array(b + e, np.int32)
+        cubes.append(cube)
+        nbk = lib.qsref_overlap_blocks(nx, ny, nz, _i(cube), _i(blocks_buf), 4096, ctypes.byref(gsz))
+        assert nbk <= 4096
+        pts = []
+        for k in range(nbk):
+            bx0, by0, bz0, bx1, by1, bz1, sx, sy, sz = blocks_buf[9 * k: 9 * k + 9]
+            zz, yy, xx = np.meshgrid(np.arange(bz0, bz1), np.arange(by0, by1), np.arange(bx0, bx1), indexing="ij")
+            pts.append(np.stack([xx.ravel() - sx, yy.ravel() - sy, zz.ravel() - sz], axis=1))
+        P = np.concatenate(pts) if pts else np.zeros((0, 3), np.int64)
+        assert len(P) == gsz.value
+        x = P[:, 0] * dx - R[0]; y = P[:, 1] * dy - R[1]; z = P[:, 2] * dz - R[2]
+        r2 = x * x + y * y + z * z
+        r = np.sqrt(r2)
+        cols = []
+        if nl >= 1:
+            pre0 = math.sqrt(2.0) / (rl[0] ** 1.5 * math.sqrt(math.sqrt(math.pi) / 2.0)) / math.sqrt(4.0 * math.pi)
+            cols.append(np.where(r <= rcut_factor * rl[0], pre0 * np.exp(-r2 / (2.0 * rl[0] ** 2)), 0.0))
+            energy.append(sp["h"][0])
+        if nl >= 2:
+            pre1 = (math.sqrt(2.0) / (rl[1] ** 2.5 * math.sqrt(3.0 * math.sqrt(math.pi) / 4.0))
+                    * math.sqrt(3.0 / (4.0 * math.pi)))
+            e1 = np.where(r <= rcut_factor * rl[1], pre1 * np.exp(-r2 / (2.0 * rl[1] ** 2)), 0.0)
+            cols += [e1 * x, e1 * y, e1 * z]
+            energy += [sp["h"][1]] * 3
+        widths.append(w)
+        if w:
+            proj.append(np.concatenate(cols))
+        npts.append(len(P))
+        coords.append(P.astype(np.int32).ravel())
+    cat = lambda L, dt: np.ascontiguousarray(np.concatenate(L).astype(dt)) if L else np.zeros(0, dt)
+    return dict(cubes=cat(cubes, np.int32), widths=np.array(widths, np.int32), proj=cat(proj, np.float64),
+                energy=np.array(energy, np.float64), npts=np.array(npts, np.int32), coords=cat(coords, np.int32))
+
+
+def seeded_psi(seed, nb, N, complex_=False, dtype=np.float64):
+    """psi ~ U[-0.5, 0.5] from numpy PCG64(seed), layout of the reference bundle."""
+    rng = np.random.default_rng(seed)
+    return rng.uniform(-0.5, 0.5, size=(nb * (2 if complex_ else 1), N)).astype(dtype)
+
+
+def seeded_potential(seed, N, scale=1.0):
+    rng = np.random.default_rng(seed + 1000)
+    return rng.uniform(-scale, scale, size=N)
+
+
+# --------------------------------------------------------------------------
+# C restatement wrappers
+# --------------------------------------------------------------------------
+def laplacian8th(nx, ny, nz, out, p, coef, dx, dy, dz):
+    """out += coef * FD8 Laplacian(p) for every band row of p (restatement)."""
+    lib = oracle_lib()
+    N = nx * ny * nz
+    p = np.ascontiguousarray(p, np.float64).reshape(-1, N)
+    assert out.dtype == np.float64 and out.flags.c_contiguous
+    o = out.reshape(-1, N)
+    for b in range(p.shape[0]):
+        lib.qso_laplacian8th(nx, ny, nz, _d(o[b]), _d(p[b]), ctypes.c_double(coef), ctypes.c_double(dx),
+                             ctypes.c_double(dy), ctypes.c_double(dz))
+    return out
+
+
+def laplacian_kpoint8th(nx, ny, nz, out, src, coef, dx, dy, dz, g):
+    lib = oracle_lib()
+    N = nx * ny * nz
+    s = np.ascontiguousarray(src, np.float64).reshape(-1, 2, N)
+    o = out.reshape(-1, 2, N)
+    for b in range(s.shape[0]):
+        lib.qso_laplacian_kpoint8th(nx, ny, nz, _d(o[b, 0]), _d(o[b, 1]), _d(s[b, 0]), _d(s[b, 1]),
+                                    *[ctypes.c_double(v) for v in (coef, dx, dy, dz, g[0], g[1], g[2])])
+    return out
+
+
+def hamiltonian(grid, V, tables, psi, nb, is_complex=False, g=(0.0, 0.0, 0.0)):
+    """H psi (restatement of mHamiltonianMatrix_ddm), FP64."""
+    lib = oracle_lib()
+    nx, ny, nz, dx, dy, dz = grid
+    npts, widths, coords, beta, energy = tables
+    psi = np.ascontiguousarray(psi, np.float64)
+    hp = np.zeros_like(psi)
+    V = np.ascontiguousarray(V, np.float64)
+    lib.qso_hamiltonian(nx, ny, nz, *[ctypes.c_double(v) for v in (dx, dy, dz)], _d(V), len(npts), _i(npts),
+                        _i(widths), _i(coords), _d(beta), _d(energy), nb, int(is_complex), _d(hp), _d(psi),
+                        *[ctypes.c_double(v) for v in g])
+    return hp
+
+
+def nonlocal_apply(grid, tables, psi, nb, is_complex=False, g=(0.0, 0.0, 0.0), hp=None):
+    lib = oracle_lib()
+    nx, ny, nz, dx, dy, dz = grid
+    npts, widths, coords, beta, energy = tables
+    psi = np.ascontiguousarray(psi, np.float64)
+    if hp is None:
+        hp = np.zeros_like(psi)
+    lib.qso_nonlocal_apply(nx, ny, nz, *[ctypes.c_double(v) for v in (dx, dy, dz)], len(npts), _i(npts), _i(widths),
+                           _i(coords), _d(beta), _d(energy), nb, int(is_complex), _d(hp), _d(psi),
+                           *[ctypes.c_double(v) for v in g])
+    return hp
+
+
+def nonlocal_project(grid, tables, psi, nb, is_complex=False, g=(0.0, 0.0, 0.0)):
+    lib = oracle_lib()
+    nx, ny, nz, dx, dy, dz = grid
+    npts, widths, coords, beta, energy = tables
+    P = int(widths.sum())
+    ncol = 2 * nb if is_complex else nb
+    out = np.zeros((ncol, P))
+    psi = np.ascontiguousarray(psi, np.float64)
+    lib.qso_nonlocal_project(nx, ny, nz, *[ctypes.c_double(v) for v in (dx, dy, dz)], len(npts), _i(npts),
+                             _i(widths), _i(coords), _d(beta), nb, int(is_complex), _d(psi),
+                             *[ctypes.c_double(v) for v in g], _d(out))
+    return out
+
+
+# --------------------------------------------------------------------------
+# the reference's own code (oracle/_ref)
+# --------------------------------------------------------------------------
+def ref_laplacian8th(nx, ny, nz, out, p, coef, dx, dy, dz):
+    lib = ref_lib()
+    N = nx * ny * nz
+    p = np.ascontiguousarray(p, np.float64).reshape(-1, N)
+    o = out.reshape(-1, N)
+    for b in range(p.shape[0]):
+        lib.qsref_laplacian8th(nx, ny, nz, _d(o[b]), _d(p[b]), *[ctypes.c_double(v) for v in (coef, dx, dy, dz)])
+    return out
+
+
+def ref_laplacian_kpoint8th(nx, ny, nz, out, src, coef, dx, dy, dz, g):
+    lib = ref_lib()
+    N = nx * ny * nz
+    s = np.ascontiguousarray(src, np.float64).reshape(-1, 2, N)
+    o = out.reshape(-1, 2, N)
+    for b in range(s.shape[0]):
+        lib.qsref_laplacian_kpoint8th(nx, ny, nz, _d(o[b, 0]), _d(o[b, 1]), _d(s[b, 0]), _d(s[b, 1]),
+                                      *[ctypes.c_double(v) for v in (coef, dx, dy, dz, g[0], g[1], g[2])])
+    return out
+
+
+def ref_hamiltonian(grid, V, cube, psi, nb, is_complex=False, g=(0.0, 0.0, 0.0)):
+    """H psi by the reference's own operators (mHamiltonianMatrix_ddm composition)."""
+    lib = ref_lib()
+    nx, ny, nz, dx, dy, dz = grid
+    psi = np.ascontiguousarray(psi, np.float64)
+    hp = np.zeros_like(psi)
+    V = np.ascontiguousarray(V, np.float64)
+    args = [nx, ny, nz, *[ctypes.c_double(v) for v in (dx, dy, dz)], _d(V), len(cube["widths"]), _i(cube["cubes"]),
+            _i(cube["widths"]), _d(cube["proj"]), _d(cube["energy"]), nb, _d(hp), _d(psi)]
+    if is_complex:
+        lib.qsref_hamiltonian_complex(*args, *[ctypes.c_double(v) for v in g])
+    else:
+        lib.qsref_hamiltonian_real(*args)
+    return hp
+
+
+def ref_set_threads(n):
+    ref_lib().qsref_set_threads(int(n))

@@ -1,0 +1,428 @@
+// Nonlocal Kleinman-Bylander projector apply for sm_100a.
+//
+//   Hpsi_c += sum_a sum_w |beta_aw> E_w dV <beta_aw | psi_c>
+//
+// The order of operations is the reference's ProjectionPP_bundle_1 /
+// mInnerNonlocalPsi_v4_bundle (source/PseudoPotNonlocal_SvF2_kpoint.h:3911-4046,
+// :4463-4576): gather psi on each atom's points, multiply by exp(+i k.r) (k != 0),
+// contract with the projector table (DGEMM_t, times dV), scale by E_w, expand
+// (DGEMM_n), multiply by exp(-i k.r), scatter-add.
+//
+// B200 layout: the projector points are held twice.
+//  * atom-major ("gather") order, cut into chunks of one atom's points, for the
+//    projection.  Each CTA reduces one chunk for a group of bands in registers
+//    and shared memory and writes one partial sum per (chunk, w, column); a
+//    second tiny kernel sums the chunks of each atom in a fixed order, so the
+//    result is deterministic (no floating-point atomics).
+//  * grid-ordered CSR (entries of grid point g are [grid_ptr[g], grid_ptr[g+1]))
+//    for the expansion, done as a PULL: each output point sums its own entries.
+//    Overlapping spheres (different atoms, or an atom and its own periodic
+//    images) therefore need no atomics and no non-overlap grouping
+//    (mCreateNonoverlapList, :3410-3487), and the pull can be fused into the H
+//    stencil so Hpsi is written once.
+#include "qsb_internal.h"
+#include <algorithm>
+#include <numeric>
+#include <cstring>
+
+namespace qsb {
+
+namespace {
+
+constexpr int PROJ_THREADS = 256;
+constexpr int CHUNK = 2048;          // points per projection chunk
+constexpr int APPLY_THREADS = 256;
+
+template <typename T>
+void dfree(T*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+template <typename T>
+qsb_status dupload(T*& dst, const T* src, size_t n) {
+    dfree(dst);
+    if (n == 0) return QSB_OK;
+    cudaError_t e = cudaMalloc((void**)&dst, n * sizeof(T));
+    if (e != cudaSuccess) { dst = nullptr; return fail(QSB_ERR_NOMEM, "nonlocal tables: cudaMalloc failed"); }
+    QSB_CUDA_TRY(cudaMemcpy(dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+    return QSB_OK;
+}
+
+inline int fold(int v, int n) {
+    int m = v % n;
+    return m < 0 ? m + n : m;
+}
+
+// ---------------------------------------------------------------------------
+// projection: partial[chunk][w][col] = sum_{p in chunk} beta[p][w] * phi_col[idx_p]
+// phi = psi (real) or psi*exp(+i k.r) (complex; columns 2b = re, 2b+1 = im)
+// ---------------------------------------------------------------------------
+template <typename T, bool CPLX, int WM, int CB>
+__global__ void __launch_bounds__(PROJ_THREADS)
+nl_proj_kernel(const int* __restrict__ chunk_begin, const int* __restrict__ chunk_end,
+               const int* __restrict__ pt_idx, const int* __restrict__ pt_xyz, const T* __restrict__ pt_beta,
+               int wmax, const T* __restrict__ psi, size_t N, int nb, double gx_dx, double gy_dy, double gz_dz,
+               double* __restrict__ partial, int ncol) {
+    constexpr int NCB = CPLX ? 2 * CB : CB;
+    constexpr int NV = WM * NCB;
+    const int chunk = blockIdx.x;
+    const int band0 = blockIdx.y * CB;
+    const int nbl = min(CB, nb - band0);
+    const int p0 = chunk_begin[chunk], p1 = chunk_end[chunk];
+
+    double acc[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) acc[i] = 0.0;
+
+    for (int p = p0 + threadIdx.x; p < p1; p += PROJ_THREADS) {
+        const int idx = __ldg(pt_idx + p);
+        double b[WM];
+#pragma unroll
+        for (int w = 0; w < WM; ++w) b[w] = (w < wmax) ? (double)__ldg(pt_beta + (size_t)p * wmax + w) : 0.0;
+        double cs = 1.0, sn = 0.0;
+        if (CPLX) {
+            // mCreateBlochExp (source/PseudoPotNonlocal_SvF2_kpoint.h:3580-3590)
+            const double kxx = gx_dx * (double)__ldg(pt_xyz + 3 * (size_t)p + 0);
+            const double kyy = gy_dy * (double)__ldg(pt_xyz + 3 * (size_t)p + 1);
+            const double kzz = gz_dz * (double)__ldg(pt_xyz + 3 * (size_t)p + 2);
+            sincos(kxx + kyy + kzz, &sn, &cs);
+        }
+#pragma unroll
+        for (int j = 0; j < CB; ++j) {
+            if (j < nbl) {
+                if (CPLX) {
+                    const size_t base = (size_t)(2 * (band0 + j)) * N;
+                    const double pr = (double)__ldg(psi + base + idx);
+                    const double pi = (double)__ldg(psi + base + N + idx);
+                    const double fr = cs * pr - sn * pi;   // :4514-4515
+                    const double fi = cs * pi + sn * pr;
+#pragma unroll
+                    for (int w = 0; w < WM; ++w) {
+                        acc[w * NCB + 2 * j] += b[w] * fr;
+                        acc[w * NCB + 2 * j + 1] += b[w] * fi;
+                    }
+                } else {
+                    const double v = (double)__ldg(psi + (size_t)(band0 + j) * N + idx);
+#pragma unroll
+                    for (int w = 0; w < WM; ++w) acc[w * NCB + j] += b[w] * v;
+                }
+            }
+        }
+    }
+
+    __shared__ double red[PROJ_THREADS / 32][NV];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+        double v = acc[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][i] = v;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < NV; i += PROJ_THREADS) {
+        const int w = i / NCB, jc = i % NCB;
+        if (w >= wmax) continue;
+        const int col = (CPLX ? 2 * band0 : band0) + jc;
+        if (jc >= (CPLX ? 2 * nbl : nbl)) continue;
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < PROJ_THREADS / 32; ++k) s += red[k][i];
+        partial[((size_t)chunk * wmax + w) * ncol + col] = s;
+    }
+}
+
+// coef[a][w][col] = dV * (E_w) * sum_{chunks of a} partial
+__global__ void nl_finalize_kernel(const int* __restrict__ atom_chunk_begin, const int* __restrict__ atom_chunk_end,
+                                   const double* __restrict__ atom_E, const int* __restrict__ atom_width, int wmax,
+                                   const double* __restrict__ partial, int ncol, double dV, int inner_only,
+                                   double* __restrict__ coef) {
+    const int a = blockIdx.x;
+    const int c0 = atom_chunk_begin[a], c1 = atom_chunk_end[a];
+    const int wa = atom_width[a];
+    for (int i = threadIdx.x; i < wmax * ncol; i += blockDim.x) {
+        const int w = i / ncol, col = i % ncol;
+        double s = 0.0;
+        if (w < wa)
+            for (int ch = c0; ch < c1; ++ch) s += partial[((size_t)ch * wmax + w) * ncol + col];
+        const double e = inner_only ? 1.0 : atom_E[(size_t)a * wmax + w];
+        coef[((size_t)a * wmax + w) * ncol + col] = (w < wa) ? (s * dV) * e : 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// separate pull apply over covered grid points: hpsi += sum_e beta_e . coef
+// ---------------------------------------------------------------------------
+template <typename T, bool CPLX, int CB>
+__global__ void __launch_bounds__(APPLY_THREADS)
+nl_apply_kernel(const int* __restrict__ cov_grid, int n_cov, const int* __restrict__ grid_ptr,
+                const int* __restrict__ ent_atom, const int* __restrict__ ent_xyz, const T* __restrict__ ent_beta,
+                int wmax, const double* __restrict__ coef, int ncol, T* __restrict__ hpsi, size_t N, int nb,
+                double gx_dx, double gy_dy, double gz_dz) {
+    const int r = blockIdx.x * APPLY_THREADS + threadIdx.x;
+    if (r >= n_cov) return;
+    const int band0 = blockIdx.y * CB;
+    const int nbl = min(CB, nb - band0);
+    const int g = __ldg(cov_grid + r);
+    const int e0 = __ldg(grid_ptr + g), e1 = __ldg(grid_ptr + g + 1);
+    constexpr int NCB = CPLX ? 2 * CB : CB;
+    double acc[NCB];
+#pragma unroll
+    for (int i = 0; i < NCB; ++i) acc[i] = 0.0;
+    for (int e = e0; e < e1; ++e) {
+        const int a = __ldg(ent_atom + e);
+        const double* cf = coef + (size_t)a * wmax * ncol;
+        double cs = 1.0, sn = 0.0;
+        if (CPLX) {
+            const double kxx = gx_dx * (double)__ldg(ent_xyz + 3 * (size_t)e + 0);
+            const double kyy = gy_dy * (double)__ldg(ent_xyz + 3 * (size_t)e + 1);
+            const double kzz = gz_dz * (double)__ldg(ent_xyz + 3 * (size_t)e + 2);
+            sincos(kxx + kyy + kzz, &sn, &cs);
+        }
+#pragma unroll
+        for (int j = 0; j < CB; ++j) {
+            if (j < nbl) {
+                double tr = 0.0, ti = 0.0;
+                for (int w = 0; w < wmax; ++w) {
+                    const double b = (double)__ldg(ent_beta + (size_t)e * wmax + w);
+                    if (CPLX) {
+                        tr += b * __ldg(cf + (size_t)w * ncol + 2 * (band0 + j));
+                        ti += b * __ldg(cf + (size_t)w * ncol + 2 * (band0 + j) + 1);
+                    } else {
+                        tr += b * __ldg(cf + (size_t)w * ncol + band0 + j);
+                    }
+                }
+                if (CPLX) {
+                    // exp(-i k.r) (source/PseudoPotNonlocal_SvF2_kpoint.h:4026-4027)
+                    acc[2 * j] += cs * tr + sn * ti;
+                    acc[2 * j + 1] += cs * ti - sn * tr;
+                } else {
+                    acc[j] += tr;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < CB; ++j) {
+        if (j < nbl) {
+            if (CPLX) {
+                const size_t base = (size_t)(2 * (band0 + j)) * N;
+                hpsi[base + g] += (T)acc[2 * j];
+                hpsi[base + N + g] += (T)acc[2 * j + 1];
+            } else {
+                hpsi[(size_t)(band0 + j) * N + g] += (T)acc[j];
+            }
+        }
+    }
+}
+
+template <typename T, bool CPLX, int WM>
+void launch_proj(const NLDevice& d, int nb, const void* psi, size_t N, double gx_dx, double gy_dy, double gz_dz,
+                 double* partial, int ncol, cudaStream_t s) {
+    constexpr int CB = CPLX ? 4 : 8;
+    dim3 grid(d.n_chunks, (nb + CB - 1) / CB);
+    const T* beta = std::is_same<T, double>::value ? (const T*)d.pt_beta64 : (const T*)d.pt_beta32;
+    nl_proj_kernel<T, CPLX, WM, CB><<<grid, PROJ_THREADS, 0, s>>>(d.chunk_begin, d.chunk_end, d.pt_idx, d.pt_xyz, beta,
+                                                                  d.wmax, (const T*)psi, N, nb, gx_dx, gy_dy, gz_dz,
+                                                                  partial, ncol);
+}
+
+template <typename T, bool CPLX>
+void launch_proj_w(const NLDevice& d, int nb, const void* psi, size_t N, double gx_dx, double gy_dy, double gz_dz,
+                   double* partial, int ncol, cudaStream_t s) {
+    if (d.wmax <= 1) launch_proj<T, CPLX, 1>(d, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+    else if (d.wmax <= 4) launch_proj<T, CPLX, 4>(d, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+    else if (d.wmax <= 9) launch_proj<T, CPLX, 9>(d, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+    else launch_proj<T, CPLX, 16>(d, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+}
+
+}  // namespace
+
+void nl_free(NLDevice& d) {
+    dfree(d.pt_idx); dfree(d.pt_xyz); dfree(d.pt_beta64); dfree(d.pt_beta32);
+    dfree(d.atom_width); dfree(d.atom_proj_off); dfree(d.atom_E);
+    dfree(d.chunk_atom); dfree(d.chunk_begin); dfree(d.chunk_end);
+    dfree(d.atom_chunk_begin); dfree(d.atom_chunk_end);
+    dfree(d.grid_ptr); dfree(d.cov_grid); dfree(d.ent_atom); dfree(d.ent_xyz);
+    dfree(d.ent_beta64); dfree(d.ent_beta32);
+    d.n_atoms = 0; d.wmax = 0; d.n_points = 0; d.total_proj = 0; d.n_chunks = 0; d.n_cov = 0;
+    d.h_atom_width.clear(); d.h_atom_proj_off.clear();
+}
+
+qsb_status nl_upload(NLDevice& d, int nx, int ny, int nz, int n_atoms, const int* npts, const int* widths,
+                     const int* coords, const double* beta, const double* energy) {
+    nl_free(d);
+    if (n_atoms < 0) return fail(QSB_ERR_INVALID, "set_projectors: n_atoms < 0");
+    const size_t N = (size_t)nx * ny * nz;
+    int64_t total = 0;
+    int wmax = 0, total_proj = 0;
+    for (int a = 0; a < n_atoms; ++a) {
+        if (npts[a] < 0 || widths[a] < 0) return fail(QSB_ERR_INVALID, "set_projectors: negative npts/width");
+        if (widths[a] > 16) return fail(QSB_ERR_INVALID, "set_projectors: width > 16 per atom is not supported");
+        total += npts[a];
+        wmax = std::max(wmax, widths[a]);
+        total_proj += widths[a];
+    }
+    if (total >= (int64_t)1 << 31) return fail(QSB_ERR_INVALID, "set_projectors: more than 2^31 points");
+    d.n_atoms = n_atoms;
+    d.wmax = wmax;
+    d.n_points = total;
+    d.total_proj = total_proj;
+    d.h_atom_width.assign(widths, widths + n_atoms);
+    d.h_atom_proj_off.resize(n_atoms);
+    {
+        int off = 0;
+        for (int a = 0; a < n_atoms; ++a) { d.h_atom_proj_off[a] = off; off += widths[a]; }
+    }
+    if (total == 0 || wmax == 0) {
+        // nothing to apply; keep an empty CSR so the fused stencil can skip it
+        d.n_points = 0;
+        return QSB_OK;
+    }
+
+    // atom-major points, sorted by folded grid index within each atom
+    std::vector<int> idx(total), xyz(3 * total), atom_of(total);
+    std::vector<double> b64((size_t)total * wmax, 0.0);
+    std::vector<double> E((size_t)n_atoms * wmax, 0.0);
+    std::vector<int> chunk_atom, chunk_b, chunk_e, acb(n_atoms), ace(n_atoms);
+    {
+        int64_t off = 0, boff = 0;
+        std::vector<int> order;
+        for (int a = 0; a < n_atoms; ++a) {
+            const int np = npts[a], w = widths[a];
+            for (int k = 0; k < w; ++k) E[(size_t)a * wmax + k] = energy[d.h_atom_proj_off[a] + k];
+            order.resize(np);
+            std::vector<int> fidx(np);
+            for (int i = 0; i < np; ++i) {
+                const int* c = coords + 3 * (off + i);
+                fidx[i] = fold(c[0], nx) + nx * (fold(c[1], ny) + ny * fold(c[2], nz));
+            }
+            std::iota(order.begin(), order.end(), 0);
+            std::stable_sort(order.begin(), order.end(), [&](int u, int v) { return fidx[u] < fidx[v]; });
+            for (int i = 0; i < np; ++i) {
+                const int src = order[i];
+                const int64_t dst = off + i;
+                idx[dst] = fidx[src];
+                atom_of[dst] = a;
+                for (int c = 0; c < 3; ++c) xyz[3 * dst + c] = coords[3 * (off + src) + c];
+                for (int k = 0; k < w; ++k) b64[(size_t)dst * wmax + k] = beta[boff + (int64_t)k * np + src];
+            }
+            acb[a] = (int)chunk_b.size();
+            if (w > 0)
+                for (int i = 0; i < np; i += CHUNK) {
+                    chunk_atom.push_back(a);
+                    chunk_b.push_back((int)(off + i));
+                    chunk_e.push_back((int)(off + std::min(np, i + CHUNK)));
+                }
+            ace[a] = (int)chunk_b.size();
+            off += np;
+            boff += (int64_t)np * w;
+        }
+    }
+    d.n_chunks = (int)chunk_b.size();
+
+    // grid-ordered CSR (counting sort by folded index, stable in atom-major order)
+    std::vector<int> gptr(N + 1, 0);
+    for (int64_t p = 0; p < total; ++p) gptr[idx[p] + 1]++;
+    for (size_t g = 0; g < N; ++g) gptr[g + 1] += gptr[g];
+    std::vector<int> fillp(gptr.begin(), gptr.end() - 1);
+    std::vector<int> e_atom(total), e_xyz(3 * total);
+    std::vector<double> e_b64((size_t)total * wmax);
+    for (int64_t p = 0; p < total; ++p) {
+        const int e = fillp[idx[p]]++;
+        e_atom[e] = atom_of[p];
+        for (int c = 0; c < 3; ++c) e_xyz[3 * e + c] = xyz[3 * p + c];
+        for (int k = 0; k < wmax; ++k) e_b64[(size_t)e * wmax + k] = b64[(size_t)p * wmax + k];
+    }
+    std::vector<int> cov;
+    for (size_t g = 0; g < N; ++g)
+        if (gptr[g + 1] > gptr[g]) cov.push_back((int)g);
+    d.n_cov = (int)cov.size();
+
+    std::vector<float> b32(b64.begin(), b64.end()), e_b32(e_b64.begin(), e_b64.end());
+    QSB_TRY(dupload(d.pt_idx, idx.data(), idx.size()));
+    QSB_TRY(dupload(d.pt_xyz, xyz.data(), xyz.size()));
+    QSB_TRY(dupload(d.pt_beta64, b64.data(), b64.size()));
+    QSB_TRY(dupload(d.pt_beta32, b32.data(), b32.size()));
+    QSB_TRY(dupload(d.atom_width, widths, (size_t)n_atoms));
+    QSB_TRY(dupload(d.atom_proj_off, d.h_atom_proj_off.data(), (size_t)n_atoms));
+    QSB_TRY(dupload(d.atom_E, E.data(), E.size()));
+    QSB_TRY(dupload(d.chunk_atom, chunk_atom.data(), chunk_atom.size()));
+    QSB_TRY(dupload(d.chunk_begin, chunk_b.data(), chunk_b.size()));
+    QSB_TRY(dupload(d.chunk_end, chunk_e.data(), chunk_e.size()));
+    QSB_TRY(dupload(d.atom_chunk_begin, acb.data(), acb.size()));
+    QSB_TRY(dupload(d.atom_chunk_end, ace.data(), ace.size()));
+    QSB_TRY(dupload(d.grid_ptr, gptr.data(), gptr.size()));
+    QSB_TRY(dupload(d.cov_grid, cov.data(), cov.size()));
+    QSB_TRY(dupload(d.ent_atom, e_atom.data(), e_atom.size()));
+    QSB_TRY(dupload(d.ent_xyz, e_xyz.data(), e_xyz.size()));
+    QSB_TRY(dupload(d.ent_beta64, e_b64.data(), e_b64.size()));
+    QSB_TRY(dupload(d.ent_beta32, e_b32.data(), e_b32.size()));
+    return QSB_OK;
+}
+
+size_t nl_workspace_bytes(const NLDevice& d, int ncol) {
+    if (d.n_points == 0) return 0;
+    const size_t part = (size_t)d.n_chunks * d.wmax * ncol * sizeof(double);
+    const size_t coef = (size_t)d.n_atoms * d.wmax * ncol * sizeof(double);
+    return ((part + 255) / 256) * 256 + ((coef + 255) / 256) * 256;
+}
+
+qsb_status nl_project(qsb_dtype dt, const NLDevice& d, int nx, int ny, int nz, int nb, int is_complex,
+                      const void* psi, double dV, double gx_dx, double gy_dy, double gz_dz, bool inner_only, void* ws,
+                      double** coef_out, cudaStream_t s) {
+    const size_t N = (size_t)nx * ny * nz;
+    const int ncol = is_complex ? 2 * nb : nb;
+    const size_t part = (size_t)d.n_chunks * d.wmax * ncol * sizeof(double);
+    double* partial = (double*)ws;
+    double* coef = (double*)((char*)ws + ((part + 255) / 256) * 256);
+    *coef_out = coef;
+    if (d.n_points == 0) return QSB_OK;
+    if ((nb + 7) / 8 > 65535) return fail(QSB_ERR_INVALID, "nonlocal: too many bands");
+    if (dt == QSB_F64) {
+        if (is_complex) launch_proj_w<double, true>(d, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+        else launch_proj_w<double, false>(d, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+    } else {
+        if (is_complex) launch_proj_w<float, true>(d, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+        else launch_proj_w<float, false>(d, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+    }
+    QSB_CUDA_TRY(cudaGetLastError());
+    nl_finalize_kernel<<<d.n_atoms, 256, 0, s>>>(d.atom_chunk_begin, d.atom_chunk_end, d.atom_E, d.atom_width, d.wmax,
+                                                 partial, ncol, dV, inner_only ? 1 : 0, coef);
+    QSB_CUDA_TRY(cudaGetLastError());
+    return QSB_OK;
+}
+
+qsb_status nl_apply(qsb_dtype dt, const NLDevice& d, int N, int nb, int is_complex, void* hpsi, const double* coef,
+                    double gx_dx, double gy_dy, double gz_dz, cudaStream_t s) {
+    if (d.n_points == 0 || d.n_cov == 0) return QSB_OK;
+    const int ncol = is_complex ? 2 * nb : nb;
+    constexpr int CBR = 8, CBC = 4;
+    const int CB = is_complex ? CBC : CBR;
+    dim3 grid((d.n_cov + APPLY_THREADS - 1) / APPLY_THREADS, (nb + CB - 1) / CB);
+    if (grid.y > 65535) return fail(QSB_ERR_INVALID, "nonlocal: too many bands");
+    if (dt == QSB_F64) {
+        if (is_complex)
+            nl_apply_kernel<double, true, CBC><<<grid, APPLY_THREADS, 0, s>>>(
+                d.cov_grid, d.n_cov, d.grid_ptr, d.ent_atom, d.ent_xyz, d.ent_beta64, d.wmax, coef, ncol,
+                (double*)hpsi, (size_t)N, nb, gx_dx, gy_dy, gz_dz);
+        else
+            nl_apply_kernel<double, false, CBR><<<grid, APPLY_THREADS, 0, s>>>(
+                d.cov_grid, d.n_cov, d.grid_ptr, d.ent_atom, d.ent_xyz, d.ent_beta64, d.wmax, coef, ncol,
+                (double*)hpsi, (size_t)N, nb, gx_dx, gy_dy, gz_dz);
+    } else {
+        if (is_complex)
+            nl_apply_kernel<float, true, CBC><<<grid, APPLY_THREADS, 0, s>>>(
+                d.cov_grid, d.n_cov, d.grid_ptr, d.ent_atom, d.ent_xyz, d.ent_beta32, d.wmax, coef, ncol,
+                (float*)hpsi, (size_t)N, nb, gx_dx, gy_dy, gz_dz);
+        else
+            nl_apply_kernel<float, false, CBR><<<grid, APPLY_THREADS, 0, s>>>(
+                d.cov_grid, d.n_cov, d.grid_ptr, d.ent_atom, d.ent_xyz, d.ent_beta32, d.wmax, coef, ncol,
+                (float*)hpsi, (size_t)N, nb, gx_dx, gy_dy, gz_dz);
+    }
+    QSB_CUDA_TRY(cudaGetLastError());
+    return QSB_OK;
+}
+
+}  // namespace qsb

@@ -1,0 +1,136 @@
+// Internal declarations shared by the CUDA translation units of the
+// qumasun_b200 library.  Not part of the public ABI (include/qumasun_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+
+#include "../../include/qumasun_b200.h"
+
+namespace qsb {
+
+// Records the message for qsb_last_error() and returns the status.
+qsb_status fail(qsb_status st, const std::string& msg);
+qsb_status cuda_fail(cudaError_t e, const char* where);
+
+#define QSB_CUDA_TRY(expr)                                   \
+    do {                                                     \
+        cudaError_t qsb_e_ = (expr);                         \
+        if (qsb_e_ != cudaSuccess) return ::qsb::cuda_fail(qsb_e_, #expr); \
+    } while (0)
+
+#define QSB_TRY(expr)                                        \
+    do {                                                     \
+        qsb_status qsb_s_ = (expr);                          \
+        if (qsb_s_ != QSB_OK) return qsb_s_;                 \
+    } while (0)
+
+// FD8 coefficients in the reference's formulas
+// (source/GridDifference8th.h:89-101, source/GridDifferenceKpoint8th.h:26-57).
+struct FD8Coef {
+    double c0;        // centre (includes -coef*|g|^2 for the k-point form)
+    double cx[4], cy[4], cz[4];   // second-derivative weights for offsets 1..4
+    double ax[4], ay[4], az[4];   // first-derivative weights (k-point form), offsets 1..4
+    bool has_grad;                // any |g_d| >= 1e-8
+};
+FD8Coef make_fd8_coef(double coef, double dx, double dy, double dz, double gx, double gy, double gz);
+
+// Fused nonlocal pull inside the H stencil: hpsi_col[g] += sum over projector
+// points e on grid point g of sum_w beta_e[w] * coef[atom_e][w][col] (times
+// exp(-i g.r_e) in the complex case).
+struct NLView {
+    const int* grid_ptr;      // [N+1] entry ranges per grid point
+    const int* ent_atom;
+    const int* ent_xyz;
+    const void* ent_beta;     // T[n_points][wmax]
+    const double* coef;       // [atom][wmax][ncol]
+    int wmax;
+    int ncol;
+    double gx_dx, gy_dy, gz_dz;
+};
+
+// Launch configuration of the stencil kernels.
+struct StencilLaunch {
+    int nx, ny, nz;
+    int nb;                  // bands
+    int is_complex;          // SoA complex bundle
+    int mode;                // 0: out += coef*L(psi); 1: out = V psi + coef*L(psi) (+ NL)
+    const void* in;
+    void* out;
+    const void* V;           // mode 1 only
+    const NLView* nl;        // fused nonlocal apply (mode 1), or nullptr
+};
+
+qsb_status launch_stencil(qsb_dtype dt, const StencilLaunch& L, const FD8Coef& c, cudaStream_t s);
+
+// Device-side nonlocal tables (owned by qsb_ham).
+struct NLDevice {
+    int n_atoms = 0;
+    int wmax = 0;                  // max projectors per atom (tables padded to wmax)
+    int64_t n_points = 0;          // total points over atoms
+    int total_proj = 0;            // sum of widths
+    // atom-major point arrays
+    int* pt_idx = nullptr;         // folded grid index
+    int* pt_xyz = nullptr;         // unfolded coords, 3 per point
+    double* pt_beta64 = nullptr;   // [point][wmax]
+    float* pt_beta32 = nullptr;
+    // per-atom
+    int* atom_width = nullptr;     // [n_atoms]
+    int* atom_proj_off = nullptr;  // [n_atoms] offset in the global projector numbering
+    double* atom_E = nullptr;      // [n_atoms][wmax], zero-padded
+    // projection chunks: each chunk is a run of points of one atom
+    int n_chunks = 0;
+    int* chunk_atom = nullptr;
+    int* chunk_begin = nullptr;
+    int* chunk_end = nullptr;
+    int* atom_chunk_begin = nullptr;  // [n_atoms]
+    int* atom_chunk_end = nullptr;    // [n_atoms]
+    // grid-ordered (CSR over all N grid points) view of the same points for
+    // the pull-form apply: entries of grid point g are [grid_ptr[g], grid_ptr[g+1])
+    int* grid_ptr = nullptr;       // [N+1]
+    int n_cov = 0;                 // grid points with at least one entry
+    int* cov_grid = nullptr;       // [n_cov]
+    int* ent_atom = nullptr;       // [n_points]
+    int* ent_xyz = nullptr;        // [n_points][3]
+    double* ent_beta64 = nullptr;  // [n_points][wmax]
+    float* ent_beta32 = nullptr;
+    // host copies kept for bookkeeping
+    std::vector<int> h_atom_width;
+    std::vector<int> h_atom_proj_off;
+};
+
+void nl_free(NLDevice& d);
+qsb_status nl_upload(NLDevice& d, int nx, int ny, int nz, int n_atoms, const int* npts, const int* widths,
+                     const int* coords, const double* beta, const double* energy);
+
+// Workspace needed by nl_project for nb bands (bytes).
+size_t nl_workspace_bytes(const NLDevice& d, int ncol);
+// coef[atom][w][col] = dV * E_w * <beta|psi_col> (Bloch-phased for complex); ws must hold
+// nl_workspace_bytes.  If inner_only, the E_w factor is omitted.
+qsb_status nl_project(qsb_dtype dt, const NLDevice& d, int nx, int ny, int nz, int nb, int is_complex,
+                      const void* psi, double dV, double gx_dx, double gy_dy, double gz_dz,
+                      bool inner_only, void* ws, double** coef_out, cudaStream_t s);
+// hpsi[grid][col] += sum_e beta_e . coef  (pull over covered grid points)
+qsb_status nl_apply(qsb_dtype dt, const NLDevice& d, int N, int nb, int is_complex, void* hpsi,
+                    const double* coef, double gx_dx, double gy_dy, double gz_dz, cudaStream_t s);
+
+}  // namespace qsb
+
+struct qsb_ham {
+    int nx = 0, ny = 0, nz = 0;
+    size_t N = 0;
+    double dx = 0, dy = 0, dz = 0;
+    double* V64 = nullptr;
+    float* V32 = nullptr;
+    qsb::NLDevice nl;
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    // optional per-kernel event timing of qsb_ham_apply
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;      // free events
+    std::vector<cudaEvent_t> ev_rec;       // recorded triples: start, after projection, after stencil
+    int launches = 0;
+};

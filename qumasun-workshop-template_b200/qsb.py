@@ -1,0 +1,210 @@
+"""Python binding of libqumasun_b200.so (the C ABI in include/qumasun_b200.h).
+
+Mirrors the reference's call surfaces for the H.psi / LOBPCG path:
+
+  laplacian8th(out, p, coef, dx, dy, dz)        ~ Laplacian8th<T>            (GridDifference8th.h:177)
+  laplacian_kpoint8th(out, src, coef, d, g)     ~ LaplacianKpoint8th_ddm      (GridDifferenceKpoint8th.h:324)
+  Hamiltonian.apply(psi, hpsi, g)               ~ mHamiltonianMatrix_ddm      (qumasun_base1.matrix.h:263)
+  Hamiltonian.nonlocal_apply(psi, hpsi, g)      ~ ProjectionPP_bundle         (PseudoPotNonlocal_SvF2_kpoint.h:4239)
+  Hamiltonian.nonlocal_project(psi, g)          ~ mInnerNonlocalPsi_v4_bundle (PseudoPotNonlocal_SvF2_kpoint.h:4463)
+
+Arrays are torch CUDA tensors in the reference's band-bundle layouts (real:
+[nb, N]; complex SoA: [nb, 2, N] i.e. re plane then im plane per band), float64
+or float32.  Calls run on torch's current CUDA stream.  There is no CPU path:
+if the CUDA library is missing or fails to load, import raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqumasun_b200.so")
+
+QSB_F64 = 0
+QSB_F32 = 1
+
+_STATUS = {0: "QSB_OK", 1: "QSB_ERR_INVALID", 2: "QSB_ERR_CUDA", 3: "QSB_ERR_NOMEM", 4: "QSB_ERR_STATE",
+           5: "QSB_ERR_SOLVER", 6: "QSB_ERR_NUMERIC"}
+
+
+class QsbError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{_STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libqumasun_b200.so not built at {LIB_PATH}; run "
+                          "python qumasun-workshop-template_b200/build_lib.py")
+    lib = ctypes.CDLL(LIB_PATH)
+    lib.qsb_last_error.restype = ctypes.c_char_p
+    lib.qsb_version.restype = ctypes.c_char_p
+    return lib
+
+
+lib = _load()
+_c_d = ctypes.c_double
+_vp = ctypes.c_void_p
+
+
+def _check(st):
+    if st != 0:
+        raise QsbError(st, lib.qsb_last_error().decode())
+
+
+def version():
+    return lib.qsb_version().decode()
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _dtype_code(t):
+    torch = _torch()
+    if t.dtype == torch.float64:
+        return QSB_F64
+    if t.dtype == torch.float32:
+        return QSB_F32
+    raise TypeError(f"unsupported dtype {t.dtype}")
+
+
+def _stream_ptr(t):
+    torch = _torch()
+    return _vp(torch.cuda.current_stream(t.device).cuda_stream)
+
+
+def _dev_ptr(t):
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return _vp(t.data_ptr())
+
+
+def laplacian8th(out, p, coef, dx, dy, dz, shape):
+    """out += coef * FD8 Laplacian(p); p, out: [nb, N] (or [N]) CUDA tensors."""
+    nx, ny, nz = shape
+    N = nx * ny * nz
+    nb = p.numel() // N
+    assert out.dtype == p.dtype and out.numel() == p.numel()
+    _check(lib.qsb_laplacian8th(_dtype_code(p), nx, ny, nz, nb, _dev_ptr(out), _dev_ptr(p), _c_d(coef), _c_d(dx),
+                                _c_d(dy), _c_d(dz), _stream_ptr(p)))
+    return out
+
+
+def laplacian_kpoint8th(out, src, coef, dx, dy, dz, g, shape):
+    """out += coef*(Lap + 2i g.grad - g^2) src for complex SoA bands [nb, 2, N]."""
+    nx, ny, nz = shape
+    N = nx * ny * nz
+    nb = src.numel() // (2 * N)
+    assert out.dtype == src.dtype and out.numel() == src.numel()
+    _check(lib.qsb_laplacian_kpoint8th(_dtype_code(src), nx, ny, nz, nb, _dev_ptr(out), _dev_ptr(src), _c_d(coef),
+                                       _c_d(dx), _c_d(dy), _c_d(dz), _c_d(g[0]), _c_d(g[1]), _c_d(g[2]),
+                                       _stream_ptr(src)))
+    return out
+
+
+def _i32(a):
+    a = np.ascontiguousarray(a, np.int32)
+    return a, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def _f64(a):
+    a = np.ascontiguousarray(a, np.float64)
+    return a, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Hamiltonian:
+    """Kohn-Sham H = -1/2 FD8 Laplacian + V + V_NL on one periodic grid (device resident)."""
+
+    def __init__(self, nx, ny, nz, dx, dy, dz):
+        self.shape = (nx, ny, nz)
+        self.spacing = (dx, dy, dz)
+        self.N = nx * ny * nz
+        h = ctypes.c_void_p()
+        _check(lib.qsb_ham_create(ctypes.byref(h), nx, ny, nz, _c_d(dx), _c_d(dy), _c_d(dz)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.qsb_ham_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_potential(self, V):
+        """V: numpy array (host) or CUDA tensor of N float64 values."""
+        if hasattr(V, "is_cuda") and V.is_cuda:
+            _check(lib.qsb_ham_set_potential(self._h, _dev_ptr(V), 1))
+        else:
+            v, vp = _f64(V)
+            _check(lib.qsb_ham_set_potential(self._h, vp, 0))
+
+    def set_projectors(self, npts, widths, coords, beta, energy):
+        """Point-list projector tables (host numpy), as in include/qumasun_b200.h."""
+        n, np_ = _i32(npts)
+        w, wp = _i32(widths)
+        c, cp = _i32(coords)
+        b, bp = _f64(beta)
+        e, ep = _f64(energy)
+        _check(lib.qsb_ham_set_projectors(self._h, len(n), np_, wp, cp, bp, ep))
+
+    def set_gth_projectors(self, pos, species, nl, r_l, h_l, rcut_factor=6.0):
+        p, pp = _f64(np.asarray(pos, np.float64).ravel())
+        s, sp = _i32(species)
+        n, nlp = _i32(nl)
+        r, rp = _f64(np.asarray(r_l, np.float64).ravel())
+        hh, hp = _f64(np.asarray(h_l, np.float64).ravel())
+        _check(lib.qsb_ham_set_gth_projectors(self._h, len(s), pp, sp, len(n), nlp, rp, hp, _c_d(rcut_factor)))
+
+    def projector_info(self):
+        tp = ctypes.c_int64()
+        tw = ctypes.c_int()
+        _check(lib.qsb_ham_projector_info(self._h, ctypes.byref(tp), ctypes.byref(tw)))
+        return tp.value, tw.value
+
+    def set_timing(self, enable=True):
+        _check(lib.qsb_ham_set_timing(self._h, int(bool(enable))))
+
+    def get_timing(self):
+        """(projection_ms, stencil_ms, applies, kernel_launches) since the last call."""
+        pm, sm = ctypes.c_double(), ctypes.c_double()
+        n, k = ctypes.c_int(), ctypes.c_int()
+        _check(lib.qsb_ham_get_timing(self._h, ctypes.byref(pm), ctypes.byref(sm), ctypes.byref(n), ctypes.byref(k)))
+        return pm.value, sm.value, n.value, k.value
+
+    def _nb(self, psi, is_complex):
+        return psi.numel() // ((2 if is_complex else 1) * self.N)
+
+    def apply(self, psi, hpsi, is_complex=False, g=(0.0, 0.0, 0.0)):
+        """hpsi = H psi."""
+        nb = self._nb(psi, is_complex)
+        assert hpsi.dtype == psi.dtype and hpsi.numel() == psi.numel()
+        _check(lib.qsb_ham_apply(self._h, _dtype_code(psi), int(is_complex), nb, _dev_ptr(psi), _dev_ptr(hpsi),
+                                 _c_d(g[0]), _c_d(g[1]), _c_d(g[2]), _stream_ptr(psi)))
+        return hpsi
+
+    def nonlocal_apply(self, psi, hpsi, is_complex=False, g=(0.0, 0.0, 0.0)):
+        """hpsi += V_NL psi."""
+        nb = self._nb(psi, is_complex)
+        _check(lib.qsb_ham_nonlocal_apply(self._h, _dtype_code(psi), int(is_complex), nb, _dev_ptr(psi),
+                                          _dev_ptr(hpsi), _c_d(g[0]), _c_d(g[1]), _c_d(g[2]), _stream_ptr(psi)))
+        return hpsi
+
+    def nonlocal_project(self, psi, is_complex=False, g=(0.0, 0.0, 0.0)):
+        """<beta|psi> dV as a numpy [ncol, total_projectors] array."""
+        nb = self._nb(psi, is_complex)
+        _, P = self.projector_info()
+        out = np.zeros(((2 if is_complex else 1) * nb, max(P, 1)))
+        _check(lib.qsb_ham_nonlocal_project(self._h, _dtype_code(psi), int(is_complex), nb, _dev_ptr(psi),
+                                            _c_d(g[0]), _c_d(g[1]), _c_d(g[2]),
+                                            out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _stream_ptr(psi)))
+        return out[:, :P]

@@ -1,0 +1,94 @@
+"""Seeded golden cases shared by make_golden.py and the tests.
+
+Each case: inputs() -> dict of arrays (regenerated from seeds), reference(inp)
+-> output of the reference's own code, oracle(inp) -> output of the C
+restatement, and "checked" arrays whose sums are stored as checksums.
+"""
+import math
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
+import oracle as O  # noqa: E402
+
+SMALL = (12, 10, 8, 0.3, 0.25, 0.35)          # non-cubic, non-tile-multiple grid
+TINY = (5, 4, 6, 0.4, 0.5, 0.45)              # dimensions smaller than the stencil reach
+C0_24 = (24, 24, 24, 0.25, 0.25, 0.25)        # config-0 bcc cell (a = 6 bohr) on a 24^3 grid
+C0_20 = (20, 20, 20, 0.3, 0.3, 0.3)           # same cell on a 20^3 grid (complex case)
+A_BCC = 6.0
+
+
+def _lap_inputs(grid, seed, nb, cplx=False):
+    nx, ny, nz = grid[:3]
+    N = nx * ny * nz
+    p = O.seeded_psi(seed, nb, N, cplx)
+    out0 = O.seeded_psi(seed + 50, nb, N, cplx)        # non-zero initial out: tests "+="
+    return dict(grid=grid, p=p, out0=out0, checked=[p, out0])
+
+
+def _lap_ref(inp, fn):
+    nx, ny, nz, dx, dy, dz = inp["grid"]
+    out = inp["out0"].copy()
+    fn(nx, ny, nz, out, inp["p"], -0.5, dx, dy, dz)
+    return out
+
+
+def _kp_ref(inp, g, fn):
+    nx, ny, nz, dx, dy, dz = inp["grid"]
+    out = inp["out0"].copy()
+    fn(nx, ny, nz, out, inp["p"], -0.5, dx, dy, dz, g)
+    return out
+
+
+def _ham_inputs(grid, seed, nb, cplx):
+    nx, ny, nz, dx, dy, dz = grid
+    N = nx * ny * nz
+    pos = O.bcc_positions(A_BCC, 1) + np.array([0.11, -0.07, 0.05])   # off-grid atoms
+    sp = [O.GTH_BCC] * len(pos)
+    psi = O.seeded_psi(seed, nb, N, cplx)
+    V = O.seeded_potential(seed, N)
+    return dict(grid=grid, pos=pos, sp=sp, psi=psi, V=V, nb=nb, checked=[psi, V])
+
+
+def _ham_ref(inp, cplx, g):
+    nx, ny, nz, dx, dy, dz = inp["grid"]
+    cube = O.gth_cube_tables(inp["pos"], inp["sp"], nx, ny, nz, dx, dy, dz)
+    return O.ref_hamiltonian(inp["grid"], inp["V"], cube, inp["psi"], inp["nb"], cplx, g)
+
+
+def _ham_oracle(inp, cplx, g):
+    nx, ny, nz, dx, dy, dz = inp["grid"]
+    tab = O.gth_tables(inp["pos"], inp["sp"], dx, dy, dz)
+    return O.hamiltonian(inp["grid"], inp["V"], tab, inp["psi"], inp["nb"], cplx, g)
+
+
+G_KP = (0.3, 0.0, -0.2)
+G_SMALL = (1.0e-9, 0.4, 0.1)    # |gx| below the 1e-8 dispatch threshold
+G_C0 = (2 * math.pi / A_BCC * 0.25, 2 * math.pi / A_BCC * 0.5, 0.0)
+
+CASES = {
+    "lap_real_small": dict(inputs=lambda: _lap_inputs(SMALL, 0, 2),
+                           reference=lambda i: _lap_ref(i, O.ref_laplacian8th),
+                           oracle=lambda i: _lap_ref(i, O.laplacian8th)),
+    "lap_real_tiny": dict(inputs=lambda: _lap_inputs(TINY, 3, 1),
+                          reference=lambda i: _lap_ref(i, O.ref_laplacian8th),
+                          oracle=lambda i: _lap_ref(i, O.laplacian8th)),
+    "lap_kpoint_small": dict(inputs=lambda: _lap_inputs(SMALL, 1, 2, True),
+                             reference=lambda i: _kp_ref(i, G_KP, O.ref_laplacian_kpoint8th),
+                             oracle=lambda i: _kp_ref(i, G_KP, O.laplacian_kpoint8th)),
+    "lap_kpoint_thresh": dict(inputs=lambda: _lap_inputs(SMALL, 2, 1, True),
+                              reference=lambda i: _kp_ref(i, G_SMALL, O.ref_laplacian_kpoint8th),
+                              oracle=lambda i: _kp_ref(i, G_SMALL, O.laplacian_kpoint8th)),
+    "lap_kpoint_gamma": dict(inputs=lambda: _lap_inputs(TINY, 4, 1, True),
+                             reference=lambda i: _kp_ref(i, (0.0, 0.0, 0.0), O.ref_laplacian_kpoint8th),
+                             oracle=lambda i: _kp_ref(i, (0.0, 0.0, 0.0), O.laplacian_kpoint8th)),
+    "ham_real_c0": dict(inputs=lambda: _ham_inputs(C0_24, 0, 3, False),
+                        reference=lambda i: _ham_ref(i, False, (0.0, 0.0, 0.0)),
+                        oracle=lambda i: _ham_oracle(i, False, (0.0, 0.0, 0.0))),
+    "ham_cplx_c0": dict(inputs=lambda: _ham_inputs(C0_20, 5, 2, True),
+                        reference=lambda i: _ham_ref(i, True, G_C0),
+                        oracle=lambda i: _ham_oracle(i, True, G_C0)),
+}

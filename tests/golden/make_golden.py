@@ -1,0 +1,34 @@
+"""Generate the golden fixtures in this folder from the REFERENCE's own code.
+
+Runs the reference's hot-path templates, compiled from its source tree into
+oracle/_ref/libqsref.so (oracle/Makefile, oracle/ref_entry.cpp), on small
+seeded inputs and stores the outputs.  Inputs are regenerated from the seeds
+by the tests (numpy PCG64), and each fixture stores input checksums so RNG
+drift is detected.
+
+    make -C oracle ref && python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
+import oracle as O  # noqa: E402
+
+from cases import CASES  # noqa: E402
+
+
+def main():
+    assert O.ref_available(), "build oracle/_ref first: make -C oracle ref"
+    for name, case in CASES.items():
+        inp = case["inputs"]()
+        out = case["reference"](inp)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), out=out,
+                            checksum=np.array([float(np.sum(v)) for v in inp["checked"]]))
+        print(name, out.shape, float(np.linalg.norm(out)))
+
+
+if __name__ == "__main__":
+    main()

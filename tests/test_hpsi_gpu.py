@@ -1,0 +1,246 @@
+"""GPU parity of the H.psi path (FD8 + V + KB nonlocal), called through the C ABI.
+
+Tolerances: FP64 drop-in 1e-12 relative L2 (the stated H.psi bar); FP32 forms
+2e-5 relative L2 against the FP64 oracle.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from cases import CASES, C0_24, C0_20, G_C0
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+TOL64 = 1e-12
+TOL32 = 2e-5
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def dev(a, dtype=None):
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    if dtype is not None:
+        t = t.to(dtype)
+    return t.cuda()
+
+
+def host(t):
+    import torch
+    torch.cuda.synchronize()
+    return t.double().cpu().numpy()
+
+
+@pytest.mark.parametrize("name", ["lap_real_small", "lap_real_tiny"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_laplacian8th_golden(qsb, name, prec):
+    import torch
+    dt = torch.float64 if prec == "f64" else torch.float32
+    inp = CASES[name]["inputs"]()
+    nx, ny, nz, dx, dy, dz = inp["grid"]
+    ref = np.load(os.path.join(GOLD, name + ".npz"))["out"]
+    out = dev(inp["out0"], dt)
+    qsb.laplacian8th(out, dev(inp["p"], dt), -0.5, dx, dy, dz, (nx, ny, nz))
+    assert rel(host(out), ref) < (TOL64 if prec == "f64" else TOL32)
+
+
+@pytest.mark.parametrize("name,g", [("lap_kpoint_small", (0.3, 0.0, -0.2)),
+                                    ("lap_kpoint_thresh", (1.0e-9, 0.4, 0.1)),
+                                    ("lap_kpoint_gamma", (0.0, 0.0, 0.0))])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_laplacian_kpoint_golden(qsb, name, g, prec):
+    import torch
+    dt = torch.float64 if prec == "f64" else torch.float32
+    inp = CASES[name]["inputs"]()
+    nx, ny, nz, dx, dy, dz = inp["grid"]
+    ref = np.load(os.path.join(GOLD, name + ".npz"))["out"]
+    out = dev(inp["out0"], dt)
+    qsb.laplacian_kpoint8th(out, dev(inp["p"], dt), -0.5, dx, dy, dz, g, (nx, ny, nz))
+    assert rel(host(out), ref) < (TOL64 if prec == "f64" else TOL32)
+
+
+def _ham_from_case(qsb, inp, gth_builder):
+    nx, ny, nz, dx, dy, dz = inp["grid"]
+    H = qsb.Hamiltonian(nx, ny, nz, dx, dy, dz)
+    H.set_potential(inp["V"])
+    if gth_builder:
+        sp = inp["sp"]
+        H.set_gth_projectors(inp["pos"], [0] * len(sp), [sp[0]["nl"]], [sp[0]["r"]], [sp[0]["h"]], O.RCUT_FACTOR)
+    else:
+        H.set_projectors(*O.gth_tables(inp["pos"], inp["sp"], dx, dy, dz))
+    return H
+
+
+@pytest.mark.parametrize("gth_builder", [True, False])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_hamiltonian_real_golden(qsb, gth_builder, prec):
+    import torch
+    dt = torch.float64 if prec == "f64" else torch.float32
+    inp = CASES["ham_real_c0"]["inputs"]()
+    ref = np.load(os.path.join(GOLD, "ham_real_c0.npz"))["out"]
+    H = _ham_from_case(qsb, inp, gth_builder)
+    psi = dev(inp["psi"], dt)
+    hp = torch.empty_like(psi)
+    H.apply(psi, hp)
+    assert rel(host(hp), ref) < (TOL64 if prec == "f64" else TOL32)
+
+
+@pytest.mark.parametrize("gth_builder", [True, False])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_hamiltonian_complex_golden(qsb, gth_builder, prec):
+    import torch
+    dt = torch.float64 if prec == "f64" else torch.float32
+    inp = CASES["ham_cplx_c0"]["inputs"]()
+    ref = np.load(os.path.join(GOLD, "ham_cplx_c0.npz"))["out"]
+    H = _ham_from_case(qsb, inp, gth_builder)
+    psi = dev(inp["psi"], dt)
+    hp = torch.empty_like(psi)
+    H.apply(psi, hp, True, G_C0)
+    assert rel(host(hp), ref) < (TOL64 if prec == "f64" else TOL32)
+
+
+def _setup(qsb, grid, nb, cplx, seed, reps=1, jitter=0.0):
+    nx, ny, nz, dx, dy, dz = grid
+    a = nx * dx / reps
+    pos = O.bcc_positions(a, reps, jitter, seed) + np.array([0.13, 0.02, -0.09])
+    sp = [O.GTH_BCC] * len(pos)
+    tab = O.gth_tables(pos, sp, dx, dy, dz)
+    V = O.seeded_potential(seed, nx * ny * nz)
+    psi = O.seeded_psi(seed, nb, nx * ny * nz, cplx)
+    H = qsb.Hamiltonian(nx, ny, nz, dx, dy, dz)
+    H.set_potential(V)
+    H.set_projectors(*tab)
+    return H, tab, V, psi
+
+
+@pytest.mark.parametrize("grid,nb", [((32, 32, 32, 0.1875, 0.1875, 0.1875), 16),   # config 0 shape
+                                      ((33, 17, 9, 0.2, 0.3, 0.25), 3),           # ragged tiles
+                                      ((64, 8, 40, 0.15, 0.2, 0.1), 2),
+                                      ((4, 4, 4, 1.5, 1.5, 1.5), 1)])             # smallest grid the reference handles
+def test_hamiltonian_real_vs_oracle(qsb, grid, nb):
+    import torch
+    H, tab, V, psi = _setup(qsb, grid, nb, False, 21)
+    ref = O.hamiltonian(grid, V, tab, psi, nb)
+    p = dev(psi)
+    hp = torch.empty_like(p)
+    H.apply(p, hp)
+    assert rel(host(hp), ref) < TOL64
+
+
+@pytest.mark.parametrize("g", [(0.0, 0.0, 0.0), (0.26, 0.52, 0.0), (0.3, -0.2, 0.7)])
+def test_hamiltonian_complex_vs_oracle(qsb, g):
+    import torch
+    grid = (24, 20, 16, 0.25, 0.3, 0.375)
+    H, tab, V, psi = _setup(qsb, grid, 3, True, 22)
+    ref = O.hamiltonian(grid, V, tab, psi, 3, True, g)
+    p = dev(psi)
+    hp = torch.empty_like(p)
+    H.apply(p, hp, True, g)
+    assert rel(host(hp), ref) < TOL64
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_nonlocal_apply_and_project_vs_oracle(qsb, cplx, prec):
+    import torch
+    dt = torch.float64 if prec == "f64" else torch.float32
+    grid = (24, 24, 24, 0.25, 0.25, 0.25)
+    g = (0.26, 0.52, -0.1) if cplx else (0.0, 0.0, 0.0)
+    H, tab, V, psi = _setup(qsb, grid, 5, cplx, 23)
+    base = O.seeded_psi(99, 5, 24 ** 3, cplx)
+    ref = O.nonlocal_apply(grid, tab, psi, 5, cplx, g, hp=base.copy())
+    hp = dev(base, dt)
+    H.nonlocal_apply(dev(psi, dt), hp, cplx, g)
+    # compare the nonlocal increment itself (the base is much larger)
+    tol = TOL64 if prec == "f64" else TOL32
+    assert rel(host(hp) - base, ref - base) < tol
+    proj = H.nonlocal_project(dev(psi, dt), cplx, g)
+    assert rel(proj, O.nonlocal_project(grid, tab, psi, 5, cplx, g)) < tol
+
+
+def test_water_molecule_projectors(qsb):
+    """O has one s projector and H none (config-1 species): widths 1, 0, 0."""
+    import torch
+    n = 40
+    h = 20.0 / 112
+    grid = (n, n, n, h, h, h)
+    pos = np.array([[3.5, 3.5, 3.5], [3.5 + 1.43, 3.5 + 1.11, 3.5], [3.5 - 1.43, 3.5 + 1.11, 3.5]])
+    sp = [O.GTH_O, O.GTH_H, O.GTH_H]
+    tab = O.gth_tables(pos, sp, h, h, h)
+    assert list(tab[1]) == [1, 0, 0]
+    H = qsb.Hamiltonian(n, n, n, h, h, h)
+    V = O.seeded_potential(5, n ** 3)
+    H.set_potential(V)
+    H.set_gth_projectors(pos, [0, 1, 1], [1, 0], [[0.222, 0.0], [0.0, 0.0]], [[18.27, 0.0], [0.0, 0.0]], 6.0)
+    assert H.projector_info() == (int(tab[0].sum()), 1)
+    psi = O.seeded_psi(6, 2, n ** 3)
+    p = dev(psi)
+    hp = torch.empty_like(p)
+    H.apply(p, hp)
+    assert rel(host(hp), O.hamiltonian(grid, V, tab, psi, 2)) < TOL64
+
+
+def test_no_projectors_and_zero_bands(qsb):
+    import torch
+    grid = (16, 16, 16, 0.3, 0.3, 0.3)
+    H = qsb.Hamiltonian(16, 16, 16, 0.3, 0.3, 0.3)
+    V = O.seeded_potential(1, 16 ** 3)
+    H.set_potential(V)
+    psi = O.seeded_psi(2, 2, 16 ** 3)
+    p = dev(psi)
+    hp = torch.empty_like(p)
+    H.apply(p, hp)
+    empty = (np.zeros(0, np.int32),) * 3 + (np.zeros(0), np.zeros(0))
+    assert rel(host(hp), O.hamiltonian(grid, V, empty, psi, 2)) < TOL64
+    e = torch.empty(0, dtype=torch.float64, device="cuda")
+    H.apply(e, e)   # nb = 0 is a no-op
+
+
+def test_errors_are_reported(qsb):
+    import torch
+    H = qsb.Hamiltonian(8, 8, 8, 0.5, 0.5, 0.5)
+    p = torch.zeros(8 ** 3, dtype=torch.float64, device="cuda")
+    with pytest.raises(qsb.QsbError, match="potential not set"):
+        H.apply(p, torch.empty_like(p))
+    with pytest.raises(qsb.QsbError):
+        qsb.Hamiltonian(0, 8, 8, 0.5, 0.5, 0.5)
+    with pytest.raises(qsb.QsbError, match="non-finite"):
+        H.set_potential(np.full(8 ** 3, np.nan))
+
+
+def test_full_size_properties_config2(qsb):
+    """96^3 x 128 bands (config 2) at full size: symmetry, linearity, band
+    independence and run-to-run determinism of the FP64 H.psi."""
+    import torch
+    grid = (96, 96, 96, 0.125, 0.125, 0.125)
+    nb = 128
+    N = 96 ** 3
+    H, tab, V, _ = _setup(qsb, grid, 1, False, 2, reps=2)
+    g = torch.Generator(device="cuda").manual_seed(2)
+    psi = torch.rand(nb, N, dtype=torch.float64, device="cuda", generator=g) - 0.5
+    hp = torch.empty_like(psi)
+    H.apply(psi, hp)
+    hp2 = torch.empty_like(psi)
+    H.apply(psi, hp2)
+    assert torch.equal(hp, hp2)                       # deterministic (no atomics)
+    one = torch.empty_like(psi[5:6])
+    H.apply(psi[5:6].contiguous(), one)
+    assert torch.equal(one[0], hp[5])                 # bands are independent
+    a, b = psi[0], psi[1]
+    lhs = torch.dot(b, hp[0]).item()
+    rhs = torch.dot(hp[1], a).item()
+    assert abs(lhs - rhs) <= 1e-11 * abs(lhs)         # symmetric operator
+    comb = (0.3 * psi[2] - 1.7 * psi[3]).unsqueeze(0).contiguous()
+    hc = torch.empty_like(comb)
+    H.apply(comb, hc)
+    lin = 0.3 * hp[2] - 1.7 * hp[3]
+    assert (torch.linalg.norm(hc[0] - lin) / torch.linalg.norm(lin)).item() < 1e-13
+    # one band against the oracle at full size
+    ref = O.hamiltonian(grid, V, tab, psi[7].cpu().numpy(), 1)
+    assert rel(host(hp[7]), ref.ravel()) < TOL64
