@@ -143,13 +143,14 @@ QSB_API qsb_status qsb_ham_nonlocal_project(qsb_ham* ham, qsb_dtype dtype, int i
 /* Per-kernel device timing of qsb_ham_apply, in the spirit of the reference's
  * StopWatch sectors (source/StopWatch.h:11-60, watch_pp in
  * source/PseudoPotNonlocal_SvF2_kpoint.h:261-272).  While enabled, every
- * qsb_ham_apply records CUDA events on its stream around the nonlocal
- * projection kernels and the fused stencil kernel.  qsb_ham_get_timing
- * synchronizes those events, returns the summed milliseconds and the number of
- * applies since the last call, and resets the counters. */
+ * qsb_ham_apply records CUDA events on its stream around its three phases:
+ * the nonlocal projection, the FD8 + V stencil, and the nonlocal expansion.
+ * qsb_ham_get_timing synchronizes those events, returns the summed
+ * milliseconds of each phase, the number of applies and of kernel launches
+ * since the last call, and resets the counters. */
 QSB_API qsb_status qsb_ham_set_timing(qsb_ham* ham, int enable);
-QSB_API qsb_status qsb_ham_get_timing(qsb_ham* ham, double* project_ms, double* stencil_ms, int* applies,
-                                      int* kernel_launches);
+QSB_API qsb_status qsb_ham_get_timing(qsb_ham* ham, double* project_ms, double* stencil_ms, double* expand_ms,
+                                      int* applies, int* kernel_launches);
 
 #ifdef __cplusplus
 }

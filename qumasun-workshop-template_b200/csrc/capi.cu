@@ -100,7 +100,7 @@ qsb_status qsb_laplacian8th(qsb_dtype dtype, int nx, int ny, int nz, int nb, voi
     if (dtype != QSB_F64 && dtype != QSB_F32) return fail(QSB_ERR_INVALID, "laplacian8th: bad dtype");
     if (dx <= 0 || dy <= 0 || dz <= 0) return fail(QSB_ERR_INVALID, "laplacian8th: spacing must be > 0");
     if (nb == 0) return QSB_OK;
-    StencilLaunch L{nx, ny, nz, nb, 0, 0, p_dev, out_dev, nullptr, nullptr};
+    StencilLaunch L{nx, ny, nz, nb, 0, 0, p_dev, out_dev, nullptr};
     return launch_stencil(dtype, L, make_fd8_coef(coef, dx, dy, dz, 0, 0, 0), (cudaStream_t)stream);
 }
 
@@ -112,7 +112,7 @@ qsb_status qsb_laplacian_kpoint8th(qsb_dtype dtype, int nx, int ny, int nz, int 
     if (dtype != QSB_F64 && dtype != QSB_F32) return fail(QSB_ERR_INVALID, "laplacian_kpoint8th: bad dtype");
     if (dx <= 0 || dy <= 0 || dz <= 0) return fail(QSB_ERR_INVALID, "laplacian_kpoint8th: spacing must be > 0");
     if (nb == 0) return QSB_OK;
-    StencilLaunch L{nx, ny, nz, nb, 1, 0, src_dev, out_dev, nullptr, nullptr};
+    StencilLaunch L{nx, ny, nz, nb, 1, 0, src_dev, out_dev, nullptr};
     return launch_stencil(dtype, L, make_fd8_coef(coef, dx, dy, dz, gx, gy, gz), (cudaStream_t)stream);
 }
 
@@ -223,30 +223,29 @@ qsb_status qsb_ham_apply(qsb_ham* h, qsb_dtype dtype, int is_complex, int nb, co
     cudaStream_t s = (cudaStream_t)stream;
     if (!is_complex) gx = gy = gz = 0.0;
     const double dV = h->dx * h->dy * h->dz;
-    NLView nv{};
     const bool has_nl = h->nl.n_points > 0;
+    const int ncol = is_complex ? 2 * nb : nb;
+    double* coef = nullptr;
+    if (has_nl) QSB_TRY(ensure_ws(h, nl_workspace_bytes(h->nl, ncol)));
     if (h->timing) QSB_TRY(timing_event(h, s));
+    // 1) <beta|psi>: deterministic chunked projection (mInnerNonlocalPsi_v4_bundle)
     if (has_nl) {
-        const int ncol = is_complex ? 2 * nb : nb;
-        QSB_TRY(ensure_ws(h, nl_workspace_bytes(h->nl, ncol)));
-        double* coef = nullptr;
         QSB_TRY(nl_project(dtype, h->nl, h->nx, h->ny, h->nz, nb, is_complex, psi_dev, dV, gx * h->dx, gy * h->dy,
                            gz * h->dz, false, h->ws, &coef, s));
-        nv.grid_ptr = h->nl.grid_ptr;
-        nv.ent_atom = h->nl.ent_atom;
-        nv.ent_xyz = h->nl.ent_xyz;
-        nv.ent_beta = dtype == QSB_F64 ? (const void*)h->nl.ent_beta64 : (const void*)h->nl.ent_beta32;
-        nv.coef = coef;
-        nv.wmax = h->nl.wmax;
-        nv.ncol = ncol;
-        nv.gx_dx = gx * h->dx; nv.gy_dy = gy * h->dy; nv.gz_dz = gz * h->dz;
         h->launches += 2;
     }
     if (h->timing) QSB_TRY(timing_event(h, s));
+    // 2) hpsi = V psi - 1/2 FD8(psi)   (mPotentialMatrix_ddm + mKineticMatrixAdd_ddm_kpint)
     StencilLaunch L{h->nx, h->ny, h->nz, nb, is_complex ? 1 : 0, 1, psi_dev, hpsi_dev,
-                    dtype == QSB_F64 ? (const void*)h->V64 : (const void*)h->V32, has_nl ? &nv : nullptr};
+                    dtype == QSB_F64 ? (const void*)h->V64 : (const void*)h->V32};
     QSB_TRY(launch_stencil(dtype, L, make_fd8_coef(-0.5, h->dx, h->dy, h->dz, gx, gy, gz), s));
     h->launches += 1;
+    if (h->timing) QSB_TRY(timing_event(h, s));
+    // 3) hpsi += sum |beta> E <beta|psi>   (ProjectionPP_bundle expansion, pull form)
+    if (has_nl) {
+        QSB_TRY(nl_apply(dtype, h->nl, (int)h->N, nb, is_complex, hpsi_dev, coef, gx * h->dx, gy * h->dy, gz * h->dz, s));
+        h->launches += 1;
+    }
     if (h->timing) QSB_TRY(timing_event(h, s));
     return QSB_OK;
 }
@@ -257,22 +256,26 @@ qsb_status qsb_ham_set_timing(qsb_ham* h, int enable) {
     return QSB_OK;
 }
 
-qsb_status qsb_ham_get_timing(qsb_ham* h, double* project_ms, double* stencil_ms, int* applies, int* kernel_launches) {
+qsb_status qsb_ham_get_timing(qsb_ham* h, double* project_ms, double* stencil_ms, double* expand_ms, int* applies,
+                              int* kernel_launches) {
     if (!h) return fail(QSB_ERR_INVALID, "get_timing: null context");
-    double pm = 0.0, sm = 0.0;
-    const size_t n = h->ev_rec.size() / 3;
+    double pm = 0.0, sm = 0.0, em = 0.0;
+    const size_t n = h->ev_rec.size() / 4;
     for (size_t i = 0; i < n; ++i) {
-        float a = 0.f, b = 0.f;
-        QSB_CUDA_TRY(cudaEventSynchronize(h->ev_rec[3 * i + 2]));
-        QSB_CUDA_TRY(cudaEventElapsedTime(&a, h->ev_rec[3 * i], h->ev_rec[3 * i + 1]));
-        QSB_CUDA_TRY(cudaEventElapsedTime(&b, h->ev_rec[3 * i + 1], h->ev_rec[3 * i + 2]));
+        float a = 0.f, b = 0.f, c = 0.f;
+        QSB_CUDA_TRY(cudaEventSynchronize(h->ev_rec[4 * i + 3]));
+        QSB_CUDA_TRY(cudaEventElapsedTime(&a, h->ev_rec[4 * i], h->ev_rec[4 * i + 1]));
+        QSB_CUDA_TRY(cudaEventElapsedTime(&b, h->ev_rec[4 * i + 1], h->ev_rec[4 * i + 2]));
+        QSB_CUDA_TRY(cudaEventElapsedTime(&c, h->ev_rec[4 * i + 2], h->ev_rec[4 * i + 3]));
         pm += a;
         sm += b;
+        em += c;
     }
     h->ev_pool.insert(h->ev_pool.end(), h->ev_rec.begin(), h->ev_rec.end());
     h->ev_rec.clear();
     if (project_ms) *project_ms = pm;
     if (stencil_ms) *stencil_ms = sm;
+    if (expand_ms) *expand_ms = em;
     if (applies) *applies = (int)n;
     if (kernel_launches) *kernel_launches = h->launches;
     h->launches = 0;

@@ -38,30 +38,15 @@ struct FD8Coef {
 };
 FD8Coef make_fd8_coef(double coef, double dx, double dy, double dz, double gx, double gy, double gz);
 
-// Fused nonlocal pull inside the H stencil: hpsi_col[g] += sum over projector
-// points e on grid point g of sum_w beta_e[w] * coef[atom_e][w][col] (times
-// exp(-i g.r_e) in the complex case).
-struct NLView {
-    const int* grid_ptr;      // [N+1] entry ranges per grid point
-    const int* ent_atom;
-    const int* ent_xyz;
-    const void* ent_beta;     // T[n_points][wmax]
-    const double* coef;       // [atom][wmax][ncol]
-    int wmax;
-    int ncol;
-    double gx_dx, gy_dy, gz_dz;
-};
-
 // Launch configuration of the stencil kernels.
 struct StencilLaunch {
     int nx, ny, nz;
     int nb;                  // bands
     int is_complex;          // SoA complex bundle
-    int mode;                // 0: out += coef*L(psi); 1: out = V psi + coef*L(psi) (+ NL)
+    int mode;                // 0: out += coef*L(psi); 1: out = V psi + coef*L(psi)
     const void* in;
     void* out;
     const void* V;           // mode 1 only
-    const NLView* nl;        // fused nonlocal apply (mode 1), or nullptr
 };
 
 qsb_status launch_stencil(qsb_dtype dt, const StencilLaunch& L, const FD8Coef& c, cudaStream_t s);

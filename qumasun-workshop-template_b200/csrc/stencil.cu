@@ -47,9 +47,8 @@ FD8Coef make_fd8_coef(double coef, double dx, double dy, double dz, double gx, d
 namespace {
 
 constexpr int TX = 32;        // tile width (one warp)
-constexpr int BY = 8;         // thread rows per CTA
-constexpr int RY = 2;         // grid rows per thread
-constexpr int TY = BY * RY;   // tile height
+constexpr int BY = 8;         // warps per CTA, stacked in y
+constexpr int NT = TX * BY;   // threads per CTA
 constexpr int HW = 4;         // halo width of the 8th-order stencil
 
 template <typename T>
@@ -75,13 +74,27 @@ __device__ __forceinline__ int wrapi(int v, int n) {
     return m < 0 ? m + n : m;
 }
 
-// MODE 0: out += coef*L(psi).  MODE 1: out = V psi + coef*L(psi) [+ NL].
-template <typename T, bool CPLX, int MODE, bool GRAD, bool NL>
-__global__ void __launch_bounds__(TX * BY, 2)
+// One CTA: a TX x TY tile (TY = BY*RY) of one band (both SoA planes for
+// complex), marching z over [z0, z1).  Thread (tx, ty) owns the RY
+// consecutive grid rows y0 + ty*RY + i at x0 + tx and keeps their z columns
+// (z-4 .. z+4) in registers; the current plane plus its 4-wide x/y halo sits in
+// a double-buffered shared tile.  Every global load is issued ahead of use:
+// centre values 4 planes ahead (the z queue), halo values 2 planes ahead (a
+// register shift of two planes), so a single __syncthreads per plane is the
+// only wait.  The y derivative of the RY rows is read as one column of RY+8
+// shared values (instead of 8 per point).
+//
+// MODE 0: out += L(psi)      (Laplacian8th / LaplacianKpoint8th "+=")
+// MODE 1: out = V psi + L(psi)   (the local part of mHamiltonianMatrix_ddm)
+template <typename T, bool CPLX, int MODE, bool GRAD, int RY>
+__global__ void __launch_bounds__(NT, 2)
 fd8_kernel(const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ V,
-           int nx, int ny, int nz, int zchunk, KC<T> k, NLView nl) {
+           int nx, int ny, int nz, int zchunk, KC<T> k) {
     constexpr int NC = CPLX ? 2 : 1;
-    __shared__ T sm[2][NC][TY + 2 * HW][TX + 2 * HW];
+    constexpr int TY = BY * RY;
+    constexpr int SW = TX + 2 * HW;
+    constexpr int SH = TY + 2 * HW;
+    __shared__ T sm[2][NC][SH][SW];
 
     const int ntx = (nx + TX - 1) / TX;
     const int x0 = (blockIdx.x % ntx) * TX;
@@ -104,203 +117,176 @@ fd8_kernel(const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ 
     }
 
     const int tx = threadIdx.x, ty = threadIdx.y;
+    const int t = ty * TX + tx;
     const int x = x0 + tx;
     const bool xin = tx < wx;
-
-    bool rvalid[RY];
-    int yrow[RY];
+    bool rv[RY];
 #pragma unroll
-    for (int r = 0; r < RY; ++r) {
-        yrow[r] = y0 + ty + BY * r;
-        rvalid[r] = xin && (ty + BY * r < wy);
+    for (int i = 0; i < RY; ++i) rv[i] = xin && (ty * RY + i < wy);
+    const size_t rowoff = (size_t)x + (size_t)nx * (y0 + ty * RY);   // grid offset of row 0 of this thread
+
+    // x-halo role: 8*TY positions (left/right, TY rows, 4 columns)
+    bool xh_ok = false;
+    size_t xh_g = 0;
+    int xh_s = 0;
+    if (t < 8 * TY) {
+        const int side = t / (4 * TY), rem = t % (4 * TY), hrow = rem / 4, hk = rem % 4;
+        xh_ok = hrow < wy;
+        const int gxx = side == 0 ? wrapi(x0 - HW + hk, nx) : wrapi(x0 + wx + hk, nx);
+        xh_g = (size_t)gxx + (size_t)nx * (y0 + min(hrow, wy - 1));
+        xh_s = (HW + hrow) * SW + (side == 0 ? hk : wx + HW + hk);
+    }
+    // y-halo role: 8*TX positions (top/bottom, 4 rows, TX columns)
+    bool yh_ok = false;
+    size_t yh_g = 0;
+    int yh_s = 0;
+    if (t < 8 * TX) {
+        const int side = t / (4 * TX), rem = t % (4 * TX), hr = rem / TX, hc = rem % TX;
+        yh_ok = hc < wx;
+        const int gyy = side == 0 ? wrapi(y0 - HW + hr, ny) : wrapi(y0 + wy + hr, ny);
+        yh_g = (size_t)(x0 + min(hc, wx - 1)) + (size_t)nx * gyy;
+        yh_s = (side == 0 ? hr : wy + HW + hr) * SW + HW + hc;
     }
 
-    // register queue: q[c][r][j] = psi(x, y_r, z - 4 + j)
+    // prefetched halos of planes z (index 0) and z+1 (index 1)
+    T hx[2][NC], hy[2][NC];
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+        const size_t zo = nxy * (size_t)wrapi(z0 + d, nz);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            hx[d][c] = xh_ok ? __ldg(src[c] + xh_g + zo) : T(0);
+            hy[d][c] = yh_ok ? __ldg(src[c] + yh_g + zo) : T(0);
+        }
+    }
+    // z queues: q[c][i][j] = psi(x, y_i, z - 4 + j)
     T q[NC][RY][9];
 #pragma unroll
     for (int c = 0; c < NC; ++c)
 #pragma unroll
-        for (int r = 0; r < RY; ++r) {
-            q[c][r][0] = T(0);
+        for (int i = 0; i < RY; ++i) {
+            q[c][i][0] = T(0);
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                const int zz = wrapi(z0 - HW + j, nz);
-                q[c][r][j + 1] = rvalid[r] ? __ldg(src[c] + x + (size_t)nx * yrow[r] + nxy * zz) : T(0);
+                const size_t zo = nxy * (size_t)wrapi(z0 - HW + j, nz);
+                q[c][i][j + 1] = rv[i] ? __ldg(src[c] + rowoff + (size_t)nx * i + zo) : T(0);
             }
         }
-
-    // halo roles
-    const int hx_left = (tx < HW);
-    const int hx_right = (tx >= HW && tx < 2 * HW);
-    const int xl = wrapi(x0 - HW + tx, nx);             // for left-halo threads
-    const int xr = wrapi(x0 + wx + (tx - HW), nx);      // for right-halo threads
-    const int ytop = wrapi(y0 - HW + ty, ny);           // ty < 4
-    const int ybot = wrapi(y0 + wy + (ty - HW), ny);    // 4 <= ty < 8
 
     for (int z = z0; z < z1; ++z) {
         const int buf = (z - z0) & 1;
-        const int zn = wrapi(z + HW, nz);
-        const size_t zoff = nxy * (size_t)z;
+        T* sb = &sm[buf][0][0][0];
+        // halos of plane z into shared memory, then prefetch plane z+2
+        const size_t zo2 = nxy * (size_t)wrapi(z + 2, nz);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            if (xh_ok) sb[c * SH * SW + xh_s] = hx[0][c];
+            if (yh_ok) sb[c * SH * SW + yh_s] = hy[0][c];
+            hx[0][c] = hx[1][c];
+            hy[0][c] = hy[1][c];
+            hx[1][c] = xh_ok ? __ldg(src[c] + xh_g + zo2) : T(0);
+            hy[1][c] = yh_ok ? __ldg(src[c] + yh_g + zo2) : T(0);
+        }
+        // advance the z queues (load plane z+4) and write the centre of plane z
+        const size_t zo4 = nxy * (size_t)wrapi(z + HW, nz);
 #pragma unroll
         for (int c = 0; c < NC; ++c)
 #pragma unroll
-            for (int r = 0; r < RY; ++r) {
+            for (int i = 0; i < RY; ++i) {
 #pragma unroll
-                for (int j = 0; j < 8; ++j) q[c][r][j] = q[c][r][j + 1];
-                q[c][r][8] = rvalid[r] ? __ldg(src[c] + x + (size_t)nx * yrow[r] + nxy * zn) : T(0);
-                sm[buf][c][ty + BY * r + HW][tx + HW] = q[c][r][4];
+                for (int j = 0; j < 8; ++j) q[c][i][j] = q[c][i][j + 1];
+                q[c][i][8] = rv[i] ? __ldg(src[c] + rowoff + (size_t)nx * i + zo4) : T(0);
+                // only in-tile threads write centres: for a partial tile the cells of
+                // out-of-tile threads alias the right / bottom halo
+                if (rv[i]) sm[buf][c][ty * RY + i + HW][tx + HW] = q[c][i][4];
             }
-        // x halos of this plane
-        if (hx_left || hx_right) {
-            const int xs = hx_left ? xl : xr;
-            const int col = hx_left ? tx : (wx + HW + (tx - HW));
-#pragma unroll
-            for (int r = 0; r < RY; ++r) {
-                if (ty + BY * r < wy) {
-#pragma unroll
-                    for (int c = 0; c < NC; ++c)
-                        sm[buf][c][ty + BY * r + HW][col] = __ldg(src[c] + xs + (size_t)nx * yrow[r] + zoff);
-                }
-            }
-        }
-        // y halos of this plane
-        if (xin) {
-            if (ty < HW) {
-#pragma unroll
-                for (int c = 0; c < NC; ++c)
-                    sm[buf][c][ty][tx + HW] = __ldg(src[c] + x + (size_t)nx * ytop + zoff);
-            } else if (ty < 2 * HW) {
-#pragma unroll
-                for (int c = 0; c < NC; ++c)
-                    sm[buf][c][wy + HW + (ty - HW)][tx + HW] = __ldg(src[c] + x + (size_t)nx * ybot + zoff);
-            }
-        }
         __syncthreads();
 
+        T res[NC][RY];
+        T grd[NC][RY];
 #pragma unroll
-        for (int r = 0; r < RY; ++r) {
-            if (!rvalid[r]) continue;
-            const int sy = ty + BY * r + HW;
-            const int sx = tx + HW;
-            T lap[NC], grd[NC];
+        for (int c = 0; c < NC; ++c) {
+            const T(*s)[SW] = sm[buf][c];
+            T col[RY + 8];
 #pragma unroll
-            for (int c = 0; c < NC; ++c) {
-                const T(*s)[TX + 2 * HW] = sm[buf][c];
-                const T* qq = q[c][r];
+            for (int j = 0; j < RY + 8; ++j) col[j] = s[ty * RY + j][tx + HW];
+#pragma unroll
+            for (int i = 0; i < RY; ++i) {
+                const int sy = ty * RY + i + HW, sx = tx + HW;
+                const T* qq = q[c][i];
+                const T xm4 = s[sy][sx - 4], xm3 = s[sy][sx - 3], xm2 = s[sy][sx - 2], xm1 = s[sy][sx - 1];
+                const T xp1 = s[sy][sx + 1], xp2 = s[sy][sx + 2], xp3 = s[sy][sx + 3], xp4 = s[sy][sx + 4];
                 T d = k.c0 * qq[4];
-                d += k.cx[3] * (s[sy][sx + 4] + s[sy][sx - 4]) + k.cx[2] * (s[sy][sx + 3] + s[sy][sx - 3]) +
-                     k.cx[1] * (s[sy][sx + 2] + s[sy][sx - 2]) + k.cx[0] * (s[sy][sx + 1] + s[sy][sx - 1]);
-                d += k.cy[3] * (s[sy + 4][sx] + s[sy - 4][sx]) + k.cy[2] * (s[sy + 3][sx] + s[sy - 3][sx]) +
-                     k.cy[1] * (s[sy + 2][sx] + s[sy - 2][sx]) + k.cy[0] * (s[sy + 1][sx] + s[sy - 1][sx]);
+                d += k.cx[3] * (xp4 + xm4) + k.cx[2] * (xp3 + xm3) + k.cx[1] * (xp2 + xm2) + k.cx[0] * (xp1 + xm1);
+                d += k.cy[3] * (col[i + 8] + col[i]) + k.cy[2] * (col[i + 7] + col[i + 1]) +
+                     k.cy[1] * (col[i + 6] + col[i + 2]) + k.cy[0] * (col[i + 5] + col[i + 3]);
                 d += k.cz[3] * (qq[8] + qq[0]) + k.cz[2] * (qq[7] + qq[1]) + k.cz[1] * (qq[6] + qq[2]) +
                      k.cz[0] * (qq[5] + qq[3]);
-                lap[c] = d;
+                res[c][i] = d;
                 if (GRAD) {
-                    T g = k.ax[3] * (s[sy][sx + 4] - s[sy][sx - 4]) + k.ax[2] * (s[sy][sx + 3] - s[sy][sx - 3]) +
-                          k.ax[1] * (s[sy][sx + 2] - s[sy][sx - 2]) + k.ax[0] * (s[sy][sx + 1] - s[sy][sx - 1]);
-                    g += k.ay[3] * (s[sy + 4][sx] - s[sy - 4][sx]) + k.ay[2] * (s[sy + 3][sx] - s[sy - 3][sx]) +
-                         k.ay[1] * (s[sy + 2][sx] - s[sy - 2][sx]) + k.ay[0] * (s[sy + 1][sx] - s[sy - 1][sx]);
+                    T g = k.ax[3] * (xp4 - xm4) + k.ax[2] * (xp3 - xm3) + k.ax[1] * (xp2 - xm2) + k.ax[0] * (xp1 - xm1);
+                    g += k.ay[3] * (col[i + 8] - col[i]) + k.ay[2] * (col[i + 7] - col[i + 1]) +
+                         k.ay[1] * (col[i + 6] - col[i + 2]) + k.ay[0] * (col[i + 5] - col[i + 3]);
                     g += k.az[3] * (qq[8] - qq[0]) + k.az[2] * (qq[7] - qq[1]) + k.az[1] * (qq[6] - qq[2]) +
                          k.az[0] * (qq[5] - qq[3]);
-                    grd[c] = g;
-                } else {
-                    grd[c] = T(0);
+                    grd[c][i] = g;
                 }
             }
-            T res[NC];
-            if (CPLX) {
-                // out.re: Lap(re) - D(im);  out.im: Lap(im) + D(re)
-                res[0] = GRAD ? lap[0] - grd[NC - 1] : lap[0];
-                res[NC - 1] = GRAD ? lap[NC - 1] + grd[0] : lap[NC - 1];
-            } else {
-                res[0] = lap[0];
-            }
-            const size_t gidx = (size_t)x + (size_t)nx * yrow[r] + zoff;
-            if (MODE == 0) {
+        }
+        const size_t zo = nxy * (size_t)z;
 #pragma unroll
-                for (int c = 0; c < NC; ++c) dst[c][gidx] += res[c];
+        for (int i = 0; i < RY; ++i) {
+            if (!rv[i]) continue;
+            const size_t gidx = rowoff + (size_t)nx * i + zo;
+            T r0 = res[0][i], r1 = res[NC - 1][i];
+            if (CPLX && GRAD) {
+                // out.re: Lap(re) - D(im);  out.im: Lap(im) + D(re)
+                r0 = res[0][i] - grd[NC - 1][i];
+                r1 = res[NC - 1][i] + grd[0][i];
+            }
+            if (MODE == 0) {
+                dst[0][gidx] += r0;
+                if (CPLX) dst[NC - 1][gidx] += r1;
             } else {
                 const T v = __ldg(V + gidx);
-                T nlv[NC];
-#pragma unroll
-                for (int c = 0; c < NC; ++c) nlv[c] = T(0);
-                if (NL) {
-                    const int e0 = __ldg(nl.grid_ptr + gidx), e1 = __ldg(nl.grid_ptr + gidx + 1);
-                    {
-                        const T* beta = (const T*)nl.ent_beta;
-                        for (int e = e0; e < e1; ++e) {
-                            const int a = __ldg(nl.ent_atom + e);
-                            const double* cf = nl.coef + (size_t)a * nl.wmax * nl.ncol;
-                            double tr = 0.0, ti = 0.0;
-                            for (int w = 0; w < nl.wmax; ++w) {
-                                const double b = (double)__ldg(beta + (size_t)e * nl.wmax + w);
-                                if (CPLX) {
-                                    tr += b * __ldg(cf + (size_t)w * nl.ncol + 2 * band);
-                                    ti += b * __ldg(cf + (size_t)w * nl.ncol + 2 * band + 1);
-                                } else {
-                                    tr += b * __ldg(cf + (size_t)w * nl.ncol + band);
-                                }
-                            }
-                            if (CPLX) {
-                                const int* xyz = nl.ent_xyz + 3 * (size_t)e;
-                                const double kxx = nl.gx_dx * (double)__ldg(xyz + 0);
-                                const double kyy = nl.gy_dy * (double)__ldg(xyz + 1);
-                                const double kzz = nl.gz_dz * (double)__ldg(xyz + 2);
-                                double sn, cs;
-                                sincos(kxx + kyy + kzz, &sn, &cs);
-                                // multiply by exp(-i k.r): (cs*tr + sn*ti, cs*ti - sn*tr)
-                                nlv[0] += (T)(cs * tr + sn * ti);
-                                nlv[NC - 1] += (T)(cs * ti - sn * tr);
-                            } else {
-                                nlv[0] += (T)tr;
-                            }
-                        }
-                    }
-                }
-#pragma unroll
-                for (int c = 0; c < NC; ++c) dst[c][gidx] = v * q[c][r][4] + nlv[c] + res[c];
+                dst[0][gidx] = v * q[0][i][4] + r0;
+                if (CPLX) dst[NC - 1][gidx] = v * q[NC - 1][i][4] + r1;
             }
         }
     }
 }
 
-template <typename T, bool CPLX, int MODE, bool NL>
-void launch_t(const StencilLaunch& L, const FD8Coef& c, const NLView& nv, cudaStream_t s) {
+template <typename T, bool CPLX, int MODE>
+void launch_t(const StencilLaunch& L, const FD8Coef& c, cudaStream_t s) {
+    constexpr int RY = CPLX ? 2 : 4;
+    constexpr int TY = BY * RY;
     const int ntx = (L.nx + TX - 1) / TX, nty = (L.ny + TY - 1) / TY;
     const int tiles = ntx * nty;
-    // Enough CTAs to fill 148 SMs x 2 resident CTAs several times over;
-    // split z only when tiles x bands is small.
+    // enough CTAs for 148 SMs x 2 resident CTAs x 3 waves; split z only when
+    // tiles x bands is small, keeping chunks of >= 16 planes
     int zsplit = 1;
     const long long ctas = (long long)tiles * L.nb;
-    while (ctas * zsplit < 148LL * 2 * 4 && L.nz / (zsplit * 2) >= 8) zsplit *= 2;
+    while (ctas * zsplit < 148LL * 2 * 3 && L.nz / (zsplit * 2) >= 16) zsplit *= 2;
     const int zchunk = (L.nz + zsplit - 1) / zsplit;
     const int nzc = (L.nz + zchunk - 1) / zchunk;
     dim3 grid(tiles, nzc, L.nb), block(TX, BY);
     const KC<T> k = to_kc<T>(c);
-    if (c.has_grad && CPLX)
-        fd8_kernel<T, CPLX, MODE, CPLX, NL><<<grid, block, 0, s>>>((const T*)L.in, (T*)L.out, (const T*)L.V, L.nx, L.ny,
-                                                                  L.nz, zchunk, k, nv);
+    if (CPLX && c.has_grad)
+        fd8_kernel<T, CPLX, MODE, CPLX, RY><<<grid, block, 0, s>>>((const T*)L.in, (T*)L.out, (const T*)L.V, L.nx,
+                                                                   L.ny, L.nz, zchunk, k);
     else
-        fd8_kernel<T, CPLX, MODE, false, NL><<<grid, block, 0, s>>>((const T*)L.in, (T*)L.out, (const T*)L.V, L.nx, L.ny,
-                                                                   L.nz, zchunk, k, nv);
+        fd8_kernel<T, CPLX, MODE, false, RY><<<grid, block, 0, s>>>((const T*)L.in, (T*)L.out, (const T*)L.V, L.nx,
+                                                                    L.ny, L.nz, zchunk, k);
 }
 
 template <typename T>
 qsb_status launch_dtype(const StencilLaunch& L, const FD8Coef& c, cudaStream_t s) {
-    NLView nv{};
-    const bool nl = (L.nl != nullptr);
-    if (nl) nv = *L.nl;
     if (L.mode == 0) {
-        if (L.is_complex) launch_t<T, true, 0, false>(L, c, nv, s);
-        else launch_t<T, false, 0, false>(L, c, nv, s);
+        if (L.is_complex) launch_t<T, true, 0>(L, c, s);
+        else launch_t<T, false, 0>(L, c, s);
     } else {
-        if (L.is_complex) {
-            if (nl) launch_t<T, true, 1, true>(L, c, nv, s);
-            else launch_t<T, true, 1, false>(L, c, nv, s);
-        } else {
-            if (nl) launch_t<T, false, 1, true>(L, c, nv, s);
-            else launch_t<T, false, 1, false>(L, c, nv, s);
-        }
+        if (L.is_complex) launch_t<T, true, 1>(L, c, s);
+        else launch_t<T, false, 1>(L, c, s);
     }
     QSB_CUDA_TRY(cudaGetLastError());
     return QSB_OK;

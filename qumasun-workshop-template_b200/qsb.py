@@ -175,11 +175,12 @@ class Hamiltonian:
         _check(lib.qsb_ham_set_timing(self._h, int(bool(enable))))
 
     def get_timing(self):
-        """(projection_ms, stencil_ms, applies, kernel_launches) since the last call."""
-        pm, sm = ctypes.c_double(), ctypes.c_double()
+        """(projection_ms, stencil_ms, expansion_ms, applies, kernel_launches) since the last call."""
+        pm, sm, em = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         n, k = ctypes.c_int(), ctypes.c_int()
-        _check(lib.qsb_ham_get_timing(self._h, ctypes.byref(pm), ctypes.byref(sm), ctypes.byref(n), ctypes.byref(k)))
-        return pm.value, sm.value, n.value, k.value
+        _check(lib.qsb_ham_get_timing(self._h, ctypes.byref(pm), ctypes.byref(sm), ctypes.byref(em), ctypes.byref(n),
+                                      ctypes.byref(k)))
+        return pm.value, sm.value, em.value, n.value, k.value
 
     def _nb(self, psi, is_complex):
         return psi.numel() // ((2 if is_complex else 1) * self.N)
