@@ -49,6 +49,13 @@ QSB_API const char* qsb_last_error(void);
 /* Library version string. */
 QSB_API const char* qsb_version(void);
 
+/* Device-side error word of the current device (synchronizes with it): bit 0
+ * set means a kernel's bounded wait on an asynchronous copy ran out and that
+ * kernel returned early (its output is incomplete).  clear != 0 resets it.
+ * The reference has no counterpart (it exits on CUDA errors,
+ * source/gyield/gy_cuda.h:95-100). */
+QSB_API qsb_status qsb_device_status(int* code, int clear);
+
 /* ---------------------------------------------------------------------------
  * FD8 stencils (stateless).
  * ------------------------------------------------------------------------- */

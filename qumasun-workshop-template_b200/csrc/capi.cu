@@ -21,6 +21,22 @@ qsb_status cuda_fail(cudaError_t e, const char* where) {
     return e == cudaErrorMemoryAllocation ? QSB_ERR_NOMEM : QSB_ERR_CUDA;
 }
 
+// Error word written by kernels whose bounded waits ran out (bit 0); one per
+// device, its address looked up once per device.
+static __device__ int g_device_error = 0;
+
+int* device_error_word() {
+    static int* addr[64] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    if (!addr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_device_error) != cudaSuccess) return nullptr;
+        addr[dev] = (int*)p;
+    }
+    return addr[dev];
+}
+
 static qsb_status check_grid(int nx, int ny, int nz) {
     if (nx < 1 || ny < 1 || nz < 1) return fail(QSB_ERR_INVALID, "grid dimensions must be >= 1");
     if ((long long)nx * ny * nz >= (1LL << 31)) return fail(QSB_ERR_INVALID, "grid has 2^31 or more points");
@@ -91,6 +107,18 @@ using namespace qsb;
 extern "C" {
 
 const char* qsb_last_error(void) { return g_last_error.c_str(); }
+
+qsb_status qsb_device_status(int* code, int clear) {
+    if (!code) return fail(QSB_ERR_INVALID, "device_status: null code");
+    int v = 0;
+    QSB_CUDA_TRY(cudaMemcpyFromSymbol(&v, g_device_error, sizeof(int)));
+    *code = v;
+    if (clear && v) {
+        const int zero = 0;
+        QSB_CUDA_TRY(cudaMemcpyToSymbol(g_device_error, &zero, sizeof(int)));
+    }
+    return QSB_OK;
+}
 const char* qsb_version(void) { return "qumasun_b200 0.1.0 (sm_100a)"; }
 
 qsb_status qsb_laplacian8th(qsb_dtype dtype, int nx, int ny, int nz, int nb, void* out_dev, const void* p_dev,

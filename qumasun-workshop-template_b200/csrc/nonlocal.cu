@@ -30,7 +30,7 @@ namespace qsb {
 namespace {
 
 constexpr int PROJ_THREADS = 256;
-constexpr int CHUNK = 2048;          // points per projection chunk
+constexpr int CHUNK = 8192;          // points per projection chunk (32 per thread: amortizes the block reduction)
 constexpr int APPLY_THREADS = 256;
 
 template <typename T>
@@ -152,66 +152,91 @@ __global__ void nl_finalize_kernel(const int* __restrict__ atom_chunk_begin, con
 }
 
 // ---------------------------------------------------------------------------
-// separate pull apply over covered grid points: hpsi += sum_e beta_e . coef
+// expansion, pull form over covered grid points:
+//   hpsi_col[g] += sum_{e on g} sum_w beta_e[w] * coef[atom_e][w][col]
+// One thread per covered grid point loops over every band, so the point's
+// entries (atom, beta, Bloch phase) are loaded once into registers and the
+// band loop streams the read-modify-write of hpsi, coalesced along x.
+// Entries are taken MAXE at a time (points covered by more spheres loop).
 // ---------------------------------------------------------------------------
-template <typename T, bool CPLX, int CB>
-__global__ void __launch_bounds__(APPLY_THREADS)
+template <typename T, bool CPLX, int WM>
+__global__ void __launch_bounds__(APPLY_THREADS, 2)
 nl_apply_kernel(const int* __restrict__ cov_grid, int n_cov, const int* __restrict__ grid_ptr,
                 const int* __restrict__ ent_atom, const int* __restrict__ ent_xyz, const T* __restrict__ ent_beta,
                 int wmax, const double* __restrict__ coef, int ncol, T* __restrict__ hpsi, size_t N, int nb,
                 double gx_dx, double gy_dy, double gz_dz) {
+    constexpr int MAXE = 4;
     const int r = blockIdx.x * APPLY_THREADS + threadIdx.x;
     if (r >= n_cov) return;
-    const int band0 = blockIdx.y * CB;
-    const int nbl = min(CB, nb - band0);
     const int g = __ldg(cov_grid + r);
     const int e0 = __ldg(grid_ptr + g), e1 = __ldg(grid_ptr + g + 1);
-    constexpr int NCB = CPLX ? 2 * CB : CB;
-    double acc[NCB];
+    for (int eb = e0; eb < e1; eb += MAXE) {
+        const int ne = min(MAXE, e1 - eb);
+        const double* cf[MAXE];
+        double b[MAXE][WM];
+        double cs[MAXE], sn[MAXE];
 #pragma unroll
-    for (int i = 0; i < NCB; ++i) acc[i] = 0.0;
-    for (int e = e0; e < e1; ++e) {
-        const int a = __ldg(ent_atom + e);
-        const double* cf = coef + (size_t)a * wmax * ncol;
-        double cs = 1.0, sn = 0.0;
-        if (CPLX) {
-            const double kxx = gx_dx * (double)__ldg(ent_xyz + 3 * (size_t)e + 0);
-            const double kyy = gy_dy * (double)__ldg(ent_xyz + 3 * (size_t)e + 1);
-            const double kzz = gz_dz * (double)__ldg(ent_xyz + 3 * (size_t)e + 2);
-            sincos(kxx + kyy + kzz, &sn, &cs);
-        }
+        for (int q = 0; q < MAXE; ++q) {
+            const int e = eb + min(q, ne - 1);
+            cf[q] = coef + (size_t)__ldg(ent_atom + e) * wmax * ncol;
 #pragma unroll
-        for (int j = 0; j < CB; ++j) {
-            if (j < nbl) {
-                double tr = 0.0, ti = 0.0;
-                for (int w = 0; w < wmax; ++w) {
-                    const double b = (double)__ldg(ent_beta + (size_t)e * wmax + w);
-                    if (CPLX) {
-                        tr += b * __ldg(cf + (size_t)w * ncol + 2 * (band0 + j));
-                        ti += b * __ldg(cf + (size_t)w * ncol + 2 * (band0 + j) + 1);
-                    } else {
-                        tr += b * __ldg(cf + (size_t)w * ncol + band0 + j);
-                    }
-                }
-                if (CPLX) {
-                    // exp(-i k.r) (source/PseudoPotNonlocal_SvF2_kpoint.h:4026-4027)
-                    acc[2 * j] += cs * tr + sn * ti;
-                    acc[2 * j + 1] += cs * ti - sn * tr;
-                } else {
-                    acc[j] += tr;
-                }
+            for (int w = 0; w < WM; ++w)
+                b[q][w] = (q < ne && w < wmax) ? (double)__ldg(ent_beta + (size_t)e * wmax + w) : 0.0;
+            cs[q] = 1.0;
+            sn[q] = 0.0;
+            if (CPLX) {
+                const double kxx = gx_dx * (double)__ldg(ent_xyz + 3 * (size_t)e + 0);
+                const double kyy = gy_dy * (double)__ldg(ent_xyz + 3 * (size_t)e + 1);
+                const double kzz = gz_dz * (double)__ldg(ent_xyz + 3 * (size_t)e + 2);
+                sincos(kxx + kyy + kzz, &sn[q], &cs[q]);
             }
         }
-    }
+        // bands in groups of BG: all hpsi loads of a group are issued before any
+        // use, so BG (x2 for complex) independent loads per thread are in flight
+        constexpr int BG = CPLX ? 4 : 8;
+        for (int b0 = 0; b0 < nb; b0 += BG) {
+            T cur[BG][CPLX ? 2 : 1];
 #pragma unroll
-    for (int j = 0; j < CB; ++j) {
-        if (j < nbl) {
-            if (CPLX) {
-                const size_t base = (size_t)(2 * (band0 + j)) * N;
-                hpsi[base + g] += (T)acc[2 * j];
-                hpsi[base + N + g] += (T)acc[2 * j + 1];
-            } else {
-                hpsi[(size_t)(band0 + j) * N + g] += (T)acc[j];
+            for (int j = 0; j < BG; ++j) {
+                const int bnd = min(b0 + j, nb - 1);
+                if (CPLX) {
+                    cur[j][0] = hpsi[(size_t)(2 * bnd) * N + g];
+                    cur[j][CPLX ? 1 : 0] = hpsi[(size_t)(2 * bnd + 1) * N + g];
+                } else {
+                    cur[j][0] = hpsi[(size_t)bnd * N + g];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < BG; ++j) {
+                const int bnd = b0 + j;
+                if (bnd >= nb) break;
+                if (CPLX) {
+                    double ar = 0.0, ai = 0.0;
+#pragma unroll
+                    for (int q = 0; q < MAXE; ++q) {
+                        double tr = 0.0, ti = 0.0;
+#pragma unroll
+                        for (int w = 0; w < WM; ++w) {
+                            if (w < wmax) {
+                                tr += b[q][w] * __ldg(cf[q] + (size_t)w * ncol + 2 * bnd);
+                                ti += b[q][w] * __ldg(cf[q] + (size_t)w * ncol + 2 * bnd + 1);
+                            }
+                        }
+                        // exp(-i k.r) (source/PseudoPotNonlocal_SvF2_kpoint.h:4026-4027)
+                        ar += cs[q] * tr + sn[q] * ti;
+                        ai += cs[q] * ti - sn[q] * tr;
+                    }
+                    hpsi[(size_t)(2 * bnd) * N + g] = cur[j][0] + (T)ar;
+                    hpsi[(size_t)(2 * bnd + 1) * N + g] = cur[j][CPLX ? 1 : 0] + (T)ai;
+                } else {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int q = 0; q < MAXE; ++q)
+#pragma unroll
+                        for (int w = 0; w < WM; ++w)
+                            if (w < wmax) acc += b[q][w] * __ldg(cf[q] + (size_t)w * ncol + bnd);
+                    hpsi[(size_t)bnd * N + g] = cur[j][0] + (T)acc;
+                }
             }
         }
     }
@@ -398,29 +423,27 @@ qsb_status nl_apply(qsb_dtype dt, const NLDevice& d, int N, int nb, int is_compl
                     double gx_dx, double gy_dy, double gz_dz, cudaStream_t s) {
     if (d.n_points == 0 || d.n_cov == 0) return QSB_OK;
     const int ncol = is_complex ? 2 * nb : nb;
-    constexpr int CBR = 8, CBC = 4;
-    const int CB = is_complex ? CBC : CBR;
-    dim3 grid((d.n_cov + APPLY_THREADS - 1) / APPLY_THREADS, (nb + CB - 1) / CB);
-    if (grid.y > 65535) return fail(QSB_ERR_INVALID, "nonlocal: too many bands");
+    const dim3 grid((d.n_cov + APPLY_THREADS - 1) / APPLY_THREADS);
+#define QSB_APPLY(T, C, W, B)                                                                                      \
+    nl_apply_kernel<T, C, W><<<grid, APPLY_THREADS, 0, s>>>(d.cov_grid, d.n_cov, d.grid_ptr, d.ent_atom, d.ent_xyz, \
+                                                            B, d.wmax, coef, ncol, (T*)hpsi, (size_t)N, nb, gx_dx,  \
+                                                            gy_dy, gz_dz)
+#define QSB_APPLY_W(T, C, B)                      \
+    do {                                          \
+        if (d.wmax <= 1) QSB_APPLY(T, C, 1, B);   \
+        else if (d.wmax <= 4) QSB_APPLY(T, C, 4, B); \
+        else if (d.wmax <= 9) QSB_APPLY(T, C, 9, B); \
+        else QSB_APPLY(T, C, 16, B);              \
+    } while (0)
     if (dt == QSB_F64) {
-        if (is_complex)
-            nl_apply_kernel<double, true, CBC><<<grid, APPLY_THREADS, 0, s>>>(
-                d.cov_grid, d.n_cov, d.grid_ptr, d.ent_atom, d.ent_xyz, d.ent_beta64, d.wmax, coef, ncol,
-                (double*)hpsi, (size_t)N, nb, gx_dx, gy_dy, gz_dz);
-        else
-            nl_apply_kernel<double, false, CBR><<<grid, APPLY_THREADS, 0, s>>>(
-                d.cov_grid, d.n_cov, d.grid_ptr, d.ent_atom, d.ent_xyz, d.ent_beta64, d.wmax, coef, ncol,
-                (double*)hpsi, (size_t)N, nb, gx_dx, gy_dy, gz_dz);
+        if (is_complex) QSB_APPLY_W(double, true, d.ent_beta64);
+        else QSB_APPLY_W(double, false, d.ent_beta64);
     } else {
-        if (is_complex)
-            nl_apply_kernel<float, true, CBC><<<grid, APPLY_THREADS, 0, s>>>(
-                d.cov_grid, d.n_cov, d.grid_ptr, d.ent_atom, d.ent_xyz, d.ent_beta32, d.wmax, coef, ncol,
-                (float*)hpsi, (size_t)N, nb, gx_dx, gy_dy, gz_dz);
-        else
-            nl_apply_kernel<float, false, CBR><<<grid, APPLY_THREADS, 0, s>>>(
-                d.cov_grid, d.n_cov, d.grid_ptr, d.ent_atom, d.ent_xyz, d.ent_beta32, d.wmax, coef, ncol,
-                (float*)hpsi, (size_t)N, nb, gx_dx, gy_dy, gz_dz);
+        if (is_complex) QSB_APPLY_W(float, true, d.ent_beta32);
+        else QSB_APPLY_W(float, false, d.ent_beta32);
     }
+#undef QSB_APPLY_W
+#undef QSB_APPLY
     QSB_CUDA_TRY(cudaGetLastError());
     return QSB_OK;
 }

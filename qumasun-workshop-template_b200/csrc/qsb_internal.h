@@ -47,7 +47,12 @@ struct StencilLaunch {
     const void* in;
     void* out;
     const void* V;           // mode 1 only
+    bool tma_ok = true;      // allow the TMA-pipelined kernel (else the register-prefetch one)
 };
+
+// Device-side error word (bit 0: a bounded wait in a kernel ran out), shared by
+// all kernels of the library; read and cleared with qsb_device_status().
+int* device_error_word();
 
 qsb_status launch_stencil(qsb_dtype dt, const StencilLaunch& L, const FD8Coef& c, cudaStream_t s);
 

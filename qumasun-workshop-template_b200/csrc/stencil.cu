@@ -15,6 +15,7 @@
 //   d = c0 p; d += x terms (offsets 4,3,2,1); d += y terms; d += z terms.
 #include "qsb_internal.h"
 #include <cmath>
+#include <cuda.h>
 
 namespace qsb {
 
@@ -87,7 +88,7 @@ __device__ __forceinline__ int wrapi(int v, int n) {
 // MODE 0: out += L(psi)      (Laplacian8th / LaplacianKpoint8th "+=")
 // MODE 1: out = V psi + L(psi)   (the local part of mHamiltonianMatrix_ddm)
 template <typename T, bool CPLX, int MODE, bool GRAD, int RY>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, (CPLX && sizeof(T) == 8) ? 1 : 2)
 fd8_kernel(const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ V,
            int nx, int ny, int nz, int zchunk, KC<T> k) {
     constexpr int NC = CPLX ? 2 : 1;
@@ -148,8 +149,11 @@ fd8_kernel(const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ 
         yh_s = (side == 0 ? hr : wy + HW + hr) * SW + HW + hc;
     }
 
-    // prefetched halos of planes z (index 0) and z+1 (index 1)
-    T hx[2][NC], hy[2][NC];
+    // Register rotation without moves: the z loop is unrolled by 9, so at phase
+    // p (z = zb + p) plane z-4+k lives in queue slot (p+k) % 9 and the halo of
+    // plane z+d in halo slot (p+d) % 3, all compile-time indices.  A load issued
+    // at phase p is first read 4 (centre) or 2 (halo) planes later.
+    T hx[3][NC], hy[3][NC];
 #pragma unroll
     for (int d = 0; d < 2; ++d) {
         const size_t zo = nxy * (size_t)wrapi(z0 + d, nz);
@@ -159,106 +163,504 @@ fd8_kernel(const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ 
             hy[d][c] = yh_ok ? __ldg(src[c] + yh_g + zo) : T(0);
         }
     }
-    // z queues: q[c][i][j] = psi(x, y_i, z - 4 + j)
+    // epilogue operand prefetched 2 planes ahead like the halos: V (MODE 1) or
+    // the accumulated output (MODE 0), 3-slot rotation
+    constexpr int NE = MODE == 0 ? NC : 1;
+    T ep[3][NE][RY];
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+        const size_t zo = nxy * (size_t)wrapi(z0 + d, nz);
+#pragma unroll
+        for (int i = 0; i < RY; ++i) {
+            if (MODE == 0) {
+#pragma unroll
+                for (int c = 0; c < NE; ++c) ep[d][c][i] = rv[i] ? dst[c][rowoff + (size_t)nx * i + zo] : T(0);
+            } else {
+                ep[d][0][i] = rv[i] ? __ldg(V + rowoff + (size_t)nx * i + zo) : T(0);
+            }
+        }
+    }
     T q[NC][RY][9];
 #pragma unroll
     for (int c = 0; c < NC; ++c)
 #pragma unroll
-        for (int i = 0; i < RY; ++i) {
-            q[c][i][0] = T(0);
+        for (int i = 0; i < RY; ++i)
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
                 const size_t zo = nxy * (size_t)wrapi(z0 - HW + j, nz);
-                q[c][i][j + 1] = rv[i] ? __ldg(src[c] + rowoff + (size_t)nx * i + zo) : T(0);
+                q[c][i][j] = rv[i] ? __ldg(src[c] + rowoff + (size_t)nx * i + zo) : T(0);
             }
-        }
 
-    for (int z = z0; z < z1; ++z) {
-        const int buf = (z - z0) & 1;
-        T* sb = &sm[buf][0][0][0];
-        // halos of plane z into shared memory, then prefetch plane z+2
-        const size_t zo2 = nxy * (size_t)wrapi(z + 2, nz);
+    for (int zb = z0; zb < z1; zb += 9) {
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
-            if (xh_ok) sb[c * SH * SW + xh_s] = hx[0][c];
-            if (yh_ok) sb[c * SH * SW + yh_s] = hy[0][c];
-            hx[0][c] = hx[1][c];
-            hy[0][c] = hy[1][c];
-            hx[1][c] = xh_ok ? __ldg(src[c] + xh_g + zo2) : T(0);
-            hy[1][c] = yh_ok ? __ldg(src[c] + yh_g + zo2) : T(0);
-        }
-        // advance the z queues (load plane z+4) and write the centre of plane z
-        const size_t zo4 = nxy * (size_t)wrapi(z + HW, nz);
+        for (int p = 0; p < 9; ++p) {
+            const int z = zb + p;
+            if (z < z1) {
+                const int buf = (z - z0) & 1;
+                T* sb = &sm[buf][0][0][0];
+                const size_t zo2 = nxy * (size_t)wrapi(z + 2, nz);
 #pragma unroll
-        for (int c = 0; c < NC; ++c)
-#pragma unroll
-            for (int i = 0; i < RY; ++i) {
-#pragma unroll
-                for (int j = 0; j < 8; ++j) q[c][i][j] = q[c][i][j + 1];
-                q[c][i][8] = rv[i] ? __ldg(src[c] + rowoff + (size_t)nx * i + zo4) : T(0);
-                // only in-tile threads write centres: for a partial tile the cells of
-                // out-of-tile threads alias the right / bottom halo
-                if (rv[i]) sm[buf][c][ty * RY + i + HW][tx + HW] = q[c][i][4];
-            }
-        __syncthreads();
-
-        T res[NC][RY];
-        T grd[NC][RY];
-#pragma unroll
-        for (int c = 0; c < NC; ++c) {
-            const T(*s)[SW] = sm[buf][c];
-            T col[RY + 8];
-#pragma unroll
-            for (int j = 0; j < RY + 8; ++j) col[j] = s[ty * RY + j][tx + HW];
-#pragma unroll
-            for (int i = 0; i < RY; ++i) {
-                const int sy = ty * RY + i + HW, sx = tx + HW;
-                const T* qq = q[c][i];
-                const T xm4 = s[sy][sx - 4], xm3 = s[sy][sx - 3], xm2 = s[sy][sx - 2], xm1 = s[sy][sx - 1];
-                const T xp1 = s[sy][sx + 1], xp2 = s[sy][sx + 2], xp3 = s[sy][sx + 3], xp4 = s[sy][sx + 4];
-                T d = k.c0 * qq[4];
-                d += k.cx[3] * (xp4 + xm4) + k.cx[2] * (xp3 + xm3) + k.cx[1] * (xp2 + xm2) + k.cx[0] * (xp1 + xm1);
-                d += k.cy[3] * (col[i + 8] + col[i]) + k.cy[2] * (col[i + 7] + col[i + 1]) +
-                     k.cy[1] * (col[i + 6] + col[i + 2]) + k.cy[0] * (col[i + 5] + col[i + 3]);
-                d += k.cz[3] * (qq[8] + qq[0]) + k.cz[2] * (qq[7] + qq[1]) + k.cz[1] * (qq[6] + qq[2]) +
-                     k.cz[0] * (qq[5] + qq[3]);
-                res[c][i] = d;
-                if (GRAD) {
-                    T g = k.ax[3] * (xp4 - xm4) + k.ax[2] * (xp3 - xm3) + k.ax[1] * (xp2 - xm2) + k.ax[0] * (xp1 - xm1);
-                    g += k.ay[3] * (col[i + 8] - col[i]) + k.ay[2] * (col[i + 7] - col[i + 1]) +
-                         k.ay[1] * (col[i + 6] - col[i + 2]) + k.ay[0] * (col[i + 5] - col[i + 3]);
-                    g += k.az[3] * (qq[8] - qq[0]) + k.az[2] * (qq[7] - qq[1]) + k.az[1] * (qq[6] - qq[2]) +
-                         k.az[0] * (qq[5] - qq[3]);
-                    grd[c][i] = g;
+                for (int c = 0; c < NC; ++c) {
+                    if (xh_ok) sb[c * SH * SW + xh_s] = hx[p % 3][c];
+                    if (yh_ok) sb[c * SH * SW + yh_s] = hy[p % 3][c];
+                    hx[(p + 2) % 3][c] = xh_ok ? __ldg(src[c] + xh_g + zo2) : T(0);
+                    hy[(p + 2) % 3][c] = yh_ok ? __ldg(src[c] + yh_g + zo2) : T(0);
                 }
-            }
-        }
-        const size_t zo = nxy * (size_t)z;
 #pragma unroll
-        for (int i = 0; i < RY; ++i) {
-            if (!rv[i]) continue;
-            const size_t gidx = rowoff + (size_t)nx * i + zo;
-            T r0 = res[0][i], r1 = res[NC - 1][i];
-            if (CPLX && GRAD) {
-                // out.re: Lap(re) - D(im);  out.im: Lap(im) + D(re)
-                r0 = res[0][i] - grd[NC - 1][i];
-                r1 = res[NC - 1][i] + grd[0][i];
-            }
-            if (MODE == 0) {
-                dst[0][gidx] += r0;
-                if (CPLX) dst[NC - 1][gidx] += r1;
-            } else {
-                const T v = __ldg(V + gidx);
-                dst[0][gidx] = v * q[0][i][4] + r0;
-                if (CPLX) dst[NC - 1][gidx] = v * q[NC - 1][i][4] + r1;
+                for (int i = 0; i < RY; ++i) {
+                    // z + 2 < z1 keeps MODE 0's read of out ahead of this CTA's own writes
+                    const bool ok = rv[i] && (MODE == 1 || z + 2 < z1);
+                    const size_t o2 = rowoff + (size_t)nx * i + zo2;
+                    if (MODE == 0) {
+#pragma unroll
+                        for (int c = 0; c < NE; ++c) ep[(p + 2) % 3][c][i] = ok ? dst[c][o2] : T(0);
+                    } else {
+                        ep[(p + 2) % 3][0][i] = ok ? __ldg(V + o2) : T(0);
+                    }
+                }
+                const size_t zo4 = nxy * (size_t)wrapi(z + HW, nz);
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+#pragma unroll
+                    for (int i = 0; i < RY; ++i) {
+                        q[c][i][(p + 8) % 9] = rv[i] ? __ldg(src[c] + rowoff + (size_t)nx * i + zo4) : T(0);
+                        // only in-tile threads write centres: for a partial tile the cells of
+                        // out-of-tile threads alias the right / bottom halo
+                        if (rv[i]) sm[buf][c][ty * RY + i + HW][tx + HW] = q[c][i][(p + 4) % 9];
+                    }
+                __syncthreads();
+
+                T res[NC][RY];
+                T grd[NC][RY];
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    const T(*s)[SW] = sm[buf][c];
+                    T col[RY + 8];
+#pragma unroll
+                    for (int j = 0; j < RY + 8; ++j) col[j] = s[ty * RY + j][tx + HW];
+#pragma unroll
+                    for (int i = 0; i < RY; ++i) {
+                        const int sy = ty * RY + i + HW, sx = tx + HW;
+#define QZ(k) q[c][i][(p + (k)) % 9]
+                        const T xm4 = s[sy][sx - 4], xm3 = s[sy][sx - 3], xm2 = s[sy][sx - 2], xm1 = s[sy][sx - 1];
+                        const T xp1 = s[sy][sx + 1], xp2 = s[sy][sx + 2], xp3 = s[sy][sx + 3], xp4 = s[sy][sx + 4];
+                        T d = k.c0 * QZ(4);
+                        d += k.cx[3] * (xp4 + xm4) + k.cx[2] * (xp3 + xm3) + k.cx[1] * (xp2 + xm2) +
+                             k.cx[0] * (xp1 + xm1);
+                        d += k.cy[3] * (col[i + 8] + col[i]) + k.cy[2] * (col[i + 7] + col[i + 1]) +
+                             k.cy[1] * (col[i + 6] + col[i + 2]) + k.cy[0] * (col[i + 5] + col[i + 3]);
+                        d += k.cz[3] * (QZ(8) + QZ(0)) + k.cz[2] * (QZ(7) + QZ(1)) + k.cz[1] * (QZ(6) + QZ(2)) +
+                             k.cz[0] * (QZ(5) + QZ(3));
+                        res[c][i] = d;
+                        if (GRAD) {
+                            T g = k.ax[3] * (xp4 - xm4) + k.ax[2] * (xp3 - xm3) + k.ax[1] * (xp2 - xm2) +
+                                  k.ax[0] * (xp1 - xm1);
+                            g += k.ay[3] * (col[i + 8] - col[i]) + k.ay[2] * (col[i + 7] - col[i + 1]) +
+                                 k.ay[1] * (col[i + 6] - col[i + 2]) + k.ay[0] * (col[i + 5] - col[i + 3]);
+                            g += k.az[3] * (QZ(8) - QZ(0)) + k.az[2] * (QZ(7) - QZ(1)) + k.az[1] * (QZ(6) - QZ(2)) +
+                                 k.az[0] * (QZ(5) - QZ(3));
+                            grd[c][i] = g;
+                        }
+#undef QZ
+                    }
+                }
+                const size_t zo = nxy * (size_t)z;
+#pragma unroll
+                for (int i = 0; i < RY; ++i) {
+                    if (!rv[i]) continue;
+                    const size_t gidx = rowoff + (size_t)nx * i + zo;
+                    T r0 = res[0][i], r1 = res[NC - 1][i];
+                    if (CPLX && GRAD) {
+                        // out.re: Lap(re) - D(im);  out.im: Lap(im) + D(re)
+                        r0 = res[0][i] - grd[NC - 1][i];
+                        r1 = res[NC - 1][i] + grd[0][i];
+                    }
+                    if (MODE == 0) {
+                        dst[0][gidx] = ep[p % 3][0][i] + r0;
+                        if (CPLX) dst[NC - 1][gidx] = ep[p % 3][NE - 1][i] + r1;
+                    } else {
+                        const T v = ep[p % 3][0][i];
+                        dst[0][gidx] = v * q[0][i][(p + 4) % 9] + r0;
+                        if (CPLX) dst[NC - 1][gidx] = v * q[NC - 1][i][(p + 4) % 9] + r1;
+                    }
+                }
             }
         }
     }
 }
 
+// ---------------------------------------------------------------------------
+// TMA-pipelined stencil (primary path on sm_100a).
+//
+// The planes of a CTA's tile, with the 4-wide x/y halo, stream through an
+// 8-stage shared-memory ring: one 3-D tensor copy (cp.async.bulk.tensor, box
+// (TX+8) x (TY+8) x 1) per plane and SoA component, completing on one mbarrier
+// per stage.  The tensor copy zero-fills coordinates outside the grid; the
+// periodic halo cells of edge tiles (the only out-of-range ones) are written by
+// threads from values prefetched two planes ahead.  Plane j (z = z0-4+j) is read
+// twice from shared memory: its tile centres into the register z queue when it
+// is the newest plane (step j-8) and its x/y neighbours when it is the current
+// plane (step j-4); its stage is refilled with plane j+8 once every thread has
+// passed the barrier of step j-3 (one barrier per step).  The FD sums are
+// evaluated as trees per direction (short FP64 dependency chains); the result
+// differs from the reference's left-to-right order only by rounding.
+//
+// Every wait is bounded: a wait that runs out sets an error bit in *err, all
+// threads leave together (a block-wide vote), and the producer first waits (also
+// bounded) for the copies it still has in flight.
+// ---------------------------------------------------------------------------
+constexpr unsigned WAIT_LIMIT = 1u << 22;   // try_wait polls before declaring a timeout
+constexpr int ERR_STENCIL_TIMEOUT = 1;
+constexpr int S_RING = 8;                  // stages: planes stp+4 .. stp+8 in use, three in flight
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait; false after WAIT_LIMIT polls
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    for (unsigned it = 0; it < WAIT_LIMIT; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(smem_u32(dst)),
+        "l"((uint64_t)map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+template <typename T, bool CPLX, int RY>
+struct TmaCfg {
+    static constexpr int NC = CPLX ? 2 : 1;
+    static constexpr int TY = BY * RY;
+    static constexpr int SW = TX + 2 * HW;
+    static constexpr int SH = TY + 2 * HW;
+    static constexpr int COMP = SH * SW;           // elements of one component's box
+    static constexpr int STAGE = NC * COMP;
+    static constexpr size_t SMEM = (size_t)S_RING * STAGE * sizeof(T) + S_RING * sizeof(uint64_t) + 128;
+    // two CTAs per SM when two rings fit in the SM's 228 KB of shared memory
+    static constexpr int MINB = SMEM <= 112 * 1024 ? 2 : 1;
+    static_assert((COMP * sizeof(T)) % 128 == 0, "stage components must stay 128-byte aligned");
+};
+
+template <typename T, bool CPLX, int MODE, bool GRAD, int RY>
+__global__ void __launch_bounds__(NT, (TmaCfg<T, CPLX, RY>::MINB))
+fd8_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ out, const T* __restrict__ in,
+               const T* __restrict__ V, int nx, int ny, int nz, int zchunk, KC<T> k, int* __restrict__ err) {
+    using C = TmaCfg<T, CPLX, RY>;
+    constexpr int NC = C::NC, TY = C::TY, SW = C::SW, S = S_RING;
+    extern __shared__ unsigned char smraw_[];
+    unsigned char* smraw = (unsigned char*)(((uintptr_t)smraw_ + 127) & ~(uintptr_t)127);
+    T* ring = reinterpret_cast<T*>(smraw);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smraw + (size_t)S * C::STAGE * sizeof(T));
+
+    const int ntx = (nx + TX - 1) / TX;
+    const int x0 = (blockIdx.x % ntx) * TX;
+    const int y0 = (blockIdx.x / ntx) * TY;
+    const int wx = min(TX, nx - x0);
+    const int wy = min(TY, ny - y0);
+    const int z0 = blockIdx.y * zchunk;
+    const int z1 = min(nz, z0 + zchunk);
+    const int nsteps = z1 - z0;
+    const int nplanes = nsteps + 2 * HW;
+    const int band = blockIdx.z;
+    const size_t nxy = (size_t)nx * ny;
+    const size_t N = nxy * nz;
+    const T* src[NC];
+    T* dst[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const size_t plane = CPLX ? (size_t)(2 * band + c) : (size_t)band;
+        src[c] = in + plane * N;
+        dst[c] = out + plane * N;
+    }
+
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int t = ty * TX + tx;
+    const bool xin = tx < wx;
+    bool rv[RY];
+#pragma unroll
+    for (int i = 0; i < RY; ++i) rv[i] = xin && (ty * RY + i < wy);
+    const size_t rowoff = (size_t)(x0 + tx) + (size_t)nx * (y0 + ty * RY);
+
+    // periodic halo cells (outside [0,nx) x [0,ny), zero-filled by the tensor copy)
+    bool xh_ok = false, yh_ok = false;
+    size_t xh_g = 0, yh_g = 0;
+    int xh_s = 0, yh_s = 0;
+    if (t < 8 * TY) {
+        const int side = t / (4 * TY), rem = t % (4 * TY), hrow = rem / 4, hk = rem % 4;
+        const int gxu = side == 0 ? x0 - HW + hk : x0 + wx + hk;   // unwrapped
+        xh_ok = hrow < wy && (gxu < 0 || gxu >= nx);
+        xh_g = (size_t)wrapi(gxu, nx) + (size_t)nx * (y0 + min(hrow, wy - 1));
+        xh_s = (HW + hrow) * SW + (side == 0 ? hk : wx + HW + hk);
+    }
+    if (t < 8 * TX) {
+        const int side = t / (4 * TX), rem = t % (4 * TX), hr = rem / TX, hc = rem % TX;
+        const int gyu = side == 0 ? y0 - HW + hr : y0 + wy + hr;
+        yh_ok = hc < wx && (gyu < 0 || gyu >= ny);
+        yh_g = (size_t)(x0 + min(hc, wx - 1)) + (size_t)nx * wrapi(gyu, ny);
+        yh_s = (side == 0 ? hr : wy + HW + hr) * SW + HW + hc;
+    }
+
+    if (t == 0) {
+        for (int st = 0; st < S; ++st) mbar_init(&bar[st], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    // producer: plane j -> stage j % S (thread 0)
+    constexpr uint32_t PLANE_BYTES = (uint32_t)(C::STAGE * sizeof(T));
+    int issued = 0;
+    auto issue = [&](int j) {
+        issued = j + 1;
+        const int st = j % S;
+        T* stage = ring + (size_t)st * C::STAGE;
+        const int zz = wrapi(z0 - HW + j, nz);
+        // order the threads' earlier generic-proxy writes (halo cells) to this
+        // stage before the tensor copy's async-proxy writes
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&bar[st], PLANE_BYTES);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const int zplane = (CPLX ? 2 * band + c : band) * nz + zz;
+            tma_load_3d(stage + c * C::COMP, &tmap, x0 - HW, y0 - HW, zplane, &bar[st]);
+        }
+    };
+    if (t == 0)
+        for (int j = 0; j < min(S, nplanes); ++j) issue(j);
+
+    int failed = 0;
+    auto wait_plane = [&](int j) {
+        if (!failed && !mbar_wait(&bar[j % S], (uint32_t)((j / S) & 1))) failed = 1;
+    };
+
+    // periodic halo values, prefetched two planes ahead (3-slot rotation)
+    T hx[3][NC], hy[3][NC];
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+        const size_t zo = nxy * (size_t)wrapi(z0 + d, nz);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            hx[d][c] = xh_ok ? __ldg(src[c] + xh_g + zo) : T(0);
+            hy[d][c] = yh_ok ? __ldg(src[c] + yh_g + zo) : T(0);
+        }
+    }
+    // V (MODE 1) / accumulated output (MODE 0) prefetched one plane ahead
+    constexpr int NE = MODE == 0 ? NC : 1;
+    T ep[3][NE][RY];
+#pragma unroll
+    for (int i = 0; i < RY; ++i) {
+        const size_t o = rowoff + (size_t)nx * i + nxy * (size_t)z0;
+        if (MODE == 0) {
+#pragma unroll
+            for (int c = 0; c < NE; ++c) ep[0][c][i] = rv[i] ? dst[c][o] : T(0);
+        } else {
+            ep[0][0][i] = rv[i] ? __ldg(V + o) : T(0);
+        }
+    }
+
+    // z queues from planes 0..7
+    T q[NC][RY][9];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        wait_plane(j);
+        const T* stage = ring + (size_t)(j % S) * C::STAGE;
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+#pragma unroll
+            for (int i = 0; i < RY; ++i)
+                q[c][i][j] = stage[c * C::COMP + (ty * RY + i + HW) * SW + tx + HW];
+    }
+    // planes 0..3 are only needed for the queues: refill their stages
+    if (__syncthreads_or(failed)) goto drain;
+    if (t == 0)
+        for (int j = 0; j < HW; ++j)
+            if (j + S < nplanes) issue(j + S);
+
+    for (int zb = 0; zb < nsteps; zb += 9) {
+#pragma unroll
+        for (int p = 0; p < 9; ++p) {
+            const int stp = zb + p;
+            if (stp < nsteps) {
+                const int z = z0 + stp;
+                T* cur = ring + (size_t)((stp + HW) % S) * C::STAGE;
+                // periodic halo cells of plane z, then prefetch those of plane z+2
+                {
+                    int z2 = z + 2;
+                    if (z2 >= nz) z2 -= nz;
+                    const size_t zo2 = nxy * (size_t)z2;
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        if (xh_ok) cur[c * C::COMP + xh_s] = hx[p % 3][c];
+                        if (yh_ok) cur[c * C::COMP + yh_s] = hy[p % 3][c];
+                        hx[(p + 2) % 3][c] = xh_ok ? __ldg(src[c] + xh_g + zo2) : T(0);
+                        hy[(p + 2) % 3][c] = yh_ok ? __ldg(src[c] + yh_g + zo2) : T(0);
+                    }
+                }
+                // newest plane (z+4) into the queue
+                wait_plane(stp + 8);
+                {
+                    const T* stage = ring + (size_t)((stp + 8) % S) * C::STAGE;
+#pragma unroll
+                    for (int c = 0; c < NC; ++c)
+#pragma unroll
+                        for (int i = 0; i < RY; ++i)
+                            q[c][i][(p + 8) % 9] = stage[c * C::COMP + (ty * RY + i + HW) * SW + tx + HW];
+                }
+                // epilogue operand of plane z+1
+                {
+                    const bool ahead = stp + 1 < nsteps;
+                    const size_t zo1 = nxy * (size_t)(z + 1);
+#pragma unroll
+                    for (int i = 0; i < RY; ++i) {
+                        const bool ok = rv[i] && ahead;
+                        const size_t o1 = rowoff + (size_t)nx * i + zo1;
+                        if (MODE == 0) {
+#pragma unroll
+                            for (int c = 0; c < NE; ++c) ep[(p + 1) % 3][c][i] = ok ? dst[c][o1] : T(0);
+                        } else {
+                            ep[(p + 1) % 3][0][i] = ok ? __ldg(V + o1) : T(0);
+                        }
+                    }
+                }
+                // one barrier per step: halo cells of plane z are written, and every
+                // thread has finished step stp-1, so plane stp+3's stage is free
+                if (__syncthreads_or(failed)) goto drain;
+                if (t == 0 && stp > 0 && stp + HW - 1 + S < nplanes) issue(stp + HW - 1 + S);
+
+                T res[NC][RY];
+                T grd[NC][RY];
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    const T(*s)[SW] = reinterpret_cast<const T(*)[SW]>(cur + c * C::COMP);
+                    T col[RY + 8];
+#pragma unroll
+                    for (int jj = 0; jj < RY + 8; ++jj) col[jj] = s[ty * RY + jj][tx + HW];
+#pragma unroll
+                    for (int i = 0; i < RY; ++i) {
+                        const int sy = ty * RY + i + HW, sx = tx + HW;
+#define QZ(kk) q[c][i][(p + (kk)) % 9]
+                        const T xm4 = s[sy][sx - 4], xm3 = s[sy][sx - 3], xm2 = s[sy][sx - 2], xm1 = s[sy][sx - 1];
+                        const T xp1 = s[sy][sx + 1], xp2 = s[sy][sx + 2], xp3 = s[sy][sx + 3], xp4 = s[sy][sx + 4];
+                        // tree-shaped sums (depth ~6 instead of a 19-deep chain): the
+                        // per-direction partial sums are independent
+                        const T sxx = (k.cx[3] * (xp4 + xm4) + k.cx[2] * (xp3 + xm3)) +
+                                      (k.cx[1] * (xp2 + xm2) + k.cx[0] * (xp1 + xm1));
+                        const T syy = (k.cy[3] * (col[i + 8] + col[i]) + k.cy[2] * (col[i + 7] + col[i + 1])) +
+                                      (k.cy[1] * (col[i + 6] + col[i + 2]) + k.cy[0] * (col[i + 5] + col[i + 3]));
+                        const T szz = (k.cz[3] * (QZ(8) + QZ(0)) + k.cz[2] * (QZ(7) + QZ(1))) +
+                                      (k.cz[1] * (QZ(6) + QZ(2)) + k.cz[0] * (QZ(5) + QZ(3)));
+                        res[c][i] = k.c0 * QZ(4) + ((sxx + syy) + szz);
+                        if (GRAD) {
+                            const T gx_ = (k.ax[3] * (xp4 - xm4) + k.ax[2] * (xp3 - xm3)) +
+                                          (k.ax[1] * (xp2 - xm2) + k.ax[0] * (xp1 - xm1));
+                            const T gy_ = (k.ay[3] * (col[i + 8] - col[i]) + k.ay[2] * (col[i + 7] - col[i + 1])) +
+                                          (k.ay[1] * (col[i + 6] - col[i + 2]) + k.ay[0] * (col[i + 5] - col[i + 3]));
+                            const T gz_ = (k.az[3] * (QZ(8) - QZ(0)) + k.az[2] * (QZ(7) - QZ(1))) +
+                                          (k.az[1] * (QZ(6) - QZ(2)) + k.az[0] * (QZ(5) - QZ(3)));
+                            grd[c][i] = (gx_ + gy_) + gz_;
+                        }
+#undef QZ
+                    }
+                }
+                const size_t zo = nxy * (size_t)z;
+#pragma unroll
+                for (int i = 0; i < RY; ++i) {
+                    if (!rv[i]) continue;
+                    const size_t gidx = rowoff + (size_t)nx * i + zo;
+                    T r0 = res[0][i], r1 = res[NC - 1][i];
+                    if (CPLX && GRAD) {
+                        r0 = res[0][i] - grd[NC - 1][i];
+                        r1 = res[NC - 1][i] + grd[0][i];
+                    }
+                    if (MODE == 0) {
+                        dst[0][gidx] = ep[p % 3][0][i] + r0;
+                        if (CPLX) dst[NC - 1][gidx] = ep[p % 3][NE - 1][i] + r1;
+                    } else {
+                        const T v = ep[p % 3][0][i];
+                        dst[0][gidx] = v * q[0][i][(p + 4) % 9] + r0;
+                        if (CPLX) dst[NC - 1][gidx] = v * q[NC - 1][i][(p + 4) % 9] + r1;
+                    }
+                }
+            }
+        }
+    }
+    return;
+
+drain:
+    // a wait ran out: record it and wait (bounded) for this CTA's copies in flight
+    if (t == 0) {
+        atomicOr(err, ERR_STENCIL_TIMEOUT);
+        for (int st = 0; st < S; ++st) {
+            int jmax = -1;
+            for (int j = st; j < issued; j += S) jmax = j;
+            if (jmax >= 0) (void)mbar_wait(&bar[st], (uint32_t)((jmax / S) & 1));
+        }
+    }
+    __syncthreads();
+}
+
+// cuTensorMapEncodeTiled, looked up once through the runtime (no libcuda link)
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// 3-D map over the band bundle viewed as [planes*nz][ny][nx], box (TX+8, TY+8, 1)
+template <typename T>
+bool make_plane_map(CUtensorMap* map, const void* base, int nx, int ny, long long zplanes, int box_y) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)zplanes};
+    const cuuint64_t strides[2] = {(cuuint64_t)nx * sizeof(T), (cuuint64_t)nx * ny * sizeof(T)};
+    const cuuint32_t box[3] = {(cuuint32_t)(TX + 2 * HW), (cuuint32_t)box_y, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = fn(map, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                          const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 template <typename T, bool CPLX, int MODE>
 void launch_t(const StencilLaunch& L, const FD8Coef& c, cudaStream_t s) {
-    constexpr int RY = CPLX ? 2 : 4;
+    // rows per thread: as many as fit 128 registers without spilling
+    constexpr int RY = (CPLX || sizeof(T) == 8) ? 2 : 4;
     constexpr int TY = BY * RY;
     const int ntx = (L.nx + TX - 1) / TX, nty = (L.ny + TY - 1) / TY;
     const int tiles = ntx * nty;
@@ -271,6 +673,26 @@ void launch_t(const StencilLaunch& L, const FD8Coef& c, cudaStream_t s) {
     const int nzc = (L.nz + zchunk - 1) / zchunk;
     dim3 grid(tiles, nzc, L.nb), block(TX, BY);
     const KC<T> k = to_kc<T>(c);
+    // TMA path: the tensor map needs 16-byte aligned base and row pitch
+    const int vec = 16 / (int)sizeof(T);
+    const bool aligned = (L.nx % vec == 0) && (((uintptr_t)L.in) % 16 == 0);
+    CUtensorMap map;
+    if (aligned && L.tma_ok &&
+        make_plane_map<T>(&map, L.in, L.nx, L.ny, (long long)L.nz * L.nb * (CPLX ? 2 : 1), TY + 2 * HW)) {
+        using C = TmaCfg<T, CPLX, RY>;
+        if (CPLX && c.has_grad) {
+            cudaFuncSetAttribute(fd8_tma_kernel<T, CPLX, MODE, CPLX, RY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)C::SMEM);
+            fd8_tma_kernel<T, CPLX, MODE, CPLX, RY><<<grid, block, C::SMEM, s>>>(
+                map, (T*)L.out, (const T*)L.in, (const T*)L.V, L.nx, L.ny, L.nz, zchunk, k, device_error_word());
+        } else {
+            cudaFuncSetAttribute(fd8_tma_kernel<T, CPLX, MODE, false, RY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)C::SMEM);
+            fd8_tma_kernel<T, CPLX, MODE, false, RY><<<grid, block, C::SMEM, s>>>(
+                map, (T*)L.out, (const T*)L.in, (const T*)L.V, L.nx, L.ny, L.nz, zchunk, k, device_error_word());
+        }
+        return;
+    }
     if (CPLX && c.has_grad)
         fd8_kernel<T, CPLX, MODE, CPLX, RY><<<grid, block, 0, s>>>((const T*)L.in, (T*)L.out, (const T*)L.V, L.nx,
                                                                    L.ny, L.nz, zchunk, k);

@@ -58,6 +58,13 @@ def version():
     return lib.qsb_version().decode()
 
 
+def device_status(clear=False):
+    """Device error word (bit 0: a kernel's bounded wait ran out); synchronizes."""
+    code = ctypes.c_int()
+    _check(lib.qsb_device_status(ctypes.byref(code), int(bool(clear))))
+    return code.value
+
+
 def _torch():
     import torch
     return torch

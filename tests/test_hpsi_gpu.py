@@ -244,3 +244,8 @@ def test_full_size_properties_config2(qsb):
     # one band against the oracle at full size
     ref = O.hamiltonian(grid, V, tab, psi[7].cpu().numpy(), 1)
     assert rel(host(hp[7]), ref.ravel()) < TOL64
+
+
+def test_device_error_word_clean(qsb):
+    """No bounded wait ran out in any of the kernels above."""
+    assert qsb.device_status() == 0
