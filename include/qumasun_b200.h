@@ -147,6 +147,53 @@ QSB_API qsb_status qsb_ham_nonlocal_project(qsb_ham* ham, qsb_dtype dtype, int i
                                     const void* psi_dev, double gx, double gy, double gz,
                                     double* out_host, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Block LOBPCG eigensolvers (device resident).
+ * ------------------------------------------------------------------------- */
+typedef struct qsb_eigensolver qsb_eigensolver;
+
+/* Operator callback: ax = A x for nb bands (device pointers, same layout as the
+ * solver's bundles), enqueued on `stream`; returns 0 on success.  This is the
+ * reference's OpeA functor (source/qumasun_kpoint.lobpcg.h:97-99,
+ * source/lobpcg_d_multi.h:70), one call per bundle instead of per band. */
+typedef int (*qsb_apply_fn)(void* user, int nb, const double* x_dev, double* ax_dev, void* stream);
+
+/* Solver context for bundles of up to n bands of N grid points (complex SoA
+ * when is_complex), holding the device work bundles R, AX, AR, AP and a
+ * temporary (the reference's `work`/`temporary` arenas,
+ * source/lobpcg_z_multi_mpi.h:2862-2881) and the cuBLAS / cuSOLVER handles. */
+QSB_API qsb_status qsb_eigensolver_create(qsb_eigensolver** es, int64_t N, int n, int is_complex);
+QSB_API qsb_status qsb_eigensolver_destroy(qsb_eigensolver* es);
+/* H of a qsb_ham context (Bloch vector g for complex bands) as the operator. */
+QSB_API qsb_status qsb_eigensolver_set_hamiltonian(qsb_eigensolver* es, qsb_ham* ham, double gx, double gy, double gz);
+/* A user callback as the operator. */
+QSB_API qsb_status qsb_eigensolver_set_operator(qsb_eigensolver* es, qsb_apply_fn op, void* user);
+/* Iterations done by the last solve, and whether it ended with the norm-check rollback. */
+QSB_API qsb_status qsb_eigensolver_last_stats(const qsb_eigensolver* es, int* iterations, int* rolled_back);
+
+/* Complex block LOBPCG.  Replaces LOBPCG::Eigen_z_multi_mpi(l_grid, dVol,
+ * num_solution, iter_max, eigen_values, eigen_vectors, keep, work, temporary,
+ * p_num_fix, residual_threshold, keep_S_matrix, SCF_step, sk, OpeA, watch)
+ * (source/lobpcg_z_multi_mpi.h:1732-1742) on one rank:
+ *   eigen_values  host, n values; in: previous eigenvalues, out: Ritz values of
+ *                 the active bands (fixed bands keep theirs)
+ *   X             device, n complex SoA bands, in/out (returned normalized, dV-weighted)
+ *   keep          device, n complex SoA bands: the P directions kept between
+ *                 calls (zeroed when scf_step == 0)
+ *   p_num_fix     in/out soft-locking count (leading converged bands), <= n/2
+ *   residual_threshold  bands with ||r|| below it (leading run) are fixed
+ * Errors: QSB_ERR_SOLVER when the overlap matrix is not positive definite. */
+QSB_API qsb_status qsb_lobpcg_z(qsb_eigensolver* es, double dVol, int n, int iter_max, double* eigen_values,
+                                double* X, double* keep, int* p_num_fix, double residual_threshold, int scf_step,
+                                void* stream);
+
+/* Real block LOBPCG.  Replaces EigenLOBPCG_d_multi(N, dVol, num_solution,
+ * iter_max, eigen_values, eigen_vectors, keep, work, is_first_time, OpeA, watch)
+ * (source/lobpcg_d_multi.h:23-27): X and keep are device real bundles (n x N),
+ * eigen_values host; stops early when max ||r||^2 dV < 1e-10 dV (:525). */
+QSB_API qsb_status qsb_lobpcg_d(qsb_eigensolver* es, double dVol, int n, int iter_max, double* eigen_values,
+                                double* X, double* keep, int is_first_time, void* stream);
+
 /* Per-kernel device timing of qsb_ham_apply, in the spirit of the reference's
  * StopWatch sectors (source/StopWatch.h:11-60, watch_pp in
  * source/PseudoPotNonlocal_SvF2_kpoint.h:261-272).  While enabled, every

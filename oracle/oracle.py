@@ -58,7 +58,6 @@ def ref_lib():
     global _ref
     if _ref is None:
         _ref = ctypes.CDLL(LIB_REF)
-        _ref.qsref_lobpcg_z_work_doubles.restype = ctypes.c_size_t
     return _ref
 
 
@@ -311,3 +310,76 @@ def ref_hamiltonian(grid, V, cube, psi, nb, is_complex=False, g=(0.0, 0.0, 0.0))
 
 def ref_set_threads(n):
     ref_lib().qsref_set_threads(int(n))
+
+
+# --------------------------------------------------------------------------
+# eigensolver oracles
+# --------------------------------------------------------------------------
+def orthonormal_psi(seed, nb, N, dV, complex_=False):
+    """Seeded psi ~ U[-0.5,0.5], orthonormalized with the dV-weighted inner product
+    (the role of GramSchmidt_ddm, source/GramSchmidt_mpi.h:56-96: same span, done by QR)."""
+    a = seeded_psi(seed, nb, N, complex_)
+    if complex_:
+        z = (a[0::2] + 1j * a[1::2]).T
+        q, _ = np.linalg.qr(z)
+        q = q.T / math.sqrt(dV)
+        out = np.empty((2 * nb, N))
+        out[0::2] = q.real
+        out[1::2] = q.imag
+        return out
+    q, _ = np.linalg.qr(a.T)
+    return np.ascontiguousarray(q.T / math.sqrt(dV))
+
+
+def _cube_args(cube):
+    return (len(cube["widths"]), _i(cube["cubes"]), _i(cube["widths"]), _d(cube["proj"]), _d(cube["energy"]))
+
+
+def ref_lobpcg_z(grid, V, cube, X, keep, n, iter_max, eigen_values, num_fix, residual_threshold, scf_step,
+                 g=(0.0, 0.0, 0.0)):
+    """LOBPCG::Eigen_z_multi_mpi of the reference (in place on X, keep, eigen_values); returns num_fix."""
+    lib = ref_lib()
+    nx, ny, nz, dx, dy, dz = grid
+    for a in (X, keep, eigen_values):
+        assert a.dtype == np.float64 and a.flags.c_contiguous
+    V = np.ascontiguousarray(V, np.float64)
+    nf = ctypes.c_int(int(num_fix))
+    lib.qsref_lobpcg_z(nx, ny, nz, *[ctypes.c_double(v) for v in (dx, dy, dz)], _d(V), *_cube_args(cube), n, iter_max,
+                       _d(eigen_values), _d(X), _d(keep), ctypes.byref(nf), ctypes.c_double(residual_threshold),
+                       int(scf_step), *[ctypes.c_double(v) for v in g])
+    return nf.value
+
+
+def ref_lobpcg_d(grid, V, cube, X, keep, n, iter_max, eigen_values, is_first_time):
+    """EigenLOBPCG_d_multi of the reference (in place on X, keep, eigen_values)."""
+    lib = ref_lib()
+    nx, ny, nz, dx, dy, dz = grid
+    N = nx * ny * nz
+    V = np.ascontiguousarray(V, np.float64)
+    work = np.zeros(5 * N * n)
+    lib.qsref_lobpcg_d(nx, ny, nz, *[ctypes.c_double(v) for v in (dx, dy, dz)], _d(V), *_cube_args(cube), n, iter_max,
+                       _d(eigen_values), _d(X), _d(keep), _d(work), int(is_first_time))
+
+
+def dense_eigenvalues(grid, V, tables, k, is_complex=False, g=(0.0, 0.0, 0.0)):
+    """Lowest k eigenvalues of H built column by column with the C restatement (small grids only)."""
+    nx, ny, nz = grid[:3]
+    N = nx * ny * nz
+    if is_complex:
+        M = np.zeros((N, N), complex)
+        e = np.zeros((2, N))
+        for j in range(N):
+            e[:] = 0.0
+            e[0, j] = 1.0
+            h = hamiltonian(grid, V, tables, e.reshape(1, 2, N), 1, True, g).reshape(2, N)
+            M[:, j] = h[0] + 1j * h[1]
+        M = 0.5 * (M + M.conj().T)
+    else:
+        M = np.zeros((N, N))
+        e = np.zeros((1, N))
+        for j in range(N):
+            e[:] = 0.0
+            e[0, j] = 1.0
+            M[:, j] = hamiltonian(grid, V, tables, e, 1)[0]
+        M = 0.5 * (M + M.T)
+    return np.linalg.eigvalsh(M)[:k]

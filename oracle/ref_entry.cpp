@@ -369,8 +369,24 @@ void qsref_lobpcg_d(int nx, int ny, int nz, double dx, double dy, double dz, con
 }
 
 #ifdef QSREF_WITH_Z
-size_t qsref_lobpcg_z_work_doubles(int N, int n) {
-    return LOBPCG::WorkSize_z_multi_mpi_temporary(N, n) / sizeof(double) + 64;
+/* LOBPCG::Eigen_z_multi_mpi on the reference Hamiltonian at Bloch vector g:
+ * X and keep are SoA complex bundles (2*n*N doubles each), eigen_values n,
+ * num_fix in/out.  Work arenas sized by the reference's own WorkSize functions. */
+void qsref_lobpcg_z(int nx, int ny, int nz, double dx, double dy, double dz, const double* V, int n_atoms,
+                    const int* cubes, const int* widths, const double* proj, const double* energy, int n, int iter_max,
+                    double* eigen_values, double* X, double* keep, int* num_fix, double residual_threshold,
+                    int scf_step, double gx, double gy, double gz) {
+    RefHamiltonian H{nx, ny, nz, dx, dy, dz, V, build_nonlocal(nx, ny, nz, n_atoms, cubes, widths, proj, energy), gx, gy, gz};
+    GridRangeMPI grid = make_grid(nx, ny, nz);
+    const size_t N = (size_t)nx * ny * nz;
+    std::vector<double> work(LOBPCG::WorkSize_z_multi_mpi_keep((int)N, n) + 1024);
+    std::vector<double> temporary(LOBPCG::WorkSize_z_multi_mpi_temporary((int)N, n) + 1024);
+    std::vector<SoAComplex> xs(n);
+    for (int k = 0; k < n; ++k) xs[k] = SoAComplex{X + 2 * k * N, X + (2 * k + 1) * N};
+    NullWatch watch;
+    LOBPCG::Eigen_z_multi_mpi(grid, dx * dy * dz, n, iter_max, eigen_values, xs.data(), keep, work.data(),
+                              temporary.data(), num_fix, residual_threshold, nullptr, scf_step, 0,
+                              [&](SoAComplex* Ax, SoAComplex* x, int nb) { apply_h_complex(H, Ax, x, nb); }, watch);
 }
 #endif
 

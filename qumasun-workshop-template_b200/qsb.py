@@ -216,3 +216,65 @@ class Hamiltonian:
                                             _c_d(g[0]), _c_d(g[1]), _c_d(g[2]),
                                             out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _stream_ptr(psi)))
         return out[:, :P]
+
+
+APPLY_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                            ctypes.c_void_p)
+
+
+class EigenSolver:
+    """Device block LOBPCG (qsb_lobpcg_z ~ LOBPCG::Eigen_z_multi_mpi, qsb_lobpcg_d ~
+    EigenLOBPCG_d_multi) for bundles of up to n bands of N points."""
+
+    def __init__(self, N, n, is_complex):
+        h = ctypes.c_void_p()
+        _check(lib.qsb_eigensolver_create(ctypes.byref(h), ctypes.c_int64(N), n, int(bool(is_complex))))
+        self._h = h
+        self.N, self.n, self.is_complex = N, n, bool(is_complex)
+        self._cb = None
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.qsb_eigensolver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_hamiltonian(self, ham, g=(0.0, 0.0, 0.0)):
+        self._ham = ham
+        _check(lib.qsb_eigensolver_set_hamiltonian(self._h, ham._h, _c_d(g[0]), _c_d(g[1]), _c_d(g[2])))
+
+    def set_operator(self, fn):
+        """fn(nb, x_ptr, ax_ptr, stream_ptr) -> int, device pointers as ints."""
+        def tramp(user, nb, x, ax, stream):
+            try:
+                return int(fn(nb, x, ax, stream))
+            except Exception:
+                return 4
+        self._cb = APPLY_FN(tramp)
+        _check(lib.qsb_eigensolver_set_operator(self._h, self._cb, None))
+
+    def last_stats(self):
+        it, rb = ctypes.c_int(), ctypes.c_int()
+        _check(lib.qsb_eigensolver_last_stats(self._h, ctypes.byref(it), ctypes.byref(rb)))
+        return it.value, rb.value
+
+    def lobpcg_z(self, dV, n, iter_max, eigen_values, X, keep, num_fix, residual_threshold, scf_step):
+        """In place on X, keep (CUDA) and eigen_values (numpy float64); returns the new num_fix."""
+        assert eigen_values.dtype == np.float64 and eigen_values.flags.c_contiguous
+        nf = ctypes.c_int(int(num_fix))
+        _check(lib.qsb_lobpcg_z(self._h, _c_d(dV), n, iter_max,
+                                eigen_values.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _dev_ptr(X),
+                                _dev_ptr(keep), ctypes.byref(nf), _c_d(residual_threshold), int(scf_step),
+                                _stream_ptr(X)))
+        return nf.value
+
+    def lobpcg_d(self, dV, n, iter_max, eigen_values, X, keep, is_first_time):
+        assert eigen_values.dtype == np.float64 and eigen_values.flags.c_contiguous
+        _check(lib.qsb_lobpcg_d(self._h, _c_d(dV), n, iter_max,
+                                eigen_values.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _dev_ptr(X),
+                                _dev_ptr(keep), int(bool(is_first_time)), _stream_ptr(X)))

@@ -92,3 +92,63 @@ CASES = {
                         reference=lambda i: _ham_ref(i, True, G_C0),
                         oracle=lambda i: _ham_oracle(i, True, G_C0)),
 }
+
+
+# ---------------------------------------------------------------------------
+# LOBPCG: the reference's solvers on the reference Hamiltonian, 12^3 bcc cell
+# ---------------------------------------------------------------------------
+EIG_GRID = (12, 12, 12, 0.5, 0.5, 0.5)
+EIG_NB = 8
+EIG_G = (2 * math.pi / A_BCC * 0.25, 2 * math.pi / A_BCC * 0.5, 0.0)
+
+
+def eig_inputs(seed=0, cplx=False):
+    nx, ny, nz, dx, dy, dz = EIG_GRID
+    N = nx * ny * nz
+    dV = dx * dy * dz
+    pos = O.bcc_positions(A_BCC, 1) + 0.1
+    sp = [O.GTH_BCC] * len(pos)
+    V = 0.3 * O.seeded_potential(seed, N)
+    X = O.orthonormal_psi(seed, EIG_NB, N, dV, cplx)
+    return dict(grid=EIG_GRID, pos=pos, sp=sp, V=V, X=X, dV=dV, checked=[V, X])
+
+
+def eig_ref_z(inp, calls=3, iter_max=4, g=EIG_G):
+    """Sequence of Eigen_z_multi_mpi calls (SCF steps 0..calls-1): eigenvalues after each."""
+    nx, ny, nz, dx, dy, dz = inp["grid"]
+    cube = O.gth_cube_tables(inp["pos"], inp["sp"], nx, ny, nz, dx, dy, dz)
+    X = inp["X"].copy()
+    keep = np.zeros_like(X)
+    ev = np.zeros(EIG_NB)
+    out, nf = [], 0
+    for step in range(calls):
+        nf = O.ref_lobpcg_z(inp["grid"], inp["V"], cube, X, keep, EIG_NB, iter_max, ev, nf, 1e-4, step, g)
+        out.append(np.concatenate([ev, [nf]]))
+    return np.array(out)
+
+
+def eig_ref_d(inp, calls=3, iter_max=4):
+    nx, ny, nz, dx, dy, dz = inp["grid"]
+    cube = O.gth_cube_tables(inp["pos"], inp["sp"], nx, ny, nz, dx, dy, dz)
+    X = inp["X"].copy()
+    keep = np.zeros_like(X)
+    ev = np.zeros(EIG_NB)
+    out = []
+    for step in range(calls):
+        O.ref_lobpcg_d(inp["grid"], inp["V"], cube, X, keep, EIG_NB, iter_max, ev, step == 0)
+        out.append(ev.copy())
+    return np.array(out)
+
+
+def eig_exact(inp, cplx, g=EIG_G):
+    nx, ny, nz, dx, dy, dz = inp["grid"]
+    tab = O.gth_tables(inp["pos"], inp["sp"], dx, dy, dz)
+    return O.dense_eigenvalues(inp["grid"], inp["V"], tab, EIG_NB, cplx, g if cplx else (0.0, 0.0, 0.0))
+
+
+CASES.update({
+    "lobpcg_z_ref": dict(inputs=lambda: eig_inputs(0, True), reference=eig_ref_z, oracle=None),
+    "lobpcg_d_ref": dict(inputs=lambda: eig_inputs(0, False), reference=eig_ref_d, oracle=None),
+    "eig_exact_z": dict(inputs=lambda: eig_inputs(0, True), reference=lambda i: eig_exact(i, True), oracle=None),
+    "eig_exact_d": dict(inputs=lambda: eig_inputs(0, False), reference=lambda i: eig_exact(i, False), oracle=None),
+})
