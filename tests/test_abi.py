@@ -48,3 +48,38 @@ def test_version_and_error_strings():
     st = lib.qsb_laplacian8th(0, 0, 4, 4, 1, None, None, ctypes.c_double(1.0), ctypes.c_double(1.0),
                               ctypes.c_double(1.0), ctypes.c_double(1.0), None)
     assert st == 1 and b"grid" in lib.qsb_last_error()
+
+
+DROPIN_PROGRAM = r"""
+#include <cstdio>
+#include <cstddef>
+struct GridRange { int begin_x, begin_y, begin_z, end_x, end_y, end_z;
+  int SizeX() const { return end_x - begin_x; } int SizeY() const { return end_y - begin_y; }
+  int SizeZ() const { return end_z - begin_z; } };
+struct SoAComplex { double* re; double* im; };
+struct OneComplex { double r, i; };
+#include "qumasun_dropin.hpp"
+struct W { void Record(int) {} };
+int main() {
+  GridRange g{0, 0, 0, 8, 8, 8};
+  qsb_dropin::Hamiltonian H(g, 0.5, 0.5, 0.5);          // host-side context, no GPU work
+  GridRange bad{0, 0, 0, 0, 8, 8};
+  try { qsb_dropin::Laplacian8th<double>(bad, nullptr, nullptr, -0.5, 0.5, 0.5, 0.5); }
+  catch (const std::exception& e) { std::printf("caught: %s\n", e.what()); return 0; }
+  return 1;
+}
+"""
+
+
+def test_dropin_header_compiles_and_reports_errors(tmp_path):
+    """The reference-signature adapter header compiles against reference-style
+    types, links to the library and turns an error status into an exception."""
+    src = tmp_path / "dropin.cpp"
+    src.write_text(DROPIN_PROGRAM)
+    exe = tmp_path / "dropin"
+    libdir = os.path.dirname(LIB)
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L", libdir, "-lqumasun_b200", f"-Wl,-rpath,{libdir}"], check=True, capture_output=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "grid dimensions" in out.stdout
