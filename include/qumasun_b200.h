@@ -138,6 +138,35 @@ QSB_API qsb_status qsb_ham_nonlocal_apply(qsb_ham* ham, qsb_dtype dtype, int is_
                                   const void* psi_dev, void* hpsi_dev,
                                   double gx, double gy, double gz, void* stream);
 
+/* Size of the fixed device scratch used by qsb_ham_nonlocal_apply_static. */
+#define QSB_NL_STATIC_SCRATCH_BYTES (4u << 20)
+
+/* hpsi += V_NL psi exactly like qsb_ham_nonlocal_apply, but the call allocates
+ * no device memory: its scratch (the <beta|psi> partial sums and per-atom
+ * coefficients) is a fixed array of QSB_NL_STATIC_SCRATCH_BYTES (4 MiB) in the
+ * library's device memory, present on every GPU that loads the library until
+ * the process exits.  No counterpart in the reference (its nonlocal apply
+ * sub-allocates from the caller's work buffer).
+ * For callers that cannot allocate device memory while they run: codes that
+ * reserve the whole device memory for their own arena at start-up, and loops
+ * that cannot take the device-wide synchronization of cudaMalloc/cudaFree (the
+ * regular entry point grows its workspace with cudaMalloc when a larger bundle
+ * first arrives).
+ *   - Requests needing more scratch than the array holds are rejected with
+ *     QSB_ERR_INVALID and a message giving both sizes; split the bands into
+ *     smaller bundles.  The need is about 8*(projector points/8192 + atoms)*
+ *     (max projectors per atom)*(nb, or 2*nb for complex) bytes.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) and caches it; make that first call before any
+ *     stream capture on that device.
+ *   - All calls share the one array: calls that overlap on the GPU (other
+ *     streams, other host threads, without ordering between them) race on it.
+ *     Nothing in it needs to start at zero (each call writes every element it
+ *     reads before reading it); it keeps the last call's values. */
+QSB_API qsb_status qsb_ham_nonlocal_apply_static(qsb_ham* ham, qsb_dtype dtype, int is_complex, int nb,
+                                                 const void* psi_dev, void* hpsi_dev,
+                                                 double gx, double gy, double gz, void* stream);
+
 /* <beta_aw | psi_c> * dV for every projector and column into out_host
  * (double, layout [column][projector], projectors in atom order, columns:
  * real -> band b; complex -> 2b (re), 2b+1 (im)), the quantity
