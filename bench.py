@@ -64,6 +64,20 @@ def algorithmic_bytes(nb, N, n_proj_points, wmax, elem=8):
     return nb * N * 2 * elem + N * elem + n_proj_points * wmax * elem
 
 
+def max_over_ranks(values, dist, device):
+    """Per-rank timings -> their maxima over all ranks (the job's time)."""
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def whole_job_gbs(bytes_per_rank, world, ms):
+    """Whole-job throughput: every rank moves bytes_per_rank in the (max-over-ranks) time ms."""
+    return world * bytes_per_rank / (ms * 1e-3) / 1e9
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -340,14 +354,10 @@ def main():
         del X, keep
     clk = clocks.stop()
 
-    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, e2e_ms = t.tolist()
-
+    ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist, "cuda")
     alg = algorithmic_bytes(NB, N, n_pts, 4)
-    value = world * alg / (ms * 1e-3) / 1e9
-    e2e_value = world * alg / (e2e_ms * 1e-3) / 1e9
+    value = whole_job_gbs(alg, world, ms)
+    e2e_value = whole_job_gbs(alg, world, e2e_ms)
     peak, peak_kind = load_peaks()
     # dominant kernel: the FD8 + V stencil; its algorithmic bytes are psi read +
     # Hpsi write + V
