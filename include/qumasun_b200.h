@@ -223,6 +223,19 @@ QSB_API qsb_status qsb_lobpcg_z(qsb_eigensolver* es, double dVol, int n, int ite
 QSB_API qsb_status qsb_lobpcg_d(qsb_eigensolver* es, double dVol, int n, int iter_max, double* eigen_values,
                                 double* X, double* keep, int is_first_time, void* stream);
 
+/* Gram product T = U^T V on the tcgen05 tensor cores as split-BF16x3
+ * compensated products (u = u_hi + u_lo in bfloat16, three products
+ * hi.hi + hi.lo + lo.hi) with FP32 accumulation per CTA and FP64 summation of
+ * the split-K partials: the mixed-precision form of the LOBPCG Gram blocks
+ * (MakeMatrix_z_blas's DGEMM_t(2n, 2n, N) on the 2n-real view,
+ * source/lobpcg_z_multi_mpi.h:300-558).
+ *   U (N x p), V (N x q): device, column-major with leading dimension N, FP32
+ *   or FP64 (V == U with p == q converts once); T: device FP64, p x q, ld ldt.
+ *   workspace: device, at least the bytes qsb_gram_bf16x3_workspace returns. */
+QSB_API qsb_status qsb_gram_bf16x3_workspace(int64_t N, int p, int q, int same, size_t* bytes);
+QSB_API qsb_status qsb_gram_bf16x3(qsb_dtype dtype, int64_t N, int p, int q, const void* U, const void* V,
+                                   double* T, int ldt, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Per-kernel device timing of qsb_ham_apply, in the spirit of the reference's
  * StopWatch sectors (source/StopWatch.h:11-60, watch_pp in
  * source/PseudoPotNonlocal_SvF2_kpoint.h:261-272).  While enabled, every

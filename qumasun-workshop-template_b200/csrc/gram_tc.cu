@@ -1,0 +1,395 @@
+// Gram products T = U^T V on the 5th-generation tensor cores (tcgen05 + TMEM),
+// as split-BF16x3 compensated products with FP32 accumulation:
+//   u = u_hi + u_lo (two bfloat16),  u.v ~ u_hi.v_hi + u_hi.v_lo + u_lo.v_hi
+// This is the mixed-precision form of the LOBPCG Gram blocks (MakeMatrix_z_blas,
+// source/lobpcg_z_multi_mpi.h:300-558: DGEMM_t(2n, 2n, N) on the 2n-real view;
+// EigenLOBPCG_d_multi's pairwise inner products, source/lobpcg_d_multi.h:103-133).
+//
+// Shapes: U is N x p, V is N x q, column-major with leading dimension N (each
+// column one grid plane); N is huge (grid points), p, q <= a few hundred.
+// Both operands are K-major for the MMA (K = grid index is contiguous).
+//
+// Pipeline per CTA (128 threads): warp 0 allocates the TMEM accumulator
+// (128 lanes x 128 fp32 columns) and its lane 0 streams 64-wide K stages of
+// U_hi, U_lo, V_hi, V_lo tiles with 2-D TMA copies (128B swizzle) into a 3-stage
+// ring; warp 1 lane 0 issues 12 tcgen05.mma (3 products x 4 K-steps of 16) per
+// stage and frees the stage with tcgen05.commit; after the CTA's K range all
+// four warps read the accumulator (tcgen05.ld) and write an FP32 partial tile.
+// CTAs split K; a second kernel sums the partials in FP64 in fixed order.
+//
+// All waits are bounded; a wait that runs out sets the device error word, the
+// CTA stops issuing, drains (bounded) and frees its TMEM before returning.
+#include "qsb_internal.h"
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cstring>
+
+namespace qsb {
+namespace {
+
+constexpr int GT_M = 128;          // UMMA M (rows of T per CTA)
+constexpr int GT_N = 128;          // UMMA N (columns of T per CTA)
+constexpr int GT_K = 64;           // K elements per stage (one 128-byte swizzle row of bf16)
+constexpr int GT_STAGES = 3;
+constexpr int GT_THREADS = 128;
+constexpr int TILE_BYTES_A = GT_M * GT_K * 2;   // 16 KB
+constexpr int TILE_BYTES_B = GT_N * GT_K * 2;   // 16 KB
+constexpr int STAGE_BYTES = 2 * TILE_BYTES_A + 2 * TILE_BYTES_B;
+constexpr size_t GT_SMEM = (size_t)GT_STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers, tmem addr*/;
+constexpr unsigned GT_WAIT_LIMIT = 1u << 22;
+constexpr unsigned GT_DRAIN_LIMIT = 1u << 16;
+constexpr int ERR_GEMM_TIMEOUT = 2;
+
+__device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void bar_init(uint64_t* b, uint32_t n) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(n) : "memory");
+}
+__device__ __forceinline__ void bar_expect_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool bar_try(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity, unsigned limit) {
+    for (unsigned i = 0; i < limit; ++i)
+        if (bar_try(b, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void tma_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* b) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(su32(dst)),
+        "l"((uint64_t)map), "r"(x), "r"(y), "r"(su32(b))
+        : "memory");
+}
+
+// UMMA shared-memory descriptor of a K-major tile stored in 128-byte swizzle
+// atoms (8 rows x 128 B): start address >> 4, leading offset 1 (unused for
+// swizzled K-major), stride offset 1024 B >> 4 between 8-row groups, descriptor
+// version 1, layout SWIZZLE_128B (2).
+__device__ __forceinline__ uint64_t sw128_kmajor_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// Instruction descriptor: kind::f16 with bf16 A and B, fp32 D, both K-major,
+// M = 128, N = 128.
+constexpr uint32_t GT_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(GT_N >> 3) << 17) |
+                              ((uint32_t)(GT_M >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(GT_IDESC), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* b) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(b))
+                 : "memory");
+}
+
+// u (fp32 or fp64, N x p, ld N) -> hi, lo bf16 (ldk x p, rows N..ldk zero)
+template <typename T>
+__global__ void split_bf16_kernel(const T* __restrict__ src, int64_t N, int p, int64_t ldk,
+                                  __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
+    const int col = blockIdx.y;
+    const T* s = src + (size_t)col * N;
+    __nv_bfloat16* h = hi + (size_t)col * ldk;
+    __nv_bfloat16* l = lo + (size_t)col * ldk;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ldk; i += (int64_t)gridDim.x * blockDim.x) {
+        if (i < N) {
+            const double v = (double)s[i];
+            const __nv_bfloat16 vh = __float2bfloat16_rn((float)v);
+            const __nv_bfloat16 vl = __float2bfloat16_rn((float)(v - (double)__bfloat162float(vh)));
+            h[i] = vh;
+            l[i] = vl;
+        } else {
+            h[i] = __float2bfloat16_rn(0.0f);
+            l[i] = __float2bfloat16_rn(0.0f);
+        }
+    }
+}
+
+// One CTA: output tile (m0, n0) of T over the K stages [kb0, kb1) (units of GT_K).
+// partial[(split * pq_tiles_rows + m) * ldpart + n] fp32, rows m in [0, 128).
+__global__ void __launch_bounds__(GT_THREADS, 1)
+gram_tc_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
+               const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, int kstages,
+               int ksplit, float* __restrict__ partial, int* __restrict__ err) {
+    extern __shared__ unsigned char gt_raw[];
+    unsigned char* base = (unsigned char*)(((uintptr_t)gt_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* full = reinterpret_cast<uint64_t*>(base + (size_t)GT_STAGES * STAGE_BYTES);
+    uint64_t* empty = full + GT_STAGES;
+    uint64_t* done = empty + GT_STAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mt = blockIdx.x, nt = blockIdx.y, split = blockIdx.z;
+    // this CTA's K stages: a contiguous share of the kstages
+    const int per = (kstages + ksplit - 1) / ksplit;
+    const int kb0 = min(kstages, split * per), kb1 = min(kstages, kb0 + per);
+    const int nk = kb1 - kb0;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < GT_STAGES; ++s) {
+            bar_init(&full[s], 1);
+            bar_init(&empty[s], 1);
+        }
+        bar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tmem_slot)),
+                     "r"(GT_N)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    int issued = 0;   // stages issued by the producer
+    if (warp == 0 && lane == 0) {
+        // ---- TMA producer ----
+        for (int it = 0; it < nk; ++it) {
+            const int s = it % GT_STAGES;
+            if (it >= GT_STAGES && !bar_wait(&empty[s], (uint32_t)(((it / GT_STAGES) - 1) & 1), GT_WAIT_LIMIT)) {
+                atomicOr(err, ERR_GEMM_TIMEOUT);
+                atomicExch(abort_flag, 1);
+                break;
+            }
+            if (*(volatile int*)abort_flag) break;
+            unsigned char* st = base + (size_t)s * STAGE_BYTES;
+            const int kx = (kb0 + it) * GT_K;
+            bar_expect_tx(&full[s], STAGE_BYTES);
+            tma_2d(st, &mAhi, kx, mt * GT_M, &full[s]);
+            tma_2d(st + TILE_BYTES_A, &mAlo, kx, mt * GT_M, &full[s]);
+            tma_2d(st + 2 * TILE_BYTES_A, &mBhi, kx, nt * GT_N, &full[s]);
+            tma_2d(st + 2 * TILE_BYTES_A + TILE_BYTES_B, &mBlo, kx, nt * GT_N, &full[s]);
+            issued = it + 1;
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMA issuer ----
+        for (int it = 0; it < nk; ++it) {
+            const int s = it % GT_STAGES;
+            if (!bar_wait(&full[s], (uint32_t)((it / GT_STAGES) & 1), GT_WAIT_LIMIT)) {
+                atomicOr(err, ERR_GEMM_TIMEOUT);
+                atomicExch(abort_flag, 1);
+                break;
+            }
+            if (*(volatile int*)abort_flag) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t st = su32(base + (size_t)s * STAGE_BYTES);
+            const uint32_t a_hi = st, a_lo = st + TILE_BYTES_A;
+            const uint32_t b_hi = st + 2 * TILE_BYTES_A, b_lo = b_hi + TILE_BYTES_B;
+#pragma unroll
+            for (int kk = 0; kk < GT_K / 16; ++kk) {
+                const uint32_t koff = kk * 32;   // 16 bf16 = 32 bytes along the swizzled row
+                const uint32_t acc0 = (it > 0 || kk > 0) ? 1u : 0u;
+                umma_bf16(tmem, sw128_kmajor_desc(a_hi + koff), sw128_kmajor_desc(b_hi + koff), acc0);
+                umma_bf16(tmem, sw128_kmajor_desc(a_hi + koff), sw128_kmajor_desc(b_lo + koff), 1u);
+                umma_bf16(tmem, sw128_kmajor_desc(a_lo + koff), sw128_kmajor_desc(b_hi + koff), 1u);
+            }
+            umma_commit(&empty[s]);   // stage s free once these MMAs complete
+        }
+        umma_commit(done);            // accumulator complete (or nothing in flight after an abort)
+    }
+    __syncwarp();
+
+    // ---- epilogue: all warps; warp w owns TMEM lanes (rows) 32w .. 32w+31 ----
+    bool ok = bar_wait(done, 0, GT_WAIT_LIMIT);
+    if (!ok) {
+        atomicOr(err, ERR_GEMM_TIMEOUT);
+        atomicExch(abort_flag, 1);
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int row = warp * 32 + lane;
+    float* prow = partial + ((size_t)split * (gridDim.x * GT_M) + (size_t)mt * GT_M + row) * (gridDim.y * GT_N) +
+                  (size_t)nt * GT_N;
+    const bool have = ok && nk > 0;
+#pragma unroll 1
+    for (int c0 = 0; c0 < GT_N; c0 += 32) {
+        uint32_t r[32];
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+              "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+              "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int j = 0; j < 32; j += 4) {
+            float4 v = have ? make_float4(__uint_as_float(r[j]), __uint_as_float(r[j + 1]), __uint_as_float(r[j + 2]),
+                                          __uint_as_float(r[j + 3]))
+                            : make_float4(0.f, 0.f, 0.f, 0.f);
+            *reinterpret_cast<float4*>(prow + c0 + j) = v;
+        }
+    }
+
+    // ---- teardown: drain copies still in flight after an abort, free TMEM ----
+    __syncthreads();
+    if (threadIdx.x == 0 && *(volatile int*)abort_flag) {
+        // only the last phase of each stage can still have copies in flight
+        for (int it = max(0, issued - GT_STAGES); it < issued; ++it)
+            (void)bar_wait(&full[it % GT_STAGES], (uint32_t)((it / GT_STAGES) & 1), GT_DRAIN_LIMIT);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(GT_N) : "memory");
+    }
+}
+
+// T[m + ldt*n] (+)= sum over splits of partial (fixed order, FP64)
+__global__ void gram_reduce_kernel(const float* __restrict__ partial, int ksplit, int rows_pad, int cols_pad, int p,
+                                   int q, double* __restrict__ T, int ldt, double alpha, int accumulate) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = blockIdx.y;
+    if (m >= p || n >= q) return;
+    double s = 0.0;
+    for (int k = 0; k < ksplit; ++k) s += (double)partial[((size_t)k * rows_pad + m) * cols_pad + n];
+    double* t = T + m + (size_t)ldt * n;
+    *t = accumulate ? *t + alpha * s : alpha * s;
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn gt_encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// 2-D map over a bf16 operand [cols][ldk], box (64 K, rows), 128-byte swizzle
+bool make_operand_map(CUtensorMap* map, const void* base, int64_t ldk, int cols, int box_rows) {
+    EncodeTiledFn fn = gt_encode_fn();
+    if (!fn) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)ldk, (cuuint64_t)cols};
+    const cuuint64_t strides[1] = {(cuuint64_t)ldk * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)GT_K, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+struct GramPlan {
+    int64_t ldk;
+    int mtiles, ntiles, kstages, ksplit;
+    size_t off_ahi, off_alo, off_bhi, off_blo, off_part, total;
+};
+
+GramPlan plan_gram(int64_t N, int p, int q, bool same) {
+    GramPlan g{};
+    g.ldk = ((N + GT_K - 1) / GT_K) * GT_K;
+    g.mtiles = (p + GT_M - 1) / GT_M;
+    g.ntiles = (q + GT_N - 1) / GT_N;
+    g.kstages = (int)(g.ldk / GT_K);
+    const int tiles = g.mtiles * g.ntiles;
+    g.ksplit = std::max(1, std::min(g.kstages, (148 + tiles - 1) / tiles));
+    auto al = [](size_t b) { return (b + 1023) & ~(size_t)1023; };
+    size_t off = 0;
+    g.off_ahi = off; off += al((size_t)g.ldk * p * 2);
+    g.off_alo = off; off += al((size_t)g.ldk * p * 2);
+    if (same) {
+        g.off_bhi = g.off_ahi;
+        g.off_blo = g.off_alo;
+    } else {
+        g.off_bhi = off; off += al((size_t)g.ldk * q * 2);
+        g.off_blo = off; off += al((size_t)g.ldk * q * 2);
+    }
+    g.off_part = off; off += al((size_t)g.ksplit * g.mtiles * GT_M * g.ntiles * GT_N * 4);
+    g.total = off;
+    return g;
+}
+
+}  // namespace
+
+size_t gram_bf16x3_workspace(int64_t N, int p, int q, bool same) { return plan_gram(N, p, q, same).total; }
+
+// T (p x q, ld ldt, FP64) = alpha * U^T V  (+ T when accumulate), U: N x p, V: N x q
+// (ld N, fp32 or fp64; V == U allowed), via split-BF16x3 tcgen05 products.
+qsb_status gram_bf16x3(qsb_dtype dt, int64_t N, int p, int q, const void* U, const void* V, double* T, int ldt,
+                       double alpha, bool accumulate, void* ws, size_t ws_bytes, cudaStream_t s) {
+    if (p <= 0 || q <= 0 || N <= 0) return QSB_OK;
+    const bool same = (U == V) && (p == q);
+    const GramPlan g = plan_gram(N, p, q, same);
+    if (ws_bytes < g.total) return fail(QSB_ERR_INVALID, "gram_bf16x3: workspace too small");
+    unsigned char* w = (unsigned char*)ws;
+    __nv_bfloat16 *ahi = (__nv_bfloat16*)(w + g.off_ahi), *alo = (__nv_bfloat16*)(w + g.off_alo);
+    __nv_bfloat16 *bhi = (__nv_bfloat16*)(w + g.off_bhi), *blo = (__nv_bfloat16*)(w + g.off_blo);
+    float* part = (float*)(w + g.off_part);
+    const int cblocks = (int)std::min<int64_t>((g.ldk + 255) / 256, 1024);
+    if (dt == QSB_F64) {
+        split_bf16_kernel<double><<<dim3(cblocks, p), 256, 0, s>>>((const double*)U, N, p, g.ldk, ahi, alo);
+        if (!same) split_bf16_kernel<double><<<dim3(cblocks, q), 256, 0, s>>>((const double*)V, N, q, g.ldk, bhi, blo);
+    } else {
+        split_bf16_kernel<float><<<dim3(cblocks, p), 256, 0, s>>>((const float*)U, N, p, g.ldk, ahi, alo);
+        if (!same) split_bf16_kernel<float><<<dim3(cblocks, q), 256, 0, s>>>((const float*)V, N, q, g.ldk, bhi, blo);
+    }
+    QSB_CUDA_TRY(cudaGetLastError());
+    CUtensorMap mahi, malo, mbhi, mblo;
+    if (!make_operand_map(&mahi, ahi, g.ldk, p, GT_M) || !make_operand_map(&malo, alo, g.ldk, p, GT_M) ||
+        !make_operand_map(&mbhi, bhi, g.ldk, q, GT_N) || !make_operand_map(&mblo, blo, g.ldk, q, GT_N))
+        return fail(QSB_ERR_CUDA, "gram_bf16x3: tensor map encoding failed");
+    QSB_CUDA_TRY(cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GT_SMEM));
+    gram_tc_kernel<<<dim3(g.mtiles, g.ntiles, g.ksplit), GT_THREADS, GT_SMEM, s>>>(
+        mahi, malo, mbhi, mblo, g.kstages, g.ksplit, part, device_error_word());
+    QSB_CUDA_TRY(cudaGetLastError());
+    gram_reduce_kernel<<<dim3((p + 127) / 128, q), 128, 0, s>>>(part, g.ksplit, g.mtiles * GT_M, g.ntiles * GT_N, p, q,
+                                                                 T, ldt, alpha, accumulate ? 1 : 0);
+    QSB_CUDA_TRY(cudaGetLastError());
+    return QSB_OK;
+}
+
+}  // namespace qsb
+
+extern "C" {
+
+qsb_status qsb_gram_bf16x3_workspace(int64_t N, int p, int q, int same, size_t* bytes) {
+    if (!bytes || N < 1 || p < 1 || q < 1) return qsb::fail(QSB_ERR_INVALID, "gram_bf16x3_workspace: bad arguments");
+    *bytes = qsb::gram_bf16x3_workspace(N, p, q, same != 0);
+    return QSB_OK;
+}
+
+qsb_status qsb_gram_bf16x3(qsb_dtype dtype, int64_t N, int p, int q, const void* U, const void* V, double* T, int ldt,
+                           void* workspace, size_t workspace_bytes, void* stream) {
+    if (dtype != QSB_F64 && dtype != QSB_F32) return qsb::fail(QSB_ERR_INVALID, "gram_bf16x3: bad dtype");
+    if (N < 1 || p < 1 || q < 1 || !U || !V || !T || ldt < p || !workspace)
+        return qsb::fail(QSB_ERR_INVALID, "gram_bf16x3: bad arguments");
+    if (p > 65535 || q > 65535) return qsb::fail(QSB_ERR_INVALID, "gram_bf16x3: p, q must be < 65536");
+    return qsb::gram_bf16x3(dtype, N, p, q, U, V, T, ldt, 1.0, false, workspace, workspace_bytes,
+                            (cudaStream_t)stream);
+}
+
+}  // extern "C"

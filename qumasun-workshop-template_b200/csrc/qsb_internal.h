@@ -107,6 +107,12 @@ qsb_status nl_project(qsb_dtype dt, const NLDevice& d, int nx, int ny, int nz, i
 qsb_status nl_apply(qsb_dtype dt, const NLDevice& d, int N, int nb, int is_complex, void* hpsi,
                     const double* coef, double gx_dx, double gy_dy, double gz_dz, cudaStream_t s);
 
+// Split-BF16x3 tensor-core Gram product (gram_tc.cu): T (p x q, FP64, ld ldt)
+// = alpha * U^T V (+ T), U: N x p, V: N x q, column-major ld N, fp32 or fp64.
+size_t gram_bf16x3_workspace(int64_t N, int p, int q, bool same);
+qsb_status gram_bf16x3(qsb_dtype dt, int64_t N, int p, int q, const void* U, const void* V, double* T, int ldt,
+                       double alpha, bool accumulate, void* ws, size_t ws_bytes, cudaStream_t s);
+
 }  // namespace qsb
 
 struct qsb_ham {
