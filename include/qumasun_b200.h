@@ -192,13 +192,45 @@ typedef int (*qsb_apply_fn)(void* user, int nb, const double* x_dev, double* ax_
  * temporary (the reference's `work`/`temporary` arenas,
  * source/lobpcg_z_multi_mpi.h:2862-2881) and the cuBLAS / cuSOLVER handles. */
 QSB_API qsb_status qsb_eigensolver_create(qsb_eigensolver** es, int64_t N, int n, int is_complex);
+
+/* Precision of a solver context.
+ *   QSB_PREC_FP64   everything in FP64 (the reference's arithmetic).
+ *   QSB_PREC_MIXED  the bundles X, R, P, AX, AR, AP live in FP32 inside the
+ *                   context and the operator runs in FP32 (qsb_ham_apply with
+ *                   QSB_F32, or an fp32 callback); the Gram / Rayleigh-Ritz
+ *                   products run on the tensor cores as split-BF16x3 products
+ *                   with FP32 accumulation (qsb_gram_bf16x3); the rotations
+ *                   X' = X Cx + R Cr + P Cp are FP32 GEMMs; the pencil solve,
+ *                   Rayleigh quotients, norms and the convergence tests stay
+ *                   FP64.  The caller's X, keep and eigenvalues stay FP64 and
+ *                   the qsb_lobpcg_z / qsb_lobpcg_d calls are unchanged; X and
+ *                   keep come back with FP32 resolution. */
+typedef enum qsb_precision { QSB_PREC_FP64 = 0, QSB_PREC_MIXED = 1 } qsb_precision;
+QSB_API qsb_status qsb_eigensolver_create_ex(qsb_eigensolver** es, int64_t N, int n, int is_complex,
+                                             qsb_precision precision);
 QSB_API qsb_status qsb_eigensolver_destroy(qsb_eigensolver* es);
 /* H of a qsb_ham context (Bloch vector g for complex bands) as the operator. */
 QSB_API qsb_status qsb_eigensolver_set_hamiltonian(qsb_eigensolver* es, qsb_ham* ham, double gx, double gy, double gz);
 /* A user callback as the operator. */
 QSB_API qsb_status qsb_eigensolver_set_operator(qsb_eigensolver* es, qsb_apply_fn op, void* user);
+/* FP32 operator callback for QSB_PREC_MIXED contexts (fp32 bundles, same layouts). */
+typedef int (*qsb_apply_f32_fn)(void* user, int nb, const float* x_dev, float* ax_dev, void* stream);
+QSB_API qsb_status qsb_eigensolver_set_operator_f32(qsb_eigensolver* es, qsb_apply_f32_fn op, void* user);
 /* Iterations done by the last solve, and whether it ended with the norm-check rollback. */
 QSB_API qsb_status qsb_eigensolver_last_stats(const qsb_eigensolver* es, int* iterations, int* rolled_back);
+/* QSB_PREC_MIXED only.  The Rayleigh-Ritz step scales the pencil to a unit
+ * diagonal, eigendecomposes the overlap matrix and drops the directions whose
+ * overlap eigenvalue is below tol * (largest); the Ritz pairs are taken in the
+ * rest (Stathopoulos-Wu's SVQB basis, as Hetmaniuk-Lehoucq use it in LOBPCG).
+ * This replaces the Cholesky of ZHEGVD, which the split-BF16x3 overlap errors
+ * (~2^-17 / sqrt(N) of the diagonal) make fail once the basis [X R P] turns
+ * ill-conditioned near convergence.  Default: 1e-5 / sqrt(N) within [1e-8, 1e-5]. */
+QSB_API qsb_status qsb_eigensolver_set_drop_tolerance(qsb_eigensolver* es, double tol);
+/* Of the last call (mixed precision): most directions dropped in one
+ * iteration, smallest kept overlap eigenvalue relative to the largest, and the
+ * tolerance in force. */
+QSB_API qsb_status qsb_eigensolver_overlap_stats(const qsb_eigensolver* es, int* max_dropped, double* min_kept_ratio,
+                                                 double* drop_tolerance);
 
 /* Complex block LOBPCG.  Replaces LOBPCG::Eigen_z_multi_mpi(l_grid, dVol,
  * num_solution, iter_max, eigen_values, eigen_vectors, keep, work, temporary,
@@ -231,10 +263,14 @@ QSB_API qsb_status qsb_lobpcg_d(qsb_eigensolver* es, double dVol, int n, int ite
  * source/lobpcg_z_multi_mpi.h:300-558).
  *   U (N x p), V (N x q): device, column-major with leading dimension N, FP32
  *   or FP64 (V == U with p == q converts once); T: device FP64, p x q, ld ldt.
+ *   upper != 0 (p == q): only the 128 x 128 output tiles on or above the
+ *   diagonal are computed and written (all upper-triangle entries among them),
+ *   the form the symmetric / Hermitian pencils use; other entries are untouched.
  *   workspace: device, at least the bytes qsb_gram_bf16x3_workspace returns. */
 QSB_API qsb_status qsb_gram_bf16x3_workspace(int64_t N, int p, int q, int same, size_t* bytes);
 QSB_API qsb_status qsb_gram_bf16x3(qsb_dtype dtype, int64_t N, int p, int q, const void* U, const void* V,
-                                   double* T, int ldt, void* workspace, size_t workspace_bytes, void* stream);
+                                   double* T, int ldt, int upper, void* workspace, size_t workspace_bytes,
+                                   void* stream);
 
 /* Per-kernel device timing of qsb_ham_apply, in the spirit of the reference's
  * StopWatch sectors (source/StopWatch.h:11-60, watch_pp in

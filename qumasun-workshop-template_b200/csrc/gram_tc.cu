@@ -102,12 +102,29 @@ __device__ __forceinline__ void umma_commit(uint64_t* b) {
                  : "memory");
 }
 
-// u (fp32 or fp64, N x p, ld N) -> hi, lo bf16 (ldk x p, rows N..ldk zero)
+// Column c of the gathered operand (fp32 or fp64, one column every N elements)
+// -> hi, lo bf16 columns of length ldk (rows N..ldk zero).  The columns come
+// from up to kMaxSegments arrays, so the active bands of separate bundles form
+// one operand without a copy.
 template <typename T>
-__global__ void split_bf16_kernel(const T* __restrict__ src, int64_t N, int p, int64_t ldk,
-                                  __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
+__global__ void split_bf16_kernel(ColumnSet src, int64_t N, int64_t ldk, __nv_bfloat16* __restrict__ hi,
+                                  __nv_bfloat16* __restrict__ lo) {
     const int col = blockIdx.y;
-    const T* s = src + (size_t)col * N;
+    int local = col;
+    const void* b = src.base[0];
+    bool found = false;
+#pragma unroll
+    for (int k = 0; k < kMaxSegments; ++k) {
+        if (!found) {
+            if (k + 1 >= src.nseg || local < src.cols[k]) {
+                b = src.base[k];
+                found = true;
+            } else {
+                local -= src.cols[k];
+            }
+        }
+    }
+    const T* s = static_cast<const T*>(b) + (size_t)local * N;
     __nv_bfloat16* h = hi + (size_t)col * ldk;
     __nv_bfloat16* l = lo + (size_t)col * ldk;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ldk; i += (int64_t)gridDim.x * blockDim.x) {
@@ -124,12 +141,33 @@ __global__ void split_bf16_kernel(const T* __restrict__ src, int64_t N, int p, i
     }
 }
 
-// One CTA: output tile (m0, n0) of T over the K stages [kb0, kb1) (units of GT_K).
-// partial[(split * pq_tiles_rows + m) * ldpart + n] fp32, rows m in [0, 128).
+// Output tile of list entry t: all mtiles x ntiles tiles (column order), or
+// only the tiles on and above the diagonal (mt <= nt, column order).
+__host__ __device__ __forceinline__ void tile_of(int t, int mtiles, bool upper, int* mt, int* nt) {
+    if (upper) {
+        int c = 0;
+        while (t > c) {
+            t -= c + 1;
+            ++c;
+        }
+        *mt = t;
+        *nt = c;
+    } else {
+        *mt = t % mtiles;
+        *nt = t / mtiles;
+    }
+}
+__host__ __device__ __forceinline__ int tile_index(int mt, int nt, int mtiles, bool upper) {
+    return upper ? nt * (nt + 1) / 2 + mt : nt * mtiles + mt;
+}
+
+// One CTA: output tile t of the tile list (blockIdx.x) over the K stages
+// [kb0, kb1) of split blockIdx.y (units of GT_K); the fp32 tile goes to
+// partial[((split * ntl + t) * GT_M + row) * GT_N + col].
 __global__ void __launch_bounds__(GT_THREADS, 1)
 gram_tc_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
                const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, int kstages,
-               int ksplit, float* __restrict__ partial, int* __restrict__ err) {
+               int ksplit, int mtiles, int upper, float* __restrict__ partial, int* __restrict__ err) {
     extern __shared__ unsigned char gt_raw[];
     unsigned char* base = (unsigned char*)(((uintptr_t)gt_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* full = reinterpret_cast<uint64_t*>(base + (size_t)GT_STAGES * STAGE_BYTES);
@@ -139,7 +177,9 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int mt = blockIdx.x, nt = blockIdx.y, split = blockIdx.z;
+    const int t = blockIdx.x, ntl = gridDim.x, split = blockIdx.y;
+    int mt, nt;
+    tile_of(t, mtiles, upper != 0, &mt, &nt);
     // this CTA's K stages: a contiguous share of the kstages
     const int per = (kstages + ksplit - 1) / ksplit;
     const int kb0 = min(kstages, split * per), kb1 = min(kstages, kb0 + per);
@@ -221,8 +261,7 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const int row = warp * 32 + lane;
-    float* prow = partial + ((size_t)split * (gridDim.x * GT_M) + (size_t)mt * GT_M + row) * (gridDim.y * GT_N) +
-                  (size_t)nt * GT_N;
+    float* prow = partial + ((size_t)split * ntl + t) * (GT_M * GT_N) + (size_t)row * GT_N;
     const bool have = ok && nk > 0;
 #pragma unroll 1
     for (int c0 = 0; c0 < GT_N; c0 += 32) {
@@ -260,16 +299,23 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__
     }
 }
 
-// T[m + ldt*n] (+)= sum over splits of partial (fixed order, FP64)
-__global__ void gram_reduce_kernel(const float* __restrict__ partial, int ksplit, int rows_pad, int cols_pad, int p,
-                                   int q, double* __restrict__ T, int ldt, double alpha, int accumulate) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    const int n = blockIdx.y;
+// T[m + ldt*n] (+)= alpha * sum over splits of the partial tiles (fixed order,
+// FP64).  Threads run along n, the contiguous index of a partial tile row.
+// Entries of tiles below the diagonal are left alone in upper mode.
+__global__ void gram_reduce_kernel(const float* __restrict__ partial, int ksplit, int ntl, int mtiles, int upper,
+                                   int p, int q, double* __restrict__ T, int ldt, double alpha, int accumulate) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = blockIdx.y;
     if (m >= p || n >= q) return;
+    const int mt = m / GT_M, nt = n / GT_N;
+    if (upper && mt > nt) return;
+    const int t = tile_index(mt, nt, mtiles, upper != 0);
+    const size_t off = (size_t)t * (GT_M * GT_N) + (size_t)(m % GT_M) * GT_N + (n % GT_N);
+    const size_t stride = (size_t)ntl * (GT_M * GT_N);
     double s = 0.0;
-    for (int k = 0; k < ksplit; ++k) s += (double)partial[((size_t)k * rows_pad + m) * cols_pad + n];
-    double* t = T + m + (size_t)ldt * n;
-    *t = accumulate ? *t + alpha * s : alpha * s;
+    for (int k = 0; k < ksplit; ++k) s += (double)partial[off + (size_t)k * stride];
+    double* d = T + m + (size_t)ldt * n;
+    *d = accumulate ? *d + alpha * s : alpha * s;
 }
 
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -303,73 +349,100 @@ bool make_operand_map(CUtensorMap* map, const void* base, int64_t ldk, int cols,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+int64_t split_ldk(int64_t N) { return ((N + GT_K - 1) / GT_K) * GT_K; }
+size_t align1k(size_t b) { return (b + 1023) & ~(size_t)1023; }
+size_t split_half_bytes(int64_t N, int cols) { return align1k((size_t)split_ldk(N) * cols * 2); }
+
 struct GramPlan {
-    int64_t ldk;
-    int mtiles, ntiles, kstages, ksplit;
-    size_t off_ahi, off_alo, off_bhi, off_blo, off_part, total;
+    int mtiles, ntiles, ntl, kstages, ksplit;
+    size_t partial_bytes;
 };
 
-GramPlan plan_gram(int64_t N, int p, int q, bool same) {
+// Tile list and K split: at most one wave of CTAs (one CTA per SM), each with
+// a contiguous share of the K stages.
+GramPlan plan_gram(int64_t N, int p, int q, bool upper) {
     GramPlan g{};
-    g.ldk = ((N + GT_K - 1) / GT_K) * GT_K;
     g.mtiles = (p + GT_M - 1) / GT_M;
     g.ntiles = (q + GT_N - 1) / GT_N;
-    g.kstages = (int)(g.ldk / GT_K);
-    const int tiles = g.mtiles * g.ntiles;
-    g.ksplit = std::max(1, std::min(g.kstages, (148 + tiles - 1) / tiles));
-    auto al = [](size_t b) { return (b + 1023) & ~(size_t)1023; };
-    size_t off = 0;
-    g.off_ahi = off; off += al((size_t)g.ldk * p * 2);
-    g.off_alo = off; off += al((size_t)g.ldk * p * 2);
-    if (same) {
-        g.off_bhi = g.off_ahi;
-        g.off_blo = g.off_alo;
-    } else {
-        g.off_bhi = off; off += al((size_t)g.ldk * q * 2);
-        g.off_blo = off; off += al((size_t)g.ldk * q * 2);
-    }
-    g.off_part = off; off += al((size_t)g.ksplit * g.mtiles * GT_M * g.ntiles * GT_N * 4);
-    g.total = off;
+    g.ntl = upper ? g.ntiles * (g.ntiles + 1) / 2 : g.mtiles * g.ntiles;
+    g.kstages = (int)(split_ldk(N) / GT_K);
+    g.ksplit = std::max(1, std::min(g.kstages, 148 / std::max(1, g.ntl)));
+    g.partial_bytes = align1k((size_t)g.ksplit * g.ntl * GT_M * GT_N * sizeof(float));
     return g;
 }
 
 }  // namespace
 
-size_t gram_bf16x3_workspace(int64_t N, int p, int q, bool same) { return plan_gram(N, p, q, same).total; }
+size_t split_bf16_bytes(int64_t N, int cols) { return 2 * split_half_bytes(N, cols); }
 
-// T (p x q, ld ldt, FP64) = alpha * U^T V  (+ T when accumulate), U: N x p, V: N x q
-// (ld N, fp32 or fp64; V == U allowed), via split-BF16x3 tcgen05 products.
-qsb_status gram_bf16x3(qsb_dtype dt, int64_t N, int p, int q, const void* U, const void* V, double* T, int ldt,
-                       double alpha, bool accumulate, void* ws, size_t ws_bytes, cudaStream_t s) {
-    if (p <= 0 || q <= 0 || N <= 0) return QSB_OK;
-    const bool same = (U == V) && (p == q);
-    const GramPlan g = plan_gram(N, p, q, same);
-    if (ws_bytes < g.total) return fail(QSB_ERR_INVALID, "gram_bf16x3: workspace too small");
-    unsigned char* w = (unsigned char*)ws;
-    __nv_bfloat16 *ahi = (__nv_bfloat16*)(w + g.off_ahi), *alo = (__nv_bfloat16*)(w + g.off_alo);
-    __nv_bfloat16 *bhi = (__nv_bfloat16*)(w + g.off_bhi), *blo = (__nv_bfloat16*)(w + g.off_blo);
-    float* part = (float*)(w + g.off_part);
-    const int cblocks = (int)std::min<int64_t>((g.ldk + 255) / 256, 1024);
-    if (dt == QSB_F64) {
-        split_bf16_kernel<double><<<dim3(cblocks, p), 256, 0, s>>>((const double*)U, N, p, g.ldk, ahi, alo);
-        if (!same) split_bf16_kernel<double><<<dim3(cblocks, q), 256, 0, s>>>((const double*)V, N, q, g.ldk, bhi, blo);
-    } else {
-        split_bf16_kernel<float><<<dim3(cblocks, p), 256, 0, s>>>((const float*)U, N, p, g.ldk, ahi, alo);
-        if (!same) split_bf16_kernel<float><<<dim3(cblocks, q), 256, 0, s>>>((const float*)V, N, q, g.ldk, bhi, blo);
-    }
-    QSB_CUDA_TRY(cudaGetLastError());
-    CUtensorMap mahi, malo, mbhi, mblo;
-    if (!make_operand_map(&mahi, ahi, g.ldk, p, GT_M) || !make_operand_map(&malo, alo, g.ldk, p, GT_M) ||
-        !make_operand_map(&mbhi, bhi, g.ldk, q, GT_N) || !make_operand_map(&mblo, blo, g.ldk, q, GT_N))
-        return fail(QSB_ERR_CUDA, "gram_bf16x3: tensor map encoding failed");
-    QSB_CUDA_TRY(cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GT_SMEM));
-    gram_tc_kernel<<<dim3(g.mtiles, g.ntiles, g.ksplit), GT_THREADS, GT_SMEM, s>>>(
-        mahi, malo, mbhi, mblo, g.kstages, g.ksplit, part, device_error_word());
-    QSB_CUDA_TRY(cudaGetLastError());
-    gram_reduce_kernel<<<dim3((p + 127) / 128, q), 128, 0, s>>>(part, g.ksplit, g.mtiles * GT_M, g.ntiles * GT_N, p, q,
-                                                                 T, ldt, alpha, accumulate ? 1 : 0);
+qsb_status split_bf16(qsb_dtype dt, int64_t N, const ColumnSet& src, void* dst, cudaStream_t s) {
+    const int cols = column_count(src);
+    if (cols <= 0) return QSB_OK;
+    if (cols > 65535) return fail(QSB_ERR_INVALID, "split_bf16: too many columns");
+    const int64_t ldk = split_ldk(N);
+    __nv_bfloat16* hi = (__nv_bfloat16*)dst;
+    __nv_bfloat16* lo = (__nv_bfloat16*)((unsigned char*)dst + split_half_bytes(N, cols));
+    const int cblocks = (int)std::min<int64_t>((ldk + 255) / 256, 512);
+    if (dt == QSB_F64)
+        split_bf16_kernel<double><<<dim3(cblocks, cols), 256, 0, s>>>(src, N, ldk, hi, lo);
+    else
+        split_bf16_kernel<float><<<dim3(cblocks, cols), 256, 0, s>>>(src, N, ldk, hi, lo);
     QSB_CUDA_TRY(cudaGetLastError());
     return QSB_OK;
+}
+
+size_t gram_partial_bytes(int64_t N, int p, int q, bool upper) { return plan_gram(N, p, q, upper).partial_bytes; }
+
+// ksplit * ntl <= max(148, ntl) for every call, and ntl grows with p and q.
+size_t gram_partial_bytes_bound(int p, int q, bool upper) {
+    const GramPlan g = plan_gram(GT_K, p, q, upper);
+    return align1k((size_t)std::max(148, g.ntl) * GT_M * GT_N * sizeof(float));
+}
+
+qsb_status gram_split_tc(int64_t N, const void* A, int p, const void* B, int q, bool upper, double* T, int ldt,
+                         double alpha, bool accumulate, void* partial, size_t partial_bytes, cudaStream_t s) {
+    if (p <= 0 || q <= 0 || N <= 0) return QSB_OK;
+    if (upper && p != q) return fail(QSB_ERR_INVALID, "gram_split_tc: upper mode needs p == q");
+    const GramPlan g = plan_gram(N, p, q, upper);
+    if (partial_bytes < g.partial_bytes) return fail(QSB_ERR_INVALID, "gram_split_tc: partial workspace too small");
+    const int64_t ldk = split_ldk(N);
+    const unsigned char* a = (const unsigned char*)A;
+    const unsigned char* b = (const unsigned char*)B;
+    CUtensorMap mahi, malo, mbhi, mblo;
+    if (!make_operand_map(&mahi, a, ldk, p, GT_M) || !make_operand_map(&malo, a + split_half_bytes(N, p), ldk, p, GT_M) ||
+        !make_operand_map(&mbhi, b, ldk, q, GT_N) || !make_operand_map(&mblo, b + split_half_bytes(N, q), ldk, q, GT_N))
+        return fail(QSB_ERR_CUDA, "gram_split_tc: tensor map encoding failed");
+    QSB_CUDA_TRY(cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GT_SMEM));
+    gram_tc_kernel<<<dim3(g.ntl, g.ksplit), GT_THREADS, GT_SMEM, s>>>(mahi, malo, mbhi, mblo, g.kstages, g.ksplit,
+                                                                       g.mtiles, upper ? 1 : 0, (float*)partial,
+                                                                       device_error_word());
+    QSB_CUDA_TRY(cudaGetLastError());
+    gram_reduce_kernel<<<dim3((q + 127) / 128, p), 128, 0, s>>>((const float*)partial, g.ksplit, g.ntl, g.mtiles,
+                                                                 upper ? 1 : 0, p, q, T, ldt, alpha,
+                                                                 accumulate ? 1 : 0);
+    QSB_CUDA_TRY(cudaGetLastError());
+    return QSB_OK;
+}
+
+size_t gram_bf16x3_workspace(int64_t N, int p, int q, bool same) {
+    return split_bf16_bytes(N, p) + (same ? 0 : split_bf16_bytes(N, q)) + gram_partial_bytes(N, p, q, false);
+}
+
+// T (p x q, ld ldt, FP64) = alpha * U^T V  (+ T when accumulate), U: N x p, V: N x q
+// (ld N, fp32 or fp64; V == U with p == q splits once).
+qsb_status gram_bf16x3(qsb_dtype dt, int64_t N, int p, int q, const void* U, const void* V, double* T, int ldt,
+                       double alpha, bool accumulate, bool upper, void* ws, size_t ws_bytes, cudaStream_t s) {
+    if (p <= 0 || q <= 0 || N <= 0) return QSB_OK;
+    const bool same = (U == V) && (p == q);
+    const size_t need = gram_bf16x3_workspace(N, p, q, same);
+    if (ws_bytes < need) return fail(QSB_ERR_INVALID, "gram_bf16x3: workspace too small");
+    unsigned char* w = (unsigned char*)ws;
+    unsigned char* sa = w;
+    unsigned char* sb = same ? sa : sa + split_bf16_bytes(N, p);
+    unsigned char* part = sb + (same ? split_bf16_bytes(N, p) : split_bf16_bytes(N, q));
+    QSB_TRY(split_bf16(dt, N, column_set(U, p), sa, s));
+    if (!same) QSB_TRY(split_bf16(dt, N, column_set(V, q), sb, s));
+    return gram_split_tc(N, sa, p, sb, q, upper, T, ldt, alpha, accumulate, part, gram_partial_bytes(N, p, q, false), s);
 }
 
 }  // namespace qsb
@@ -383,12 +456,13 @@ qsb_status qsb_gram_bf16x3_workspace(int64_t N, int p, int q, int same, size_t* 
 }
 
 qsb_status qsb_gram_bf16x3(qsb_dtype dtype, int64_t N, int p, int q, const void* U, const void* V, double* T, int ldt,
-                           void* workspace, size_t workspace_bytes, void* stream) {
+                           int upper, void* workspace, size_t workspace_bytes, void* stream) {
     if (dtype != QSB_F64 && dtype != QSB_F32) return qsb::fail(QSB_ERR_INVALID, "gram_bf16x3: bad dtype");
     if (N < 1 || p < 1 || q < 1 || !U || !V || !T || ldt < p || !workspace)
         return qsb::fail(QSB_ERR_INVALID, "gram_bf16x3: bad arguments");
     if (p > 65535 || q > 65535) return qsb::fail(QSB_ERR_INVALID, "gram_bf16x3: p, q must be < 65536");
-    return qsb::gram_bf16x3(dtype, N, p, q, U, V, T, ldt, 1.0, false, workspace, workspace_bytes,
+    if (upper && p != q) return qsb::fail(QSB_ERR_INVALID, "gram_bf16x3: upper needs p == q");
+    return qsb::gram_bf16x3(dtype, N, p, q, U, V, T, ldt, 1.0, false, upper != 0, workspace, workspace_bytes,
                             (cudaStream_t)stream);
 }
 

@@ -36,14 +36,16 @@ constexpr int RED_THREADS = 256;
 constexpr int RED_CHUNK = 1 << 16;   // doubles per reduction block
 
 // partial[s * nch + ch] = sum over chunk ch of segment s of a[i]*b[i]
-__global__ void seg_dot_partial(const double* __restrict__ a, const double* __restrict__ b, size_t L, int nch,
+// (fp64 or fp32 bundles, fp64 sums)
+template <typename T>
+__global__ void seg_dot_partial(const T* __restrict__ a, const T* __restrict__ b, size_t L, int nch,
                                 double* __restrict__ partial) {
     const int s = blockIdx.y, ch = blockIdx.x;
     const size_t i0 = (size_t)ch * RED_CHUNK, i1 = min(L, i0 + RED_CHUNK);
-    const double* A = a + (size_t)s * L;
-    const double* B = b + (size_t)s * L;
+    const T* A = a + (size_t)s * L;
+    const T* B = b + (size_t)s * L;
     double acc = 0.0;
-    for (size_t i = i0 + threadIdx.x; i < i1; i += RED_THREADS) acc += A[i] * B[i];
+    for (size_t i = i0 + threadIdx.x; i < i1; i += RED_THREADS) acc += (double)A[i] * (double)B[i];
     __shared__ double red[RED_THREADS / 32];
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
@@ -56,18 +58,18 @@ __global__ void seg_dot_partial(const double* __restrict__ a, const double* __re
 }
 
 // r = ax - eps[s]*x; partial sums of r^2 (if partial != nullptr)
-__global__ void seg_residual_partial(double* __restrict__ r, const double* __restrict__ ax,
-                                     const double* __restrict__ x, const double* __restrict__ eps, size_t L, int nch,
-                                     double* __restrict__ partial) {
+template <typename T>
+__global__ void seg_residual_partial(T* __restrict__ r, const T* __restrict__ ax, const T* __restrict__ x,
+                                     const double* __restrict__ eps, size_t L, int nch, double* __restrict__ partial) {
     const int s = blockIdx.y, ch = blockIdx.x;
     const size_t i0 = (size_t)ch * RED_CHUNK, i1 = min(L, i0 + RED_CHUNK);
     const size_t off = (size_t)s * L;
     const double e = eps[s];
     double acc = 0.0;
     for (size_t i = i0 + threadIdx.x; i < i1; i += RED_THREADS) {
-        const double v = ax[off + i] - e * x[off + i];
+        const T v = (T)((double)ax[off + i] - e * (double)x[off + i]);
         r[off + i] = v;
-        acc += v * v;
+        acc += (double)v * (double)v;
     }
     if (!partial) return;
     __shared__ double red[RED_THREADS / 32];
@@ -91,12 +93,31 @@ __global__ void seg_finalize(const double* __restrict__ partial, int nseg, int n
 }
 
 // x[s] *= scale[s]  (or a single scalar when scale == nullptr)
-__global__ void seg_scale(double* __restrict__ x, size_t L, const double* __restrict__ scale, double scalar) {
+template <typename T>
+__global__ void seg_scale(T* __restrict__ x, size_t L, const double* __restrict__ scale, double scalar) {
     const int s = blockIdx.y;
     const double c = scale ? scale[s] : scalar;
-    double* X = x + (size_t)s * L;
+    T* X = x + (size_t)s * L;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < L; i += (size_t)gridDim.x * blockDim.x)
-        X[i] *= c;
+        X[i] = (T)((double)X[i] * c);
+}
+
+// out[s] = in[s] * scale[s] (or scalar) with a type change (fp64 <-> fp32 bundles)
+template <typename Ti, typename To>
+__global__ void seg_convert(const Ti* __restrict__ in, To* __restrict__ out, size_t L, const double* __restrict__ scale,
+                            double scalar) {
+    const int s = blockIdx.y;
+    const double c = scale ? scale[s] : scalar;
+    const Ti* I = in + (size_t)s * L;
+    To* O = out + (size_t)s * L;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < L; i += (size_t)gridDim.x * blockDim.x)
+        O[i] = (To)((double)I[i] * c);
+}
+
+// small matrices: out[i] = (float)in[i]
+__global__ void to_f32(const double* __restrict__ in, float* __restrict__ out, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
 }
 
 // Complex block from the 2n x 2n real Gram T (column-major, ld 2na x ...):
@@ -221,6 +242,24 @@ struct qsb_eigensolver {
     // statistics of the last call
     int last_iters = 0;
     int last_rollback = 0;
+    // mixed precision (QSB_PREC_MIXED): fp32 bundles, split-BF16x3 tensor-core
+    // Gram products, fp64 pencil / norms; the fp64 bundles above stay unallocated
+    int mixed = 0;
+    float *X32 = nullptr, *R32 = nullptr, *P32 = nullptr, *AX32 = nullptr, *AR32 = nullptr, *AP32 = nullptr,
+          *TMP32 = nullptr;
+    void* su = nullptr;      // bf16 hi/lo split of the basis [X R P] (active bands)
+    void* sau = nullptr;     // split of [AX AR AP]
+    size_t split_bytes = 0;
+    void* gpart = nullptr;   // split-K partial tiles of the Gram products
+    size_t gpart_bytes = 0;
+    double* T2 = nullptr;    // full-pencil real Gram (up to (2*3n)^2)
+    float* rc32 = nullptr;   // fp32 copies of the rotation coefficients / orthogonalization matrix
+    double* svq = nullptr;   // overlap-basis pencil solve: W, scratch, reduced matrix (m x m each), lambda, d
+    double drop_tol = 0.0;   // overlap eigenvalues below drop_tol * max are dropped
+    int last_dropped = 0;    // most directions dropped in one iteration of the last call
+    double last_min_kept = 1.0;   // smallest kept overlap eigenvalue / max in the last call
+    qsb_apply_f32_fn op32 = nullptr;
+    void* user32 = nullptr;
 };
 
 namespace qsb {
@@ -234,9 +273,29 @@ qsb_status apply_op(qsb_eigensolver* es, int nb, const double* x, double* ax, cu
     return QSB_OK;
 }
 
-// out[s] = scale * sum(a_s * b_s) over nseg segments of L doubles (device out)
-qsb_status seg_dot(qsb_eigensolver* es, int nseg, const double* a, const double* b, double scale, double* out,
-                   cudaStream_t s) {
+qsb_status apply_op32(qsb_eigensolver* es, int nb, const float* x, float* ax, cudaStream_t s) {
+    if (nb <= 0) return QSB_OK;
+    if (es->ham) return qsb_ham_apply(es->ham, QSB_F32, es->cplx, nb, x, ax, es->g[0], es->g[1], es->g[2], s);
+    if (!es->op32)
+        return fail(QSB_ERR_STATE, "eigensolver: mixed precision needs the built-in Hamiltonian or an fp32 operator");
+    const int st = es->op32(es->user32, nb, x, ax, (void*)s);
+    if (st != 0) return fail((qsb_status)(st > 0 && st <= 6 ? st : QSB_ERR_STATE), "eigensolver: operator callback failed");
+    return QSB_OK;
+}
+
+template <typename Ti, typename To>
+qsb_status seg_convert_by(qsb_eigensolver* es, int nseg, const Ti* in, To* out, const double* scale_dev, double scalar,
+                          cudaStream_t s) {
+    if (nseg <= 0) return QSB_OK;
+    const int bx = (int)std::min<size_t>((es->L + 255) / 256, 512);
+    seg_convert<Ti, To><<<dim3(bx, nseg), 256, 0, s>>>(in, out, es->L, scale_dev, scalar);
+    QSB_CUDA_TRY(cudaGetLastError());
+    return QSB_OK;
+}
+
+// out[s] = scale * sum(a_s * b_s) over nseg segments of L values (device out)
+template <typename T>
+qsb_status seg_dot(qsb_eigensolver* es, int nseg, const T* a, const T* b, double scale, double* out, cudaStream_t s) {
     if (nseg <= 0) return QSB_OK;
     const int nch = (int)((es->L + RED_CHUNK - 1) / RED_CHUNK);
     seg_dot_partial<<<dim3(nch, nseg), RED_THREADS, 0, s>>>(a, b, es->L, nch, es->partial);
@@ -245,7 +304,8 @@ qsb_status seg_dot(qsb_eigensolver* es, int nseg, const double* a, const double*
     return QSB_OK;
 }
 
-qsb_status seg_residual(qsb_eigensolver* es, int nseg, double* r, const double* ax, const double* x, const double* eps,
+template <typename T>
+qsb_status seg_residual(qsb_eigensolver* es, int nseg, T* r, const T* ax, const T* x, const double* eps,
                         double* norms, double scale, cudaStream_t s) {
     if (nseg <= 0) return QSB_OK;
     const int nch = (int)((es->L + RED_CHUNK - 1) / RED_CHUNK);
@@ -256,8 +316,8 @@ qsb_status seg_residual(qsb_eigensolver* es, int nseg, double* r, const double* 
     return QSB_OK;
 }
 
-qsb_status seg_scale_by(qsb_eigensolver* es, int nseg, double* x, const double* scale_dev, double scalar,
-                        cudaStream_t s) {
+template <typename T>
+qsb_status seg_scale_by(qsb_eigensolver* es, int nseg, T* x, const double* scale_dev, double scalar, cudaStream_t s) {
     if (nseg <= 0) return QSB_OK;
     const int bx = (int)std::min<size_t>((es->L + 255) / 256, 512);
     seg_scale<<<dim3(bx, nseg), 256, 0, s>>>(x, es->L, scale_dev, scalar);
@@ -277,6 +337,14 @@ qsb_status gemm_tn(qsb_eigensolver* es, int p, int q, const double* U, const dou
 qsb_status gemm_nn(qsb_eigensolver* es, int p, int q, double alpha, const double* U, const double* C, double beta,
                    double* OUT, int ldo) {
     QSB_BLAS_TRY(cublasDgemm(es->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)es->N, q, p, &alpha, U, (int)es->N, C, p, &beta,
+                             OUT, ldo));
+    return QSB_OK;
+}
+
+// OUT (N x q, ldo) = beta*OUT + alpha * U (N x p, ld N) . C (p x q, ld p), fp32
+qsb_status sgemm_nn(qsb_eigensolver* es, int p, int q, float alpha, const float* U, const float* C, float beta,
+                    float* OUT, int ldo) {
+    QSB_BLAS_TRY(cublasSgemm(es->blas, CUBLAS_OP_N, CUBLAS_OP_N, (int)es->N, q, p, &alpha, U, (int)es->N, C, p, &beta,
                              OUT, ldo));
     return QSB_OK;
 }
@@ -372,17 +440,469 @@ qsb_status make_coefficients(qsb_eigensolver* es, int na, int m, int nblk, cudaS
 }  // namespace
 }  // namespace qsb
 
+// ---------------------------------------------------------------------------
+// Mixed precision (QSB_PREC_MIXED): fp32 bundles, split-BF16x3 tensor-core
+// Gram products, fp32 rotations, fp64 pencil / Rayleigh quotients / norms.
+// The steps and their order are those of the fp64 solvers above.
+// ---------------------------------------------------------------------------
+namespace qsb {
+namespace {
+
+// Sb = U^H U, Sa = U^H AU over the whole basis (m bands) in two tensor-core
+// Gram products (upper tiles; the pencil's lower triangle is the mirror, as
+// MakeMatrix_z_blas computes only the upper blocks).  scale: dV for the real solver.
+qsb_status mixed_pencil(qsb_eigensolver* es, const ColumnSet& U, const ColumnSet& AU, int m, double scale,
+                        cudaStream_t s) {
+    const int p = column_count(U);   // real columns: m (real) or 2m (complex)
+    QSB_TRY(split_bf16(QSB_F32, es->N, U, es->su, s));
+    QSB_TRY(split_bf16(QSB_F32, es->N, AU, es->sau, s));
+    const dim3 grid((m + 127) / 128, m);
+    QSB_TRY(gram_split_tc(es->N, es->su, p, es->su, p, true, es->T2, p, 1.0, false, es->gpart, es->gpart_bytes, s));
+    if (es->cplx)
+        assemble_complex_block<<<grid, 128, 0, s>>>(es->T2, m, m, p, (double2*)es->Sb, m, 0, 0, 1);
+    else
+        assemble_real_block<<<grid, 128, 0, s>>>(es->T2, m, m, p, es->Sb, m, 0, 0, 1, scale);
+    QSB_CUDA_TRY(cudaGetLastError());
+    QSB_TRY(gram_split_tc(es->N, es->su, p, es->sau, p, true, es->T2, p, 1.0, false, es->gpart, es->gpart_bytes, s));
+    if (es->cplx)
+        assemble_complex_block<<<grid, 128, 0, s>>>(es->T2, m, m, p, (double2*)es->Sa, m, 0, 0, 1);
+    else
+        assemble_real_block<<<grid, 128, 0, s>>>(es->T2, m, m, p, es->Sa, m, 0, 0, 1, scale);
+    QSB_CUDA_TRY(cudaGetLastError());
+    return QSB_OK;
+}
+
+// ---- overlap-basis pencil solve (mixed precision) --------------------------
+// d_i = 1 / sqrt(B_ii) (0 for a vanishing column)
+__global__ void pencil_diag(const double* __restrict__ B, int m, int cplx, double* __restrict__ d) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const double b = cplx ? B[2 * ((size_t)i + (size_t)m * i)] : B[(size_t)i + (size_t)m * i];
+    d[i] = b > 0.0 ? 1.0 / sqrt(b) : 0.0;
+}
+// A_ij *= d_i d_j, B_ij *= d_i d_j
+__global__ void pencil_scale(double* __restrict__ A, double* __restrict__ B, int m, int cplx,
+                             const double* __restrict__ d) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= m) return;
+    const double f = d[i] * d[j];
+    const size_t e = (size_t)i + (size_t)m * j;
+    if (cplx) {
+        A[2 * e] *= f; A[2 * e + 1] *= f;
+        B[2 * e] *= f; B[2 * e + 1] *= f;
+    } else {
+        A[e] *= f;
+        B[e] *= f;
+    }
+}
+// Wm[:, j] = V[:, c0 + j] / sqrt(lam[c0 + j])  (m x k)
+__global__ void overlap_basis(const double* __restrict__ V, const double* __restrict__ lam, int m, int c0, int k,
+                              int cplx, double* __restrict__ Wm) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= m || j >= k) return;
+    const double f = 1.0 / sqrt(lam[c0 + j]);
+    const size_t src = (size_t)i + (size_t)m * (c0 + j), dst = (size_t)i + (size_t)m * j;
+    if (cplx) {
+        Wm[2 * dst] = V[2 * src] * f;
+        Wm[2 * dst + 1] = V[2 * src + 1] * f;
+    } else {
+        Wm[dst] = V[src] * f;
+    }
+}
+// C_ij = d_i Z_ij  (m x ncol, ld m)
+__global__ void rows_scale(const double* __restrict__ Z, const double* __restrict__ d, int m, int ncol, int cplx,
+                           double* __restrict__ C) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= m || j >= ncol) return;
+    const size_t e = (size_t)i + (size_t)m * j;
+    if (cplx) {
+        C[2 * e] = Z[2 * e] * d[i];
+        C[2 * e + 1] = Z[2 * e + 1] * d[i];
+    } else {
+        C[e] = Z[e] * d[i];
+    }
+}
+
+qsb_status ensure_swork(qsb_eigensolver* es, size_t bytes) {
+    if ((size_t)es->slwork >= bytes) return QSB_OK;
+    if (es->swork) cudaFree(es->swork);
+    es->swork = nullptr;
+    es->slwork = 0;
+    QSB_CUDA_TRY(cudaMalloc(&es->swork, bytes));
+    es->slwork = (int)bytes;
+    return QSB_OK;
+}
+
+// Hermitian / symmetric eigendecomposition in place (ascending eigenvalues in w)
+qsb_status dense_evd(qsb_eigensolver* es, int k, double* A, int lda, double* w, cudaStream_t s) {
+    int lwork = 0;
+    if (es->cplx) {
+        QSB_SOLVER_TRY(cusolverDnZheevd_bufferSize(es->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, k,
+                                                   (cuDoubleComplex*)A, lda, w, &lwork));
+        QSB_TRY(ensure_swork(es, (size_t)lwork * sizeof(cuDoubleComplex)));
+        QSB_SOLVER_TRY(cusolverDnZheevd(es->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, k,
+                                        (cuDoubleComplex*)A, lda, w, (cuDoubleComplex*)es->swork, lwork, es->info));
+    } else {
+        QSB_SOLVER_TRY(cusolverDnDsyevd_bufferSize(es->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, k, A, lda,
+                                                   w, &lwork));
+        QSB_TRY(ensure_swork(es, (size_t)lwork * sizeof(double)));
+        QSB_SOLVER_TRY(cusolverDnDsyevd(es->sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, k, A, lda, w,
+                                        (double*)es->swork, lwork, es->info));
+    }
+    int info = 0;
+    QSB_CUDA_TRY(cudaMemcpyAsync(&info, es->info, sizeof(int), cudaMemcpyDeviceToHost, s));
+    QSB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (info != 0) return fail(QSB_ERR_SOLVER, "eigensolver: dense eigendecomposition failed, info = " + std::to_string(info));
+    return QSB_OK;
+}
+
+// OUT (r x c, ld ldo) = op(X) (r x kk) . Y (kk x c); op = conjugate transpose when herm
+qsb_status small_gemm(qsb_eigensolver* es, bool herm, int r, int c, int kk, const double* X, int ldx, const double* Y,
+                      int ldy, double* OUT, int ldo) {
+    const cublasOperation_t opx = herm ? (es->cplx ? CUBLAS_OP_C : CUBLAS_OP_T) : CUBLAS_OP_N;
+    if (es->cplx) {
+        const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+        QSB_BLAS_TRY(cublasZgemm(es->blas, opx, CUBLAS_OP_N, r, c, kk, &one, (const cuDoubleComplex*)X, ldx,
+                                 (const cuDoubleComplex*)Y, ldy, &zero, (cuDoubleComplex*)OUT, ldo));
+    } else {
+        const double one = 1.0, zero = 0.0;
+        QSB_BLAS_TRY(cublasDgemm(es->blas, opx, CUBLAS_OP_N, r, c, kk, &one, X, ldx, Y, ldy, &zero, OUT, ldo));
+    }
+    return QSB_OK;
+}
+
+// Lowest nout Ritz pairs of the pencil (Sa, Sb) (m x m, full Hermitian) on the
+// well-conditioned part of the basis: scale to a unit diagonal, eigendecompose
+// the overlap, keep the directions with eigenvalue above drop_tol * max, and
+// solve the standard problem there (the overlap-basis "SVQB" form of
+// Stathopoulos & Wu, used in LOBPCG by Hetmaniuk & Lehoucq).  Eigenvalues go to
+// es->W, B-orthonormal eigenvectors to the first nout columns of Sa (ld m),
+// where the cholesky-based solve_pencil leaves them.
+qsb_status solve_pencil_overlap_basis(qsb_eigensolver* es, int m, int nout, cudaStream_t s) {
+    const int c2 = es->cplx ? 2 : 1;
+    const size_t mm = (size_t)m * m * c2;
+    double* Wm = es->svq;
+    double* tmp = Wm + mm;
+    double* Ah = tmp + mm;
+    double* lam = Ah + mm;
+    double* d = lam + m;
+    pencil_diag<<<(m + 127) / 128, 128, 0, s>>>(es->Sb, m, es->cplx, d);
+    pencil_scale<<<dim3((m + 127) / 128, m), 128, 0, s>>>(es->Sa, es->Sb, m, es->cplx, d);
+    QSB_CUDA_TRY(cudaGetLastError());
+    QSB_TRY(dense_evd(es, m, es->Sb, m, lam, s));
+    std::vector<double> hl(m);
+    QSB_CUDA_TRY(cudaMemcpyAsync(hl.data(), lam, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
+    QSB_CUDA_TRY(cudaStreamSynchronize(s));
+    const double lmax = hl[m - 1];
+    if (!(lmax > 0.0) || !std::isfinite(lmax)) return fail(QSB_ERR_NUMERIC, "eigensolver: overlap matrix vanishes");
+    int c0 = 0;
+    while (c0 < m && !(hl[c0] > es->drop_tol * lmax)) ++c0;
+    const int k = m - c0;
+    es->last_dropped = std::max(es->last_dropped, c0);
+    if (c0 < m) es->last_min_kept = std::min(es->last_min_kept, hl[c0] / lmax);
+    if (k < nout)
+        return fail(QSB_ERR_SOLVER, "eigensolver: search basis rank " + std::to_string(k) + " below the " +
+                                        std::to_string(nout) + " bands sought");
+    overlap_basis<<<dim3((m + 127) / 128, k), 128, 0, s>>>(es->Sb, lam, m, c0, k, es->cplx, Wm);
+    QSB_CUDA_TRY(cudaGetLastError());
+    QSB_TRY(small_gemm(es, false, m, k, m, es->Sa, m, Wm, m, tmp, m));   // A Wm
+    QSB_TRY(small_gemm(es, true, k, k, m, Wm, m, tmp, m, Ah, k));        // Wm^H A Wm
+    QSB_TRY(dense_evd(es, k, Ah, k, es->W, s));
+    QSB_TRY(small_gemm(es, false, m, nout, k, Wm, m, Ah, k, tmp, m));    // Wm Y
+    rows_scale<<<dim3((m + 127) / 128, nout), 128, 0, s>>>(tmp, d, m, nout, es->cplx, es->Sa);
+    QSB_CUDA_TRY(cudaGetLastError());
+    return QSB_OK;
+}
+
+// fp32 copies of the first count rotation coefficients
+qsb_status coefficients_f32(qsb_eigensolver* es, size_t count, cudaStream_t s) {
+    to_f32<<<(int)std::min<size_t>((count + 255) / 256, 1024), 256, 0, s>>>(es->rc, es->rc32, count);
+    QSB_CUDA_TRY(cudaGetLastError());
+    return QSB_OK;
+}
+
+qsb_status rotate_real32(qsb_eigensolver* es, int na, float* OUT, const float* U, int cu, float beta) {
+    return sgemm_nn(es, na, na, 1.0f, U, es->rc32 + (size_t)cu * na * na, beta, OUT, (int)es->N);
+}
+
+qsb_status rotate_complex32(qsb_eigensolver* es, int na, float* OUT, const float* U, int cu, float beta) {
+    const size_t blk = (size_t)2 * na * na;
+    const int ldo = (int)(2 * es->N);
+    QSB_TRY(sgemm_nn(es, 2 * na, na, 1.0f, U, es->rc32 + (size_t)(2 * cu) * blk, beta, OUT, ldo));
+    QSB_TRY(sgemm_nn(es, 2 * na, na, 1.0f, U, es->rc32 + (size_t)(2 * cu + 1) * blk, beta, OUT + es->N, ldo));
+    return QSB_OK;
+}
+
+// B_act -= X_fix (X_fix^H B_act) for complex fp32 bundles (VectorOrthogonalization)
+qsb_status orthogonalize32(qsb_eigensolver* es, int nf, int na, const float* Xfix, float* B, cudaStream_t s) {
+    QSB_TRY(split_bf16(QSB_F32, es->N, column_set(Xfix, 2 * nf), es->su, s));
+    QSB_TRY(split_bf16(QSB_F32, es->N, column_set(B, 2 * na), es->sau, s));
+    QSB_TRY(gram_split_tc(es->N, es->su, 2 * nf, es->sau, 2 * na, false, es->T2, 2 * nf, 1.0, false, es->gpart,
+                          es->gpart_bytes, s));
+    pack_orth<<<dim3((nf + 127) / 128, na), 128, 0, s>>>(es->T2, nf, na);
+    QSB_CUDA_TRY(cudaGetLastError());
+    const size_t cnt = (size_t)2 * nf * 2 * na;
+    to_f32<<<(int)std::min<size_t>((cnt + 255) / 256, 1024), 256, 0, s>>>(es->T2, es->rc32, cnt);
+    QSB_CUDA_TRY(cudaGetLastError());
+    return sgemm_nn(es, 2 * nf, 2 * na, -1.0f, Xfix, es->rc32, 1.0f, B, (int)es->N);
+}
+
+qsb_status copy32(float* dst, const float* src, size_t count, cudaStream_t s) {
+    QSB_CUDA_TRY(cudaMemcpyAsync(dst, src, sizeof(float) * count, cudaMemcpyDeviceToDevice, s));
+    return QSB_OK;
+}
+
+// EigenLOBPCG_d_multi (source/lobpcg_d_multi.h:23-545) on fp32 bundles.
+qsb_status lobpcg_d_mixed(qsb_eigensolver* es, double dVol, int n, int iter_max, double* eigen_values, double* X64,
+                          double* keep64, int is_first_time, cudaStream_t s) {
+    const size_t L = es->L;
+    double* eps_d = es->vec;
+    double* nrm_d = es->vec + n;
+    double* scl_d = es->vec + 2 * n;
+    std::vector<double> v(n), scl(n);
+    auto host_vec = [&](const double* d, std::vector<double>& h) -> qsb_status {
+        QSB_CUDA_TRY(cudaMemcpyAsync(h.data(), d, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+        QSB_CUDA_TRY(cudaStreamSynchronize(s));
+        for (int k = 0; k < n; ++k)
+            if (!std::isfinite(h[k])) return fail(QSB_ERR_NUMERIC, "lobpcg_d: non-finite value");
+        return QSB_OK;
+    };
+    // x /= sqrt(|x|^2 dV) per band (Normalize, source/vecmath.h:128-134), fp64 sums
+    auto inv_norms = [&](const float* B, std::vector<double>& out) -> qsb_status {
+        QSB_TRY(seg_dot(es, n, B, B, dVol, nrm_d, s));
+        QSB_TRY(host_vec(nrm_d, v));
+        for (int k = 0; k < n; ++k) out[k] = 1.0 / std::sqrt(v[k]);
+        return QSB_OK;
+    };
+    auto scale_bands = [&](float* B, const std::vector<double>& f) -> qsb_status {
+        QSB_CUDA_TRY(cudaMemcpyAsync(scl_d, f.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        return seg_scale_by(es, n, B, scl_d, 0.0, s);
+    };
+
+    QSB_TRY(seg_convert_by(es, n, X64, es->X32, nullptr, 1.0, s));
+    QSB_TRY(inv_norms(es->X32, scl));
+    QSB_TRY(scale_bands(es->X32, scl));
+    QSB_TRY(apply_op32(es, n, es->X32, es->AX32, s));
+    if (is_first_time) {
+        QSB_CUDA_TRY(cudaMemsetAsync(es->P32, 0, sizeof(float) * L * n, s));
+        QSB_CUDA_TRY(cudaMemsetAsync(es->AP32, 0, sizeof(float) * L * n, s));
+    } else {
+        QSB_TRY(seg_convert_by(es, n, keep64, es->P32, nullptr, 1.0, s));
+        QSB_TRY(apply_op32(es, n, es->P32, es->AP32, s));
+    }
+    QSB_TRY(seg_dot(es, n, es->X32, es->AX32, dVol, eps_d, s));
+    QSB_TRY(seg_residual(es, n, es->R32, es->AX32, es->X32, eps_d, (double*)nullptr, 1.0, s));
+    QSB_TRY(inv_norms(es->R32, scl));
+    QSB_TRY(scale_bands(es->R32, scl));
+    std::vector<double> eps(n), sx(n), sp(n);
+    QSB_TRY(host_vec(eps_d, eps));
+    for (int k = 0; k < n; ++k) eigen_values[k] = eps[k];
+
+    int iter;
+    for (iter = 0; iter < iter_max; ++iter) {
+        QSB_TRY(apply_op32(es, n, es->R32, es->AR32, s));
+        const bool two = is_first_time && iter == 0;
+        const int nblk = two ? 2 : 3;
+        const int m = nblk * n;
+        const ColumnSet U = column_set(es->X32, n, es->R32, n, es->P32, two ? 0 : n);
+        const ColumnSet AU = column_set(es->AX32, n, es->AR32, n, es->AP32, two ? 0 : n);
+        QSB_TRY(mixed_pencil(es, U, AU, m, dVol, s));
+        QSB_TRY(solve_pencil_overlap_basis(es, m, n, s));
+        QSB_TRY(make_coefficients(es, n, m, nblk, s));
+        QSB_TRY(coefficients_f32(es, (size_t)nblk * n * n, s));
+        // P' = R Cr (+ P Cp); X' = X Cx + P'; the same on the A-bundles (:226-365)
+        QSB_TRY(rotate_real32(es, n, es->TMP32, es->R32, 1, 0.0f));
+        if (!two) QSB_TRY(rotate_real32(es, n, es->TMP32, es->P32, 2, 1.0f));
+        std::swap(es->P32, es->TMP32);
+        QSB_TRY(copy32(es->TMP32, es->P32, L * n, s));
+        QSB_TRY(rotate_real32(es, n, es->TMP32, es->X32, 0, 1.0f));
+        std::swap(es->X32, es->TMP32);
+        QSB_TRY(rotate_real32(es, n, es->TMP32, es->AR32, 1, 0.0f));
+        if (!two) QSB_TRY(rotate_real32(es, n, es->TMP32, es->AP32, 2, 1.0f));
+        std::swap(es->AP32, es->TMP32);
+        QSB_TRY(copy32(es->TMP32, es->AP32, L * n, s));
+        QSB_TRY(rotate_real32(es, n, es->TMP32, es->AX32, 0, 1.0f));
+        std::swap(es->AX32, es->TMP32);
+        // renormalize x, p and Ax, Ap (:493-505)
+        QSB_TRY(inv_norms(es->X32, sx));
+        QSB_TRY(inv_norms(es->P32, sp));
+        QSB_TRY(scale_bands(es->X32, sx));
+        QSB_TRY(scale_bands(es->AX32, sx));
+        QSB_TRY(scale_bands(es->P32, sp));
+        QSB_TRY(scale_bands(es->AP32, sp));
+        // eps = <x|Ax> dV; r = Ax - eps x; ||r||^2 dV (:507-513)
+        QSB_TRY(seg_dot(es, n, es->X32, es->AX32, dVol, eps_d, s));
+        QSB_TRY(seg_residual(es, n, es->R32, es->AX32, es->X32, eps_d, nrm_d, dVol, s));
+        QSB_TRY(host_vec(eps_d, eps));
+        QSB_TRY(host_vec(nrm_d, v));
+        double rmax = 0.0;
+        for (int k = 0; k < n; ++k) {
+            eigen_values[k] = eps[k];
+            rmax = std::max(rmax, v[k]);
+        }
+        if (rmax < 1.0e-10 * dVol) { ++iter; break; }   // :525
+    }
+    es->last_iters = iter;
+    QSB_TRY(seg_convert_by(es, n, es->X32, X64, nullptr, 1.0, s));
+    QSB_TRY(seg_convert_by(es, n, es->P32, keep64, nullptr, 1.0, s));
+    QSB_CUDA_TRY(cudaStreamSynchronize(s));
+    return QSB_OK;
+}
+
+// LOBPCG::Eigen_z_multi_mpi (source/lobpcg_z_multi_mpi.h:1732-2852) on fp32
+// bundles.  The fixed (locked) bands of the caller's X are read, never written.
+qsb_status lobpcg_z_mixed(qsb_eigensolver* es, double dVol, int n, int iter_max, double* eigen_values, double* X64,
+                          double* keep64, int* p_num_fix, double residual_threshold, int scf_step, cudaStream_t s) {
+    const size_t L = es->L;
+    auto b32 = [&](float* base, int k) { return base + (size_t)k * L; };
+    auto b64 = [&](double* base, int k) { return base + (size_t)k * L; };
+    double* eps_d = es->vec;
+    double* nrm_d = es->vec + n;
+    double* scl_d = es->vec + 2 * n;
+    std::vector<double> eps(n), nr(n), nx(n), scl(n);
+
+    int num_fix = std::max(0, std::min(*p_num_fix, n));
+    int num_active = n - num_fix;
+    const int head0 = num_fix;
+    // X32 = sqrt(dV) X (:1851), all bands: the fixed ones orthogonalize the active ones
+    QSB_TRY(seg_convert_by(es, n, X64, es->X32, nullptr, std::sqrt(dVol), s));
+    QSB_TRY(apply_op32(es, num_active, b32(es->X32, head0), b32(es->AX32, head0), s));
+    QSB_TRY(seg_dot(es, num_active, b32(es->X32, head0), b32(es->AX32, head0), 1.0, eps_d + head0, s));
+    QSB_TRY(seg_residual(es, num_active, b32(es->R32, head0), b32(es->AX32, head0), b32(es->X32, head0), eps_d + head0,
+                         nrm_d + head0, 1.0, s));
+    QSB_CUDA_TRY(cudaMemcpyAsync(eps.data() + head0, eps_d + head0, sizeof(double) * num_active, cudaMemcpyDeviceToHost, s));
+    QSB_CUDA_TRY(cudaMemcpyAsync(nr.data() + head0, nrm_d + head0, sizeof(double) * num_active, cudaMemcpyDeviceToHost, s));
+    QSB_CUDA_TRY(cudaStreamSynchronize(s));
+    for (int k = head0; k < n; ++k)
+        if (!std::isfinite(eps[k]) || !std::isfinite(nr[k])) return fail(QSB_ERR_NUMERIC, "lobpcg_z: non-finite Rayleigh quotient");
+    // soft locking (:1962-1986)
+    int fix_pos = n;
+    const double th2 = residual_threshold * residual_threshold;
+    for (int k = head0; k < n; ++k)
+        if (th2 < nr[k]) { fix_pos = k; break; }
+    const int org_active = num_active;
+    num_fix = std::min(fix_pos, n / 2);
+    num_active = n - num_fix;
+    if (num_active != org_active) *p_num_fix = num_fix;
+    if (iter_max < 1) return QSB_OK;
+    const int head = num_fix;
+    const int N_ = num_active;
+    const bool is_first_time = (scf_step == 0);
+    float* Xa = b32(es->X32, head);
+    float* Ra = b32(es->R32, head);
+    float* Pa = b32(es->P32, head);
+    float* AXa = b32(es->AX32, head);
+    float* ARa = b32(es->AR32, head);
+    float* APa = b32(es->AP32, head);
+    float* TMP = es->TMP32;
+    if (is_first_time) {
+        QSB_CUDA_TRY(cudaMemsetAsync(es->P32, 0, sizeof(float) * L * n, s));
+        QSB_CUDA_TRY(cudaMemsetAsync(es->AP32, 0, sizeof(float) * L * n, s));
+    } else {
+        QSB_TRY(seg_convert_by(es, N_, b64(keep64, head), Pa, nullptr, 1.0, s));
+        if (num_active != org_active && num_fix > 0) QSB_TRY(orthogonalize32(es, num_fix, N_, es->X32, Pa, s));
+        QSB_TRY(apply_op32(es, N_, Pa, APa, s));
+    }
+    // X64 (active) <- X32 (active) / sqrt(|x'|^2 dV)  (:2792-2803, and the rollback's rescale :2651)
+    auto write_back_x = [&]() -> qsb_status {
+        for (int k = 0; k < N_; ++k) scl[k] = 1.0 / std::sqrt(nx[k] * dVol);
+        QSB_CUDA_TRY(cudaMemcpyAsync(scl_d, scl.data(), sizeof(double) * N_, cudaMemcpyHostToDevice, s));
+        return seg_convert_by(es, N_, Xa, b64(X64, head), scl_d, 0.0, s);
+    };
+    int iter;
+    for (iter = 0; iter < iter_max; ++iter) {
+        if (num_fix > 0) QSB_TRY(orthogonalize32(es, num_fix, N_, es->X32, Ra, s));   // :2080
+        QSB_TRY(apply_op32(es, N_, Ra, ARa, s));                                          // :2084
+        const bool use_p = !(is_first_time && iter == 0);
+        const int nblk = use_p ? 3 : 2;
+        const int m = nblk * N_;
+        const ColumnSet U = column_set(Xa, 2 * N_, Ra, 2 * N_, Pa, use_p ? 2 * N_ : 0);
+        const ColumnSet AU = column_set(AXa, 2 * N_, ARa, 2 * N_, APa, use_p ? 2 * N_ : 0);
+        QSB_TRY(mixed_pencil(es, U, AU, m, 1.0, s));
+        QSB_TRY(solve_pencil_overlap_basis(es, m, N_, s));
+        QSB_TRY(make_coefficients(es, N_, m, nblk, s));
+        QSB_TRY(coefficients_f32(es, (size_t)nblk * 2 * (2 * N_) * N_, s));
+        // P' = R Cr + P Cp; X' = X Cx + P'  (NextVector_z2)
+        QSB_TRY(rotate_complex32(es, N_, TMP, Ra, 1, 0.0f));
+        if (use_p) QSB_TRY(rotate_complex32(es, N_, TMP, Pa, 2, 1.0f));
+        QSB_TRY(copy32(Pa, TMP, L * N_, s));
+        QSB_TRY(rotate_complex32(es, N_, TMP, Xa, 0, 1.0f));
+        QSB_TRY(seg_dot(es, N_, TMP, TMP, 1.0, nrm_d, s));                               // :2570
+        QSB_CUDA_TRY(cudaMemcpyAsync(nx.data(), nrm_d, sizeof(double) * N_, cudaMemcpyDeviceToHost, s));
+        QSB_CUDA_TRY(cudaStreamSynchronize(s));
+        double maxdiff = 0.0;
+        for (int k = 0; k < N_; ++k) {
+            if (!std::isfinite(nx[k])) return fail(QSB_ERR_NUMERIC, "lobpcg_z: non-finite vector norm");
+            maxdiff = std::max(maxdiff, std::fabs(1.0 - nx[k]));
+        }
+        if (maxdiff > 1.0e-3) {   // rollback (:2611-2666): keep X, P <- R
+            es->last_rollback = 1;
+            QSB_TRY(copy32(Pa, Ra, L * N_, s));
+            QSB_TRY(write_back_x());
+            ++iter;
+            break;
+        }
+        QSB_TRY(copy32(Xa, TMP, L * N_, s));
+        // AP' = AR Cr + AP Cp; AX' = AX Cx + AP' (:2718), on the last iteration too:
+        // the eigenvalues are the Rayleigh quotients <x'|Ax'> / <x'|x'> summed in
+        // fp64, not the pencil's Ritz values.  Split-BF16x3 leaves out lo*lo,
+        // which on the overlap diagonal is sum(lo^2) > 0, so the pencil's values
+        // sit ~2^-16/3 (relative) high; the vectors themselves are unaffected.
+        QSB_TRY(rotate_complex32(es, N_, TMP, ARa, 1, 0.0f));
+        if (use_p) QSB_TRY(rotate_complex32(es, N_, TMP, APa, 2, 1.0f));
+        QSB_TRY(copy32(APa, TMP, L * N_, s));
+        QSB_TRY(rotate_complex32(es, N_, TMP, AXa, 0, 1.0f));
+        QSB_TRY(copy32(AXa, TMP, L * N_, s));
+        QSB_TRY(seg_dot(es, N_, Xa, AXa, 1.0, eps_d, s));
+        std::vector<double> w(N_);
+        QSB_CUDA_TRY(cudaMemcpyAsync(w.data(), eps_d, sizeof(double) * N_, cudaMemcpyDeviceToHost, s));
+        QSB_CUDA_TRY(cudaStreamSynchronize(s));
+        for (int k = 0; k < N_; ++k) {
+            w[k] /= nx[k];
+            if (!std::isfinite(w[k])) return fail(QSB_ERR_NUMERIC, "lobpcg_z: non-finite Rayleigh quotient");
+            eps[head + k] = w[k];
+        }
+        if (iter + 1 < iter_max) {
+            QSB_CUDA_TRY(cudaMemcpyAsync(eps_d, w.data(), sizeof(double) * N_, cudaMemcpyHostToDevice, s));
+            QSB_TRY(seg_residual(es, N_, Ra, AXa, Xa, eps_d, (double*)nullptr, 1.0, s));   // :2750
+        } else {
+            QSB_TRY(write_back_x());
+        }
+    }
+    es->last_iters = iter;
+    for (int k = head; k < n; ++k) eigen_values[k] = eps[k];
+    QSB_TRY(seg_convert_by(es, N_, Pa, b64(keep64, head), nullptr, 1.0, s));
+    QSB_CUDA_TRY(cudaStreamSynchronize(s));
+    return QSB_OK;
+}
+
+}  // namespace
+}  // namespace qsb
+
 extern "C" {
 
 qsb_status qsb_eigensolver_create(qsb_eigensolver** out, int64_t N, int n, int is_complex) {
+    return qsb_eigensolver_create_ex(out, N, n, is_complex, QSB_PREC_FP64);
+}
+
+qsb_status qsb_eigensolver_create_ex(qsb_eigensolver** out, int64_t N, int n, int is_complex, qsb_precision precision) {
     if (!out) return fail(QSB_ERR_INVALID, "eigensolver_create: null handle pointer");
     *out = nullptr;
     if (N < 1 || n < 1) return fail(QSB_ERR_INVALID, "eigensolver_create: N and n must be >= 1");
+    if (precision != QSB_PREC_FP64 && precision != QSB_PREC_MIXED)
+        return fail(QSB_ERR_INVALID, "eigensolver_create: unknown precision");
+    const int c2 = is_complex ? 2 : 1;
+    if (precision == QSB_PREC_MIXED && 3 * n * c2 > 65535)
+        return fail(QSB_ERR_INVALID, "eigensolver_create: too many bands for the mixed-precision Gram");
     qsb_eigensolver* es = new qsb_eigensolver();
     es->N = N;
     es->nmax = n;
     es->cplx = is_complex ? 1 : 0;
-    es->L = (size_t)N * (is_complex ? 2 : 1);
+    es->mixed = precision == QSB_PREC_MIXED ? 1 : 0;
+    es->L = (size_t)N * c2;
     auto cleanup = [&](qsb_status st) {
         qsb_eigensolver_destroy(es);
         return st;
@@ -390,10 +910,32 @@ qsb_status qsb_eigensolver_create(qsb_eigensolver** out, int64_t N, int n, int i
     if (cublasCreate(&es->blas) != CUBLAS_STATUS_SUCCESS) return cleanup(fail(QSB_ERR_CUDA, "cublasCreate failed"));
     if (cusolverDnCreate(&es->sol) != CUSOLVER_STATUS_SUCCESS)
         return cleanup(fail(QSB_ERR_CUDA, "cusolverDnCreate failed"));
-    const size_t big = es->L * n * sizeof(double);
-    double** bigs[5] = {&es->R, &es->AX, &es->AR, &es->AP, &es->TMP};
-    for (double** p : bigs)
-        if (cudaMalloc((void**)p, big) != cudaSuccess) return cleanup(fail(QSB_ERR_NOMEM, "eigensolver: bundle allocation"));
+    if (!es->mixed) {
+        const size_t big = es->L * n * sizeof(double);
+        double** bigs[5] = {&es->R, &es->AX, &es->AR, &es->AP, &es->TMP};
+        for (double** p : bigs)
+            if (cudaMalloc((void**)p, big) != cudaSuccess)
+                return cleanup(fail(QSB_ERR_NOMEM, "eigensolver: bundle allocation"));
+    } else {
+        const size_t big = es->L * n * sizeof(float);
+        float** bigs[7] = {&es->X32, &es->R32, &es->P32, &es->AX32, &es->AR32, &es->AP32, &es->TMP32};
+        for (float** p : bigs)
+            if (cudaMalloc((void**)p, big) != cudaSuccess)
+                return cleanup(fail(QSB_ERR_NOMEM, "eigensolver: fp32 bundle allocation"));
+        // split-BF16x3 Gram entries carry random errors ~ 2^-17 / sqrt(N) of the
+        // (unit) diagonal: overlap directions weaker than about that are noise
+        es->drop_tol = std::min(1e-5, std::max(1e-8, 1e-5 / std::sqrt((double)N)));
+        const int pmax = 3 * n * c2;
+        es->split_bytes = split_bf16_bytes(N, pmax);
+        es->gpart_bytes = std::max(gram_partial_bytes_bound(pmax, pmax, true), gram_partial_bytes_bound(n, 2 * n, false));
+        if (cudaMalloc(&es->su, es->split_bytes) != cudaSuccess || cudaMalloc(&es->sau, es->split_bytes) != cudaSuccess ||
+            cudaMalloc(&es->gpart, es->gpart_bytes) != cudaSuccess ||
+            cudaMalloc((void**)&es->T2, sizeof(double) * (size_t)pmax * pmax) != cudaSuccess ||
+            cudaMalloc((void**)&es->rc32, sizeof(float) * (size_t)6 * 2 * n * n) != cudaSuccess ||
+            cudaMalloc((void**)&es->svq, sizeof(double) * ((size_t)3 * (3 * n) * (3 * n) * c2 + 2 * (3 * n))) !=
+                cudaSuccess)
+            return cleanup(fail(QSB_ERR_NOMEM, "eigensolver: mixed-precision workspace allocation"));
+    }
     const int m = 3 * n;
     const size_t cm = (size_t)m * m * (is_complex ? 2 : 1);
     const size_t tsz = (size_t)(2 * n) * (2 * n);
@@ -420,6 +962,12 @@ qsb_status qsb_eigensolver_destroy(qsb_eigensolver* es) {
     double* bigs[5] = {es->R, es->AX, es->AR, es->AP, es->TMP};
     for (double* p : bigs)
         if (p) cudaFree(p);
+    float* b32[7] = {es->X32, es->R32, es->P32, es->AX32, es->AR32, es->AP32, es->TMP32};
+    for (float* p : b32)
+        if (p) cudaFree(p);
+    void* mw[6] = {es->su, es->sau, es->gpart, es->T2, es->rc32, es->svq};
+    for (void* p : mw)
+        if (p) cudaFree(p);
     if (es->T) cudaFree(es->T);
     if (es->swork) cudaFree(es->swork);
     if (es->info) cudaFree(es->info);
@@ -435,6 +983,8 @@ qsb_status qsb_eigensolver_set_hamiltonian(qsb_eigensolver* es, qsb_ham* ham, do
     es->ham = ham;
     es->op = nullptr;
     es->user = nullptr;
+    es->op32 = nullptr;
+    es->user32 = nullptr;
     es->g[0] = gx; es->g[1] = gy; es->g[2] = gz;
     return QSB_OK;
 }
@@ -444,6 +994,35 @@ qsb_status qsb_eigensolver_set_operator(qsb_eigensolver* es, qsb_apply_fn op, vo
     es->ham = nullptr;
     es->op = op;
     es->user = user;
+    es->op32 = nullptr;
+    es->user32 = nullptr;
+    return QSB_OK;
+}
+
+qsb_status qsb_eigensolver_set_operator_f32(qsb_eigensolver* es, qsb_apply_f32_fn op, void* user) {
+    if (!es || !op) return fail(QSB_ERR_INVALID, "set_operator_f32: null argument");
+    es->ham = nullptr;
+    es->op = nullptr;
+    es->user = nullptr;
+    es->op32 = op;
+    es->user32 = user;
+    return QSB_OK;
+}
+
+qsb_status qsb_eigensolver_set_drop_tolerance(qsb_eigensolver* es, double tol) {
+    if (!es) return fail(QSB_ERR_INVALID, "set_drop_tolerance: null solver");
+    if (!es->mixed) return fail(QSB_ERR_STATE, "set_drop_tolerance: only mixed-precision contexts drop directions");
+    if (!(tol > 0.0 && tol < 1.0)) return fail(QSB_ERR_INVALID, "set_drop_tolerance: needs 0 < tol < 1");
+    es->drop_tol = tol;
+    return QSB_OK;
+}
+
+qsb_status qsb_eigensolver_overlap_stats(const qsb_eigensolver* es, int* max_dropped, double* min_kept_ratio,
+                                         double* drop_tolerance) {
+    if (!es) return fail(QSB_ERR_INVALID, "overlap_stats: null solver");
+    if (max_dropped) *max_dropped = es->last_dropped;
+    if (min_kept_ratio) *min_kept_ratio = es->last_min_kept;
+    if (drop_tolerance) *drop_tolerance = es->drop_tol;
     return QSB_OK;
 }
 
@@ -460,7 +1039,9 @@ qsb_status qsb_eigensolver_last_stats(const qsb_eigensolver* es, int* iterations
 qsb_status qsb_lobpcg_z(qsb_eigensolver* es, double dVol, int n, int iter_max, double* eigen_values, double* X,
                         double* keep, int* p_num_fix, double residual_threshold, int scf_step, void* stream) {
     if (!es || !es->cplx) return fail(QSB_ERR_INVALID, "lobpcg_z: needs a complex eigensolver context");
-    if (!es->ham && !es->op) return fail(QSB_ERR_STATE, "lobpcg_z: no operator set");
+    if (!es->ham && !(es->mixed ? (void*)es->op32 : (void*)es->op))
+        return fail(QSB_ERR_STATE, es->mixed ? "lobpcg_z: no fp32 operator or Hamiltonian set (mixed precision)"
+                                             : "lobpcg_z: no operator or Hamiltonian set");
     if (n < 1 || n > es->nmax || !X || !keep || !eigen_values || !p_num_fix || !(dVol > 0))
         return fail(QSB_ERR_INVALID, "lobpcg_z: bad arguments");
     cudaStream_t s = (cudaStream_t)stream;
@@ -468,6 +1049,10 @@ qsb_status qsb_lobpcg_z(qsb_eigensolver* es, double dVol, int n, int iter_max, d
     QSB_SOLVER_TRY(cusolverDnSetStream(es->sol, s));
     es->last_iters = 0;
     es->last_rollback = 0;
+    es->last_dropped = 0;
+    es->last_min_kept = 1.0;
+    if (es->mixed)
+        return lobpcg_z_mixed(es, dVol, n, iter_max, eigen_values, X, keep, p_num_fix, residual_threshold, scf_step, s);
     const size_t L = es->L;
     auto band = [&](double* base, int b) { return base + (size_t)b * L; };
     double* eps_d = es->vec;             // n
@@ -614,7 +1199,9 @@ qsb_status qsb_lobpcg_z(qsb_eigensolver* es, double dVol, int n, int iter_max, d
 qsb_status qsb_lobpcg_d(qsb_eigensolver* es, double dVol, int n, int iter_max, double* eigen_values, double* X,
                         double* keep, int is_first_time, void* stream) {
     if (!es || es->cplx) return fail(QSB_ERR_INVALID, "lobpcg_d: needs a real eigensolver context");
-    if (!es->ham && !es->op) return fail(QSB_ERR_STATE, "lobpcg_d: no operator set");
+    if (!es->ham && !(es->mixed ? (void*)es->op32 : (void*)es->op))
+        return fail(QSB_ERR_STATE, es->mixed ? "lobpcg_d: no fp32 operator or Hamiltonian set (mixed precision)"
+                                             : "lobpcg_d: no operator or Hamiltonian set");
     if (n < 1 || n > es->nmax || !X || !keep || !eigen_values || !(dVol > 0))
         return fail(QSB_ERR_INVALID, "lobpcg_d: bad arguments");
     cudaStream_t s = (cudaStream_t)stream;
@@ -622,6 +1209,9 @@ qsb_status qsb_lobpcg_d(qsb_eigensolver* es, double dVol, int n, int iter_max, d
     QSB_SOLVER_TRY(cusolverDnSetStream(es->sol, s));
     es->last_iters = 0;
     es->last_rollback = 0;
+    es->last_dropped = 0;
+    es->last_min_kept = 1.0;
+    if (es->mixed) return lobpcg_d_mixed(es, dVol, n, iter_max, eigen_values, X, keep, is_first_time, s);
     const size_t L = es->L;
     double* eps_d = es->vec;
     double* nrm_d = es->vec + n;

@@ -107,11 +107,50 @@ qsb_status nl_project(qsb_dtype dt, const NLDevice& d, int nx, int ny, int nz, i
 qsb_status nl_apply(qsb_dtype dt, const NLDevice& d, int N, int nb, int is_complex, void* hpsi,
                     const double* coef, double gx_dx, double gy_dy, double gz_dz, cudaStream_t s);
 
-// Split-BF16x3 tensor-core Gram product (gram_tc.cu): T (p x q, FP64, ld ldt)
-// = alpha * U^T V (+ T), U: N x p, V: N x q, column-major ld N, fp32 or fp64.
+// Split-BF16x3 tensor-core Gram products (gram_tc.cu).
+//
+// A tall operand is a set of columns of N grid values (fp32 or fp64, one
+// column every N elements) gathered from up to kMaxSegments separate arrays.
+constexpr int kMaxSegments = 4;
+struct ColumnSet {
+    const void* base[kMaxSegments];
+    int cols[kMaxSegments];
+    int nseg;
+};
+inline ColumnSet column_set(const void* a, int na, const void* b = nullptr, int nb = 0, const void* c = nullptr,
+                            int nc = 0) {
+    ColumnSet s{};
+    const void* bs[3] = {a, b, c};
+    const int ns[3] = {na, nb, nc};
+    for (int k = 0; k < 3; ++k)
+        if (ns[k] > 0) {
+            s.base[s.nseg] = bs[k];
+            s.cols[s.nseg++] = ns[k];
+        }
+    return s;
+}
+inline int column_count(const ColumnSet& s) {
+    int t = 0;
+    for (int k = 0; k < s.nseg; ++k) t += s.cols[k];
+    return t;
+}
+// Bytes of the bf16 hi/lo copy of a cols-column operand.
+size_t split_bf16_bytes(int64_t N, int cols);
+// dst (split_bf16_bytes) <- hi/lo bf16 copy of the gathered columns
+qsb_status split_bf16(qsb_dtype dt, int64_t N, const ColumnSet& src, void* dst, cudaStream_t s);
+// Bytes of the split-K partial tiles of one gram_split_tc call.
+size_t gram_partial_bytes(int64_t N, int p, int q, bool upper);
+// Partial bytes enough for every call with p' <= p, q' <= q (any N).
+size_t gram_partial_bytes_bound(int p, int q, bool upper);
+// T (p x q, FP64, ld ldt) = alpha * A^T B (+ T when accumulate) from split
+// operands A (p columns) and B (q columns); upper: only entries in output tiles
+// on or above the diagonal (128 x 128 tiles) are written.
+qsb_status gram_split_tc(int64_t N, const void* A, int p, const void* B, int q, bool upper, double* T, int ldt,
+                         double alpha, bool accumulate, void* partial, size_t partial_bytes, cudaStream_t s);
+// One-call form on plain operands U (N x p), V (N x q), ld N.
 size_t gram_bf16x3_workspace(int64_t N, int p, int q, bool same);
 qsb_status gram_bf16x3(qsb_dtype dt, int64_t N, int p, int q, const void* U, const void* V, double* T, int ldt,
-                       double alpha, bool accumulate, void* ws, size_t ws_bytes, cudaStream_t s);
+                       double alpha, bool accumulate, bool upper, void* ws, size_t ws_bytes, cudaStream_t s);
 
 }  // namespace qsb
 

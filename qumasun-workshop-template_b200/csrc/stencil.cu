@@ -52,9 +52,14 @@ constexpr int BY = 8;         // warps per CTA, stacked in y
 constexpr int NT = TX * BY;   // threads per CTA
 constexpr int HW = 4;         // halo width of the 8th-order stencil
 
+// Coefficients in the kernel's type.  In fp32 the centre weight is a pair
+// c0 + c0lo equal (to ~2^-48) to -2 * (sum of the ROUNDED fp32 neighbour
+// weights) - coef |g|^2, so the fp32 stencil still annihilates constants:
+// rounding c0 on its own would shift every eigenvalue of the fp32 operator by
+// ~|c0| 2^-24 (~1e-6 Ha at h = 0.5 bohr).  In fp64 c0lo is zero and unused.
 template <typename T>
 struct KC {
-    T c0;
+    T c0, c0lo;
     T cx[4], cy[4], cz[4];
     T ax[4], ay[4], az[4];
 };
@@ -62,10 +67,21 @@ struct KC {
 template <typename T>
 KC<T> to_kc(const FD8Coef& c) {
     KC<T> k;
-    k.c0 = (T)c.c0;
+    double sum_exact = 0.0, sum_rounded = 0.0;
     for (int m = 0; m < 4; ++m) {
         k.cx[m] = (T)c.cx[m]; k.cy[m] = (T)c.cy[m]; k.cz[m] = (T)c.cz[m];
         k.ax[m] = (T)c.ax[m]; k.ay[m] = (T)c.ay[m]; k.az[m] = (T)c.az[m];
+        sum_exact += c.cx[m] + c.cy[m] + c.cz[m];
+        sum_rounded += (double)k.cx[m] + (double)k.cy[m] + (double)k.cz[m];
+    }
+    if (sizeof(T) == sizeof(double)) {
+        k.c0 = (T)c.c0;
+        k.c0lo = T(0);
+    } else {
+        // c.c0 = -2 * sum_exact - coef |g|^2 (14350 = 2 * (8064 - 1008 + 128 - 9))
+        const double target = (c.c0 + 2.0 * sum_exact) - 2.0 * sum_rounded;
+        k.c0 = (T)target;
+        k.c0lo = (T)(target - (double)k.c0);
     }
     return k;
 }
@@ -251,6 +267,7 @@ fd8_kernel(const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ 
                              k.cy[1] * (col[i + 6] + col[i + 2]) + k.cy[0] * (col[i + 5] + col[i + 3]);
                         d += k.cz[3] * (QZ(8) + QZ(0)) + k.cz[2] * (QZ(7) + QZ(1)) + k.cz[1] * (QZ(6) + QZ(2)) +
                              k.cz[0] * (QZ(5) + QZ(3));
+                        if constexpr (sizeof(T) == 4) d = fmaf(k.c0lo, QZ(4), d);
                         res[c][i] = d;
                         if (GRAD) {
                             T g = k.ax[3] * (xp4 - xm4) + k.ax[2] * (xp3 - xm3) + k.ax[1] * (xp2 - xm2) +
@@ -573,6 +590,7 @@ fd8_tma_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ out, co
                         const T szz = (k.cz[3] * (QZ(8) + QZ(0)) + k.cz[2] * (QZ(7) + QZ(1))) +
                                       (k.cz[1] * (QZ(6) + QZ(2)) + k.cz[0] * (QZ(5) + QZ(3)));
                         res[c][i] = k.c0 * QZ(4) + ((sxx + syy) + szz);
+                        if constexpr (sizeof(T) == 4) res[c][i] = fmaf(k.c0lo, QZ(4), res[c][i]);
                         if (GRAD) {
                             const T gx_ = (k.ax[3] * (xp4 - xm4) + k.ax[2] * (xp3 - xm3)) +
                                           (k.ax[1] * (xp2 - xm2) + k.ax[0] * (xp1 - xm1));

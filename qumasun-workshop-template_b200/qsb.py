@@ -226,11 +226,16 @@ class EigenSolver:
     """Device block LOBPCG (qsb_lobpcg_z ~ LOBPCG::Eigen_z_multi_mpi, qsb_lobpcg_d ~
     EigenLOBPCG_d_multi) for bundles of up to n bands of N points."""
 
-    def __init__(self, N, n, is_complex):
+    PRECISIONS = {"fp64": 0, "mixed": 1}
+
+    def __init__(self, N, n, is_complex, precision="fp64"):
+        """precision "fp64" (the reference's arithmetic) or "mixed" (fp32 bundles
+        and operator, split-BF16x3 tensor-core Gram products, fp64 pencil)."""
         h = ctypes.c_void_p()
-        _check(lib.qsb_eigensolver_create(ctypes.byref(h), ctypes.c_int64(N), n, int(bool(is_complex))))
+        _check(lib.qsb_eigensolver_create_ex(ctypes.byref(h), ctypes.c_int64(N), n, int(bool(is_complex)),
+                                             self.PRECISIONS[precision]))
         self._h = h
-        self.N, self.n, self.is_complex = N, n, bool(is_complex)
+        self.N, self.n, self.is_complex, self.precision = N, n, bool(is_complex), precision
         self._cb = None
 
     def close(self):
@@ -257,6 +262,26 @@ class EigenSolver:
                 return 4
         self._cb = APPLY_FN(tramp)
         _check(lib.qsb_eigensolver_set_operator(self._h, self._cb, None))
+
+    def set_operator_f32(self, fn):
+        """Mixed precision: fn(nb, x_ptr, ax_ptr, stream_ptr) -> int on fp32 bundles."""
+        def tramp(user, nb, x, ax, stream):
+            try:
+                return int(fn(nb, x, ax, stream))
+            except Exception:
+                return 4
+        self._cb = APPLY_FN(tramp)
+        _check(lib.qsb_eigensolver_set_operator_f32(self._h, self._cb, None))
+
+    def set_drop_tolerance(self, tol):
+        _check(lib.qsb_eigensolver_set_drop_tolerance(self._h, _c_d(tol)))
+
+    def overlap_stats(self):
+        """(most directions dropped in one iteration, smallest kept overlap
+        eigenvalue / largest, drop tolerance) of the last call (mixed precision)."""
+        d, r, t = ctypes.c_int(), ctypes.c_double(), ctypes.c_double()
+        _check(lib.qsb_eigensolver_overlap_stats(self._h, ctypes.byref(d), ctypes.byref(r), ctypes.byref(t)))
+        return d.value, r.value, t.value
 
     def last_stats(self):
         it, rb = ctypes.c_int(), ctypes.c_int()

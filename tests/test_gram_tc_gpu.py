@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 TOL = 2e-5
 
 
-def _gram(qsb, U, V, p, q):
+def _gram(qsb, U, V, p, q, upper=0):
     import torch
     N = U.shape[-1]
     same = int(U.data_ptr() == V.data_ptr())
@@ -22,7 +22,7 @@ def _gram(qsb, U, V, p, q):
     T = torch.full((q, p), float("nan"), dtype=torch.float64, device="cuda")   # column-major p x q
     dt = 0 if U.dtype == torch.float64 else 1
     st = qsb.lib.qsb_gram_bf16x3(dt, ctypes.c_int64(N), p, q, ctypes.c_void_p(U.data_ptr()),
-                                 ctypes.c_void_p(V.data_ptr()), ctypes.c_void_p(T.data_ptr()), p,
+                                 ctypes.c_void_p(V.data_ptr()), ctypes.c_void_p(T.data_ptr()), p, upper,
                                  ctypes.c_void_p(ws.data_ptr()), ctypes.c_size_t(nbytes.value),
                                  ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
     assert st == 0, qsb.lib.qsb_last_error()
@@ -46,4 +46,22 @@ def test_gram_bf16x3_matches_fp64(qsb, N, p, q, same, dtype):
     ref = U.double() @ V.double().t()
     err = (T - ref).abs().max().item() / ref.abs().max().item()
     assert err < TOL, err
+    assert qsb.device_status() == 0
+
+
+def test_gram_bf16x3_upper_tiles(qsb):
+    """upper = 1: every entry m <= n is the product; tiles strictly below the
+    diagonal stay untouched (NaN here)."""
+    import torch
+    N, p = 60000, 300
+    g = torch.Generator(device="cuda").manual_seed(8)
+    U = (torch.rand(p, N, generator=g, device="cuda", dtype=torch.float64) - 0.5).float()
+    T = _gram(qsb, U, U, p, p, upper=1)
+    ref = U.double() @ U.double().t()
+    iu = torch.triu_indices(p, p, device="cuda")
+    err = (T[iu[0], iu[1]] - ref[iu[0], iu[1]]).abs().max().item() / ref.abs().max().item()
+    assert err < TOL, err
+    m = torch.arange(p, device="cuda")
+    below = (m[:, None] // 128) > (m[None, :] // 128)
+    assert torch.isnan(T[below]).all()
     assert qsb.device_status() == 0
