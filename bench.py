@@ -236,6 +236,79 @@ def cpu_baseline_sample():
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
+NB_OCC = 48          # 16 atoms x 6 valence electrons / 2 (spin-paired)
+EIG_TOL = 1e-6       # Ha, every occupied eigenvalue against the FP64 converged values
+
+
+def lobpcg_section(H, psi, N, NB, dV, n_occ, stream, max_calls=60):
+    """EigenLOBPCG_d_multi-style solves (4 iterations per call, the way an SCF
+    step calls it) from one dV-orthonormal start, FP64 drop-in and mixed
+    precision: ms per steady iteration, and device time until every occupied
+    eigenvalue is within EIG_TOL of the FP64 solver's converged values."""
+    import torch
+    import qsb
+    X0 = torch.linalg.qr(psi.t())[0].t().contiguous() / math.sqrt(dV)
+    out = {"bands": NB, "occupied": n_occ, "iterations_per_call": 4, "tolerance_ha": EIG_TOL}
+    traces = {}
+    for prec in ("fp64", "mixed"):
+        es = qsb.EigenSolver(N, NB, False, prec)
+        es.set_hamiltonian(H)
+        X = X0.clone()
+        keep = torch.zeros_like(X)
+        ev = np.zeros(NB)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        # steady-state iteration time: a first-time call and a steady call (they
+        # size the dense-solver workspaces), then 3 iterations timed
+        es.lobpcg_d(dV, NB, 1, ev, X, keep, True)
+        es.lobpcg_d(dV, NB, 1, ev, X, keep, False)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        es.lobpcg_d(dV, NB, 3, ev, X, keep, False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        it, _ = es.last_stats()
+        ms_it = e0.elapsed_time(e1) / max(it, 1)
+        # convergence run from the same start, every call timed on the device
+        X.copy_(X0)
+        keep.zero_()
+        times, evs = [], []
+        limit = max_calls if prec == "fp64" else 2 * max_calls
+        for c in range(limit):
+            e0.record(stream)
+            es.lobpcg_d(dV, NB, 4, ev, X, keep, c == 0)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+            evs.append(ev.copy())
+            if prec == "fp64" and c > 2 and np.abs(evs[-1][:n_occ] - evs[-2][:n_occ]).max() < 1e-10:
+                break
+            if prec == "mixed" and "fp64" in traces:
+                if np.abs(evs[-1][:n_occ] - traces["fp64"][1][-1][:n_occ]).max() < EIG_TOL:
+                    break
+        traces[prec] = (np.array(times), np.array(evs))
+        out[prec] = {"ms_per_iteration": ms_it}
+        if prec == "mixed":
+            out[prec]["overlap_dropped_max"], out[prec]["overlap_min_kept"], out[prec]["drop_tolerance"] = \
+                es.overlap_stats()
+        es.close()
+        del X, keep
+        torch.cuda.empty_cache()
+    ref = traces["fp64"][1][-1][:n_occ]
+    for prec in ("fp64", "mixed"):
+        times, evs = traces[prec]
+        err = np.abs(evs[:, :n_occ] - ref[None, :]).max(axis=1)
+        hit = np.nonzero(err < EIG_TOL)[0]
+        o = out[prec]
+        o["calls_to_tolerance"] = int(hit[0]) + 1 if len(hit) else None
+        o["seconds_to_tolerance"] = float(times[:hit[0] + 1].sum() * 1e-3) if len(hit) else None
+        o["final_max_error_ha"] = float(err[-1])
+    if out["fp64"]["seconds_to_tolerance"] and out["mixed"]["seconds_to_tolerance"]:
+        out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds_to_tolerance"] / out["mixed"]["seconds_to_tolerance"]
+    out["note"] = ("eigensolver part of the SCF metric on a fixed H (the SCF driver: density, Poisson, XC, "
+                   "mixing, is not built); reference eigenvalues = FP64 solver converged to 1e-10 Ha change")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -330,28 +403,10 @@ def main():
     barrier()
     e2e_ms = f0.elapsed_time(f1) / e2e_steps
 
-    # ---- one real block-LOBPCG iteration on the same H and bands (context) -----
+    # ---- block LOBPCG on the same H: FP64 drop-in vs mixed precision ----------
     lob = None
     if not args.no_lobpcg:
-        es = qsb.EigenSolver(N, NB, False)
-        es.set_hamiltonian(H)
-        X = psi.clone()
-        keep = torch.zeros_like(X)
-        ev = np.zeros(NB)
-        dV = H_GRID ** 3
-        es.lobpcg_d(dV, NB, 1, ev, X, keep, True)       # warm: first-time 2n pencil
-        torch.cuda.synchronize()
-        l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        l0.record(stream)
-        es.lobpcg_d(dV, NB, 3, ev, X, keep, False)      # 3 steady iterations (3n pencil)
-        l1.record(stream)
-        torch.cuda.synchronize()
-        it, _ = es.last_stats()
-        lob = {"ms_per_iteration": l0.elapsed_time(l1) / max(it, 1), "iterations": it, "bands": NB,
-               "note": "EigenLOBPCG_d_multi semantics: 1 H.psi of the residuals, 12 Gram DGEMMs (3n pencil), "
-                       "device dsygvd, 8 rotation DGEMMs per iteration, plus the per-call initial H.psi"}
-        es.close()
-        del X, keep
+        lob = lobpcg_section(H, psi, N, NB, H_GRID ** 3, n_occ=NB_OCC, stream=stream)
     clk = clocks.stop()
 
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist, "cuda")

@@ -226,6 +226,18 @@ QSB_API qsb_status qsb_eigensolver_last_stats(const qsb_eigensolver* es, int* it
  * (~2^-17 / sqrt(N) of the diagonal) make fail once the basis [X R P] turns
  * ill-conditioned near convergence.  Default: 1e-5 / sqrt(N) within [1e-8, 1e-5]. */
 QSB_API qsb_status qsb_eigensolver_set_drop_tolerance(qsb_eigensolver* es, double tol);
+/* QSB_PREC_MIXED: how the Gram / Rayleigh-Ritz products are formed.
+ *   QSB_GRAM_BF16X3     split-BF16x3 on the tensor cores (qsb_gram_bf16x3)
+ *   QSB_GRAM_BF16X4     the same plus lo.lo (qsb_gram_bf16x4)
+ *   QSB_GRAM_INT8_OZAKI three int8 slices, exact INT32 accumulation
+ *                       (qsb_gram_ozaki_int8); the default.
+ * The BF16 forms accumulate in the tensor core's FP32, which rounds toward
+ * zero: a same-sign sum loses ~4e-8 of itself per MMA in one accumulator chain,
+ * measured -4.8e-5 relative on overlap diagonals at 8192 grid points per CTA.
+ * That bias shifts all overlap eigenvalues; at 96^3 grids with 128 bands the
+ * BF16 solvers diverge, the INT8 one converges. */
+typedef enum qsb_gram_kind { QSB_GRAM_BF16X3 = 3, QSB_GRAM_BF16X4 = 4, QSB_GRAM_INT8_OZAKI = 8 } qsb_gram_kind;
+QSB_API qsb_status qsb_eigensolver_set_gram_kind(qsb_eigensolver* es, qsb_gram_kind kind);
 /* Of the last call (mixed precision): most directions dropped in one
  * iteration, smallest kept overlap eigenvalue relative to the largest, and the
  * tolerance in force. */
@@ -271,6 +283,27 @@ QSB_API qsb_status qsb_gram_bf16x3_workspace(int64_t N, int p, int q, int same, 
 QSB_API qsb_status qsb_gram_bf16x3(qsb_dtype dtype, int64_t N, int p, int q, const void* U, const void* V,
                                    double* T, int ldt, int upper, void* workspace, size_t workspace_bytes,
                                    void* stream);
+/* Same with the fourth product lo.lo.  The three-product form misses
+ * sum(u_lo v_lo), which on a diagonal entry u.u is sum(u_lo^2) > 0: the
+ * diagonal comes out low by ~2^-16/3 relative, a bias, not noise, that an
+ * overlap matrix turns into a shift of all its eigenvalues.  With lo.lo the
+ * remaining error is the rounding of u_lo (~2^-17 relative, no sign bias). */
+QSB_API qsb_status qsb_gram_bf16x4(qsb_dtype dtype, int64_t N, int p, int q, const void* U, const void* V,
+                                   double* T, int ldt, int upper, void* workspace, size_t workspace_bytes,
+                                   void* stream);
+
+/* Gram product T = U^T V on the INT8 tensor cores (tcgen05 kind::i8) by the
+ * Ozaki splitting: each column of U and V gets a power-of-two scale 2^e with
+ * max|u| 2^-e in [32, 64) and three int8 slices u 2^-e = s0 + s1 2^-7 + s2 2^-14
+ * (+ |r| <= 2^-15, round-to-nearest, no sign bias); the six slice products with
+ * i + j <= 2 accumulate exactly in INT32 (TMEM) and combine in FP64.  Relative
+ * error ~2^-20 per element product, random-signed, so Gram entries over N
+ * points carry ~1e-6 / sqrt(N) and no systematic part beyond ~2^-28.  Same
+ * arguments and workspace query as qsb_gram_bf16x3. */
+QSB_API qsb_status qsb_gram_ozaki_int8_workspace(int64_t N, int p, int q, int same, size_t* bytes);
+QSB_API qsb_status qsb_gram_ozaki_int8(qsb_dtype dtype, int64_t N, int p, int q, const void* U, const void* V,
+                                       double* T, int ldt, int upper, void* workspace, size_t workspace_bytes,
+                                       void* stream);
 
 /* Per-kernel device timing of qsb_ham_apply, in the spirit of the reference's
  * StopWatch sectors (source/StopWatch.h:11-60, watch_pp in

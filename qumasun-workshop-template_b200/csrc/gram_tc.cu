@@ -20,6 +20,7 @@
 // All waits are bounded; a wait that runs out sets the device error word, the
 // CTA stops issuing, drains (bounded) and frees its TMEM before returning.
 #include "qsb_internal.h"
+#include "tc_common.cuh"
 
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -29,6 +30,7 @@
 
 namespace qsb {
 namespace {
+using namespace tc;
 
 constexpr int GT_M = 128;          // UMMA M (rows of T per CTA)
 constexpr int GT_N = 128;          // UMMA N (columns of T per CTA)
@@ -43,47 +45,6 @@ constexpr unsigned GT_WAIT_LIMIT = 1u << 22;
 constexpr unsigned GT_DRAIN_LIMIT = 1u << 16;
 constexpr int ERR_GEMM_TIMEOUT = 2;
 
-__device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void bar_init(uint64_t* b, uint32_t n) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(n) : "memory");
-}
-__device__ __forceinline__ void bar_expect_tx(uint64_t* b, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool bar_try(uint64_t* b, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(su32(b)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity, unsigned limit) {
-    for (unsigned i = 0; i < limit; ++i)
-        if (bar_try(b, parity)) return true;
-    return false;
-}
-__device__ __forceinline__ void tma_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* b) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
-            "r"(su32(dst)),
-        "l"((uint64_t)map), "r"(x), "r"(y), "r"(su32(b))
-        : "memory");
-}
-
-// UMMA shared-memory descriptor of a K-major tile stored in 128-byte swizzle
-// atoms (8 rows x 128 B): start address >> 4, leading offset 1 (unused for
-// swizzled K-major), stride offset 1024 B >> 4 between 8-row groups, descriptor
-// version 1, layout SWIZZLE_128B (2).
-__device__ __forceinline__ uint64_t sw128_kmajor_desc(uint32_t saddr) {
-    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
-           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
-}
-
 // Instruction descriptor: kind::f16 with bf16 A and B, fp32 D, both K-major,
 // M = 128, N = 128.
 constexpr uint32_t GT_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(GT_N >> 3) << 17) |
@@ -96,10 +57,6 @@ __device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint6
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
         "l"(adesc), "l"(bdesc), "r"(GT_IDESC), "r"(accumulate)
         : "memory");
-}
-__device__ __forceinline__ void umma_commit(uint64_t* b) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(b))
-                 : "memory");
 }
 
 // Column c of the gathered operand (fp32 or fp64, one column every N elements)
@@ -164,6 +121,7 @@ __host__ __device__ __forceinline__ int tile_index(int mt, int nt, int mtiles, b
 // One CTA: output tile t of the tile list (blockIdx.x) over the K stages
 // [kb0, kb1) of split blockIdx.y (units of GT_K); the fp32 tile goes to
 // partial[((split * ntl + t) * GT_M + row) * GT_N + col].
+template <int PRODUCTS>
 __global__ void __launch_bounds__(GT_THREADS, 1)
 gram_tc_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__ CUtensorMap mAlo,
                const __grid_constant__ CUtensorMap mBhi, const __grid_constant__ CUtensorMap mBlo, int kstages,
@@ -246,6 +204,8 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__
                 umma_bf16(tmem, sw128_kmajor_desc(a_hi + koff), sw128_kmajor_desc(b_hi + koff), acc0);
                 umma_bf16(tmem, sw128_kmajor_desc(a_hi + koff), sw128_kmajor_desc(b_lo + koff), 1u);
                 umma_bf16(tmem, sw128_kmajor_desc(a_lo + koff), sw128_kmajor_desc(b_hi + koff), 1u);
+                if (PRODUCTS == 4)
+                    umma_bf16(tmem, sw128_kmajor_desc(a_lo + koff), sw128_kmajor_desc(b_lo + koff), 1u);
             }
             umma_commit(&empty[s]);   // stage s free once these MMAs complete
         }
@@ -267,15 +227,7 @@ gram_tc_kernel(const __grid_constant__ CUtensorMap mAhi, const __grid_constant__
     for (int c0 = 0; c0 < GT_N; c0 += 32) {
         uint32_t r[32];
         const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-              "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-              "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        tmem_ld32(taddr, r);
 #pragma unroll
         for (int j = 0; j < 32; j += 4) {
             float4 v = have ? make_float4(__uint_as_float(r[j]), __uint_as_float(r[j + 1]), __uint_as_float(r[j + 2]),
@@ -318,35 +270,8 @@ __global__ void gram_reduce_kernel(const float* __restrict__ partial, int ksplit
     *d = accumulate ? *d + alpha * s : alpha * s;
 }
 
-using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn gt_encode_fn() {
-    static EncodeTiledFn fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = (EncodeTiledFn)p;
-    }
-    return fn;
-}
-
-// 2-D map over a bf16 operand [cols][ldk], box (64 K, rows), 128-byte swizzle
 bool make_operand_map(CUtensorMap* map, const void* base, int64_t ldk, int cols, int box_rows) {
-    EncodeTiledFn fn = gt_encode_fn();
-    if (!fn) return false;
-    const cuuint64_t dims[2] = {(cuuint64_t)ldk, (cuuint64_t)cols};
-    const cuuint64_t strides[1] = {(cuuint64_t)ldk * 2};
-    const cuuint32_t box[2] = {(cuuint32_t)GT_K, (cuuint32_t)box_rows};
-    const cuuint32_t estr[2] = {1, 1};
-    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
-              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    return make_kmajor_map(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, ldk, cols, GT_K, box_rows);
 }
 
 int64_t split_ldk(int64_t N) { return ((N + GT_K - 1) / GT_K) * GT_K; }
@@ -372,6 +297,37 @@ GramPlan plan_gram(int64_t N, int p, int q, bool upper) {
 }
 
 }  // namespace
+
+namespace tc {
+
+EncodeTiledFn encode_tiled_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+bool make_kmajor_map(CUtensorMap* map, CUtensorMapDataType dt, int elem_bytes, const void* base, int64_t ldk,
+                     int cols, int box_k, int box_rows) {
+    EncodeTiledFn fn = encode_tiled_fn();
+    if (!fn) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)ldk, (cuuint64_t)cols};
+    const cuuint64_t strides[1] = {(cuuint64_t)ldk * elem_bytes};
+    const cuuint32_t box[2] = {(cuuint32_t)box_k, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace tc
 
 size_t split_bf16_bytes(int64_t N, int cols) { return 2 * split_half_bytes(N, cols); }
 
@@ -400,8 +356,10 @@ size_t gram_partial_bytes_bound(int p, int q, bool upper) {
 }
 
 qsb_status gram_split_tc(int64_t N, const void* A, int p, const void* B, int q, bool upper, double* T, int ldt,
-                         double alpha, bool accumulate, void* partial, size_t partial_bytes, cudaStream_t s) {
+                         double alpha, bool accumulate, void* partial, size_t partial_bytes, cudaStream_t s,
+                         int products) {
     if (p <= 0 || q <= 0 || N <= 0) return QSB_OK;
+    if (products != 3 && products != 4) return fail(QSB_ERR_INVALID, "gram_split_tc: products must be 3 or 4");
     if (upper && p != q) return fail(QSB_ERR_INVALID, "gram_split_tc: upper mode needs p == q");
     const GramPlan g = plan_gram(N, p, q, upper);
     if (partial_bytes < g.partial_bytes) return fail(QSB_ERR_INVALID, "gram_split_tc: partial workspace too small");
@@ -412,8 +370,9 @@ qsb_status gram_split_tc(int64_t N, const void* A, int p, const void* B, int q, 
     if (!make_operand_map(&mahi, a, ldk, p, GT_M) || !make_operand_map(&malo, a + split_half_bytes(N, p), ldk, p, GT_M) ||
         !make_operand_map(&mbhi, b, ldk, q, GT_N) || !make_operand_map(&mblo, b + split_half_bytes(N, q), ldk, q, GT_N))
         return fail(QSB_ERR_CUDA, "gram_split_tc: tensor map encoding failed");
-    QSB_CUDA_TRY(cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GT_SMEM));
-    gram_tc_kernel<<<dim3(g.ntl, g.ksplit), GT_THREADS, GT_SMEM, s>>>(mahi, malo, mbhi, mblo, g.kstages, g.ksplit,
+    auto kern = products == 4 ? gram_tc_kernel<4> : gram_tc_kernel<3>;
+    QSB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GT_SMEM));
+    kern<<<dim3(g.ntl, g.ksplit), GT_THREADS, GT_SMEM, s>>>(mahi, malo, mbhi, mblo, g.kstages, g.ksplit,
                                                                        g.mtiles, upper ? 1 : 0, (float*)partial,
                                                                        device_error_word());
     QSB_CUDA_TRY(cudaGetLastError());
@@ -431,7 +390,8 @@ size_t gram_bf16x3_workspace(int64_t N, int p, int q, bool same) {
 // T (p x q, ld ldt, FP64) = alpha * U^T V  (+ T when accumulate), U: N x p, V: N x q
 // (ld N, fp32 or fp64; V == U with p == q splits once).
 qsb_status gram_bf16x3(qsb_dtype dt, int64_t N, int p, int q, const void* U, const void* V, double* T, int ldt,
-                       double alpha, bool accumulate, bool upper, void* ws, size_t ws_bytes, cudaStream_t s) {
+                       double alpha, bool accumulate, bool upper, void* ws, size_t ws_bytes, cudaStream_t s,
+                       int products) {
     if (p <= 0 || q <= 0 || N <= 0) return QSB_OK;
     const bool same = (U == V) && (p == q);
     const size_t need = gram_bf16x3_workspace(N, p, q, same);
@@ -442,7 +402,8 @@ qsb_status gram_bf16x3(qsb_dtype dt, int64_t N, int p, int q, const void* U, con
     unsigned char* part = sb + (same ? split_bf16_bytes(N, p) : split_bf16_bytes(N, q));
     QSB_TRY(split_bf16(dt, N, column_set(U, p), sa, s));
     if (!same) QSB_TRY(split_bf16(dt, N, column_set(V, q), sb, s));
-    return gram_split_tc(N, sa, p, sb, q, upper, T, ldt, alpha, accumulate, part, gram_partial_bytes(N, p, q, false), s);
+    return gram_split_tc(N, sa, p, sb, q, upper, T, ldt, alpha, accumulate, part, gram_partial_bytes(N, p, q, false), s,
+                         products);
 }
 
 }  // namespace qsb
@@ -455,15 +416,27 @@ qsb_status qsb_gram_bf16x3_workspace(int64_t N, int p, int q, int same, size_t* 
     return QSB_OK;
 }
 
-qsb_status qsb_gram_bf16x3(qsb_dtype dtype, int64_t N, int p, int q, const void* U, const void* V, double* T, int ldt,
-                           int upper, void* workspace, size_t workspace_bytes, void* stream) {
+namespace {
+qsb_status gram_entry(qsb_dtype dtype, int64_t N, int p, int q, const void* U, const void* V, double* T, int ldt,
+                      int upper, void* workspace, size_t workspace_bytes, void* stream, int products) {
     if (dtype != QSB_F64 && dtype != QSB_F32) return qsb::fail(QSB_ERR_INVALID, "gram_bf16x3: bad dtype");
     if (N < 1 || p < 1 || q < 1 || !U || !V || !T || ldt < p || !workspace)
-        return qsb::fail(QSB_ERR_INVALID, "gram_bf16x3: bad arguments");
+        return qsb::fail(QSB_ERR_INVALID, "gram_bf16: bad arguments");
     if (p > 65535 || q > 65535) return qsb::fail(QSB_ERR_INVALID, "gram_bf16x3: p, q must be < 65536");
     if (upper && p != q) return qsb::fail(QSB_ERR_INVALID, "gram_bf16x3: upper needs p == q");
     return qsb::gram_bf16x3(dtype, N, p, q, U, V, T, ldt, 1.0, false, upper != 0, workspace, workspace_bytes,
-                            (cudaStream_t)stream);
+                            (cudaStream_t)stream, products);
+}
+}  // namespace
+
+qsb_status qsb_gram_bf16x3(qsb_dtype dtype, int64_t N, int p, int q, const void* U, const void* V, double* T, int ldt,
+                           int upper, void* workspace, size_t workspace_bytes, void* stream) {
+    return gram_entry(dtype, N, p, q, U, V, T, ldt, upper, workspace, workspace_bytes, stream, 3);
+}
+
+qsb_status qsb_gram_bf16x4(qsb_dtype dtype, int64_t N, int p, int q, const void* U, const void* V, double* T, int ldt,
+                           int upper, void* workspace, size_t workspace_bytes, void* stream) {
+    return gram_entry(dtype, N, p, q, U, V, T, ldt, upper, workspace, workspace_bytes, stream, 4);
 }
 
 }  // extern "C"

@@ -256,6 +256,7 @@ struct qsb_eigensolver {
     float* rc32 = nullptr;   // fp32 copies of the rotation coefficients / orthogonalization matrix
     double* svq = nullptr;   // overlap-basis pencil solve: W, scratch, reduced matrix (m x m each), lambda, d
     double drop_tol = 0.0;   // overlap eigenvalues below drop_tol * max are dropped
+    int gram_kind = QSB_GRAM_INT8_OZAKI;   // Gram products: BF16x3, BF16x4 or INT8 Ozaki
     int last_dropped = 0;    // most directions dropped in one iteration of the last call
     double last_min_kept = 1.0;   // smallest kept overlap eigenvalue / max in the last call
     qsb_apply_f32_fn op32 = nullptr;
@@ -451,19 +452,33 @@ namespace {
 // Sb = U^H U, Sa = U^H AU over the whole basis (m bands) in two tensor-core
 // Gram products (upper tiles; the pencil's lower triangle is the mirror, as
 // MakeMatrix_z_blas computes only the upper blocks).  scale: dV for the real solver.
+// split copy of an fp32 operand in the solver's Gram form
+qsb_status gram_split_operand(qsb_eigensolver* es, const ColumnSet& src, void* dst, cudaStream_t s) {
+    if (es->gram_kind == QSB_GRAM_INT8_OZAKI) return ozaki_split(QSB_F32, es->N, src, dst, s);
+    return split_bf16(QSB_F32, es->N, src, dst, s);
+}
+// T (ld ldt) = A^T B from split operands, in the solver's Gram form
+qsb_status gram_of_splits(qsb_eigensolver* es, const void* A, int p, const void* B, int q, bool upper, double* T,
+                          int ldt, cudaStream_t s) {
+    if (es->gram_kind == QSB_GRAM_INT8_OZAKI)
+        return gram_ozaki_tc(es->N, A, p, B, q, upper, T, ldt, 1.0, false, es->gpart, es->gpart_bytes, s);
+    return gram_split_tc(es->N, A, p, B, q, upper, T, ldt, 1.0, false, es->gpart, es->gpart_bytes, s,
+                         es->gram_kind == QSB_GRAM_BF16X4 ? 4 : 3);
+}
+
 qsb_status mixed_pencil(qsb_eigensolver* es, const ColumnSet& U, const ColumnSet& AU, int m, double scale,
                         cudaStream_t s) {
     const int p = column_count(U);   // real columns: m (real) or 2m (complex)
-    QSB_TRY(split_bf16(QSB_F32, es->N, U, es->su, s));
-    QSB_TRY(split_bf16(QSB_F32, es->N, AU, es->sau, s));
+    QSB_TRY(gram_split_operand(es, U, es->su, s));
+    QSB_TRY(gram_split_operand(es, AU, es->sau, s));
     const dim3 grid((m + 127) / 128, m);
-    QSB_TRY(gram_split_tc(es->N, es->su, p, es->su, p, true, es->T2, p, 1.0, false, es->gpart, es->gpart_bytes, s));
+    QSB_TRY(gram_of_splits(es, es->su, p, es->su, p, true, es->T2, p, s));
     if (es->cplx)
         assemble_complex_block<<<grid, 128, 0, s>>>(es->T2, m, m, p, (double2*)es->Sb, m, 0, 0, 1);
     else
         assemble_real_block<<<grid, 128, 0, s>>>(es->T2, m, m, p, es->Sb, m, 0, 0, 1, scale);
     QSB_CUDA_TRY(cudaGetLastError());
-    QSB_TRY(gram_split_tc(es->N, es->su, p, es->sau, p, true, es->T2, p, 1.0, false, es->gpart, es->gpart_bytes, s));
+    QSB_TRY(gram_of_splits(es, es->su, p, es->sau, p, true, es->T2, p, s));
     if (es->cplx)
         assemble_complex_block<<<grid, 128, 0, s>>>(es->T2, m, m, p, (double2*)es->Sa, m, 0, 0, 1);
     else
@@ -638,10 +653,9 @@ qsb_status rotate_complex32(qsb_eigensolver* es, int na, float* OUT, const float
 
 // B_act -= X_fix (X_fix^H B_act) for complex fp32 bundles (VectorOrthogonalization)
 qsb_status orthogonalize32(qsb_eigensolver* es, int nf, int na, const float* Xfix, float* B, cudaStream_t s) {
-    QSB_TRY(split_bf16(QSB_F32, es->N, column_set(Xfix, 2 * nf), es->su, s));
-    QSB_TRY(split_bf16(QSB_F32, es->N, column_set(B, 2 * na), es->sau, s));
-    QSB_TRY(gram_split_tc(es->N, es->su, 2 * nf, es->sau, 2 * na, false, es->T2, 2 * nf, 1.0, false, es->gpart,
-                          es->gpart_bytes, s));
+    QSB_TRY(gram_split_operand(es, column_set(Xfix, 2 * nf), es->su, s));
+    QSB_TRY(gram_split_operand(es, column_set(B, 2 * na), es->sau, s));
+    QSB_TRY(gram_of_splits(es, es->su, 2 * nf, es->sau, 2 * na, false, es->T2, 2 * nf, s));
     pack_orth<<<dim3((nf + 127) / 128, na), 128, 0, s>>>(es->T2, nf, na);
     QSB_CUDA_TRY(cudaGetLastError());
     const size_t cnt = (size_t)2 * nf * 2 * na;
@@ -848,9 +862,9 @@ qsb_status lobpcg_z_mixed(qsb_eigensolver* es, double dVol, int n, int iter_max,
         QSB_TRY(copy32(Xa, TMP, L * N_, s));
         // AP' = AR Cr + AP Cp; AX' = AX Cx + AP' (:2718), on the last iteration too:
         // the eigenvalues are the Rayleigh quotients <x'|Ax'> / <x'|x'> summed in
-        // fp64, not the pencil's Ritz values.  Split-BF16x3 leaves out lo*lo,
-        // which on the overlap diagonal is sum(lo^2) > 0, so the pencil's values
-        // sit ~2^-16/3 (relative) high; the vectors themselves are unaffected.
+        // fp64, not the pencil's Ritz values, which carry the Gram products'
+        // error (with 3 products, no lo*lo term, the overlap diagonal is low by
+        // sum(lo^2) ~ 2^-16/3 relative and the Ritz values sit that much high).
         QSB_TRY(rotate_complex32(es, N_, TMP, ARa, 1, 0.0f));
         if (use_p) QSB_TRY(rotate_complex32(es, N_, TMP, APa, 2, 1.0f));
         QSB_TRY(copy32(APa, TMP, L * N_, s));
@@ -926,8 +940,10 @@ qsb_status qsb_eigensolver_create_ex(qsb_eigensolver** out, int64_t N, int n, in
         // (unit) diagonal: overlap directions weaker than about that are noise
         es->drop_tol = std::min(1e-5, std::max(1e-8, 1e-5 / std::sqrt((double)N)));
         const int pmax = 3 * n * c2;
-        es->split_bytes = split_bf16_bytes(N, pmax);
-        es->gpart_bytes = std::max(gram_partial_bytes_bound(pmax, pmax, true), gram_partial_bytes_bound(n, 2 * n, false));
+        es->split_bytes = std::max(split_bf16_bytes(N, pmax), ozaki_split_bytes(N, pmax));
+        es->gpart_bytes = std::max({gram_partial_bytes_bound(pmax, pmax, true), gram_partial_bytes_bound(n, 2 * n, false),
+                                    ozaki_partial_bytes_bound(N, pmax, pmax, true),
+                                    ozaki_partial_bytes_bound(N, n, 2 * n, false)});
         if (cudaMalloc(&es->su, es->split_bytes) != cudaSuccess || cudaMalloc(&es->sau, es->split_bytes) != cudaSuccess ||
             cudaMalloc(&es->gpart, es->gpart_bytes) != cudaSuccess ||
             cudaMalloc((void**)&es->T2, sizeof(double) * (size_t)pmax * pmax) != cudaSuccess ||
@@ -1014,6 +1030,14 @@ qsb_status qsb_eigensolver_set_drop_tolerance(qsb_eigensolver* es, double tol) {
     if (!es->mixed) return fail(QSB_ERR_STATE, "set_drop_tolerance: only mixed-precision contexts drop directions");
     if (!(tol > 0.0 && tol < 1.0)) return fail(QSB_ERR_INVALID, "set_drop_tolerance: needs 0 < tol < 1");
     es->drop_tol = tol;
+    return QSB_OK;
+}
+
+qsb_status qsb_eigensolver_set_gram_kind(qsb_eigensolver* es, qsb_gram_kind kind) {
+    if (!es) return fail(QSB_ERR_INVALID, "set_gram_kind: null solver");
+    if (kind != QSB_GRAM_BF16X3 && kind != QSB_GRAM_BF16X4 && kind != QSB_GRAM_INT8_OZAKI)
+        return fail(QSB_ERR_INVALID, "set_gram_kind: unknown kind");
+    es->gram_kind = kind;
     return QSB_OK;
 }
 

@@ -145,12 +145,26 @@ size_t gram_partial_bytes_bound(int p, int q, bool upper);
 // T (p x q, FP64, ld ldt) = alpha * A^T B (+ T when accumulate) from split
 // operands A (p columns) and B (q columns); upper: only entries in output tiles
 // on or above the diagonal (128 x 128 tiles) are written.
+// products: 3 (hi.hi + hi.lo + lo.hi) or 4 (+ lo.lo).
 qsb_status gram_split_tc(int64_t N, const void* A, int p, const void* B, int q, bool upper, double* T, int ldt,
+                         double alpha, bool accumulate, void* partial, size_t partial_bytes, cudaStream_t s,
+                         int products);
+// INT8 Ozaki form (gram_i8.cu): three int8 slices per column with a per-column
+// power-of-two scale, exact INT32 accumulation on the tensor cores.
+size_t ozaki_split_bytes(int64_t N, int cols);
+qsb_status ozaki_split(qsb_dtype dt, int64_t N, const ColumnSet& src, void* dst, cudaStream_t s);
+// FP64 partial bytes enough for every call with p' <= p, q' <= q at this N.
+size_t ozaki_partial_bytes_bound(int64_t N, int p, int q, bool upper);
+qsb_status gram_ozaki_tc(int64_t N, const void* A, int p, const void* B, int q, bool upper, double* T, int ldt,
                          double alpha, bool accumulate, void* partial, size_t partial_bytes, cudaStream_t s);
+size_t gram_ozaki_workspace(int64_t N, int p, int q, bool same);
+qsb_status gram_ozaki(qsb_dtype dt, int64_t N, int p, int q, const void* U, const void* V, double* T, int ldt,
+                      double alpha, bool accumulate, bool upper, void* ws, size_t ws_bytes, cudaStream_t s);
 // One-call form on plain operands U (N x p), V (N x q), ld N.
 size_t gram_bf16x3_workspace(int64_t N, int p, int q, bool same);
 qsb_status gram_bf16x3(qsb_dtype dt, int64_t N, int p, int q, const void* U, const void* V, double* T, int ldt,
-                       double alpha, bool accumulate, bool upper, void* ws, size_t ws_bytes, cudaStream_t s);
+                       double alpha, bool accumulate, bool upper, void* ws, size_t ws_bytes, cudaStream_t s,
+                       int products);
 
 }  // namespace qsb
 

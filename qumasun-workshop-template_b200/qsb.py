@@ -276,6 +276,12 @@ class EigenSolver:
     def set_drop_tolerance(self, tol):
         _check(lib.qsb_eigensolver_set_drop_tolerance(self._h, _c_d(tol)))
 
+    GRAM_KINDS = {"bf16x3": 3, "bf16x4": 4, "int8_ozaki": 8}
+
+    def set_gram_kind(self, kind):
+        """"bf16x3", "bf16x4" or "int8_ozaki" (the default) for the mixed-precision Gram products."""
+        _check(lib.qsb_eigensolver_set_gram_kind(self._h, self.GRAM_KINDS[kind]))
+
     def overlap_stats(self):
         """(most directions dropped in one iteration, smallest kept overlap
         eigenvalue / largest, drop tolerance) of the last call (mixed precision)."""
