@@ -310,6 +310,7 @@ def lobpcg_section(H, psi, N, NB, dV, n_occ, stream, max_calls=60):
 
 
 def main():
+    global NB
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
@@ -317,7 +318,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-lobpcg", action="store_true")
+    ap.add_argument("--bands", type=int, default=NB,
+                    help="bands per GPU (default 128, the benchmark workload; smaller only for profiler captures)")
     args = ap.parse_args()
+    NB = args.bands
     if args.impl == "reference":
         return run_reference(args)
     assert args.warmup >= 3, "at least 3 warm-up steps"
@@ -430,7 +434,7 @@ def main():
         "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded psi U[-0.5,0.5], seeded potential, analytic GTH projectors)",
         "config": {"workload": "H.psi, bcc 2x2x2 supercell (16 atoms, a=12 bohr), 96^3 grid (h=0.125), "
-                               "128 bands per GPU, FP64 real Gamma, FD8 + V + GTH s+p KB nonlocal",
+                               f"{NB} bands per GPU, FP64 real Gamma, FD8 + V + GTH s+p KB nonlocal",
                    "grid": [NX, NY, NZ], "bands_per_gpu": NB, "atoms": len(pos), "projector_points": n_pts,
                    "parallelism": f"band decomposition x{world}",
                    "l2": "inputs larger than L2 (psi 906 MB per GPU)"},
