@@ -176,6 +176,33 @@ QSB_API qsb_status qsb_ham_nonlocal_project(qsb_ham* ham, qsb_dtype dtype, int i
                                     const void* psi_dev, double gx, double gy, double gz,
                                     double* out_host, void* stream);
 
+/* Projector gradients d beta / d(x, y, z) (of the grid point's coordinate) for
+ * the tables given to qsb_ham_set_projectors, needed by the forces: host array,
+ * per atom three blocks (d/dx, d/dy, d/dz), each npts[a] x widths[a]
+ * column-major like beta, atoms concatenated in order.  The reference's
+ * FORCE_DIFF_PROJ path builds the same gradients of projector_RY
+ * (source/PseudoPotNonlocal_SvF2_kpoint.h:31-45).  qsb_ham_set_gth_projectors
+ * sets them itself (analytic derivatives of the GTH projectors). */
+QSB_API qsb_status qsb_ham_set_projector_gradients(qsb_ham* ham, const double* dbeta);
+
+/* Nonlocal band energy E = sum_n occ_n sum_atoms sum_w E_w |dV <beta_w|psi_n>|^2
+ * (the Bloch-phased projection for complex bands at vector g).  occupancies:
+ * host, nb values.  Replaces EnergyPPnonlocal_bundle
+ * (source/PseudoPotNonlocal_SvF2_kpoint.h:5033-5135). */
+QSB_API qsb_status qsb_ham_nonlocal_energy(qsb_ham* ham, qsb_dtype dtype, int is_complex, int nb, const void* psi_dev,
+                                           const double* occupancies, double gx, double gy, double gz,
+                                           double* energy, void* stream);
+
+/* Same energy and the nonlocal forces, "+=" into forces (host, 3 per atom):
+ *   F_a += sum_n occ_n sum_w 2 E_w Re( conj(dV <beta_w|psi_n>) dV <grad beta_w|psi_n> )
+ * i.e. -dE/dR_a at fixed psi, computed in reverse mode: the adjoint of the
+ * projection (2 occ E_w conj(c)) contracted with the projector-gradient
+ * projections.  Replaces ForceNonlocal_bundle (grad(p) form,
+ * source/PseudoPotNonlocal_SvF2_kpoint.h:3629-3731).  Needs projector gradients. */
+QSB_API qsb_status qsb_ham_nonlocal_energy_force(qsb_ham* ham, qsb_dtype dtype, int is_complex, int nb,
+                                                 const void* psi_dev, const double* occupancies, double gx, double gy,
+                                                 double gz, double* energy, double* forces, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Block LOBPCG eigensolvers (device resident).
  * ------------------------------------------------------------------------- */

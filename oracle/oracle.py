@@ -138,13 +138,91 @@ def gth_tables(pos, species_params, dx, dy, dz, rcut_factor=RCUT_FACTOR):
             np.array(energy, np.float64))
 
 
+def gth_gradient_columns(x, y, z, sp, rcut_factor=RCUT_FACTOR):
+    """d beta_w / d(x, y, z) of the GTH projectors of gth_tables at offsets
+    (x, y, z) = point - atom: grads[d][w] arrays.  Analytic derivatives:
+      s:   d/dv_d exp(-r^2/(2 r0^2))      = -v_d / r0^2 * (the Gaussian)
+      p_m: d/dv_d (v_m exp(-r^2/(2 r1^2))) = (delta_md - v_m v_d / r1^2) * (the Gaussian)
+    (the same cutoffs as the projectors)."""
+    nl, rl = sp["nl"], sp["r"]
+    r2 = x * x + y * y + z * z
+    r = np.sqrt(r2)
+    v = (x, y, z)
+    grads = [[], [], []]
+    if nl >= 1:
+        pre0 = math.sqrt(2.0) / (rl[0] ** 1.5 * math.sqrt(math.sqrt(math.pi) / 2.0)) / math.sqrt(4.0 * math.pi)
+        b0 = np.where(r <= rcut_factor * rl[0], pre0 * np.exp(-r2 / (2.0 * rl[0] ** 2)), 0.0)
+        for d in range(3):
+            grads[d].append(-v[d] / rl[0] ** 2 * b0)
+    if nl >= 2:
+        pre1 = (math.sqrt(2.0) / (rl[1] ** 2.5 * math.sqrt(3.0 * math.sqrt(math.pi) / 4.0))
+                * math.sqrt(3.0 / (4.0 * math.pi)))
+        e1 = np.where(r <= rcut_factor * rl[1], pre1 * np.exp(-r2 / (2.0 * rl[1] ** 2)), 0.0)
+        for m in range(3):
+            for d in range(3):
+                grads[d].append(e1 * ((1.0 if m == d else 0.0) - v[m] * v[d] / rl[1] ** 2))
+    return grads
+
+
+def gth_gradient_tables(pos, species_params, dx, dy, dz, tables, rcut_factor=RCUT_FACTOR):
+    """Projector gradients for the point lists of gth_tables (same points, same
+    order), in the C ABI's layout: per atom d/dx, d/dy, d/dz blocks, each
+    npts x width column-major."""
+    npts, widths, coords, _, _ = tables
+    out, off = [], 0
+    for a, (R, sp) in enumerate(zip(pos, species_params)):
+        n = int(npts[a])
+        if widths[a] == 0 or n == 0:
+            off += n
+            continue
+        C = coords[3 * off: 3 * (off + n)].reshape(n, 3)
+        g = gth_gradient_columns(C[:, 0] * dx - R[0], C[:, 1] * dy - R[1], C[:, 2] * dz - R[2], sp, rcut_factor)
+        for d in range(3):
+            out.append(np.concatenate(g[d]))
+        off += n
+    return np.ascontiguousarray(np.concatenate(out)) if out else np.zeros(0)
+
+
+def nonlocal_energy_force(grid, tables, dbeta, psi, nb, occ, is_complex=False, g=(0.0, 0.0, 0.0)):
+    """Restatement of EnergyPPnonlocal_bundle / ForceNonlocal_bundle
+    (source/PseudoPotNonlocal_SvF2_kpoint.h:5033-5135, :3629-3731):
+      c = dV <beta|psi>, d_k = dV <d beta/dk|psi> (qso_nonlocal_project on the
+      beta and the gradient tables), E = sum occ E_w |c|^2,
+      F_a,k = sum occ 2 E_w (c_re d_k,re + c_im d_k,im).
+    Returns (energy, forces[n_atoms, 3])."""
+    npts, widths, coords, beta, energy = tables
+    c = nonlocal_project(grid, tables, psi, nb, is_complex, g)            # [ncol][P]
+    d = []
+    for k in range(3):
+        parts = []
+        off_g = 0
+        for a in range(len(npts)):
+            n, w = int(npts[a]), int(widths[a])
+            parts.append(dbeta[off_g + k * n * w: off_g + (k + 1) * n * w])
+            off_g += 3 * n * w
+        tk = (npts, widths, coords, np.ascontiguousarray(np.concatenate(parts)) if parts else np.zeros(0), energy)
+        d.append(nonlocal_project(grid, tk, psi, nb, is_complex, g))
+    occ = np.asarray(occ, np.float64)
+    occ_col = np.repeat(occ, 2) if is_complex else occ
+    E = float((occ_col[:, None] * energy[None, :] * c * c).sum())
+    F = np.zeros((len(npts), 3))
+    p0 = 0
+    for a in range(len(npts)):
+        w = int(widths[a])
+        sl = slice(p0, p0 + w)
+        for k in range(3):
+            F[a, k] = (2.0 * occ_col[:, None] * energy[None, sl] * c[:, sl] * d[k][:, sl]).sum()
+        p0 += w
+    return E, F
+
+
 def gth_cube_tables(pos, species_params, nx, ny, nz, dx, dy, dz, rcut_factor=RCUT_FACTOR):
     """The same projectors on the reference's CUBE subgrid blocks (GetOverlapPeriodic,
     source/GridSubgrid.h:690-740), for the reference-side nonlocal.  Returns
     (cubes[6 per atom], widths, proj (block layout, column-major per atom), energy,
     point-list form (npts, coords) of the same blocks)."""
     lib = ref_lib()
-    cubes, widths, proj, energy, npts, coords = [], [], [], [], [], []
+    cubes, widths, proj, energy, npts, coords, grad = [], [], [], [], [], [], []
     blocks_buf = np.zeros(9 * 4096, np.int32)
     gsz = ctypes.c_int(0)
     for R, sp in zip(pos, species_params):
@@ -182,11 +260,14 @@ def gth_cube_tables(pos, species_params, nx, ny, nz, dx, dy, dz, rcut_factor=RCU
         widths.append(w)
         if w:
             proj.append(np.concatenate(cols))
+            gr = gth_gradient_columns(x, y, z, sp, rcut_factor)
+            grad.append(np.concatenate([np.concatenate(gr[k]) for k in range(3)]))
         npts.append(len(P))
         coords.append(P.astype(np.int32).ravel())
     cat = lambda L, dt: np.ascontiguousarray(np.concatenate(L).astype(dt)) if L else np.zeros(0, dt)
     return dict(cubes=cat(cubes, np.int32), widths=np.array(widths, np.int32), proj=cat(proj, np.float64),
-                energy=np.array(energy, np.float64), npts=np.array(npts, np.int32), coords=cat(coords, np.int32))
+                energy=np.array(energy, np.float64), npts=np.array(npts, np.int32), coords=cat(coords, np.int32),
+                grad=cat(grad, np.float64))
 
 
 def seeded_psi(seed, nb, N, complex_=False, dtype=np.float64):
@@ -271,6 +352,22 @@ def nonlocal_project(grid, tables, psi, nb, is_complex=False, g=(0.0, 0.0, 0.0))
 # --------------------------------------------------------------------------
 # the reference's own code (oracle/_ref)
 # --------------------------------------------------------------------------
+def ref_nonlocal_energy_force(grid, cube, psi_soa, nb, occ, g=(0.0, 0.0, 0.0)):
+    """The reference's nonlocal energy and forces (qsref_nonlocal_energy_force)
+    on cube tables (gth_cube_tables) for nb complex SoA bands."""
+    lib = ref_lib()
+    nx, ny, nz, dx, dy, dz = grid
+    e = ctypes.c_double()
+    F = np.zeros(3 * len(cube["widths"]))
+    psi = np.ascontiguousarray(psi_soa, np.float64)
+    occ = np.ascontiguousarray(occ, np.float64)
+    lib.qsref_nonlocal_energy_force(nx, ny, nz, *[ctypes.c_double(v) for v in (dx, dy, dz)], len(cube["widths"]),
+                                    _i(cube["cubes"]), _i(cube["widths"]), _d(cube["proj"]), _d(cube["grad"]),
+                                    _d(cube["energy"]), nb, _d(psi), _d(occ), *[ctypes.c_double(v) for v in g],
+                                    ctypes.byref(e), _d(F))
+    return e.value, F.reshape(-1, 3)
+
+
 def ref_laplacian8th(nx, ny, nz, out, p, coef, dx, dy, dz):
     lib = ref_lib()
     N = nx * ny * nz

@@ -18,6 +18,8 @@
  *                              mInnerNonlocalPsi_v4_bundle :4463-4576) built from the
  *                              reference's CutSubgridByRanges / AddSubgridByRanges
  *                              (GridSubgrid.h:742,751) and blas_DGEMM_t/_n (w_dgemm.h)
+ *   qsref_nonlocal_energy_force  EnergyPPnonlocal_bundle / ForceNonlocal_bundle (grad(p) form)
+ *                             (PseudoPotNonlocal_SvF2_kpoint.h:5033-5135, :3629-3731)
  *   qsref_hamiltonian         mHamiltonianMatrix_ddm composition
  *                             (qumasun_base1.matrix.h:263-317): H = V.psi + NL + FD8(-1/2)
  *   qsref_lobpcg_d            EigenLOBPCG_d_multi           lobpcg_d_multi.h:23-545
@@ -331,6 +333,68 @@ void qsref_nonlocal_apply(int nx, int ny, int nz, double dx, double dy, double d
         pr[b] = psi + 2 * b * N; pi[b] = psi + (2 * b + 1) * N;
     }
     nonlocal_apply_bundle(nl, grid, nb, hr.data(), hi.data(), pr.data(), pi.data(), dx * dy * dz, gx * dx, gy * dy, gz * dz);
+}
+
+/* Nonlocal energy and forces of nb complex SoA bands, following
+ * EnergyPPnonlocal_bundle (PseudoPotNonlocal_SvF2_kpoint.h:5033-5135) and the
+ * grad(p) form of ForceNonlocal_bundle (:3629-3731): per atom the cut psi
+ * (Bloch phase as mInnerNonlocalPsi applies it) is projected with DGEMM_t on
+ * projector_RY and on its three gradient tables (dV-scaled, the inner / diff_x,
+ * diff_y, diff_z of mInnerNonlocalPsi_diff_bundle), then
+ *   E += |inner|^2 E_w occ_n,   F_a += 2 (inner.r diff.r + inner.i diff.i) E_w occ_n.
+ * grad: per atom three block-layout tables (d/dx, d/dy, d/dz), grid_size x width each. */
+void qsref_nonlocal_energy_force(int nx, int ny, int nz, double dx, double dy, double dz, int n_atoms,
+                                 const int* cubes, const int* widths, const double* proj, const double* grad,
+                                 const double* energy, int nb, const double* psi, const double* occ, double gx,
+                                 double gy, double gz, double* energy_out, double* forces) {
+    RefNonlocal nl = build_nonlocal(nx, ny, nz, n_atoms, cubes, widths, proj, energy);
+    GridRange grid = MakeRange(nx, ny, nz);
+    const size_t N = grid.Size3D();
+    const double dV = dx * dy * dz;
+    const double gx_dx = gx * dx, gy_dy = gy * dy, gz_dz = gz * dz;
+    const bool is_gamma = (gx_dx == 0.0) && (gy_dy == 0.0) && (gz_dz == 0.0);
+    double E = 0.0;
+    size_t goff = 0;
+    for (int ai = 0; ai < n_atoms; ++ai) {
+        const RefAtom& a = nl.atoms[ai];
+        if (a.width == 0 || a.grid_size == 0) continue;
+        const int gs = a.grid_size, w = a.width;
+        std::vector<double> cut((size_t)gs * 2 * nb);
+        for (int n = 0; n < nb; ++n) {
+            CutSubgridByRanges(a.ranges, cut.data() + (size_t)gs * 2 * n, grid, psi + 2 * n * N);
+            CutSubgridByRanges(a.ranges, cut.data() + (size_t)gs * (2 * n + 1), grid, psi + (2 * n + 1) * N);
+        }
+        if (!is_gamma) {
+            std::vector<double> ere, eim;
+            bloch_exp(a, gx_dx, gy_dy, gz_dz, ere, eim);
+            for (int n = 0; n < nb; ++n) {
+                double* pr = cut.data() + (size_t)gs * 2 * n;
+                double* pi = cut.data() + (size_t)gs * (2 * n + 1);
+                for (int i = 0; i < gs; ++i) {
+                    const double p_re = pr[i], p_im = pi[i];
+                    pr[i] = ere[i] * p_re - eim[i] * p_im;
+                    pi[i] = ere[i] * p_im + eim[i] * p_re;
+                }
+            }
+        }
+        std::vector<double> inner((size_t)w * 2 * nb), diff[3];
+        blas_DGEMM_t(w, 2 * nb, gs, a.proj, cut.data(), inner.data(), w, dV, 0.0);
+        for (int k = 0; k < 3; ++k) {
+            diff[k].resize((size_t)w * 2 * nb);
+            blas_DGEMM_t(w, 2 * nb, gs, grad + goff + (size_t)k * gs * w, cut.data(), diff[k].data(), w, dV, 0.0);
+        }
+        for (int n = 0; n < nb; ++n)
+            for (int wi = 0; wi < w; ++wi) {
+                const double eo = a.energy[wi] * occ[n];
+                const double ir = inner[(size_t)w * (2 * n) + wi], ii = inner[(size_t)w * (2 * n + 1) + wi];
+                E += (ir * ir + ii * ii) * eo;
+                for (int k = 0; k < 3; ++k)
+                    forces[3 * ai + k] += 2.0 * (ir * diff[k][(size_t)w * (2 * n) + wi] +
+                                                 ii * diff[k][(size_t)w * (2 * n + 1) + wi]) * eo;
+            }
+        goff += (size_t)3 * gs * w;
+    }
+    *energy_out = E;
 }
 
 /* H psi = V psi + V_NL psi - 1/2 FD8(psi) for nb real bands (band b at psi + bN). */

@@ -61,7 +61,7 @@ static qsb_status ensure_ws(qsb_ham* h, size_t bytes) {
 //   Y_00 = 1/sqrt(4 pi),  Y_1{x,y,z} = sqrt(3/(4 pi)) {x,y,z}/r.
 static void gth_points(double Rx, double Ry, double Rz, int nl, const double* r_l, const double* h_l, double rcut_factor,
                        double dx, double dy, double dz, std::vector<int>& coords, std::vector<double>& beta_cols,
-                       std::vector<double>& energy, int& npts, int& width) {
+                       std::vector<double>& energy, int& npts, int& width, std::vector<double>& dbeta_cols) {
     width = (nl >= 1 ? 1 : 0) + (nl >= 2 ? 3 : 0);
     npts = 0;
     if (width == 0) return;
@@ -71,7 +71,7 @@ static void gth_points(double Rx, double Ry, double Rz, int nl, const double* r_
     const int ix0 = (int)std::floor((Rx - rmax) / dx), ix1 = (int)std::ceil((Rx + rmax) / dx);
     const int iy0 = (int)std::floor((Ry - rmax) / dy), iy1 = (int)std::ceil((Ry + rmax) / dy);
     const int iz0 = (int)std::floor((Rz - rmax) / dz), iz1 = (int)std::ceil((Rz + rmax) / dz);
-    std::vector<double> cols[4];
+    std::vector<double> cols[4], grads[3][4];   // grads[d][w]: d beta_w / d(x, y, z)
     const double rc0 = rcut_factor * r_l[0];
     const double rc1 = nl >= 2 ? rcut_factor * r_l[1] : 0.0;
     const double pre0 = std::sqrt(2.0) / (std::pow(r_l[0], 1.5) * std::sqrt(std::sqrt(pi) / 2.0)) / std::sqrt(4.0 * pi);
@@ -86,16 +86,26 @@ static void gth_points(double Rx, double Ry, double Rz, int nl, const double* r_
                 if (r2 > rmax * rmax) continue;
                 coords.push_back(ix); coords.push_back(iy); coords.push_back(iz);
                 const double r = std::sqrt(r2);
-                cols[0].push_back(r <= rc0 ? pre0 * std::exp(-r2 / (2.0 * r_l[0] * r_l[0])) : 0.0);
+                const double v[3] = {x, y, z};
+                const double b0 = r <= rc0 ? pre0 * std::exp(-r2 / (2.0 * r_l[0] * r_l[0])) : 0.0;
+                cols[0].push_back(b0);
+                const double s0 = 1.0 / (r_l[0] * r_l[0]);
+                for (int d = 0; d < 3; ++d) grads[d][0].push_back(-v[d] * s0 * b0);   // grad of a Gaussian
                 if (nl >= 2) {
                     const double e1 = r <= rc1 ? pre1 * std::exp(-r2 / (2.0 * r_l[1] * r_l[1])) : 0.0;
-                    cols[1].push_back(e1 * x);
-                    cols[2].push_back(e1 * y);
-                    cols[3].push_back(e1 * z);
+                    const double s1 = 1.0 / (r_l[1] * r_l[1]);
+                    for (int m = 0; m < 3; ++m) {
+                        cols[1 + m].push_back(e1 * v[m]);
+                        // d(e1 v_m)/d v_d = e1 (delta_md - v_m v_d / r1^2)
+                        for (int d = 0; d < 3; ++d)
+                            grads[d][1 + m].push_back(e1 * ((m == d ? 1.0 : 0.0) - v[m] * v[d] * s1));
+                    }
                 }
                 ++npts;
             }
     for (int w = 0; w < width; ++w) beta_cols.insert(beta_cols.end(), cols[w].begin(), cols[w].end());
+    for (int d = 0; d < 3; ++d)
+        for (int w = 0; w < width; ++w) dbeta_cols.insert(dbeta_cols.end(), grads[d][w].begin(), grads[d][w].end());
     energy.push_back(h_l[0]);
     if (nl >= 2) for (int m = 0; m < 3; ++m) energy.push_back(h_l[1]);
 }
@@ -202,7 +212,7 @@ qsb_status qsb_ham_set_gth_projectors(qsb_ham* h, int n_atoms, const double* pos
         return fail(QSB_ERR_INVALID, "set_gth_projectors: bad arguments");
     if (!(rcut_factor > 0)) return fail(QSB_ERR_INVALID, "set_gth_projectors: rcut_factor must be > 0");
     std::vector<int> npts(n_atoms), widths(n_atoms), coords;
-    std::vector<double> beta, energy;
+    std::vector<double> beta, energy, dbeta;
     for (int a = 0; a < n_atoms; ++a) {
         const int s = species[a];
         if (s < 0 || s >= n_species || nl[s] < 0 || nl[s] > 2)
@@ -210,10 +220,44 @@ qsb_status qsb_ham_set_gth_projectors(qsb_ham* h, int n_atoms, const double* pos
         for (int l = 0; l < nl[s]; ++l)
             if (!(r_l[2 * s + l] > 0)) return fail(QSB_ERR_INVALID, "set_gth_projectors: r_l must be > 0");
         gth_points(pos[3 * a], pos[3 * a + 1], pos[3 * a + 2], nl[s], r_l + 2 * s, h_l + 2 * s, rcut_factor, h->dx,
-                   h->dy, h->dz, coords, beta, energy, npts[a], widths[a]);
+                   h->dy, h->dz, coords, beta, energy, npts[a], widths[a], dbeta);
     }
-    return nl_upload(h->nl, h->nx, h->ny, h->nz, n_atoms, npts.data(), widths.data(), coords.data(), beta.data(),
-                     energy.data());
+    QSB_TRY(nl_upload(h->nl, h->nx, h->ny, h->nz, n_atoms, npts.data(), widths.data(), coords.data(), beta.data(),
+                      energy.data()));
+    return nl_upload_gradients(h->nl, dbeta.data());
+}
+
+qsb_status qsb_ham_set_projector_gradients(qsb_ham* h, const double* dbeta) {
+    if (!h) return fail(QSB_ERR_INVALID, "set_projector_gradients: null context");
+    return nl_upload_gradients(h->nl, dbeta);
+}
+
+static qsb_status energy_force(qsb_ham* h, qsb_dtype dtype, int is_complex, int nb, const void* psi,
+                               const double* occupancies, double gx, double gy, double gz, double* energy,
+                               double* forces, void* stream) {
+    if (!h || !energy) return fail(QSB_ERR_INVALID, "nonlocal energy: null argument");
+    if (dtype != QSB_F64 && dtype != QSB_F32) return fail(QSB_ERR_INVALID, "nonlocal energy: bad dtype");
+    if (nb < 0 || (nb > 0 && (!psi || !occupancies))) return fail(QSB_ERR_INVALID, "nonlocal energy: bad bands/pointers");
+    *energy = 0.0;
+    if (nb == 0 || h->nl.n_points == 0) return QSB_OK;
+    if (!is_complex) gx = gy = gz = 0.0;
+    const int ncol = is_complex ? 2 * nb : nb;
+    QSB_TRY(ensure_ws(h, nl_energy_force_bytes(h->nl, ncol, nb)));
+    return nl_energy_force(dtype, h->nl, h->nx, h->ny, h->nz, nb, is_complex, psi, occupancies, h->dx * h->dy * h->dz,
+                           gx * h->dx, gy * h->dy, gz * h->dz, energy, forces, h->ws, (cudaStream_t)stream);
+}
+
+qsb_status qsb_ham_nonlocal_energy(qsb_ham* h, qsb_dtype dtype, int is_complex, int nb, const void* psi,
+                                   const double* occupancies, double gx, double gy, double gz, double* energy,
+                                   void* stream) {
+    return energy_force(h, dtype, is_complex, nb, psi, occupancies, gx, gy, gz, energy, nullptr, stream);
+}
+
+qsb_status qsb_ham_nonlocal_energy_force(qsb_ham* h, qsb_dtype dtype, int is_complex, int nb, const void* psi,
+                                         const double* occupancies, double gx, double gy, double gz, double* energy,
+                                         double* forces, void* stream) {
+    if (!forces) return fail(QSB_ERR_INVALID, "nonlocal energy_force: null forces");
+    return energy_force(h, dtype, is_complex, nb, psi, occupancies, gx, gy, gz, energy, forces, stream);
 }
 
 qsb_status qsb_ham_projector_info(const qsb_ham* h, int64_t* total_points, int* total_projectors) {

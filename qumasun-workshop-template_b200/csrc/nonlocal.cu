@@ -21,6 +21,8 @@
 //    (mCreateNonoverlapList, :3410-3487), and the pull can be fused into the H
 //    stencil so Hpsi is written once.
 #include "qsb_internal.h"
+
+#include <cmath>
 #include <algorithm>
 #include <numeric>
 #include <cstring>
@@ -242,24 +244,66 @@ nl_apply_kernel(const int* __restrict__ cov_grid, int n_cov, const int* __restri
     }
 }
 
+// table: -1 projects on beta, 0..2 on the gradient tables d beta / d(x, y, z)
 template <typename T, bool CPLX, int WM>
-void launch_proj(const NLDevice& d, int nb, const void* psi, size_t N, double gx_dx, double gy_dy, double gz_dz,
-                 double* partial, int ncol, cudaStream_t s) {
+void launch_proj(const NLDevice& d, int table, int nb, const void* psi, size_t N, double gx_dx, double gy_dy,
+                 double gz_dz, double* partial, int ncol, cudaStream_t s) {
     constexpr int CB = CPLX ? 4 : 8;
     dim3 grid(d.n_chunks, (nb + CB - 1) / CB);
-    const T* beta = std::is_same<T, double>::value ? (const T*)d.pt_beta64 : (const T*)d.pt_beta32;
+    const size_t toff = table < 0 ? 0 : (size_t)table * d.n_points * d.wmax;
+    const T* beta = table < 0 ? (std::is_same<T, double>::value ? (const T*)d.pt_beta64 : (const T*)d.pt_beta32)
+                              : (std::is_same<T, double>::value ? (const T*)d.pt_dbeta64 + toff
+                                                                : (const T*)d.pt_dbeta32 + toff);
     nl_proj_kernel<T, CPLX, WM, CB><<<grid, PROJ_THREADS, 0, s>>>(d.chunk_begin, d.chunk_end, d.pt_idx, d.pt_xyz, beta,
                                                                   d.wmax, (const T*)psi, N, nb, gx_dx, gy_dy, gz_dz,
                                                                   partial, ncol);
 }
 
 template <typename T, bool CPLX>
-void launch_proj_w(const NLDevice& d, int nb, const void* psi, size_t N, double gx_dx, double gy_dy, double gz_dz,
-                   double* partial, int ncol, cudaStream_t s) {
-    if (d.wmax <= 1) launch_proj<T, CPLX, 1>(d, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
-    else if (d.wmax <= 4) launch_proj<T, CPLX, 4>(d, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
-    else if (d.wmax <= 9) launch_proj<T, CPLX, 9>(d, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
-    else launch_proj<T, CPLX, 16>(d, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+void launch_proj_w(const NLDevice& d, int table, int nb, const void* psi, size_t N, double gx_dx, double gy_dy,
+                   double gz_dz, double* partial, int ncol, cudaStream_t s) {
+    if (d.wmax <= 1) launch_proj<T, CPLX, 1>(d, table, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+    else if (d.wmax <= 4) launch_proj<T, CPLX, 4>(d, table, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+    else if (d.wmax <= 9) launch_proj<T, CPLX, 9>(d, table, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+    else launch_proj<T, CPLX, 16>(d, table, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+}
+
+// Per atom (one block): energy = sum over bands and projectors of occ E_w |c|^2;
+// force_d = sum 2 occ E_w Re(conj(c) g_d) with c = dV <beta|psi>, g_d = dV <d beta/dd|psi>
+// (coefficient arrays [atom][w][col], complex bands as columns 2b, 2b+1).
+// Fixed-order block reduction: the result does not depend on timing.
+__global__ void nl_energy_force_kernel(const double* __restrict__ c, const double* __restrict__ gx,
+                                       const double* __restrict__ gy, const double* __restrict__ gz,
+                                       const double* __restrict__ atom_E, const int* __restrict__ atom_width, int wmax,
+                                       int nb, int is_complex, const double* __restrict__ occ, double* __restrict__ out) {
+    const int a = blockIdx.x;
+    const int wa = atom_width[a];
+    const int ncol = is_complex ? 2 * nb : nb;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int i = threadIdx.x; i < wa * nb; i += blockDim.x) {
+        const int w = i / nb, b = i % nb;
+        const double e = atom_E[(size_t)a * wmax + w] * occ[b];
+        const size_t base = ((size_t)a * wmax + w) * ncol;
+        const int c0 = is_complex ? 2 * b : b;
+        const double cr = c[base + c0], ci = is_complex ? c[base + c0 + 1] : 0.0;
+        acc[0] += e * (cr * cr + ci * ci);
+        if (gx) {
+            acc[1] += 2.0 * e * (cr * gx[base + c0] + (is_complex ? ci * gx[base + c0 + 1] : 0.0));
+            acc[2] += 2.0 * e * (cr * gy[base + c0] + (is_complex ? ci * gy[base + c0 + 1] : 0.0));
+            acc[3] += 2.0 * e * (cr * gz[base + c0] + (is_complex ? ci * gz[base + c0 + 1] : 0.0));
+        }
+    }
+    __shared__ double red[4][256];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) red[k][threadIdx.x] = acc[k];
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) out[(size_t)a * 4 + threadIdx.x] = red[threadIdx.x][0];
 }
 
 }  // namespace
@@ -271,8 +315,9 @@ void nl_free(NLDevice& d) {
     dfree(d.atom_chunk_begin); dfree(d.atom_chunk_end);
     dfree(d.grid_ptr); dfree(d.cov_grid); dfree(d.ent_atom); dfree(d.ent_xyz);
     dfree(d.ent_beta64); dfree(d.ent_beta32);
+    dfree(d.pt_dbeta64); dfree(d.pt_dbeta32);
     d.n_atoms = 0; d.wmax = 0; d.n_points = 0; d.total_proj = 0; d.n_chunks = 0; d.n_cov = 0;
-    d.h_atom_width.clear(); d.h_atom_proj_off.clear();
+    d.h_atom_width.clear(); d.h_atom_proj_off.clear(); d.h_npts.clear(); d.h_src.clear();
 }
 
 qsb_status nl_upload(NLDevice& d, int nx, int ny, int nz, int n_atoms, const int* npts, const int* widths,
@@ -295,6 +340,7 @@ qsb_status nl_upload(NLDevice& d, int nx, int ny, int nz, int n_atoms, const int
     d.n_points = total;
     d.total_proj = total_proj;
     d.h_atom_width.assign(widths, widths + n_atoms);
+    d.h_npts.assign(npts, npts + n_atoms);
     d.h_atom_proj_off.resize(n_atoms);
     {
         int off = 0;
@@ -308,6 +354,7 @@ qsb_status nl_upload(NLDevice& d, int nx, int ny, int nz, int n_atoms, const int
 
     // atom-major points, sorted by folded grid index within each atom
     std::vector<int> idx(total), xyz(3 * total), atom_of(total);
+    d.h_src.assign(total, 0);
     std::vector<double> b64((size_t)total * wmax, 0.0);
     std::vector<double> E((size_t)n_atoms * wmax, 0.0);
     std::vector<int> chunk_atom, chunk_b, chunk_e, acb(n_atoms), ace(n_atoms);
@@ -330,6 +377,7 @@ qsb_status nl_upload(NLDevice& d, int nx, int ny, int nz, int n_atoms, const int
                 const int64_t dst = off + i;
                 idx[dst] = fidx[src];
                 atom_of[dst] = a;
+                d.h_src[dst] = src;
                 for (int c = 0; c < 3; ++c) xyz[3 * dst + c] = coords[3 * (off + src) + c];
                 for (int k = 0; k < w; ++k) b64[(size_t)dst * wmax + k] = beta[boff + (int64_t)k * np + src];
             }
@@ -394,9 +442,10 @@ size_t nl_workspace_bytes(const NLDevice& d, int ncol) {
     return ((part + 255) / 256) * 256 + ((coef + 255) / 256) * 256;
 }
 
-qsb_status nl_project(qsb_dtype dt, const NLDevice& d, int nx, int ny, int nz, int nb, int is_complex,
-                      const void* psi, double dV, double gx_dx, double gy_dy, double gz_dz, bool inner_only, void* ws,
-                      double** coef_out, cudaStream_t s) {
+namespace {
+qsb_status nl_project_table(qsb_dtype dt, const NLDevice& d, int table, int nx, int ny, int nz, int nb,
+                            int is_complex, const void* psi, double dV, double gx_dx, double gy_dy, double gz_dz,
+                            bool inner_only, void* ws, double** coef_out, cudaStream_t s) {
     const size_t N = (size_t)nx * ny * nz;
     const int ncol = is_complex ? 2 * nb : nb;
     const size_t part = (size_t)d.n_chunks * d.wmax * ncol * sizeof(double);
@@ -406,16 +455,92 @@ qsb_status nl_project(qsb_dtype dt, const NLDevice& d, int nx, int ny, int nz, i
     if (d.n_points == 0) return QSB_OK;
     if ((nb + 7) / 8 > 65535) return fail(QSB_ERR_INVALID, "nonlocal: too many bands");
     if (dt == QSB_F64) {
-        if (is_complex) launch_proj_w<double, true>(d, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
-        else launch_proj_w<double, false>(d, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+        if (is_complex) launch_proj_w<double, true>(d, table, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+        else launch_proj_w<double, false>(d, table, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
     } else {
-        if (is_complex) launch_proj_w<float, true>(d, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
-        else launch_proj_w<float, false>(d, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+        if (is_complex) launch_proj_w<float, true>(d, table, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
+        else launch_proj_w<float, false>(d, table, nb, psi, N, gx_dx, gy_dy, gz_dz, partial, ncol, s);
     }
     QSB_CUDA_TRY(cudaGetLastError());
     nl_finalize_kernel<<<d.n_atoms, 256, 0, s>>>(d.atom_chunk_begin, d.atom_chunk_end, d.atom_E, d.atom_width, d.wmax,
                                                  partial, ncol, dV, inner_only ? 1 : 0, coef);
     QSB_CUDA_TRY(cudaGetLastError());
+    return QSB_OK;
+}
+}  // namespace
+
+qsb_status nl_project(qsb_dtype dt, const NLDevice& d, int nx, int ny, int nz, int nb, int is_complex,
+                      const void* psi, double dV, double gx_dx, double gy_dy, double gz_dz, bool inner_only, void* ws,
+                      double** coef_out, cudaStream_t s) {
+    return nl_project_table(dt, d, -1, nx, ny, nz, nb, is_complex, psi, dV, gx_dx, gy_dy, gz_dz, inner_only, ws,
+                            coef_out, s);
+}
+
+qsb_status nl_upload_gradients(NLDevice& d, const double* dbeta) {
+    if (d.n_points == 0 || d.wmax == 0) return QSB_OK;
+    if (!dbeta) return fail(QSB_ERR_INVALID, "set_projector_gradients: null table");
+    const size_t per_dir = (size_t)d.n_points * d.wmax;
+    std::vector<double> g64(3 * per_dir, 0.0);
+    int64_t off = 0, goff = 0;
+    for (int a = 0; a < d.n_atoms; ++a) {
+        const int np = d.h_npts[a], w = d.h_atom_width[a];
+        for (int i = 0; i < np; ++i) {
+            const int64_t dst = off + i;
+            const int src = d.h_src[dst];
+            for (int dir = 0; dir < 3; ++dir)
+                for (int k = 0; k < w; ++k)
+                    g64[dir * per_dir + (size_t)dst * d.wmax + k] =
+                        dbeta[goff + (int64_t)dir * np * w + (int64_t)k * np + src];
+        }
+        off += np;
+        goff += (int64_t)3 * np * w;
+    }
+    std::vector<float> g32(g64.begin(), g64.end());
+    dfree(d.pt_dbeta64);
+    dfree(d.pt_dbeta32);
+    QSB_CUDA_TRY(cudaMalloc((void**)&d.pt_dbeta64, g64.size() * sizeof(double)));
+    QSB_CUDA_TRY(cudaMalloc((void**)&d.pt_dbeta32, g32.size() * sizeof(float)));
+    QSB_CUDA_TRY(cudaMemcpy(d.pt_dbeta64, g64.data(), g64.size() * sizeof(double), cudaMemcpyHostToDevice));
+    QSB_CUDA_TRY(cudaMemcpy(d.pt_dbeta32, g32.data(), g32.size() * sizeof(float), cudaMemcpyHostToDevice));
+    return QSB_OK;
+}
+
+size_t nl_energy_force_bytes(const NLDevice& d, int ncol, int nb) {
+    const size_t one = nl_workspace_bytes(d, ncol);
+    return 4 * one + (((size_t)d.n_atoms * 4 + nb) * sizeof(double) + 256);
+}
+
+qsb_status nl_energy_force(qsb_dtype dt, const NLDevice& d, int nx, int ny, int nz, int nb, int is_complex,
+                           const void* psi, const double* occ_host, double dV, double gx_dx, double gy_dy,
+                           double gz_dz, double* energy, double* forces, void* ws, cudaStream_t s) {
+    *energy = 0.0;
+    if (d.n_points == 0 || nb == 0) return QSB_OK;
+    if (forces && !d.pt_dbeta64) return fail(QSB_ERR_STATE, "nonlocal forces: no projector gradients set");
+    const int ncol = is_complex ? 2 * nb : nb;
+    const size_t one = nl_workspace_bytes(d, ncol);
+    unsigned char* w = (unsigned char*)ws;
+    double* coef[4] = {nullptr, nullptr, nullptr, nullptr};
+    const int ntab = forces ? 4 : 1;
+    for (int t = 0; t < ntab; ++t)
+        QSB_TRY(nl_project_table(dt, d, t - 1, nx, ny, nz, nb, is_complex, psi, dV, gx_dx, gy_dy, gz_dz, true,
+                                 w + t * one, &coef[t], s));
+    double* out = (double*)(w + 4 * one);
+    double* occ = out + (size_t)d.n_atoms * 4;
+    QSB_CUDA_TRY(cudaMemcpyAsync(occ, occ_host, sizeof(double) * nb, cudaMemcpyHostToDevice, s));
+    nl_energy_force_kernel<<<d.n_atoms, 256, 0, s>>>(coef[0], coef[1], coef[2], coef[3], d.atom_E, d.atom_width,
+                                                     d.wmax, nb, is_complex, occ, out);
+    QSB_CUDA_TRY(cudaGetLastError());
+    std::vector<double> h((size_t)d.n_atoms * 4);
+    QSB_CUDA_TRY(cudaMemcpyAsync(h.data(), out, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s));
+    QSB_CUDA_TRY(cudaStreamSynchronize(s));
+    double e = 0.0;
+    for (int a = 0; a < d.n_atoms; ++a) {
+        e += h[(size_t)a * 4];
+        if (forces)
+            for (int k = 0; k < 3; ++k) forces[3 * a + k] += h[(size_t)a * 4 + 1 + k];
+    }
+    if (!std::isfinite(e)) return fail(QSB_ERR_NUMERIC, "nonlocal energy: non-finite value");
+    *energy = e;
     return QSB_OK;
 }
 

@@ -87,9 +87,15 @@ struct NLDevice {
     int* ent_xyz = nullptr;        // [n_points][3]
     double* ent_beta64 = nullptr;  // [n_points][wmax]
     float* ent_beta32 = nullptr;
+    // projector gradients d beta / d(x, y, z) of the point coordinate, same
+    // layout as pt_beta per direction: [3][point][wmax] (optional; forces)
+    double* pt_dbeta64 = nullptr;
+    float* pt_dbeta32 = nullptr;
     // host copies kept for bookkeeping
     std::vector<int> h_atom_width;
     std::vector<int> h_atom_proj_off;
+    std::vector<int> h_npts;
+    std::vector<int> h_src;        // per atom-major sorted point: its index in the caller's order within its atom
 };
 
 void nl_free(NLDevice& d);
@@ -98,6 +104,16 @@ qsb_status nl_upload(NLDevice& d, int nx, int ny, int nz, int n_atoms, const int
 
 // Workspace needed by nl_project for nb bands (bytes).
 size_t nl_workspace_bytes(const NLDevice& d, int ncol);
+// Gradient tables in the caller's layout: per atom three blocks (d/dx, d/dy,
+// d/dz), each npts x width column-major, atoms concatenated in order.
+qsb_status nl_upload_gradients(NLDevice& d, const double* dbeta);
+// Workspace of nl_energy_force.
+size_t nl_energy_force_bytes(const NLDevice& d, int ncol, int nb);
+// Nonlocal band energy sum_n occ_n sum_a,w E_w |<beta|psi_n>|^2 and, when
+// forces != nullptr (host, 3 per atom, "+="), F_a = sum 2 occ E_w Re(<psi|beta><grad beta|psi>).
+qsb_status nl_energy_force(qsb_dtype dt, const NLDevice& d, int nx, int ny, int nz, int nb, int is_complex,
+                           const void* psi, const double* occ_host, double dV, double gx_dx, double gy_dy,
+                           double gz_dz, double* energy, double* forces, void* ws, cudaStream_t s);
 // coef[atom][w][col] = dV * E_w * <beta|psi_col> (Bloch-phased for complex); ws must hold
 // nl_workspace_bytes.  If inner_only, the E_w factor is omitted.
 qsb_status nl_project(qsb_dtype dt, const NLDevice& d, int nx, int ny, int nz, int nb, int is_complex,

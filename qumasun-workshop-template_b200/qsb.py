@@ -178,6 +178,34 @@ class Hamiltonian:
         _check(lib.qsb_ham_projector_info(self._h, ctypes.byref(tp), ctypes.byref(tw)))
         return tp.value, tw.value
 
+    def set_projector_gradients(self, dbeta):
+        """dbeta: per atom (d/dx, d/dy, d/dz) blocks of npts x width column-major, concatenated."""
+        g = np.ascontiguousarray(dbeta, dtype=np.float64)
+        _check(lib.qsb_ham_set_projector_gradients(self._h, g.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+
+    def nonlocal_energy(self, psi, occupancies, is_complex=False, g=(0.0, 0.0, 0.0)):
+        nb = self._nb(psi, is_complex)
+        occ = np.ascontiguousarray(occupancies, dtype=np.float64)
+        assert occ.size == nb
+        e = ctypes.c_double()
+        _check(lib.qsb_ham_nonlocal_energy(self._h, _dtype_code(psi), int(is_complex), nb, _dev_ptr(psi),
+                                           occ.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _c_d(g[0]),
+                                           _c_d(g[1]), _c_d(g[2]), ctypes.byref(e), _stream_ptr(psi)))
+        return e.value
+
+    def nonlocal_energy_force(self, psi, occupancies, n_atoms, is_complex=False, g=(0.0, 0.0, 0.0)):
+        """(energy, forces[n_atoms, 3]) of the nonlocal part."""
+        nb = self._nb(psi, is_complex)
+        occ = np.ascontiguousarray(occupancies, dtype=np.float64)
+        assert occ.size == nb
+        f = np.zeros((n_atoms, 3))
+        e = ctypes.c_double()
+        _check(lib.qsb_ham_nonlocal_energy_force(self._h, _dtype_code(psi), int(is_complex), nb, _dev_ptr(psi),
+                                                 occ.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _c_d(g[0]),
+                                                 _c_d(g[1]), _c_d(g[2]), ctypes.byref(e),
+                                                 f.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _stream_ptr(psi)))
+        return e.value, f
+
     def set_timing(self, enable=True):
         _check(lib.qsb_ham_set_timing(self._h, int(bool(enable))))
 
