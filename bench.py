@@ -236,6 +236,53 @@ def cpu_baseline_sample():
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
+def gram_section(N, p, stream, reps=5):
+    """The mixed-precision Rayleigh-Ritz Gram at the LOBPCG shape of this
+    workload (U^T U over N grid points, p = 3 x bands fp32 columns, upper
+    tiles): split-BF16x3 and INT8 Ozaki on the tensor cores (split included),
+    against the fp64 DGEMM of the drop-in.  TFLOP/s are algorithmic for the
+    full p x p product (2 N p^2), whatever part of it a kernel computes."""
+    import ctypes
+    import torch
+    import qsb
+    U = torch.rand(p, N, dtype=torch.float32, device="cuda") - 0.5
+    T = torch.empty(p, p, dtype=torch.float64, device="cuda")
+    out = {"grid_points": N, "columns": p, "upper_tiles": True}
+    for name, wsq, fn in (("bf16x3", qsb.lib.qsb_gram_bf16x3_workspace, qsb.lib.qsb_gram_bf16x3),
+                          ("int8_ozaki", qsb.lib.qsb_gram_ozaki_int8_workspace, qsb.lib.qsb_gram_ozaki_int8)):
+        nbytes = ctypes.c_size_t()
+        assert wsq(ctypes.c_int64(N), p, p, 1, ctypes.byref(nbytes)) == 0
+        ws = torch.empty(nbytes.value, dtype=torch.uint8, device="cuda")
+        call = lambda: fn(1, ctypes.c_int64(N), p, p, ctypes.c_void_p(U.data_ptr()), ctypes.c_void_p(U.data_ptr()),
+                          ctypes.c_void_p(T.data_ptr()), p, 1, ctypes.c_void_p(ws.data_ptr()),
+                          ctypes.c_size_t(nbytes.value), ctypes.c_void_p(stream.cuda_stream))
+        assert call() == 0
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            call()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out[name] = {"ms": ms, "tflops_algorithmic": 2.0 * N * p * p / (ms * 1e-3) / 1e12}
+        del ws
+    U64 = U.double()
+    U64 @ U64.t()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        U64 @ U64.t()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    out["fp64_dgemm"] = {"ms": ms, "tflops_algorithmic": 2.0 * N * p * p / (ms * 1e-3) / 1e12}
+    del U, U64, T
+    torch.cuda.empty_cache()
+    return out
+
+
 NB_OCC = 48          # 16 atoms x 6 valence electrons / 2 (spin-paired)
 EIG_TOL = 1e-6       # Ha, every occupied eigenvalue against the FP64 converged values
 
@@ -409,8 +456,9 @@ def main():
 
     # ---- block LOBPCG on the same H: FP64 drop-in vs mixed precision ----------
     lob = None
+    gram = gram_section(N, 3 * NB, stream)
     if not args.no_lobpcg:
-        lob = lobpcg_section(H, psi, N, NB, H_GRID ** 3, n_occ=NB_OCC, stream=stream)
+        lob = lobpcg_section(H, psi, N, NB, H_GRID ** 3, n_occ=min(NB_OCC, NB), stream=stream)
     clk = clocks.stop()
 
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist, "cuda")
@@ -448,6 +496,7 @@ def main():
                 "ms_per_step": e2e_ms},
         "gpu_launches": launches,
         "lobpcg": lob,
+        "gram": gram,
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

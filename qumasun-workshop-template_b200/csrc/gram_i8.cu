@@ -81,15 +81,39 @@ __device__ __forceinline__ int column_of(const ColumnSet& src, int col, const vo
     return local;
 }
 
+// Four consecutive elements of a column (zero past N); one 16-byte (fp32) or
+// two 16-byte (fp64) loads when the column start is 16-byte aligned.
+template <typename T>
+__device__ __forceinline__ void load4(const T* __restrict__ s, int64_t i, int64_t N, bool vec, double (&v)[4]) {
+    if (vec && i + 3 < N) {
+        if constexpr (sizeof(T) == 4) {
+            const float4 f = __ldg(reinterpret_cast<const float4*>(s + i));
+            v[0] = f.x; v[1] = f.y; v[2] = f.z; v[3] = f.w;
+        } else {
+            const double2 a = __ldg(reinterpret_cast<const double2*>(s + i));
+            const double2 b = __ldg(reinterpret_cast<const double2*>(s + i + 2));
+            v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[j] = (i + j < N) ? (double)s[i + j] : 0.0;
+    }
+}
+
 // maxbits[col] = bits of max_i |u_i,col| (non-negative doubles order like their bits)
 template <typename T>
 __global__ void column_absmax_kernel(ColumnSet src, int64_t N, unsigned long long* __restrict__ maxbits) {
     const void* b;
     const int local = column_of(src, blockIdx.y, &b);
     const T* s = static_cast<const T*>(b) + (size_t)local * N;
+    const bool vec = ((uintptr_t)s % 16) == 0;
     double m = 0.0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
-        m = fmax(m, fabs((double)s[i]));
+    const int64_t n4 = (N + 3) / 4;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += (int64_t)gridDim.x * blockDim.x) {
+        double v[4];
+        load4<T>(s, 4 * q, N, vec, v);
+        m = fmax(m, fmax(fmax(fabs(v[0]), fabs(v[1])), fmax(fabs(v[2]), fabs(v[3]))));
+    }
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
     __shared__ double red[32];
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
@@ -105,7 +129,8 @@ __device__ __forceinline__ int column_exponent(unsigned long long bits) {
     return m > 0.0 ? ilogb(m) - 5 : 0;   // max |u| 2^-e in [32, 64)
 }
 
-// Three int8 slices of column col (length ldk, rows N..ldk zero) and its exponent.
+// Three int8 slices of column col (length ldk, a multiple of 4; rows N..ldk
+// zero) and its exponent; four elements per thread, one 4-byte store per slice.
 template <typename T>
 __global__ void slice_kernel(ColumnSet src, int64_t N, int64_t ldk, const unsigned long long* __restrict__ maxbits,
                              int8_t* __restrict__ slices, size_t slice_stride, int* __restrict__ exps) {
@@ -113,26 +138,34 @@ __global__ void slice_kernel(ColumnSet src, int64_t N, int64_t ldk, const unsign
     const void* b;
     const int local = column_of(src, col, &b);
     const T* s = static_cast<const T*>(b) + (size_t)local * N;
+    const bool vec = ((uintptr_t)s % 16) == 0;
     const int e = column_exponent(maxbits[col]);
     if (blockIdx.x == 0 && threadIdx.x == 0) exps[col] = e;
     int8_t* o0 = slices + (size_t)col * ldk;
     int8_t* o1 = o0 + slice_stride;
     int8_t* o2 = o0 + 2 * slice_stride;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ldk; i += (int64_t)gridDim.x * blockDim.x) {
-        int a = 0, c = 0, d = 0;
-        if (i < N) {
-            const double x = ldexp((double)s[i], -e);
+    const int64_t n4 = ldk / 4;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = 4 * q;
+        double v[4];
+        load4<T>(s, i, N, vec, v);
+        char4 a, c, d;
+        signed char* pa = &a.x;
+        signed char* pc = &c.x;
+        signed char* pd = &d.x;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double x = ldexp(v[j], -e);
             const double q0 = rint(x);
             const double r1 = (x - q0) * 128.0;
             const double q1 = rint(r1);
-            const double q2 = rint((r1 - q1) * 128.0);
-            a = (int)q0;
-            c = (int)q1;
-            d = (int)q2;
+            pa[j] = (signed char)(int)q0;
+            pc[j] = (signed char)(int)q1;
+            pd[j] = (signed char)(int)rint((r1 - q1) * 128.0);
         }
-        o0[i] = (int8_t)a;
-        o1[i] = (int8_t)c;
-        o2[i] = (int8_t)d;
+        *reinterpret_cast<char4*>(o0 + i) = a;
+        *reinterpret_cast<char4*>(o1 + i) = c;
+        *reinterpret_cast<char4*>(o2 + i) = d;
     }
 }
 
@@ -349,7 +382,7 @@ qsb_status ozaki_split(qsb_dtype dt, int64_t N, const ColumnSet& src, void* dst,
     int* exps = (int*)(w + 3 * stride);
     unsigned long long* maxbits = (unsigned long long*)(w + 3 * stride + a1k((size_t)cols * sizeof(int)));
     QSB_CUDA_TRY(cudaMemsetAsync(maxbits, 0, (size_t)cols * sizeof(unsigned long long), s));
-    const int cblocks = (int)std::min<int64_t>((ldk + 255) / 256, 512);
+    const int cblocks = (int)std::min<int64_t>((ldk / 4 + 255) / 256, 256);
     if (dt == QSB_F64) {
         column_absmax_kernel<double><<<dim3(cblocks, cols), 256, 0, s>>>(src, N, maxbits);
         slice_kernel<double><<<dim3(cblocks, cols), 256, 0, s>>>(src, N, ldk, maxbits, (int8_t*)w, stride, exps);

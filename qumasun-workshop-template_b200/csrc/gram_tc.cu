@@ -60,9 +60,10 @@ __device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint6
 }
 
 // Column c of the gathered operand (fp32 or fp64, one column every N elements)
-// -> hi, lo bf16 columns of length ldk (rows N..ldk zero).  The columns come
-// from up to kMaxSegments arrays, so the active bands of separate bundles form
-// one operand without a copy.
+// -> hi, lo bf16 columns of length ldk (a multiple of 4; rows N..ldk zero).
+// The columns come from up to kMaxSegments arrays, so the active bands of
+// separate bundles form one operand without a copy.  Four elements per thread:
+// 16-byte loads when the column start allows, one 8-byte store per half.
 template <typename T>
 __global__ void split_bf16_kernel(ColumnSet src, int64_t N, int64_t ldk, __nv_bfloat16* __restrict__ hi,
                                   __nv_bfloat16* __restrict__ lo) {
@@ -82,19 +83,39 @@ __global__ void split_bf16_kernel(ColumnSet src, int64_t N, int64_t ldk, __nv_bf
         }
     }
     const T* s = static_cast<const T*>(b) + (size_t)local * N;
+    const bool vec = ((uintptr_t)s % 16) == 0;
     __nv_bfloat16* h = hi + (size_t)col * ldk;
     __nv_bfloat16* l = lo + (size_t)col * ldk;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ldk; i += (int64_t)gridDim.x * blockDim.x) {
-        if (i < N) {
-            const double v = (double)s[i];
-            const __nv_bfloat16 vh = __float2bfloat16_rn((float)v);
-            const __nv_bfloat16 vl = __float2bfloat16_rn((float)(v - (double)__bfloat162float(vh)));
-            h[i] = vh;
-            l[i] = vl;
+    const int64_t n4 = ldk / 4;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = 4 * q;
+        double v[4];
+        if (vec && i + 3 < N) {
+            if constexpr (sizeof(T) == 4) {
+                const float4 f = __ldg(reinterpret_cast<const float4*>(s + i));
+                v[0] = f.x; v[1] = f.y; v[2] = f.z; v[3] = f.w;
+            } else {
+                const double2 x0 = __ldg(reinterpret_cast<const double2*>(s + i));
+                const double2 x1 = __ldg(reinterpret_cast<const double2*>(s + i + 2));
+                v[0] = x0.x; v[1] = x0.y; v[2] = x1.x; v[3] = x1.y;
+            }
         } else {
-            h[i] = __float2bfloat16_rn(0.0f);
-            l[i] = __float2bfloat16_rn(0.0f);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = (i + j < N) ? (double)s[i + j] : 0.0;
         }
+        __nv_bfloat162 h01, h23, l01, l23;
+        __nv_bfloat16 hv[4], lv[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            hv[j] = __float2bfloat16_rn((float)v[j]);
+            lv[j] = __float2bfloat16_rn((float)(v[j] - (double)__bfloat162float(hv[j])));
+        }
+        h01.x = hv[0]; h01.y = hv[1]; h23.x = hv[2]; h23.y = hv[3];
+        l01.x = lv[0]; l01.y = lv[1]; l23.x = lv[2]; l23.y = lv[3];
+        reinterpret_cast<__nv_bfloat162*>(h + i)[0] = h01;
+        reinterpret_cast<__nv_bfloat162*>(h + i)[1] = h23;
+        reinterpret_cast<__nv_bfloat162*>(l + i)[0] = l01;
+        reinterpret_cast<__nv_bfloat162*>(l + i)[1] = l23;
     }
 }
 
@@ -338,7 +359,7 @@ qsb_status split_bf16(qsb_dtype dt, int64_t N, const ColumnSet& src, void* dst, 
     const int64_t ldk = split_ldk(N);
     __nv_bfloat16* hi = (__nv_bfloat16*)dst;
     __nv_bfloat16* lo = (__nv_bfloat16*)((unsigned char*)dst + split_half_bytes(N, cols));
-    const int cblocks = (int)std::min<int64_t>((ldk + 255) / 256, 512);
+    const int cblocks = (int)std::min<int64_t>((ldk / 4 + 255) / 256, 256);
     if (dt == QSB_F64)
         split_bf16_kernel<double><<<dim3(cblocks, cols), 256, 0, s>>>(src, N, ldk, hi, lo);
     else
