@@ -167,11 +167,16 @@ nl_apply_kernel(const int* __restrict__ cov_grid, int n_cov, const int* __restri
                 const int* __restrict__ ent_atom, const int* __restrict__ ent_xyz, const T* __restrict__ ent_beta,
                 int wmax, const double* __restrict__ coef, int ncol, T* __restrict__ hpsi, size_t N, int nb,
                 double gx_dx, double gy_dy, double gz_dz) {
-    constexpr int MAXE = 4;
+    // entries held in registers at a time
+    constexpr int MAXE = CPLX ? (WM <= 4 ? 2 : 1) : (WM <= 4 ? 4 : (WM <= 9 ? 2 : 1));
+    constexpr int BG = CPLX ? 4 : 8;   // bands per group
+    constexpr int CG = 8;              // coefficient columns per group: BG real, 2 BG complex
     const int r = blockIdx.x * APPLY_THREADS + threadIdx.x;
     if (r >= n_cov) return;
     const int g = __ldg(cov_grid + r);
     const int e0 = __ldg(grid_ptr + g), e1 = __ldg(grid_ptr + g + 1);
+    // coefficient rows are read 8 columns at a time as four 16-byte loads
+    const bool vec = (ncol % 2 == 0) && (((uintptr_t)coef) % 16 == 0);
     for (int eb = e0; eb < e1; eb += MAXE) {
         const int ne = min(MAXE, e1 - eb);
         const double* cf[MAXE];
@@ -193,52 +198,62 @@ nl_apply_kernel(const int* __restrict__ cov_grid, int n_cov, const int* __restri
                 sincos(kxx + kyy + kzz, &sn[q], &cs[q]);
             }
         }
-        // bands in groups of BG: all hpsi loads of a group are issued before any
-        // use, so BG (x2 for complex) independent loads per thread are in flight
-        constexpr int BG = CPLX ? 4 : 8;
         for (int b0 = 0; b0 < nb; b0 += BG) {
-            T cur[BG][CPLX ? 2 : 1];
+            const int c0 = CPLX ? 2 * b0 : b0;
+            const bool full = vec && (b0 + BG <= nb);
+            // hpsi of the group first: CG independent loads in flight
+            T cur[CG];
 #pragma unroll
-            for (int j = 0; j < BG; ++j) {
-                const int bnd = min(b0 + j, nb - 1);
-                if (CPLX) {
-                    cur[j][0] = hpsi[(size_t)(2 * bnd) * N + g];
-                    cur[j][CPLX ? 1 : 0] = hpsi[(size_t)(2 * bnd + 1) * N + g];
-                } else {
-                    cur[j][0] = hpsi[(size_t)bnd * N + g];
+            for (int k = 0; k < CG; ++k) {
+                const int col = c0 + k;
+                cur[k] = (col < ncol) ? hpsi[(size_t)col * N + g] : T(0);
+            }
+            double acc[CG];
+#pragma unroll
+            for (int k = 0; k < CG; ++k) acc[k] = 0.0;
+#pragma unroll
+            for (int q = 0; q < MAXE; ++q) {
+                if (q < ne) {
+                    double tq[CG];
+#pragma unroll
+                    for (int k = 0; k < CG; ++k) tq[k] = 0.0;
+#pragma unroll
+                    for (int w = 0; w < WM; ++w) {
+                        if (w < wmax) {
+                            const double* row = cf[q] + (size_t)w * ncol + c0;
+                            double c[CG];
+                            if (full) {
+#pragma unroll
+                                for (int k = 0; k < CG; k += 2) {
+                                    const double2 v = __ldg(reinterpret_cast<const double2*>(row + k));
+                                    c[k] = v.x;
+                                    c[k + 1] = v.y;
+                                }
+                            } else {
+#pragma unroll
+                                for (int k = 0; k < CG; ++k) c[k] = (c0 + k < ncol) ? __ldg(row + k) : 0.0;
+                            }
+#pragma unroll
+                            for (int k = 0; k < CG; ++k) tq[k] += b[q][w] * c[k];
+                        }
+                    }
+                    if (CPLX) {
+                        // exp(-i k.r) (source/PseudoPotNonlocal_SvF2_kpoint.h:4026-4027)
+#pragma unroll
+                        for (int j = 0; j < BG; ++j) {
+                            acc[2 * j] += cs[q] * tq[2 * j] + sn[q] * tq[2 * j + 1];
+                            acc[2 * j + 1] += cs[q] * tq[2 * j + 1] - sn[q] * tq[2 * j];
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < CG; ++k) acc[k] += tq[k];
+                    }
                 }
             }
 #pragma unroll
-            for (int j = 0; j < BG; ++j) {
-                const int bnd = b0 + j;
-                if (bnd >= nb) break;
-                if (CPLX) {
-                    double ar = 0.0, ai = 0.0;
-#pragma unroll
-                    for (int q = 0; q < MAXE; ++q) {
-                        double tr = 0.0, ti = 0.0;
-#pragma unroll
-                        for (int w = 0; w < WM; ++w) {
-                            if (w < wmax) {
-                                tr += b[q][w] * __ldg(cf[q] + (size_t)w * ncol + 2 * bnd);
-                                ti += b[q][w] * __ldg(cf[q] + (size_t)w * ncol + 2 * bnd + 1);
-                            }
-                        }
-                        // exp(-i k.r) (source/PseudoPotNonlocal_SvF2_kpoint.h:4026-4027)
-                        ar += cs[q] * tr + sn[q] * ti;
-                        ai += cs[q] * ti - sn[q] * tr;
-                    }
-                    hpsi[(size_t)(2 * bnd) * N + g] = cur[j][0] + (T)ar;
-                    hpsi[(size_t)(2 * bnd + 1) * N + g] = cur[j][CPLX ? 1 : 0] + (T)ai;
-                } else {
-                    double acc = 0.0;
-#pragma unroll
-                    for (int q = 0; q < MAXE; ++q)
-#pragma unroll
-                        for (int w = 0; w < WM; ++w)
-                            if (w < wmax) acc += b[q][w] * __ldg(cf[q] + (size_t)w * ncol + bnd);
-                    hpsi[(size_t)bnd * N + g] = cur[j][0] + (T)acc;
-                }
+            for (int k = 0; k < CG; ++k) {
+                const int col = c0 + k;
+                if (col < ncol) hpsi[(size_t)col * N + g] = cur[k] + (T)acc[k];
             }
         }
     }
