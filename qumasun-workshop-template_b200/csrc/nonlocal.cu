@@ -77,26 +77,51 @@ nl_proj_kernel(const int* __restrict__ chunk_begin, const int* __restrict__ chun
 #pragma unroll
     for (int i = 0; i < NV; ++i) acc[i] = 0.0;
 
-    for (int p = p0 + threadIdx.x; p < p1; p += PROJ_THREADS) {
-        const int idx = __ldg(pt_idx + p);
-        double b[WM];
+    // UP points per thread per pass: their index and psi loads are all issued
+    // before the first use, so UP x CB (x2 complex) gathers are in flight
+    constexpr int UP = (WM <= 4 && !CPLX) ? 2 : 1;
+    for (int pb = p0 + threadIdx.x; pb < p1; pb += PROJ_THREADS * UP) {
+        int idx[UP];
+        bool live[UP];
 #pragma unroll
-        for (int w = 0; w < WM; ++w) b[w] = (w < wmax) ? (double)__ldg(pt_beta + (size_t)p * wmax + w) : 0.0;
-        double cs = 1.0, sn = 0.0;
-        if (CPLX) {
-            // mCreateBlochExp (source/PseudoPotNonlocal_SvF2_kpoint.h:3580-3590)
-            const double kxx = gx_dx * (double)__ldg(pt_xyz + 3 * (size_t)p + 0);
-            const double kyy = gy_dy * (double)__ldg(pt_xyz + 3 * (size_t)p + 1);
-            const double kzz = gz_dz * (double)__ldg(pt_xyz + 3 * (size_t)p + 2);
-            sincos(kxx + kyy + kzz, &sn, &cs);
+        for (int u = 0; u < UP; ++u) {
+            const int p = pb + u * PROJ_THREADS;
+            live[u] = p < p1;
+            idx[u] = live[u] ? __ldg(pt_idx + p) : 0;
         }
+        double vals[UP][CPLX ? 2 * CB : CB];
 #pragma unroll
-        for (int j = 0; j < CB; ++j) {
-            if (j < nbl) {
+        for (int u = 0; u < UP; ++u)
+#pragma unroll
+            for (int j = 0; j < CB; ++j) {
+                const bool ok = live[u] && j < nbl;
                 if (CPLX) {
                     const size_t base = (size_t)(2 * (band0 + j)) * N;
-                    const double pr = (double)__ldg(psi + base + idx);
-                    const double pi = (double)__ldg(psi + base + N + idx);
+                    vals[u][2 * j] = ok ? (double)__ldg(psi + base + idx[u]) : 0.0;
+                    vals[u][2 * j + 1] = ok ? (double)__ldg(psi + base + N + idx[u]) : 0.0;
+                } else {
+                    vals[u][j] = ok ? (double)__ldg(psi + (size_t)(band0 + j) * N + idx[u]) : 0.0;
+                }
+            }
+#pragma unroll
+        for (int u = 0; u < UP; ++u) {
+            if (!live[u]) continue;
+            const int p = pb + u * PROJ_THREADS;
+            double b[WM];
+#pragma unroll
+            for (int w = 0; w < WM; ++w) b[w] = (w < wmax) ? (double)__ldg(pt_beta + (size_t)p * wmax + w) : 0.0;
+            double cs = 1.0, sn = 0.0;
+            if (CPLX) {
+                // mCreateBlochExp (source/PseudoPotNonlocal_SvF2_kpoint.h:3580-3590)
+                const double kxx = gx_dx * (double)__ldg(pt_xyz + 3 * (size_t)p + 0);
+                const double kyy = gy_dy * (double)__ldg(pt_xyz + 3 * (size_t)p + 1);
+                const double kzz = gz_dz * (double)__ldg(pt_xyz + 3 * (size_t)p + 2);
+                sincos(kxx + kyy + kzz, &sn, &cs);
+            }
+#pragma unroll
+            for (int j = 0; j < CB; ++j) {
+                if (CPLX) {
+                    const double pr = vals[u][2 * j], pi = vals[u][2 * j + 1];
                     const double fr = cs * pr - sn * pi;   // :4514-4515
                     const double fi = cs * pi + sn * pr;
 #pragma unroll
@@ -105,9 +130,8 @@ nl_proj_kernel(const int* __restrict__ chunk_begin, const int* __restrict__ chun
                         acc[w * NCB + 2 * j + 1] += b[w] * fi;
                     }
                 } else {
-                    const double v = (double)__ldg(psi + (size_t)(band0 + j) * N + idx);
 #pragma unroll
-                    for (int w = 0; w < WM; ++w) acc[w * NCB + j] += b[w] * v;
+                    for (int w = 0; w < WM; ++w) acc[w * NCB + j] += b[w] * vals[u][j];
                 }
             }
         }
