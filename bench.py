@@ -337,6 +337,7 @@ def lobpcg_section(H, psi, N, NB, dV, n_occ, stream, max_calls=60):
         if prec == "mixed":
             out[prec]["overlap_dropped_max"], out[prec]["overlap_min_kept"], out[prec]["drop_tolerance"] = \
                 es.overlap_stats()
+            out[prec]["last_call_cholesky_solves"], out[prec]["last_call_overlap_basis_solves"] = es.solve_stats()
         es.close()
         del X, keep
         torch.cuda.empty_cache()

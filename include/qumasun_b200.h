@@ -265,6 +265,12 @@ QSB_API qsb_status qsb_eigensolver_set_drop_tolerance(qsb_eigensolver* es, doubl
  * BF16 solvers diverge, the INT8 one converges. */
 typedef enum qsb_gram_kind { QSB_GRAM_BF16X3 = 3, QSB_GRAM_BF16X4 = 4, QSB_GRAM_INT8_OZAKI = 8 } qsb_gram_kind;
 QSB_API qsb_status qsb_eigensolver_set_gram_kind(qsb_eigensolver* es, qsb_gram_kind kind);
+/* Of the last call (mixed precision): how many Rayleigh-Ritz steps were solved
+ * by the Cholesky route (?hegvd on the unit-diagonal-scaled pencil, tried
+ * first) and how many fell back to the overlap-basis solve because that
+ * Cholesky found the overlap not positive definite. */
+QSB_API qsb_status qsb_eigensolver_solve_stats(const qsb_eigensolver* es, int* cholesky_solves,
+                                               int* overlap_basis_solves);
 /* Of the last call (mixed precision): most directions dropped in one
  * iteration, smallest kept overlap eigenvalue relative to the largest, and the
  * tolerance in force. */

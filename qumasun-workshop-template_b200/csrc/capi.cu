@@ -11,6 +11,8 @@ namespace qsb {
 
 static thread_local std::string g_last_error;
 
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
 qsb_status fail(qsb_status st, const std::string& msg) {
     g_last_error = msg;
     return st;

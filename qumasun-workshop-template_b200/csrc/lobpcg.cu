@@ -257,6 +257,8 @@ struct qsb_eigensolver {
     double* svq = nullptr;   // overlap-basis pencil solve: W, scratch, reduced matrix (m x m each), lambda, d
     double drop_tol = 0.0;   // overlap eigenvalues below drop_tol * max are dropped
     int gram_kind = QSB_GRAM_INT8_OZAKI;   // Gram products: BF16x3, BF16x4 or INT8 Ozaki
+    int last_chol = 0;       // pencil solves of the last call by Cholesky (?hegvd on the scaled pencil)
+    int last_svqb = 0;       // ... and by the overlap-basis fallback
     int last_dropped = 0;    // most directions dropped in one iteration of the last call
     double last_min_kept = 1.0;   // smallest kept overlap eigenvalue / max in the last call
     qsb_apply_f32_fn op32 = nullptr;
@@ -607,6 +609,24 @@ qsb_status solve_pencil_overlap_basis(qsb_eigensolver* es, int m, int nout, cuda
     pencil_diag<<<(m + 127) / 128, 128, 0, s>>>(es->Sb, m, es->cplx, d);
     pencil_scale<<<dim3((m + 127) / 128, m), 128, 0, s>>>(es->Sa, es->Sb, m, es->cplx, d);
     QSB_CUDA_TRY(cudaGetLastError());
+    // First the Cholesky route (one eigendecomposition): with an unbiased Gram the
+    // scaled overlap stays numerically positive definite in most iterations.
+    // The scaled pencil is kept in Wm / tmp for the fallback.
+    if (es->gram_kind == QSB_GRAM_INT8_OZAKI) {
+        QSB_CUDA_TRY(cudaMemcpyAsync(Wm, es->Sa, sizeof(double) * mm, cudaMemcpyDeviceToDevice, s));
+        QSB_CUDA_TRY(cudaMemcpyAsync(tmp, es->Sb, sizeof(double) * mm, cudaMemcpyDeviceToDevice, s));
+        const std::string saved_error = qsb_last_error();
+        if (solve_pencil(es, m, s) == QSB_OK) {
+            rows_scale<<<dim3((m + 127) / 128, nout), 128, 0, s>>>(es->Sa, d, m, nout, es->cplx, es->Sa);
+            QSB_CUDA_TRY(cudaGetLastError());
+            ++es->last_chol;
+            return QSB_OK;
+        }
+        set_last_error(saved_error);   // a failed Cholesky here is expected, not an error of the call
+        QSB_CUDA_TRY(cudaMemcpyAsync(es->Sa, Wm, sizeof(double) * mm, cudaMemcpyDeviceToDevice, s));
+        QSB_CUDA_TRY(cudaMemcpyAsync(es->Sb, tmp, sizeof(double) * mm, cudaMemcpyDeviceToDevice, s));
+    }
+    ++es->last_svqb;
     QSB_TRY(dense_evd(es, m, es->Sb, m, lam, s));
     std::vector<double> hl(m);
     QSB_CUDA_TRY(cudaMemcpyAsync(hl.data(), lam, sizeof(double) * m, cudaMemcpyDeviceToHost, s));
@@ -1041,6 +1061,13 @@ qsb_status qsb_eigensolver_set_gram_kind(qsb_eigensolver* es, qsb_gram_kind kind
     return QSB_OK;
 }
 
+qsb_status qsb_eigensolver_solve_stats(const qsb_eigensolver* es, int* cholesky_solves, int* overlap_basis_solves) {
+    if (!es) return fail(QSB_ERR_INVALID, "solve_stats: null solver");
+    if (cholesky_solves) *cholesky_solves = es->last_chol;
+    if (overlap_basis_solves) *overlap_basis_solves = es->last_svqb;
+    return QSB_OK;
+}
+
 qsb_status qsb_eigensolver_overlap_stats(const qsb_eigensolver* es, int* max_dropped, double* min_kept_ratio,
                                          double* drop_tolerance) {
     if (!es) return fail(QSB_ERR_INVALID, "overlap_stats: null solver");
@@ -1074,6 +1101,8 @@ qsb_status qsb_lobpcg_z(qsb_eigensolver* es, double dVol, int n, int iter_max, d
     es->last_iters = 0;
     es->last_rollback = 0;
     es->last_dropped = 0;
+    es->last_chol = 0;
+    es->last_svqb = 0;
     es->last_min_kept = 1.0;
     if (es->mixed)
         return lobpcg_z_mixed(es, dVol, n, iter_max, eigen_values, X, keep, p_num_fix, residual_threshold, scf_step, s);
@@ -1234,6 +1263,8 @@ qsb_status qsb_lobpcg_d(qsb_eigensolver* es, double dVol, int n, int iter_max, d
     es->last_iters = 0;
     es->last_rollback = 0;
     es->last_dropped = 0;
+    es->last_chol = 0;
+    es->last_svqb = 0;
     es->last_min_kept = 1.0;
     if (es->mixed) return lobpcg_d_mixed(es, dVol, n, iter_max, eigen_values, X, keep, is_first_time, s);
     const size_t L = es->L;

@@ -14,6 +14,7 @@ namespace qsb {
 
 // Records the message for qsb_last_error() and returns the status.
 qsb_status fail(qsb_status st, const std::string& msg);
+void set_last_error(const std::string& msg);   // restore the calling thread's message
 qsb_status cuda_fail(cudaError_t e, const char* where);
 
 #define QSB_CUDA_TRY(expr)                                   \

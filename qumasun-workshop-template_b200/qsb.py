@@ -310,6 +310,12 @@ class EigenSolver:
         """"bf16x3", "bf16x4" or "int8_ozaki" (the default) for the mixed-precision Gram products."""
         _check(lib.qsb_eigensolver_set_gram_kind(self._h, self.GRAM_KINDS[kind]))
 
+    def solve_stats(self):
+        """(Cholesky solves, overlap-basis fallbacks) of the last call (mixed precision)."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        _check(lib.qsb_eigensolver_solve_stats(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def overlap_stats(self):
         """(most directions dropped in one iteration, smallest kept overlap
         eigenvalue / largest, drop tolerance) of the last call (mixed precision)."""
