@@ -338,6 +338,16 @@ QSB_API qsb_status qsb_gram_ozaki_int8(qsb_dtype dtype, int64_t N, int p, int q,
                                        double* T, int ldt, int upper, void* workspace, size_t workspace_bytes,
                                        void* stream);
 
+/* Rotation OUT = U C (the NextVector_z2 / NextVector products,
+ * source/lobpcg_z_multi_mpi.h:1515-1598) on the INT8 tensor cores: U (N x K,
+ * column-major ld N, fp32 or fp64) split as in qsb_gram_ozaki_int8, C (K x q,
+ * FP64, device, ld K) scaled by U's column exponents and split per output
+ * column; OUT: N x q fp32, ld N.  Element error ~2^-20 of max|u| |c| per term
+ * (round-to-nearest slices, exact integer accumulation). */
+QSB_API qsb_status qsb_rotate_ozaki_int8_workspace(int64_t N, int K, int q, size_t* bytes);
+QSB_API qsb_status qsb_rotate_ozaki_int8(qsb_dtype dtype, int64_t N, int K, int q, const void* U, const double* C,
+                                         float* out, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Per-kernel device timing of qsb_ham_apply, in the spirit of the reference's
  * StopWatch sectors (source/StopWatch.h:11-60, watch_pp in
  * source/PseudoPotNonlocal_SvF2_kpoint.h:261-272).  While enabled, every

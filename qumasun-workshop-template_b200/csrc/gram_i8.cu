@@ -323,6 +323,209 @@ gram_i8_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Rotation OUT = U C on the INT8 tensor cores (the NextVector products of the
+// mixed-precision LOBPCG): U is an Ozaki-split operand (the Gram's slices of
+// the basis, grid-contiguous columns, read as an MN-major A operand), C a
+// small FP64 K x q matrix whose rows are first scaled by U's column exponents
+// (so one exponent per output column remains) and split into three int8
+// slices stored K-contiguous (K-major B operand).  Six MMAs per K step into
+// three INT32 accumulators, as in the Gram; the epilogue scales by the output
+// column's exponent and stores FP32 planes (one per output column).
+// ---------------------------------------------------------------------------
+constexpr int RT_K = 128;   // K per stage (rows of the MN-major A tile, bytes of the K-major B rows)
+
+// kind::i8, A MN-major (bit 15), B K-major, S32 accumulate, M = N = 128
+constexpr uint32_t RT_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | ((uint32_t)(OZ_N >> 3) << 17) |
+                              ((uint32_t)(OZ_M >> 4) << 24);
+
+__device__ __forceinline__ void umma_i8_mn(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(RT_IDESC), "r"(accumulate)
+        : "memory");
+}
+
+// MN-major A tile: K rows of 128 bytes (128 int8 along M, one 128-byte swizzle
+// atom wide), 8-row atoms 1024 bytes apart along K.  With a single atom along M
+// only the K stride matters; it is written into both offset fields.
+__device__ __forceinline__ uint64_t sw128_mnmajor_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(1024 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// C' = diag(2^e_U) C split per output column j: exponent f_j with max|C'_.j| 2^-f in
+// [32, 64), three int8 slices, written [j][kpad] (rows K..kpad zero).  One block per column.
+__global__ void rot_coef_split_kernel(const double* __restrict__ C, int ldc, int K, int kpad,
+                                      const int* __restrict__ eu, int8_t* __restrict__ slices, size_t stride,
+                                      int* __restrict__ fexp) {
+    const int j = blockIdx.x;
+    double m = 0.0;
+    for (int k = threadIdx.x; k < K; k += blockDim.x) m = fmax(m, fabs(ldexp(C[(size_t)k + (size_t)ldc * j], eu[k])));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    __shared__ double red[32];
+    __shared__ int ef;
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+        ef = m > 0.0 ? ilogb(m) - 5 : 0;
+        fexp[j] = ef;
+    }
+    __syncthreads();
+    const int f = ef;
+    int8_t* o0 = slices + (size_t)j * kpad;
+    for (int k = threadIdx.x; k < kpad; k += blockDim.x) {
+        int a = 0, b = 0, c = 0;
+        if (k < K) {
+            const double x = ldexp(C[(size_t)k + (size_t)ldc * j], eu[k] - f);
+            const double q0 = rint(x);
+            const double r1 = (x - q0) * 128.0;
+            const double q1 = rint(r1);
+            a = (int)q0;
+            b = (int)q1;
+            c = (int)rint((r1 - q1) * 128.0);
+        }
+        o0[k] = (int8_t)a;
+        o0[stride + k] = (int8_t)b;
+        o0[2 * stride + k] = (int8_t)c;
+    }
+}
+
+// One CTA: rows [mt*128, +128) of OUT, columns [nt*128, +128), all of K.
+__global__ void __launch_bounds__(OZ_THREADS, 1)
+rot_i8_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ CUtensorMap mA1,
+              const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mB0,
+              const __grid_constant__ CUtensorMap mB1, const __grid_constant__ CUtensorMap mB2, int kstages,
+              int64_t N, int q, const int* __restrict__ fexp, ColumnSet out, int* __restrict__ err) {
+    extern __shared__ unsigned char rt_raw[];
+    unsigned char* base = (unsigned char*)(((uintptr_t)rt_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* full = reinterpret_cast<uint64_t*>(base + (size_t)OZ_STAGES * OZ_STAGE_BYTES);
+    uint64_t* empty = full + OZ_STAGES;
+    uint64_t* done = empty + OZ_STAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int mt = blockIdx.x, nt = blockIdx.y;
+    const int nk = kstages;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < OZ_STAGES; ++s) {
+            bar_init(&full[s], 1);
+            bar_init(&empty[s], 1);
+        }
+        bar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tmem_slot)),
+                     "r"(512)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    int issued = 0;
+    if (warp == 0 && lane == 0) {
+        const CUtensorMap* maps[6] = {&mA0, &mA1, &mA2, &mB0, &mB1, &mB2};
+        for (int it = 0; it < nk; ++it) {
+            const int s = it % OZ_STAGES;
+            if (it >= OZ_STAGES && !bar_wait(&empty[s], (uint32_t)(((it / OZ_STAGES) - 1) & 1), OZ_WAIT_LIMIT)) {
+                atomicOr(err, ERR_GEMM_TIMEOUT);
+                atomicExch(abort_flag, 1);
+                break;
+            }
+            if (*(volatile int*)abort_flag) break;
+            unsigned char* st = base + (size_t)s * OZ_STAGE_BYTES;
+            bar_expect_tx(&full[s], OZ_STAGE_BYTES);
+            // A: box (128 grid points, 128 columns of U) at (mt*128, it*128); B: box (128 K, 128 columns of C')
+#pragma unroll
+            for (int k = 0; k < 3; ++k) tma_2d(st + k * OZ_TILE, maps[k], mt * OZ_M, it * RT_K, &full[s]);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) tma_2d(st + (3 + k) * OZ_TILE, maps[3 + k], it * RT_K, nt * OZ_N, &full[s]);
+            issued = it + 1;
+        }
+    } else if (warp == 1 && lane == 0) {
+        const uint32_t d0 = tmem, d1 = tmem + 128, d2 = tmem + 256;
+        for (int it = 0; it < nk; ++it) {
+            const int s = it % OZ_STAGES;
+            if (!bar_wait(&full[s], (uint32_t)((it / OZ_STAGES) & 1), OZ_WAIT_LIMIT)) {
+                atomicOr(err, ERR_GEMM_TIMEOUT);
+                atomicExch(abort_flag, 1);
+                break;
+            }
+            if (*(volatile int*)abort_flag) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t st = su32(base + (size_t)s * OZ_STAGE_BYTES);
+            const uint32_t a0 = st, a1 = st + OZ_TILE, a2 = st + 2 * OZ_TILE;
+            const uint32_t b0 = st + 3 * OZ_TILE, b1 = st + 4 * OZ_TILE, b2 = st + 5 * OZ_TILE;
+#pragma unroll
+            for (int kk = 0; kk < RT_K / 32; ++kk) {
+                const uint32_t ao = kk * 4096;   // 32 K rows of 128 bytes (four 8-row atoms)
+                const uint32_t bo = kk * 32;     // 32 int8 along the K-major row
+                const uint32_t acc = (it > 0 || kk > 0) ? 1u : 0u;
+                umma_i8_mn(d0, sw128_mnmajor_desc(a0 + ao), sw128_kmajor_desc(b0 + bo), acc);
+                umma_i8_mn(d1, sw128_mnmajor_desc(a0 + ao), sw128_kmajor_desc(b1 + bo), acc);
+                umma_i8_mn(d1, sw128_mnmajor_desc(a1 + ao), sw128_kmajor_desc(b0 + bo), 1u);
+                umma_i8_mn(d2, sw128_mnmajor_desc(a0 + ao), sw128_kmajor_desc(b2 + bo), acc);
+                umma_i8_mn(d2, sw128_mnmajor_desc(a1 + ao), sw128_kmajor_desc(b1 + bo), 1u);
+                umma_i8_mn(d2, sw128_mnmajor_desc(a2 + ao), sw128_kmajor_desc(b0 + bo), 1u);
+            }
+            umma_commit(&empty[s]);
+        }
+        umma_commit(done);
+    }
+    __syncwarp();
+
+    bool ok = bar_wait(done, 0, OZ_WAIT_LIMIT);
+    if (!ok) {
+        atomicOr(err, ERR_GEMM_TIMEOUT);
+        atomicExch(abort_flag, 1);
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int64_t g = (int64_t)mt * OZ_M + warp * 32 + lane;   // grid point of this TMEM lane
+    const bool have = ok && nk > 0 && !*(volatile int*)abort_flag;
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+#pragma unroll 1
+    for (int c0 = 0; c0 < OZ_N; c0 += 32) {
+        uint32_t r0[32], r1[32], r2[32];
+        tmem_ld32(tmem + lane_base + (uint32_t)c0, r0);
+        tmem_ld32(tmem + lane_base + 128u + (uint32_t)c0, r1);
+        tmem_ld32(tmem + lane_base + 256u + (uint32_t)c0, r2);
+        if (have && g < N) {
+#pragma unroll
+            for (int jj = 0; jj < 32; ++jj) {
+                const int j = nt * OZ_N + c0 + jj;
+                if (j >= q) continue;
+                const void* b;
+                const int local = column_of(out, j, &b);
+                float* dst = (float*)b + (size_t)local * N;
+                const double v =
+                    (double)(int)r0[jj] + (double)(int)r1[jj] * 0x1p-7 + (double)(int)r2[jj] * 0x1p-14;
+                dst[g] = (float)ldexp(v, __ldg(fexp + j));
+            }
+        }
+    }
+
+    __syncthreads();
+    if (threadIdx.x == 0 && *(volatile int*)abort_flag) {
+        for (int it = max(0, issued - OZ_STAGES); it < issued; ++it)
+            (void)bar_wait(&full[it % OZ_STAGES], (uint32_t)((it / OZ_STAGES) & 1), OZ_DRAIN_LIMIT);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+    }
+}
+
 // T[m + ldt n] (+)= alpha 2^(ea[m] + eb[n]) sum over splits (fixed order, FP64)
 __global__ void gram_i8_reduce_kernel(const double* __restrict__ partial, int ksplit, int ntl, int mtiles, int upper,
                                       int p, int q, const int* __restrict__ ea, const int* __restrict__ eb,
@@ -449,6 +652,43 @@ qsb_status gram_ozaki(qsb_dtype dt, int64_t N, int p, int q, const void* U, cons
                          s);
 }
 
+size_t ozaki_rot_coef_bytes(int K, int q) {
+    const size_t kpad = (size_t)((K + RT_K - 1) / RT_K) * RT_K;
+    return 3 * a1k((size_t)q * kpad) + a1k((size_t)q * sizeof(int));
+}
+
+// OUT (fp32 columns, one every N elements, gathered destinations) = U C, with U
+// an ozaki_split operand of K columns and C a K x q FP64 matrix (device, ld ldc).
+// OUT may alias the arrays U was split from: only the slices are read.
+qsb_status ozaki_rotate(int64_t N, const void* Usplit, int K, const double* C, int ldc, int q, const ColumnSet& out,
+                        void* cws, size_t cws_bytes, cudaStream_t s) {
+    if (N <= 0 || K <= 0 || q <= 0) return QSB_OK;
+    if (column_count(out) != q) return fail(QSB_ERR_INVALID, "ozaki_rotate: output column count");
+    if (cws_bytes < ozaki_rot_coef_bytes(K, q)) return fail(QSB_ERR_INVALID, "ozaki_rotate: workspace too small");
+    const int kpad = ((K + RT_K - 1) / RT_K) * RT_K;
+    const size_t cstride = a1k((size_t)q * kpad);
+    const unsigned char* a = (const unsigned char*)Usplit;
+    const size_t sa = oz_stride(N, K);
+    const int* eu = (const int*)(a + 3 * sa);
+    int8_t* cs = (int8_t*)cws;
+    int* fexp = (int*)((unsigned char*)cws + 3 * cstride);
+    rot_coef_split_kernel<<<q, 256, 0, s>>>(C, ldc, K, kpad, eu, cs, cstride, fexp);
+    QSB_CUDA_TRY(cudaGetLastError());
+    const int64_t ldk = oz_ldk(N);
+    CUtensorMap m[6];
+    for (int k = 0; k < 3; ++k) {
+        if (!make_kmajor_map(&m[k], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, a + k * sa, ldk, K, OZ_M, RT_K) ||
+            !make_kmajor_map(&m[3 + k], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, cs + k * cstride, kpad, q, RT_K, OZ_N))
+            return fail(QSB_ERR_CUDA, "ozaki_rotate: tensor map encoding failed");
+    }
+    QSB_CUDA_TRY(cudaFuncSetAttribute(rot_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)OZ_SMEM));
+    const dim3 grid((unsigned)((N + OZ_M - 1) / OZ_M), (unsigned)((q + OZ_N - 1) / OZ_N));
+    rot_i8_kernel<<<grid, OZ_THREADS, OZ_SMEM, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], kpad / RT_K, N, q, fexp, out,
+                                                    device_error_word());
+    QSB_CUDA_TRY(cudaGetLastError());
+    return QSB_OK;
+}
+
 }  // namespace qsb
 
 extern "C" {
@@ -468,6 +708,31 @@ qsb_status qsb_gram_ozaki_int8(qsb_dtype dtype, int64_t N, int p, int q, const v
     if (upper && p != q) return qsb::fail(QSB_ERR_INVALID, "gram_ozaki_int8: upper needs p == q");
     return qsb::gram_ozaki(dtype, N, p, q, U, V, T, ldt, 1.0, false, upper != 0, workspace, workspace_bytes,
                            (cudaStream_t)stream);
+}
+
+size_t qsb_rotate_ozaki_int8_bytes(int64_t N, int K, int q) {
+    return qsb::ozaki_split_bytes(N, K) + qsb::ozaki_rot_coef_bytes(K, q);
+}
+
+qsb_status qsb_rotate_ozaki_int8_workspace(int64_t N, int K, int q, size_t* bytes) {
+    if (!bytes || N < 1 || K < 1 || q < 1) return qsb::fail(QSB_ERR_INVALID, "rotate_ozaki_int8_workspace: bad arguments");
+    *bytes = qsb_rotate_ozaki_int8_bytes(N, K, q);
+    return QSB_OK;
+}
+
+qsb_status qsb_rotate_ozaki_int8(qsb_dtype dtype, int64_t N, int K, int q, const void* U, const double* C, float* out,
+                                 void* workspace, size_t workspace_bytes, void* stream) {
+    if (dtype != QSB_F64 && dtype != QSB_F32) return qsb::fail(QSB_ERR_INVALID, "rotate_ozaki_int8: bad dtype");
+    if (N < 1 || K < 1 || q < 1 || !U || !C || !out || !workspace)
+        return qsb::fail(QSB_ERR_INVALID, "rotate_ozaki_int8: bad arguments");
+    if (K > 65535 || q > 65535) return qsb::fail(QSB_ERR_INVALID, "rotate_ozaki_int8: K, q must be < 65536");
+    if (workspace_bytes < qsb_rotate_ozaki_int8_bytes(N, K, q))
+        return qsb::fail(QSB_ERR_INVALID, "rotate_ozaki_int8: workspace too small");
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char* w = (unsigned char*)workspace;
+    QSB_TRY(qsb::ozaki_split(dtype, N, qsb::column_set(U, K), w, s));
+    return qsb::ozaki_rotate(N, w, K, C, K, q, qsb::column_set(out, q), w + qsb::ozaki_split_bytes(N, K),
+                             qsb::ozaki_rot_coef_bytes(K, q), s);
 }
 
 }  // extern "C"

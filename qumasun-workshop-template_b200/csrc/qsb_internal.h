@@ -174,6 +174,12 @@ qsb_status ozaki_split(qsb_dtype dt, int64_t N, const ColumnSet& src, void* dst,
 size_t ozaki_partial_bytes_bound(int64_t N, int p, int q, bool upper);
 qsb_status gram_ozaki_tc(int64_t N, const void* A, int p, const void* B, int q, bool upper, double* T, int ldt,
                          double alpha, bool accumulate, void* partial, size_t partial_bytes, cudaStream_t s);
+// OUT (q fp32 columns, one every N elements, gathered destinations) = U C on
+// the INT8 tensor cores, U an ozaki_split operand of K columns, C K x q FP64
+// (device, ld ldc); OUT may alias the arrays U was split from.
+size_t ozaki_rot_coef_bytes(int K, int q);
+qsb_status ozaki_rotate(int64_t N, const void* Usplit, int K, const double* C, int ldc, int q, const ColumnSet& out,
+                        void* cws, size_t cws_bytes, cudaStream_t s);
 size_t gram_ozaki_workspace(int64_t N, int p, int q, bool same);
 qsb_status gram_ozaki(qsb_dtype dt, int64_t N, int p, int q, const void* U, const void* V, double* T, int ldt,
                       double alpha, bool accumulate, bool upper, void* ws, size_t ws_bytes, cudaStream_t s);

@@ -127,3 +127,32 @@ def test_gram_ozaki_int8_has_no_diagonal_bias(qsb):
     assert abs(rel) < 2e-8, rel
     assert (T - full).abs().max().item() / full.abs().max().item() < 1e-6
     assert qsb.device_status() == 0
+
+
+@pytest.mark.parametrize("N,K,q", [
+    (50021, 96, 40),       # ragged everything: grid tail, K < one stage, q < one tile
+    (65536, 384, 256),     # the mixed LOBPCG shape: three K stages, two column tiles
+    (70000, 200, 130),     # K tail inside a stage, column tail in the second tile
+])
+def test_rotation_ozaki_int8_matches_fp64(qsb, N, K, q):
+    """OUT = U C on the INT8 tensor cores (MN-major A operand) against the FP64
+    product: every element within 5e-6 of max|OUT|."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(21)
+    U = (torch.rand(K, N, generator=g, device="cuda", dtype=torch.float64) - 0.5).float()
+    U[K // 3] *= 1e-3                                    # columns of very different scale
+    C = torch.randn(q, K, generator=g, device="cuda", dtype=torch.float64)   # column-major K x q
+    nbytes = ctypes.c_size_t()
+    assert qsb.lib.qsb_rotate_ozaki_int8_workspace(ctypes.c_int64(N), K, q, ctypes.byref(nbytes)) == 0
+    ws = torch.empty(nbytes.value, dtype=torch.uint8, device="cuda")
+    out = torch.full((q, N), float("nan"), dtype=torch.float32, device="cuda")
+    st = qsb.lib.qsb_rotate_ozaki_int8(1, ctypes.c_int64(N), K, q, ctypes.c_void_p(U.data_ptr()),
+                                       ctypes.c_void_p(C.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                       ctypes.c_void_p(ws.data_ptr()), ctypes.c_size_t(nbytes.value),
+                                       ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert st == 0, qsb.lib.qsb_last_error()
+    torch.cuda.synchronize()
+    ref = C @ U.double()                                 # q x N: column j of OUT is row j here
+    err = (out.double() - ref).abs().max().item() / ref.abs().max().item()
+    assert err < 5e-6, err
+    assert qsb.device_status() == 0
