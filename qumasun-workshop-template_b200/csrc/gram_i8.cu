@@ -129,8 +129,9 @@ __device__ __forceinline__ int column_exponent(unsigned long long bits) {
     return m > 0.0 ? ilogb(m) - 5 : 0;   // max |u| 2^-e in [32, 64)
 }
 
-// Three int8 slices of column col (length ldk, a multiple of 4; rows N..ldk
+// Four int8 slices of column col (length ldk, a multiple of 4; rows N..ldk
 // zero) and its exponent; four elements per thread, one 4-byte store per slice.
+// The Gram products use the first three, the rotations all four.
 template <typename T>
 __global__ void slice_kernel(ColumnSet src, int64_t N, int64_t ldk, const unsigned long long* __restrict__ maxbits,
                              int8_t* __restrict__ slices, size_t slice_stride, int* __restrict__ exps) {
@@ -144,28 +145,34 @@ __global__ void slice_kernel(ColumnSet src, int64_t N, int64_t ldk, const unsign
     int8_t* o0 = slices + (size_t)col * ldk;
     int8_t* o1 = o0 + slice_stride;
     int8_t* o2 = o0 + 2 * slice_stride;
+    int8_t* o3 = o0 + 3 * slice_stride;
     const int64_t n4 = ldk / 4;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = 4 * q;
         double v[4];
         load4<T>(s, i, N, vec, v);
-        char4 a, c, d;
+        char4 a, c, d, f;
         signed char* pa = &a.x;
         signed char* pc = &c.x;
         signed char* pd = &d.x;
+        signed char* pf = &f.x;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const double x = ldexp(v[j], -e);
             const double q0 = rint(x);
             const double r1 = (x - q0) * 128.0;
             const double q1 = rint(r1);
+            const double r2 = (r1 - q1) * 128.0;
+            const double q2 = rint(r2);
             pa[j] = (signed char)(int)q0;
             pc[j] = (signed char)(int)q1;
-            pd[j] = (signed char)(int)rint((r1 - q1) * 128.0);
+            pd[j] = (signed char)(int)q2;
+            pf[j] = (signed char)(int)rint((r2 - q2) * 128.0);
         }
         *reinterpret_cast<char4*>(o0 + i) = a;
         *reinterpret_cast<char4*>(o1 + i) = c;
         *reinterpret_cast<char4*>(o2 + i) = d;
+        *reinterpret_cast<char4*>(o3 + i) = f;
     }
 }
 
@@ -328,15 +335,27 @@ gram_i8_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ 
 // mixed-precision LOBPCG): U is an Ozaki-split operand (the Gram's slices of
 // the basis, grid-contiguous columns, read as an MN-major A operand), C a
 // small FP64 K x q matrix whose rows are first scaled by U's column exponents
-// (so one exponent per output column remains) and split into three int8
-// slices stored K-contiguous (K-major B operand).  Six MMAs per K step into
-// three INT32 accumulators, as in the Gram; the epilogue scales by the output
-// column's exponent and stores FP32 planes (one per output column).
+// (so one exponent per output column remains) and split into int8 slices
+// stored K-contiguous (K-major B operand).  Both enter with four slices
+// (2^-27 of the column maxima, below FP32's rounding): near convergence
+// P' = R Cr + P Cp is far smaller than its two terms, and P' and AP' must stay
+// as consistent as FP32 arithmetic keeps them.  The ten products with
+// i + j <= 3 go into four INT32 accumulators (64 output columns per CTA);
+// the epilogue scales by the output column's exponent and stores FP32 planes.
 // ---------------------------------------------------------------------------
 constexpr int RT_K = 128;   // K per stage (rows of the MN-major A tile, bytes of the K-major B rows)
+constexpr int RT_N = 64;    // output columns per CTA (UMMA N)
+constexpr int RT_TILE_B = RT_N * RT_K;          // 8 KB per slice of C'
+constexpr int RT_STAGE_BYTES = 4 * OZ_TILE + 4 * RT_TILE_B;   // four slices of U, four of C'
+// One stage per CTA so that two CTAs share an SM (2 x 256 TMEM columns): each
+// CTA's tile is short (K <= a few hundred), so the overlap that matters is one
+// CTA's loads under the other's MMAs and epilogue.
+constexpr int RT_STAGES = 1;
+constexpr size_t RT_SMEM = (size_t)RT_STAGES * RT_STAGE_BYTES + 1024 + 256;
+static_assert(RT_SMEM <= 232448, "rotation stages must fit the 227 KB of shared memory per CTA");
 
-// kind::i8, A MN-major (bit 15), B K-major, S32 accumulate, M = N = 128
-constexpr uint32_t RT_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | ((uint32_t)(OZ_N >> 3) << 17) |
+// kind::i8, A MN-major (bit 15), B K-major, S32 accumulate, M = 128, N = 64
+constexpr uint32_t RT_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | ((uint32_t)(RT_N >> 3) << 17) |
                               ((uint32_t)(OZ_M >> 4) << 24);
 
 __device__ __forceinline__ void umma_i8_mn(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
@@ -357,10 +376,10 @@ __device__ __forceinline__ uint64_t sw128_mnmajor_desc(uint32_t saddr) {
 }
 
 // C' = diag(2^e_U) C split per output column j: exponent f_j with max|C'_.j| 2^-f in
-// [32, 64), three int8 slices, written [j][kpad] (rows K..kpad zero).  One block per column.
+// [32, 64), four int8 slices, written [j][kpad] (rows K..kpad zero).  One block per column.
 __global__ void rot_coef_split_kernel(const double* __restrict__ C, int ldc, int K, int kpad,
                                       const int* __restrict__ eu, int8_t* __restrict__ slices, size_t stride,
-                                      int* __restrict__ fexp) {
+                                      double* __restrict__ fscale) {
     const int j = blockIdx.x;
     double m = 0.0;
     for (int k = threadIdx.x; k < K; k += blockDim.x) m = fmax(m, fabs(ldexp(C[(size_t)k + (size_t)ldc * j], eu[k])));
@@ -372,39 +391,44 @@ __global__ void rot_coef_split_kernel(const double* __restrict__ C, int ldc, int
     if (threadIdx.x == 0) {
         for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
         ef = m > 0.0 ? ilogb(m) - 5 : 0;
-        fexp[j] = ef;
+        fscale[j] = ldexp(1.0, ef);
     }
     __syncthreads();
     const int f = ef;
     int8_t* o0 = slices + (size_t)j * kpad;
     for (int k = threadIdx.x; k < kpad; k += blockDim.x) {
-        int a = 0, b = 0, c = 0;
+        int a = 0, b = 0, c = 0, d = 0;
         if (k < K) {
             const double x = ldexp(C[(size_t)k + (size_t)ldc * j], eu[k] - f);
             const double q0 = rint(x);
             const double r1 = (x - q0) * 128.0;
             const double q1 = rint(r1);
+            const double r2 = (r1 - q1) * 128.0;
+            const double q2 = rint(r2);
             a = (int)q0;
             b = (int)q1;
-            c = (int)rint((r1 - q1) * 128.0);
+            c = (int)q2;
+            d = (int)rint((r2 - q2) * 128.0);
         }
         o0[k] = (int8_t)a;
         o0[stride + k] = (int8_t)b;
         o0[2 * stride + k] = (int8_t)c;
+        o0[3 * stride + k] = (int8_t)d;
     }
 }
 
-// One CTA: rows [mt*128, +128) of OUT, columns [nt*128, +128), all of K.
+// One CTA: rows [mt*128, +128) of OUT, columns [nt*64, +64), all of K.
 __global__ void __launch_bounds__(OZ_THREADS, 1)
 rot_i8_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ CUtensorMap mA1,
-              const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mB0,
-              const __grid_constant__ CUtensorMap mB1, const __grid_constant__ CUtensorMap mB2, int kstages,
-              int64_t N, int q, const int* __restrict__ fexp, ColumnSet out, int* __restrict__ err) {
+              const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mA3,
+              const __grid_constant__ CUtensorMap mB0, const __grid_constant__ CUtensorMap mB1,
+              const __grid_constant__ CUtensorMap mB2, const __grid_constant__ CUtensorMap mB3, int kstages,
+              int64_t N, int q, const double* __restrict__ fscale, ColumnSet out, int* __restrict__ err) {
     extern __shared__ unsigned char rt_raw[];
     unsigned char* base = (unsigned char*)(((uintptr_t)rt_raw + 1023) & ~(uintptr_t)1023);
-    uint64_t* full = reinterpret_cast<uint64_t*>(base + (size_t)OZ_STAGES * OZ_STAGE_BYTES);
-    uint64_t* empty = full + OZ_STAGES;
-    uint64_t* done = empty + OZ_STAGES;
+    uint64_t* full = reinterpret_cast<uint64_t*>(base + (size_t)RT_STAGES * RT_STAGE_BYTES);
+    uint64_t* empty = full + RT_STAGES;
+    uint64_t* done = empty + RT_STAGES;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
@@ -413,7 +437,7 @@ rot_i8_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ C
     const int nk = kstages;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < OZ_STAGES; ++s) {
+        for (int s = 0; s < RT_STAGES; ++s) {
             bar_init(&full[s], 1);
             bar_init(&empty[s], 1);
         }
@@ -423,7 +447,7 @@ rot_i8_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ C
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tmem_slot)),
-                     "r"(512)
+                     "r"(256)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -434,49 +458,61 @@ rot_i8_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ C
 
     int issued = 0;
     if (warp == 0 && lane == 0) {
-        const CUtensorMap* maps[6] = {&mA0, &mA1, &mA2, &mB0, &mB1, &mB2};
+        const CUtensorMap* amaps[4] = {&mA0, &mA1, &mA2, &mA3};
+        const CUtensorMap* bmaps[4] = {&mB0, &mB1, &mB2, &mB3};
         for (int it = 0; it < nk; ++it) {
-            const int s = it % OZ_STAGES;
-            if (it >= OZ_STAGES && !bar_wait(&empty[s], (uint32_t)(((it / OZ_STAGES) - 1) & 1), OZ_WAIT_LIMIT)) {
+            const int s = it % RT_STAGES;
+            if (it >= RT_STAGES && !bar_wait(&empty[s], (uint32_t)(((it / RT_STAGES) - 1) & 1), OZ_WAIT_LIMIT)) {
                 atomicOr(err, ERR_GEMM_TIMEOUT);
                 atomicExch(abort_flag, 1);
                 break;
             }
             if (*(volatile int*)abort_flag) break;
-            unsigned char* st = base + (size_t)s * OZ_STAGE_BYTES;
-            bar_expect_tx(&full[s], OZ_STAGE_BYTES);
-            // A: box (128 grid points, 128 columns of U) at (mt*128, it*128); B: box (128 K, 128 columns of C')
+            unsigned char* st = base + (size_t)s * RT_STAGE_BYTES;
+            bar_expect_tx(&full[s], RT_STAGE_BYTES);
+            // A: box (128 grid points, 128 columns of U) at (mt*128, it*128); B: box (128 K, 64 columns of C')
 #pragma unroll
-            for (int k = 0; k < 3; ++k) tma_2d(st + k * OZ_TILE, maps[k], mt * OZ_M, it * RT_K, &full[s]);
+            for (int k = 0; k < 4; ++k) tma_2d(st + k * OZ_TILE, amaps[k], mt * OZ_M, it * RT_K, &full[s]);
 #pragma unroll
-            for (int k = 0; k < 3; ++k) tma_2d(st + (3 + k) * OZ_TILE, maps[3 + k], it * RT_K, nt * OZ_N, &full[s]);
+            for (int k = 0; k < 4; ++k)
+                tma_2d(st + 4 * OZ_TILE + k * RT_TILE_B, bmaps[k], it * RT_K, nt * RT_N, &full[s]);
             issued = it + 1;
         }
     } else if (warp == 1 && lane == 0) {
-        const uint32_t d0 = tmem, d1 = tmem + 128, d2 = tmem + 256;
+        const uint32_t d0 = tmem, d1 = tmem + RT_N, d2 = tmem + 2 * RT_N, d3 = tmem + 3 * RT_N;
         for (int it = 0; it < nk; ++it) {
-            const int s = it % OZ_STAGES;
-            if (!bar_wait(&full[s], (uint32_t)((it / OZ_STAGES) & 1), OZ_WAIT_LIMIT)) {
+            const int s = it % RT_STAGES;
+            if (!bar_wait(&full[s], (uint32_t)((it / RT_STAGES) & 1), OZ_WAIT_LIMIT)) {
                 atomicOr(err, ERR_GEMM_TIMEOUT);
                 atomicExch(abort_flag, 1);
                 break;
             }
             if (*(volatile int*)abort_flag) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t st = su32(base + (size_t)s * OZ_STAGE_BYTES);
-            const uint32_t a0 = st, a1 = st + OZ_TILE, a2 = st + 2 * OZ_TILE;
-            const uint32_t b0 = st + 3 * OZ_TILE, b1 = st + 4 * OZ_TILE, b2 = st + 5 * OZ_TILE;
+            const uint32_t st = su32(base + (size_t)s * RT_STAGE_BYTES);
+            uint32_t a[4], b[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                a[k] = st + k * OZ_TILE;
+                b[k] = st + 4 * OZ_TILE + k * RT_TILE_B;
+            }
 #pragma unroll
             for (int kk = 0; kk < RT_K / 32; ++kk) {
                 const uint32_t ao = kk * 4096;   // 32 K rows of 128 bytes (four 8-row atoms)
                 const uint32_t bo = kk * 32;     // 32 int8 along the K-major row
                 const uint32_t acc = (it > 0 || kk > 0) ? 1u : 0u;
-                umma_i8_mn(d0, sw128_mnmajor_desc(a0 + ao), sw128_kmajor_desc(b0 + bo), acc);
-                umma_i8_mn(d1, sw128_mnmajor_desc(a0 + ao), sw128_kmajor_desc(b1 + bo), acc);
-                umma_i8_mn(d1, sw128_mnmajor_desc(a1 + ao), sw128_kmajor_desc(b0 + bo), 1u);
-                umma_i8_mn(d2, sw128_mnmajor_desc(a0 + ao), sw128_kmajor_desc(b2 + bo), acc);
-                umma_i8_mn(d2, sw128_mnmajor_desc(a1 + ao), sw128_kmajor_desc(b1 + bo), 1u);
-                umma_i8_mn(d2, sw128_mnmajor_desc(a2 + ao), sw128_kmajor_desc(b0 + bo), 1u);
+#define RT_MMA(D, I, J, ACC) umma_i8_mn(D, sw128_mnmajor_desc(a[I] + ao), sw128_kmajor_desc(b[J] + bo), ACC)
+                RT_MMA(d0, 0, 0, acc);
+                RT_MMA(d1, 0, 1, acc);
+                RT_MMA(d1, 1, 0, 1u);
+                RT_MMA(d2, 0, 2, acc);
+                RT_MMA(d2, 1, 1, 1u);
+                RT_MMA(d2, 2, 0, 1u);
+                RT_MMA(d3, 0, 3, acc);
+                RT_MMA(d3, 1, 2, 1u);
+                RT_MMA(d3, 2, 1, 1u);
+                RT_MMA(d3, 3, 0, 1u);
+#undef RT_MMA
             }
             umma_commit(&empty[s]);
         }
@@ -494,35 +530,49 @@ rot_i8_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ C
     const bool have = ok && nk > 0 && !*(volatile int*)abort_flag;
     const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
 #pragma unroll 1
-    for (int c0 = 0; c0 < OZ_N; c0 += 32) {
-        uint32_t r0[32], r1[32], r2[32];
+    for (int c0 = 0; c0 < RT_N; c0 += 32) {
+        uint32_t r0[32], r1[32], r2[32], r3[32];
         tmem_ld32(tmem + lane_base + (uint32_t)c0, r0);
-        tmem_ld32(tmem + lane_base + 128u + (uint32_t)c0, r1);
-        tmem_ld32(tmem + lane_base + 256u + (uint32_t)c0, r2);
+        tmem_ld32(tmem + lane_base + (uint32_t)(RT_N + c0), r1);
+        tmem_ld32(tmem + lane_base + (uint32_t)(2 * RT_N + c0), r2);
+        tmem_ld32(tmem + lane_base + (uint32_t)(3 * RT_N + c0), r3);
         if (have && g < N) {
+            const int j0 = nt * RT_N + c0;
+            // one destination lookup for the chunk when its 32 columns lie in one array
+            const void* bp;
+            const int local0 = column_of(out, j0, &bp);
+            const void* bl;
+            const int local31 = j0 + 31 < q ? column_of(out, j0 + 31, &bl) : -1;
+            const bool one = local31 == local0 + 31 && bl == bp;
+            float* dst0 = (float*)bp + (size_t)local0 * N + g;
 #pragma unroll
             for (int jj = 0; jj < 32; ++jj) {
-                const int j = nt * OZ_N + c0 + jj;
+                const int j = j0 + jj;
                 if (j >= q) continue;
-                const void* b;
-                const int local = column_of(out, j, &b);
-                float* dst = (float*)b + (size_t)local * N;
-                const double v =
-                    (double)(int)r0[jj] + (double)(int)r1[jj] * 0x1p-7 + (double)(int)r2[jj] * 0x1p-14;
-                dst[g] = (float)ldexp(v, __ldg(fexp + j));
+                float* dst;
+                if (one) {
+                    dst = dst0 + (size_t)jj * N;
+                } else {
+                    const void* bj;
+                    const int lj = column_of(out, j, &bj);
+                    dst = (float*)bj + (size_t)lj * N + g;
+                }
+                const double v = (double)(int)r0[jj] + (double)(int)r1[jj] * 0x1p-7 +
+                                 (double)(int)r2[jj] * 0x1p-14 + (double)(int)r3[jj] * 0x1p-21;
+                *dst = (float)(v * __ldg(fscale + j));
             }
         }
     }
 
     __syncthreads();
     if (threadIdx.x == 0 && *(volatile int*)abort_flag) {
-        for (int it = max(0, issued - OZ_STAGES); it < issued; ++it)
-            (void)bar_wait(&full[it % OZ_STAGES], (uint32_t)((it / OZ_STAGES) & 1), OZ_DRAIN_LIMIT);
+        for (int it = max(0, issued - RT_STAGES); it < issued; ++it)
+            (void)bar_wait(&full[it % RT_STAGES], (uint32_t)((it / RT_STAGES) & 1), OZ_DRAIN_LIMIT);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
     }
 }
 
@@ -572,7 +622,7 @@ OzPlan plan_oz(int64_t N, int p, int q, bool upper) {
 }  // namespace
 
 size_t ozaki_split_bytes(int64_t N, int cols) {
-    return 3 * oz_stride(N, cols) + a1k((size_t)cols * sizeof(int)) + a1k((size_t)cols * sizeof(unsigned long long));
+    return 4 * oz_stride(N, cols) + a1k((size_t)cols * sizeof(int)) + a1k((size_t)cols * sizeof(unsigned long long));
 }
 
 qsb_status ozaki_split(qsb_dtype dt, int64_t N, const ColumnSet& src, void* dst, cudaStream_t s) {
@@ -582,8 +632,8 @@ qsb_status ozaki_split(qsb_dtype dt, int64_t N, const ColumnSet& src, void* dst,
     const int64_t ldk = oz_ldk(N);
     const size_t stride = oz_stride(N, cols);
     unsigned char* w = (unsigned char*)dst;
-    int* exps = (int*)(w + 3 * stride);
-    unsigned long long* maxbits = (unsigned long long*)(w + 3 * stride + a1k((size_t)cols * sizeof(int)));
+    int* exps = (int*)(w + 4 * stride);
+    unsigned long long* maxbits = (unsigned long long*)(w + 4 * stride + a1k((size_t)cols * sizeof(int)));
     QSB_CUDA_TRY(cudaMemsetAsync(maxbits, 0, (size_t)cols * sizeof(unsigned long long), s));
     const int cblocks = (int)std::min<int64_t>((ldk / 4 + 255) / 256, 256);
     if (dt == QSB_F64) {
@@ -620,8 +670,8 @@ qsb_status gram_ozaki_tc(int64_t N, const void* A, int p, const void* B, int q, 
             !make_kmajor_map(&m[3 + k], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, b + k * sb, ldk, q, OZ_K, OZ_N))
             return fail(QSB_ERR_CUDA, "gram_ozaki_tc: tensor map encoding failed");
     }
-    const int* ea = (const int*)(a + 3 * sa);
-    const int* eb = (const int*)(b + 3 * sb);
+    const int* ea = (const int*)(a + 4 * sa);
+    const int* eb = (const int*)(b + 4 * sb);
     QSB_CUDA_TRY(cudaFuncSetAttribute(gram_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)OZ_SMEM));
     gram_i8_kernel<<<dim3(g.ntl, g.ksplit), OZ_THREADS, OZ_SMEM, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], g.kstages,
                                                                        g.ksplit, g.mtiles, upper ? 1 : 0,
@@ -654,7 +704,7 @@ qsb_status gram_ozaki(qsb_dtype dt, int64_t N, int p, int q, const void* U, cons
 
 size_t ozaki_rot_coef_bytes(int K, int q) {
     const size_t kpad = (size_t)((K + RT_K - 1) / RT_K) * RT_K;
-    return 3 * a1k((size_t)q * kpad) + a1k((size_t)q * sizeof(int));
+    return 4 * a1k((size_t)q * kpad) + a1k((size_t)q * sizeof(double));
 }
 
 // OUT (fp32 columns, one every N elements, gathered destinations) = U C, with U
@@ -669,22 +719,21 @@ qsb_status ozaki_rotate(int64_t N, const void* Usplit, int K, const double* C, i
     const size_t cstride = a1k((size_t)q * kpad);
     const unsigned char* a = (const unsigned char*)Usplit;
     const size_t sa = oz_stride(N, K);
-    const int* eu = (const int*)(a + 3 * sa);
+    const int* eu = (const int*)(a + 4 * sa);
     int8_t* cs = (int8_t*)cws;
-    int* fexp = (int*)((unsigned char*)cws + 3 * cstride);
-    rot_coef_split_kernel<<<q, 256, 0, s>>>(C, ldc, K, kpad, eu, cs, cstride, fexp);
+    double* fscale = (double*)((unsigned char*)cws + 4 * cstride);
+    rot_coef_split_kernel<<<q, 256, 0, s>>>(C, ldc, K, kpad, eu, cs, cstride, fscale);
     QSB_CUDA_TRY(cudaGetLastError());
     const int64_t ldk = oz_ldk(N);
-    CUtensorMap m[6];
-    for (int k = 0; k < 3; ++k) {
+    CUtensorMap m[8];
+    for (int k = 0; k < 4; ++k)
         if (!make_kmajor_map(&m[k], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, a + k * sa, ldk, K, OZ_M, RT_K) ||
-            !make_kmajor_map(&m[3 + k], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, cs + k * cstride, kpad, q, RT_K, OZ_N))
+            !make_kmajor_map(&m[4 + k], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, cs + k * cstride, kpad, q, RT_K, RT_N))
             return fail(QSB_ERR_CUDA, "ozaki_rotate: tensor map encoding failed");
-    }
-    QSB_CUDA_TRY(cudaFuncSetAttribute(rot_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)OZ_SMEM));
-    const dim3 grid((unsigned)((N + OZ_M - 1) / OZ_M), (unsigned)((q + OZ_N - 1) / OZ_N));
-    rot_i8_kernel<<<grid, OZ_THREADS, OZ_SMEM, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], kpad / RT_K, N, q, fexp, out,
-                                                    device_error_word());
+    QSB_CUDA_TRY(cudaFuncSetAttribute(rot_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RT_SMEM));
+    const dim3 grid((unsigned)((N + OZ_M - 1) / OZ_M), (unsigned)((q + RT_N - 1) / RT_N));
+    rot_i8_kernel<<<grid, OZ_THREADS, RT_SMEM, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7], kpad / RT_K, N, q,
+                                                    fscale, out, device_error_word());
     QSB_CUDA_TRY(cudaGetLastError());
     return QSB_OK;
 }

@@ -255,6 +255,9 @@ struct qsb_eigensolver {
     double* T2 = nullptr;    // full-pencil real Gram (up to (2*3n)^2)
     float* rc32 = nullptr;   // fp32 copies of the rotation coefficients / orthogonalization matrix
     double* svq = nullptr;   // overlap-basis pencil solve: W, scratch, reduced matrix (m x m each), lambda, d
+    double* rotw = nullptr;  // tensor-core rotations: saved overlap, rotation coefficients, their overlap product, norms
+    void* rotc = nullptr;    // int8 slices of the rotation coefficients
+    size_t rotc_bytes = 0;
     double drop_tol = 0.0;   // overlap eigenvalues below drop_tol * max are dropped
     int gram_kind = QSB_GRAM_INT8_OZAKI;   // Gram products: BF16x3, BF16x4 or INT8 Ozaki
     int last_chol = 0;       // pencil solves of the last call by Cholesky (?hegvd on the scaled pencil)
@@ -652,6 +655,67 @@ qsb_status solve_pencil_overlap_basis(qsb_eigensolver* es, int m, int nout, cuda
     return QSB_OK;
 }
 
+// a[i] /= b[i]
+__global__ void divide_by(double* __restrict__ a, const double* __restrict__ b, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] /= b[i];
+}
+
+// Rotation coefficients of the real solver for one tensor-core product per
+// bundle set: [X' | P'] = [X R P] C2 with C2 (m x 2n) = [[Cx, 0], [Cr, Cr], [Cp, Cp]]
+// (P' = R Cr + P Cp, X' = X Cx + P'), from the eigenvectors C (m x n, ld m).
+__global__ void build_rot_coef_real(const double* __restrict__ C, int m, int n, double* __restrict__ C2) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (k >= m) return;
+    C2[(size_t)k + (size_t)m * j] = j < n ? C[(size_t)k + (size_t)m * j]
+                                          : (k < n ? 0.0 : C[(size_t)k + (size_t)m * (j - n)]);
+}
+
+// Column j of C2 scaled to unit B-norm: norms_j = C2_j^T (B C2)_j (G = B C2),
+// C2_j /= sqrt(norms_j) — the per-band renormalisation of x' and p' (dV-weighted,
+// B = dV U^T U) done on the coefficients instead of on the bundles.
+__global__ void normalize_rot_coef(double* __restrict__ C2, const double* __restrict__ G, int m,
+                                   double* __restrict__ norms) {
+    const int j = blockIdx.x;
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < m; k += blockDim.x) acc += C2[(size_t)k + (size_t)m * j] * G[(size_t)k + (size_t)m * j];
+    __shared__ double red[256];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    const double nrm = red[0];
+    const double f = nrm > 0.0 ? 1.0 / sqrt(nrm) : 0.0;
+    if (threadIdx.x == 0) norms[j] = nrm;
+    for (int k = threadIdx.x; k < m; k += blockDim.x) C2[(size_t)k + (size_t)m * j] *= f;
+}
+
+// [X' | P'] and [AX' | AP'] of the real mixed solver as two INT8 tensor-core
+// rotations of the Gram's slices (es->su, es->sau hold [X R P], [AX AR AP]),
+// normalised through the coefficients; written straight into the bundles.
+qsb_status rotate_real_ozaki(qsb_eigensolver* es, int m, int n, const double* Bsave, cudaStream_t s) {
+    double* C2 = es->rotw + (size_t)m * m;
+    double* G = C2 + (size_t)m * 2 * n;
+    double* norms = G + (size_t)m * 2 * n;
+    build_rot_coef_real<<<dim3((m + 127) / 128, 2 * n), 128, 0, s>>>(es->Sa, m, n, C2);
+    QSB_CUDA_TRY(cudaGetLastError());
+    const double one = 1.0, zero = 0.0;
+    QSB_BLAS_TRY(cublasDgemm(es->blas, CUBLAS_OP_N, CUBLAS_OP_N, m, 2 * n, m, &one, Bsave, m, C2, m, &zero, G, m));
+    // only the x' columns: their B-norm is 1 up to rounding, so the coefficient
+    // route is exact enough.  p' = R Cr + P Cp can be tiny once a band has
+    // converged, and its B-norm from the overlap is then dominated by the Gram
+    // products' error: p' is normalised from its measured norm after the rotation.
+    normalize_rot_coef<<<n, 256, 0, s>>>(C2, G, m, norms);
+    QSB_CUDA_TRY(cudaGetLastError());
+    QSB_TRY(ozaki_rotate(es->N, es->su, m, C2, m, 2 * n, column_set(es->X32, n, es->P32, n), es->rotc, es->rotc_bytes,
+                         s));
+    QSB_TRY(ozaki_rotate(es->N, es->sau, m, C2, m, 2 * n, column_set(es->AX32, n, es->AP32, n), es->rotc,
+                         es->rotc_bytes, s));
+    return QSB_OK;
+}
+
 // fp32 copies of the first count rotation coefficients
 qsb_status coefficients_f32(qsb_eigensolver* es, size_t count, cudaStream_t s) {
     to_f32<<<(int)std::min<size_t>((count + 255) / 256, 1024), 256, 0, s>>>(es->rc, es->rc32, count);
@@ -744,31 +808,51 @@ qsb_status lobpcg_d_mixed(qsb_eigensolver* es, double dVol, int n, int iter_max,
         const ColumnSet U = column_set(es->X32, n, es->R32, n, es->P32, two ? 0 : n);
         const ColumnSet AU = column_set(es->AX32, n, es->AR32, n, es->AP32, two ? 0 : n);
         QSB_TRY(mixed_pencil(es, U, AU, m, dVol, s));
+        const bool tc_rot = es->gram_kind == QSB_GRAM_INT8_OZAKI;
+        if (tc_rot)   // the overlap B, kept for the coefficient norms
+            QSB_CUDA_TRY(cudaMemcpyAsync(es->rotw, es->Sb, sizeof(double) * m * m, cudaMemcpyDeviceToDevice, s));
         QSB_TRY(solve_pencil_overlap_basis(es, m, n, s));
-        QSB_TRY(make_coefficients(es, n, m, nblk, s));
-        QSB_TRY(coefficients_f32(es, (size_t)nblk * n * n, s));
-        // P' = R Cr (+ P Cp); X' = X Cx + P'; the same on the A-bundles (:226-365)
-        QSB_TRY(rotate_real32(es, n, es->TMP32, es->R32, 1, 0.0f));
-        if (!two) QSB_TRY(rotate_real32(es, n, es->TMP32, es->P32, 2, 1.0f));
-        std::swap(es->P32, es->TMP32);
-        QSB_TRY(copy32(es->TMP32, es->P32, L * n, s));
-        QSB_TRY(rotate_real32(es, n, es->TMP32, es->X32, 0, 1.0f));
-        std::swap(es->X32, es->TMP32);
-        QSB_TRY(rotate_real32(es, n, es->TMP32, es->AR32, 1, 0.0f));
-        if (!two) QSB_TRY(rotate_real32(es, n, es->TMP32, es->AP32, 2, 1.0f));
-        std::swap(es->AP32, es->TMP32);
-        QSB_TRY(copy32(es->TMP32, es->AP32, L * n, s));
-        QSB_TRY(rotate_real32(es, n, es->TMP32, es->AX32, 0, 1.0f));
-        std::swap(es->AX32, es->TMP32);
-        // renormalize x, p and Ax, Ap (:493-505)
-        QSB_TRY(inv_norms(es->X32, sx));
-        QSB_TRY(inv_norms(es->P32, sp));
-        QSB_TRY(scale_bands(es->X32, sx));
-        QSB_TRY(scale_bands(es->AX32, sx));
-        QSB_TRY(scale_bands(es->P32, sp));
-        QSB_TRY(scale_bands(es->AP32, sp));
-        // eps = <x|Ax> dV; r = Ax - eps x; ||r||^2 dV (:507-513)
+        if (tc_rot) {
+            // P' = R Cr (+ P Cp); X' = X Cx + P'; the same on the A-bundles (:226-365),
+            // on the tensor cores; x renormalised (:493-505) through the coefficients,
+            // p from its measured norm
+            QSB_TRY(rotate_real_ozaki(es, m, n, es->rotw, s));
+            QSB_TRY(inv_norms(es->P32, sp));
+            QSB_TRY(scale_bands(es->P32, sp));
+            QSB_TRY(scale_bands(es->AP32, sp));
+        } else {
+            QSB_TRY(make_coefficients(es, n, m, nblk, s));
+            QSB_TRY(coefficients_f32(es, (size_t)nblk * n * n, s));
+            // P' = R Cr (+ P Cp); X' = X Cx + P'; the same on the A-bundles (:226-365)
+            QSB_TRY(rotate_real32(es, n, es->TMP32, es->R32, 1, 0.0f));
+            if (!two) QSB_TRY(rotate_real32(es, n, es->TMP32, es->P32, 2, 1.0f));
+            std::swap(es->P32, es->TMP32);
+            QSB_TRY(copy32(es->TMP32, es->P32, L * n, s));
+            QSB_TRY(rotate_real32(es, n, es->TMP32, es->X32, 0, 1.0f));
+            std::swap(es->X32, es->TMP32);
+            QSB_TRY(rotate_real32(es, n, es->TMP32, es->AR32, 1, 0.0f));
+            if (!two) QSB_TRY(rotate_real32(es, n, es->TMP32, es->AP32, 2, 1.0f));
+            std::swap(es->AP32, es->TMP32);
+            QSB_TRY(copy32(es->TMP32, es->AP32, L * n, s));
+            QSB_TRY(rotate_real32(es, n, es->TMP32, es->AX32, 0, 1.0f));
+            std::swap(es->AX32, es->TMP32);
+            // renormalize x, p and Ax, Ap (:493-505)
+            QSB_TRY(inv_norms(es->X32, sx));
+            QSB_TRY(inv_norms(es->P32, sp));
+            QSB_TRY(scale_bands(es->X32, sx));
+            QSB_TRY(scale_bands(es->AX32, sx));
+            QSB_TRY(scale_bands(es->P32, sp));
+            QSB_TRY(scale_bands(es->AP32, sp));
+        }
+        // eps = <x|Ax> dV; r = Ax - eps x; ||r||^2 dV (:507-513).  After the tensor-core
+        // rotation |x|^2 dV is 1 only to the coefficient slices' rounding (~1e-6), so
+        // eps is taken as the normalised Rayleigh quotient <x|Ax> / <x|x>.
         QSB_TRY(seg_dot(es, n, es->X32, es->AX32, dVol, eps_d, s));
+        if (tc_rot) {
+            QSB_TRY(seg_dot(es, n, es->X32, es->X32, dVol, nrm_d, s));
+            divide_by<<<(n + 127) / 128, 128, 0, s>>>(eps_d, nrm_d, n);
+            QSB_CUDA_TRY(cudaGetLastError());
+        }
         QSB_TRY(seg_residual(es, n, es->R32, es->AX32, es->X32, eps_d, nrm_d, dVol, s));
         QSB_TRY(host_vec(eps_d, eps));
         QSB_TRY(host_vec(nrm_d, v));
@@ -969,7 +1053,11 @@ qsb_status qsb_eigensolver_create_ex(qsb_eigensolver** out, int64_t N, int n, in
             cudaMalloc((void**)&es->T2, sizeof(double) * (size_t)pmax * pmax) != cudaSuccess ||
             cudaMalloc((void**)&es->rc32, sizeof(float) * (size_t)6 * 2 * n * n) != cudaSuccess ||
             cudaMalloc((void**)&es->svq, sizeof(double) * ((size_t)3 * (3 * n) * (3 * n) * c2 + 2 * (3 * n))) !=
-                cudaSuccess)
+                cudaSuccess ||
+            cudaMalloc((void**)&es->rotw, sizeof(double) * ((size_t)(3 * n) * (3 * n) * c2 +
+                                                            (size_t)2 * (3 * n * c2) * (2 * n * c2) + 2 * n * c2)) !=
+                cudaSuccess ||
+            cudaMalloc(&es->rotc, es->rotc_bytes = ozaki_rot_coef_bytes(3 * n * c2, 2 * n * c2)) != cudaSuccess)
             return cleanup(fail(QSB_ERR_NOMEM, "eigensolver: mixed-precision workspace allocation"));
     }
     const int m = 3 * n;
@@ -1001,7 +1089,7 @@ qsb_status qsb_eigensolver_destroy(qsb_eigensolver* es) {
     float* b32[7] = {es->X32, es->R32, es->P32, es->AX32, es->AR32, es->AP32, es->TMP32};
     for (float* p : b32)
         if (p) cudaFree(p);
-    void* mw[6] = {es->su, es->sau, es->gpart, es->T2, es->rc32, es->svq};
+    void* mw[8] = {es->su, es->sau, es->gpart, es->T2, es->rc32, es->svq, es->rotw, es->rotc};
     for (void* p : mw)
         if (p) cudaFree(p);
     if (es->T) cudaFree(es->T);
