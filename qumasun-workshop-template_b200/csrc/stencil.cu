@@ -15,7 +15,9 @@
 //   d = c0 p; d += x terms (offsets 4,3,2,1); d += y terms; d += z terms.
 #include "qsb_internal.h"
 #include <cmath>
+#include <cstdlib>
 #include <cuda.h>
+#include <string>
 
 namespace qsb {
 
@@ -341,6 +343,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                  : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
@@ -640,6 +646,731 @@ drain:
     __syncthreads();
 }
 
+// ---------------------------------------------------------------------------
+// fd8_zacc_kernel: the plane ring of fd8_tma_kernel, consumed one plane per
+// step, with the z derivative carried as pending OUTPUTS.
+//
+// A thread owns RY rows x 2 x-adjacent points and reads shared memory in
+// 16-byte pairs.  When plane j lands, its x/y derivatives, centre and V terms
+// go into output j, and w_m p_j into the pending outputs j-m and j+m (m = 1..4);
+// output j-4 is then complete and stored.  A plane is read from shared memory
+// only in the step that consumes it, so the ring needs only the prefetch depth,
+// and no z queue of inputs is kept.  Shared memory read per point (RY = 2):
+// x 5 pairs per 2 points (2.5 pairs = 5 values) + y 8 pairs per 2 x 2 points
+// (4 values) = 9 values, against 14 for fd8_tma_kernel.
+//
+// Same arithmetic terms as fd8_tma_kernel (Laplacian8th_halo_f,
+// source/GridDifference8th.h:82-148; LaplacianKpoint8th_halo_f,
+// source/GridDifferenceKpoint8th.h:17-120); the z sums are accumulated in
+// arrival order, which changes only the rounding (~1e-16 relative).
+constexpr int ZX = 16;            // threads along x, two points each
+constexpr int ZTX = 2 * ZX;       // tile width in points
+
+template <typename T>
+struct Pair;
+template <>
+struct Pair<double> {
+    using type = double2;
+};
+template <>
+struct Pair<float> {
+    using type = float2;
+};
+
+// ZY threads along y, RY rows each; S ring stages; MINB resident CTAs per SM
+template <typename T, bool CPLX, int ZY, int RY, int S, int MINB>
+struct ZCfg {
+    static constexpr int NT = ZX * ZY;
+    static constexpr int NC = CPLX ? 2 : 1;
+    static constexpr int TY = ZY * RY;
+    static constexpr int SW = ZTX + 2 * HW;
+    static constexpr int SH = TY + 2 * HW;
+    static constexpr int COMP = SH * SW;
+    static constexpr int STAGE = NC * COMP;
+    static constexpr size_t SMEM = (size_t)S * STAGE * sizeof(T) + S * sizeof(uint64_t) + 128;
+    static_assert((COMP * sizeof(T)) % 128 == 0, "stage components must stay 128-byte aligned");
+    static_assert(8 * TY <= NT && 8 * ZTX <= NT, "one periodic halo cell of each kind per thread");
+    static_assert(MINB * SMEM <= 227 * 1024, "MINB CTAs per SM");
+};
+
+template <typename T, bool CPLX, int MODE, bool GRAD, int ZY, int RY, int S, int MINB>
+__global__ void __launch_bounds__(ZX * ZY, MINB)
+fd8_zacc_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ out, const T* __restrict__ in,
+                const T* __restrict__ V, int nx, int ny, int nz, int zchunk, KC<T> k, int* __restrict__ err) {
+    using C = ZCfg<T, CPLX, ZY, RY, S, MINB>;
+    using P2 = typename Pair<T>::type;
+    constexpr int NC = C::NC, TY = C::TY, SW = C::SW;
+    extern __shared__ unsigned char smraw_[];
+    unsigned char* smraw = (unsigned char*)(((uintptr_t)smraw_ + 127) & ~(uintptr_t)127);
+    T* ring = reinterpret_cast<T*>(smraw);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smraw + (size_t)S * C::STAGE * sizeof(T));
+
+    const int ntx = (nx + ZTX - 1) / ZTX;
+    const int x0 = (blockIdx.x % ntx) * ZTX;
+    const int y0 = (blockIdx.x / ntx) * TY;
+    const int wx = min(ZTX, nx - x0);
+    const int wy = min(TY, ny - y0);
+    const int z0 = blockIdx.y * zchunk;
+    const int z1 = min(nz, z0 + zchunk);
+    const int nsteps = z1 - z0;
+    const int nplanes = nsteps + 2 * HW;
+    const int band = blockIdx.z;
+    const size_t nxy = (size_t)nx * ny;
+    const size_t N = nxy * nz;
+    const T* src[NC];
+    T* dst[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const size_t plane = CPLX ? (size_t)(2 * band + c) : (size_t)band;
+        src[c] = in + plane * N;
+        dst[c] = out + plane * N;
+    }
+
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int t = ty * ZX + tx;
+    // nx is even on this path (16-byte row pitch), so a pair is valid or not as a whole
+    const bool xin = 2 * tx < wx;
+    bool rv[RY];
+#pragma unroll
+    for (int i = 0; i < RY; ++i) rv[i] = xin && (ty * RY + i < wy);
+    const size_t rowoff = (size_t)(x0 + 2 * tx) + (size_t)nx * (y0 + ty * RY);
+    const int soff = (ty * RY + HW) * SW + 2 * tx + HW;   // first centre pair in a component box
+
+    // periodic halo cells (outside [0,nx) x [0,ny), zero-filled by the tensor copy)
+    bool xh_ok = false, yh_ok = false;
+    size_t xh_g = 0, yh_g = 0;
+    int xh_s = 0, yh_s = 0;
+    if (t < 8 * TY) {
+        const int side = t / (4 * TY), rem = t % (4 * TY), hrow = rem / 4, hk = rem % 4;
+        const int gxu = side == 0 ? x0 - HW + hk : x0 + wx + hk;
+        xh_ok = hrow < wy && (gxu < 0 || gxu >= nx);
+        xh_g = (size_t)wrapi(gxu, nx) + (size_t)nx * (y0 + min(hrow, wy - 1));
+        xh_s = (HW + hrow) * SW + (side == 0 ? hk : wx + HW + hk);
+    }
+    if (t < 8 * ZTX) {
+        const int side = t / (4 * ZTX), rem = t % (4 * ZTX), hr = rem / ZTX, hc = rem % ZTX;
+        const int gyu = side == 0 ? y0 - HW + hr : y0 + wy + hr;
+        yh_ok = hc < wx && (gyu < 0 || gyu >= ny);
+        yh_g = (size_t)(x0 + min(hc, wx - 1)) + (size_t)nx * wrapi(gyu, ny);
+        yh_s = (side == 0 ? hr : wy + HW + hr) * SW + HW + hc;
+    }
+
+    if (t == 0) {
+        for (int st = 0; st < S; ++st) mbar_init(&bar[st], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    // producer (thread 0): plane j (z = z0 - 4 + j, wrapped) -> stage j % S
+    constexpr uint32_t PLANE_BYTES = (uint32_t)(C::STAGE * sizeof(T));
+    int issued = 0;
+    auto issue = [&](int j) {
+        issued = j + 1;
+        const int st = j % S;
+        T* stage = ring + (size_t)st * C::STAGE;
+        const int zz = wrapi(z0 - HW + j, nz);
+        // order the threads' earlier generic-proxy writes (halo cells) to this
+        // stage before the tensor copy's async-proxy writes
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&bar[st], PLANE_BYTES);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const int zplane = (CPLX ? 2 * band + c : band) * nz + zz;
+            tma_load_3d(stage + c * C::COMP, &tmap, x0 - HW, y0 - HW, zplane, &bar[st]);
+        }
+    };
+    if (t == 0)
+        for (int j = 0; j < min(S, nplanes); ++j) issue(j);
+
+    int failed = 0;
+    // periodic halo values of inner planes, loaded two planes ahead (4 slots)
+    T hx[4][NC], hy[4][NC];
+    // epilogue operand one step ahead: V of plane j+1 (MODE 1) or the old value
+    // of the output stored at step j+1 (MODE 0)
+    constexpr int NE = MODE == 0 ? NC : 1;
+    P2 ep[2][NE][RY];
+    // pending outputs: slot o % 8 holds output plane o (local index; plane j is
+    // z = z0 - 4 + j, output o is stored at step o + 4)
+    T A[NC][RY][2][8];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int i = 0; i < RY; ++i)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int s8 = 0; s8 < 8; ++s8) A[c][i][h][s8] = T(0);
+
+    for (int jb = 0; jb < nplanes; jb += 8) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int j = jb + u;
+            if (j < nplanes) {
+                if (!failed && !mbar_wait(&bar[j % S], (uint32_t)((j / S) & 1))) failed = 1;
+                T* cur = ring + (size_t)(j % S) * C::STAGE;
+                const bool inner = j >= HW && j < nsteps + HW;
+                if (inner) {
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        if (xh_ok) cur[c * C::COMP + xh_s] = hx[u % 4][c];
+                        if (yh_ok) cur[c * C::COMP + yh_s] = hy[u % 4][c];
+                    }
+                }
+                {
+                    const int j2 = j + 2;
+                    if (j2 >= HW && j2 < nsteps + HW) {
+                        const size_t zo2 = nxy * (size_t)(z0 + j2 - HW);
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) {
+                            hx[(u + 2) % 4][c] = xh_ok ? __ldg(src[c] + xh_g + zo2) : T(0);
+                            hy[(u + 2) % 4][c] = yh_ok ? __ldg(src[c] + yh_g + zo2) : T(0);
+                        }
+                    }
+                }
+                if (MODE == 1) {
+                    const int j1 = j + 1;
+                    if (j1 >= HW && j1 < nsteps + HW) {
+                        const size_t zo1 = nxy * (size_t)(z0 + j1 - HW);
+#pragma unroll
+                        for (int i = 0; i < RY; ++i) {
+                            P2 v{};
+                            if (rv[i]) v = __ldg(reinterpret_cast<const P2*>(V + rowoff + (size_t)nx * i + zo1));
+                            ep[(u + 1) % 2][0][i] = v;
+                        }
+                    }
+                } else {
+                    const int o1 = j + 1 - HW;
+                    if (o1 >= HW && o1 < nsteps + HW) {
+                        const size_t zo1 = nxy * (size_t)(z0 + o1 - HW);
+#pragma unroll
+                        for (int c = 0; c < NE; ++c)
+#pragma unroll
+                            for (int i = 0; i < RY; ++i) {
+                                P2 v{};
+                                if (rv[i]) v = *reinterpret_cast<const P2*>(dst[c] + rowoff + (size_t)nx * i + zo1);
+                                ep[(u + 1) % 2][c][i] = v;
+                            }
+                    }
+                }
+                // halo cells of plane j are written, and every thread has finished
+                // step j-1, so stage (j-1) % S is free
+                if (__syncthreads_or(failed)) goto drain;
+                if (t == 0 && j >= 1 && j + S - 1 < nplanes) issue(j + S - 1);
+
+                P2 pc[NC][RY];
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+#pragma unroll
+                    for (int i = 0; i < RY; ++i)
+                        pc[c][i] = *reinterpret_cast<const P2*>(cur + c * C::COMP + soff + i * SW);
+#define PV(c, i, h) ((h) ? pc[c][i].y : pc[c][i].x)
+
+                if (inner) {
+                    T lxy[NC][RY][2];
+                    T gxy[NC][RY][2];
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        const T* s = cur + c * C::COMP + soff;
+                        P2 col[RY + 8];
+#pragma unroll
+                        for (int r = 0; r < RY + 8; ++r)
+                            col[r] = (r >= HW && r < HW + RY) ? pc[c][r - HW]
+                                                             : *reinterpret_cast<const P2*>(s + (r - HW) * SW);
+#pragma unroll
+                        for (int i = 0; i < RY; ++i) {
+                            const T* row = s + i * SW;
+                            const P2 L0 = *reinterpret_cast<const P2*>(row - 4);
+                            const P2 L1 = *reinterpret_cast<const P2*>(row - 2);
+                            const P2 R0 = *reinterpret_cast<const P2*>(row + 2);
+                            const P2 R1 = *reinterpret_cast<const P2*>(row + 4);
+                            const P2 Cc = pc[c][i];
+#pragma unroll
+                            for (int h = 0; h < 2; ++h) {
+                                // x neighbours -4..-1, +1..+4 of point h of the pair
+                                const T xm4 = h ? L0.y : L0.x, xm3 = h ? L1.x : L0.y;
+                                const T xm2 = h ? L1.y : L1.x, xm1 = h ? Cc.x : L1.y;
+                                const T xp1 = h ? R0.x : Cc.y, xp2 = h ? R0.y : R0.x;
+                                const T xp3 = h ? R1.x : R0.y, xp4 = h ? R1.y : R1.x;
+                                const T ym4 = h ? col[i].y : col[i].x, yp4 = h ? col[i + 8].y : col[i + 8].x;
+                                const T ym3 = h ? col[i + 1].y : col[i + 1].x, yp3 = h ? col[i + 7].y : col[i + 7].x;
+                                const T ym2 = h ? col[i + 2].y : col[i + 2].x, yp2 = h ? col[i + 6].y : col[i + 6].x;
+                                const T ym1 = h ? col[i + 3].y : col[i + 3].x, yp1 = h ? col[i + 5].y : col[i + 5].x;
+                                const T sxx = (k.cx[3] * (xp4 + xm4) + k.cx[2] * (xp3 + xm3)) +
+                                              (k.cx[1] * (xp2 + xm2) + k.cx[0] * (xp1 + xm1));
+                                const T syy = (k.cy[3] * (yp4 + ym4) + k.cy[2] * (yp3 + ym3)) +
+                                              (k.cy[1] * (yp2 + ym2) + k.cy[0] * (yp1 + ym1));
+                                lxy[c][i][h] = sxx + syy;
+                                if (GRAD) {
+                                    const T gx_ = (k.ax[3] * (xp4 - xm4) + k.ax[2] * (xp3 - xm3)) +
+                                                  (k.ax[1] * (xp2 - xm2) + k.ax[0] * (xp1 - xm1));
+                                    const T gy_ = (k.ay[3] * (yp4 - ym4) + k.ay[2] * (yp3 - ym3)) +
+                                                  (k.ay[1] * (yp2 - ym2) + k.ay[0] * (yp1 - ym1));
+                                    gxy[c][i][h] = gx_ + gy_;
+                                }
+                            }
+                        }
+                    }
+                    // centre, V and in-plane terms of output j (slot u)
+#pragma unroll
+                    for (int c = 0; c < NC; ++c)
+#pragma unroll
+                        for (int i = 0; i < RY; ++i)
+#pragma unroll
+                            for (int h = 0; h < 2; ++h) {
+                                const T p = PV(c, i, h);
+                                T r = k.c0 * p + lxy[c][i][h];
+                                if constexpr (sizeof(T) == 4) r = fmaf(k.c0lo, p, r);
+                                if (MODE == 1) r += (h ? ep[u % 2][0][i].y : ep[u % 2][0][i].x) * p;
+                                // out_re = L(re) - D(im), out_im = L(im) + D(re)
+                                if (CPLX && GRAD) r += c == 0 ? -gxy[NC - 1][i][h] : gxy[0][i][h];
+                                A[c][i][h][u] += r;
+                            }
+                }
+
+                // plane j enters outputs j -+ m (m = 1..3); output j-4 takes its last term
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+#pragma unroll
+                    for (int i = 0; i < RY; ++i)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const T p = PV(c, i, h);
+                            A[c][i][h][(u + 7) % 8] += k.cz[0] * p;
+                            A[c][i][h][(u + 1) % 8] += k.cz[0] * p;
+                            A[c][i][h][(u + 6) % 8] += k.cz[1] * p;
+                            A[c][i][h][(u + 2) % 8] += k.cz[1] * p;
+                            A[c][i][h][(u + 5) % 8] += k.cz[2] * p;
+                            A[c][i][h][(u + 3) % 8] += k.cz[2] * p;
+                            A[c][i][h][(u + 4) % 8] += k.cz[3] * p;
+                            if (CPLX && GRAD) {
+                                // D z-part: +a_m q[o+m] (o = j-m), -a_m q[o-m] (o = j+m)
+                                const T q = PV(NC - 1 - c, i, h);
+                                const T w = c == 0 ? -q : q;
+                                A[c][i][h][(u + 7) % 8] += k.az[0] * w;
+                                A[c][i][h][(u + 1) % 8] -= k.az[0] * w;
+                                A[c][i][h][(u + 6) % 8] += k.az[1] * w;
+                                A[c][i][h][(u + 2) % 8] -= k.az[1] * w;
+                                A[c][i][h][(u + 5) % 8] += k.az[2] * w;
+                                A[c][i][h][(u + 3) % 8] -= k.az[2] * w;
+                                A[c][i][h][(u + 4) % 8] += k.az[3] * w;
+                            }
+                        }
+                // output j-4 (z = z0 + j - 8) is complete
+                if (j >= 2 * HW) {
+                    const size_t zo = nxy * (size_t)(z0 + j - 2 * HW);
+#pragma unroll
+                    for (int i = 0; i < RY; ++i) {
+                        if (!rv[i]) continue;
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) {
+                            P2 r;
+                            r.x = A[c][i][0][(u + 4) % 8];
+                            r.y = A[c][i][1][(u + 4) % 8];
+                            if (MODE == 0) {
+                                r.x += ep[u % 2][c][i].x;
+                                r.y += ep[u % 2][c][i].y;
+                            }
+                            *reinterpret_cast<P2*>(dst[c] + rowoff + (size_t)nx * i + zo) = r;
+                        }
+                    }
+                }
+                // the freed slot starts output j+4 with plane j's term
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+#pragma unroll
+                    for (int i = 0; i < RY; ++i)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            T a = k.cz[3] * PV(c, i, h);
+                            if (CPLX && GRAD) {
+                                const T q = PV(NC - 1 - c, i, h);
+                                a -= k.az[3] * (c == 0 ? -q : q);
+                            }
+                            A[c][i][h][(u + 4) % 8] = a;
+                        }
+#undef PV
+            }
+        }
+    }
+    return;
+
+drain:
+    // a wait ran out: record it and wait (bounded) for this CTA's copies in flight
+    if (t == 0) {
+        atomicOr(err, ERR_STENCIL_TIMEOUT);
+        for (int st = 0; st < S; ++st) {
+            int jmax = -1;
+            for (int j = st; j < issued; j += S) jmax = j;
+            if (jmax >= 0) (void)mbar_wait(&bar[st], (uint32_t)((jmax / S) & 1));
+        }
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// fd8_ws_kernel: the pending-output z accumulation of fd8_zacc_kernel, fed
+// only by the tensor-memory accelerator, with one producer warp.
+//
+// Per plane, one producer lane issues into a ring stage:
+//   * the 40 x (TY+8) psi box of the tile and its 4-wide halo; at a y boundary
+//     as top / body / bottom boxes at wrapped y coordinates, so the periodic
+//     halo rows land in place (same 40-element pitch);
+//   * at an x boundary, the 4 wrapped columns of the tile's rows as a side box
+//     (4-element pitch; only the tile's own rows need x neighbours); the
+//     zero-filled columns of the main box there are never read;
+//   * the 32 x TY tile of V (MODE 1) or of the old output (MODE 0).
+// The eight compute warps read shared memory only (no global load in the z
+// loop, whose latency measured as the stall of the register-prefetch form)
+// and hand each stage back through an mbarrier: no CTA-wide barrier per plane.
+// Tiles that would pass the grid edge are shifted back inside it and store only
+// the points of their own nominal tile.
+constexpr int WCW = 8;                    // compute warps: 16 x 16 threads
+constexpr int WNT = (WCW + 1) * 32;       // + one producer warp
+
+template <typename T, bool CPLX, int MODE, int RY, int S>
+struct WsCfg {
+    static constexpr int NC = CPLX ? 2 : 1;
+    static constexpr int NE = MODE == 0 ? NC : 1;
+    static constexpr int TY = 16 * RY;
+    static constexpr int SW = ZTX + 2 * HW;                 // main pitch (40)
+    static constexpr int MROWS = TY + 2 * HW;
+    static constexpr int MAIN = MROWS * SW;                 // one component's main box
+    static constexpr int SIDE = TY * HW;                    // side buffer: the tile's rows x 4
+    static constexpr int EBOX = TY * ZTX;                   // V / old-output tile
+    static constexpr int OFF_SIDE = NC * MAIN;              // side[c][L|R]
+    static constexpr int OFF_E = OFF_SIDE + NC * 2 * SIDE;
+    static constexpr int STAGE = OFF_E + NE * EBOX;
+    static constexpr size_t SMEM = (size_t)S * STAGE * sizeof(T) + 2 * S * sizeof(uint64_t) + 128;
+    static constexpr uint32_t MAIN_BYTES = (uint32_t)(MAIN * sizeof(T));
+    static constexpr uint32_t SIDE_BYTES = (uint32_t)(SIDE * sizeof(T));
+    static constexpr uint32_t E_BYTES = (uint32_t)(EBOX * sizeof(T));
+    // every tensor copy lands on a 128-byte boundary
+    static_assert((MAIN * sizeof(T)) % 128 == 0 && (SIDE * sizeof(T)) % 128 == 0 && (EBOX * sizeof(T)) % 128 == 0,
+                  "stage parts aligned");
+    static_assert((HW * SW * sizeof(T)) % 128 == 0 && ((TY + HW) * SW * sizeof(T)) % 128 == 0, "main sub-boxes");
+    static_assert(SMEM <= 227 * 1024, "one CTA per SM");
+};
+
+struct WsMaps {
+    CUtensorMap full, body, four;      // psi: 40 x (TY+8), 40 x TY, 40 x 4
+    CUtensorMap side;                  // psi: 4 x TY
+    CUtensorMap e;                     // V (MODE 1) or out (MODE 0): 32 x TY
+};
+
+template <typename T, bool CPLX, int MODE, bool GRAD, int RY, int S>
+__global__ void __launch_bounds__(WNT, 1)
+fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, int ny, int nz, int zchunk, KC<T> k,
+              int* __restrict__ err) {
+    using C = WsCfg<T, CPLX, MODE, RY, S>;
+    using P2 = typename Pair<T>::type;
+    constexpr int NC = C::NC, NE = C::NE, TY = C::TY, SW = C::SW;
+    extern __shared__ unsigned char smraw_[];
+    unsigned char* smraw = (unsigned char*)(((uintptr_t)smraw_ + 127) & ~(uintptr_t)127);
+    T* ring = reinterpret_cast<T*>(smraw);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smraw + (size_t)S * C::STAGE * sizeof(T));
+    uint64_t* empty = full + S;
+
+    const int ntx = (nx + ZTX - 1) / ZTX;
+    const int x0n = (blockIdx.x % ntx) * ZTX;          // nominal tile: the points this CTA stores
+    const int y0n = (blockIdx.x / ntx) * TY;
+    const int x0 = min(x0n, nx - ZTX);                  // loaded tile, inside the grid
+    const int y0 = min(y0n, ny - TY);
+    const bool ledge = x0 == 0, redge = x0 + ZTX == nx;
+    const bool yedge = y0 < HW || y0 + TY + HW > ny;
+    const int ytop = y0 - HW < 0 ? y0 - HW + ny : y0 - HW;
+    const int ybot = y0 + TY >= ny ? y0 + TY - ny : y0 + TY;
+    const int z0 = blockIdx.y * zchunk;
+    const int z1 = min(nz, z0 + zchunk);
+    const int nsteps = z1 - z0;
+    const int nplanes = nsteps + 2 * HW;
+    const int band = blockIdx.z;
+    const size_t nxy = (size_t)nx * ny;
+    const size_t N = nxy * nz;
+    const int t = threadIdx.y * ZX + threadIdx.x;
+    const int warp = t >> 5, lane = t & 31;
+
+    if (t == 0) {
+        for (int st = 0; st < S; ++st) {
+            mbar_init(&full[st], 1);
+            mbar_init(&empty[st], WCW);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    if (warp == WCW) {
+        // ---------------- producer ----------------
+        if (lane != 0) return;
+        const uint32_t psi_bytes = NC * (C::MAIN_BYTES + ((ledge ? 1 : 0) + (redge ? 1 : 0)) * C::SIDE_BYTES);
+        int issued = 0;
+        bool failed = false;
+        for (int j = 0; j < nplanes; ++j) {
+            const int st = j % S;
+            // stage st last held plane j - S: wait until every compute warp released it
+            if (j >= S && !mbar_wait(&empty[st], (uint32_t)(((j / S) - 1) & 1))) {
+                failed = true;
+                break;
+            }
+            const bool e_on = MODE == 1 ? (j >= HW && j < nsteps + HW) : (j >= 2 * HW);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(&full[st], psi_bytes + (e_on ? NE * C::E_BYTES : 0u));
+            T* stage = ring + (size_t)st * C::STAGE;
+            const int zz = wrapi(z0 - HW + j, nz);
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const int zp = (CPLX ? 2 * band + c : band) * nz + zz;
+                T* mb = stage + c * C::MAIN;
+                if (!yedge) {
+                    tma_load_3d(mb, &maps.full, x0 - HW, y0 - HW, zp, &full[st]);
+                } else {
+                    tma_load_3d(mb, &maps.four, x0 - HW, ytop, zp, &full[st]);
+                    tma_load_3d(mb + HW * SW, &maps.body, x0 - HW, y0, zp, &full[st]);
+                    tma_load_3d(mb + (TY + HW) * SW, &maps.four, x0 - HW, ybot, zp, &full[st]);
+                }
+#pragma unroll
+                for (int sd = 0; sd < 2; ++sd) {
+                    if (sd == 0 ? !ledge : !redge) continue;
+                    tma_load_3d(stage + C::OFF_SIDE + (c * 2 + sd) * C::SIDE, &maps.side, sd == 0 ? nx - HW : 0, y0,
+                                zp, &full[st]);
+                }
+            }
+            if (e_on) {
+                T* eb = stage + C::OFF_E;
+                if (MODE == 1) {
+                    tma_load_3d(eb, &maps.e, x0, y0, z0 + j - HW, &full[st]);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < NE; ++c)
+                        tma_load_3d(eb + c * C::EBOX, &maps.e, x0, y0,
+                                    (CPLX ? 2 * band + c : band) * nz + z0 + j - 2 * HW, &full[st]);
+                }
+            }
+            issued = j + 1;
+        }
+        if (failed) {
+            atomicOr(err, ERR_STENCIL_TIMEOUT);
+            // copies in flight must land before the CTA may exit
+            for (int st = 0; st < S; ++st) {
+                int jmax = -1;
+                for (int j = st; j < issued; j += S) jmax = j;
+                if (jmax >= 0) (void)mbar_wait(&full[st], (uint32_t)((jmax / S) & 1));
+            }
+        }
+        return;
+    }
+    // ---------------- compute warps ----------------
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int gx = x0 + 2 * tx;
+    bool own[RY];
+#pragma unroll
+    for (int i = 0; i < RY; ++i) own[i] = gx >= x0n && y0 + ty * RY + i >= y0n;
+    const size_t rowoff = (size_t)gx + (size_t)nx * (y0 + ty * RY);
+    T* dst[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) dst[c] = out + (CPLX ? (size_t)(2 * band + c) : (size_t)band) * N;
+    // the five x pairs of the thread's first row: shared offset (component 0),
+    // row pitch, and whether they sit in a side buffer
+    int xo[5], xp[5];
+    bool xs[5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+        const int cm = 2 * tx + 2 * m;          // column in the 40-wide main box
+        const int r = ty * RY + HW;             // row of the first point
+        if (ledge && cm < HW) {
+            xo[m] = C::OFF_SIDE + (r - HW) * HW + cm;
+            xp[m] = HW;
+            xs[m] = true;
+        } else if (redge && cm >= ZTX + HW) {
+            xo[m] = C::OFF_SIDE + C::SIDE + (r - HW) * HW + (cm - ZTX - HW);
+            xp[m] = HW;
+            xs[m] = true;
+        } else {
+            xo[m] = r * SW + cm;
+            xp[m] = SW;
+            xs[m] = false;
+        }
+    }
+    const int soff = (ty * RY + HW) * SW + 2 * tx + HW;    // centre pair (main box)
+    const int eoff = ty * RY * ZTX + 2 * tx;               // V / old output pair
+
+    T A[NC][RY][2][8];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int i = 0; i < RY; ++i)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int s8 = 0; s8 < 8; ++s8) A[c][i][h][s8] = T(0);
+    bool failed = false;
+    for (int jb = 0; jb < nplanes && !failed; jb += 8) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int j = jb + u;
+            if (j < nplanes && !failed) {
+                const bool ok = mbar_wait(&full[j % S], (uint32_t)((j / S) & 1));
+                if (__any_sync(0xffffffffu, !ok)) {
+                    failed = true;
+                    continue;
+                }
+                const T* cur = ring + (size_t)(j % S) * C::STAGE;
+                const bool inner = j >= HW && j < nsteps + HW;
+                P2 pc[NC][RY];
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+#pragma unroll
+                    for (int i = 0; i < RY; ++i)
+                        pc[c][i] = *reinterpret_cast<const P2*>(cur + c * C::MAIN + soff + i * SW);
+#define PV(c, i, h) ((h) ? pc[c][i].y : pc[c][i].x)
+                T lxy[NC][RY][2];
+                T gxy[NC][RY][2];
+                P2 ev[NE][RY];
+                if (inner) {
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) {
+                        const T* s = cur + c * C::MAIN + soff;
+                        P2 col[RY + 8];
+#pragma unroll
+                        for (int r = 0; r < RY + 8; ++r)
+                            col[r] = (r >= HW && r < HW + RY) ? pc[c][r - HW]
+                                                             : *reinterpret_cast<const P2*>(s + (r - HW) * SW);
+#pragma unroll
+                        for (int i = 0; i < RY; ++i) {
+                            P2 xv[5];
+#pragma unroll
+                            for (int m = 0; m < 5; ++m)
+                                xv[m] = m == 2 ? pc[c][i]
+                                               : *reinterpret_cast<const P2*>(
+                                                     cur + xo[m] + (xs[m] ? c * 2 * C::SIDE : c * C::MAIN) + i * xp[m]);
+                            const P2 L0 = xv[0], L1 = xv[1], Cc = xv[2], R0 = xv[3], R1 = xv[4];
+#pragma unroll
+                            for (int h = 0; h < 2; ++h) {
+                                // x neighbours -4..-1, +1..+4 of point h of the pair
+                                const T xm4 = h ? L0.y : L0.x, xm3 = h ? L1.x : L0.y;
+                                const T xm2 = h ? L1.y : L1.x, xm1 = h ? Cc.x : L1.y;
+                                const T xp1 = h ? R0.x : Cc.y, xp2 = h ? R0.y : R0.x;
+                                const T xp3 = h ? R1.x : R0.y, xp4 = h ? R1.y : R1.x;
+                                const T ym4 = h ? col[i].y : col[i].x, yp4 = h ? col[i + 8].y : col[i + 8].x;
+                                const T ym3 = h ? col[i + 1].y : col[i + 1].x, yp3 = h ? col[i + 7].y : col[i + 7].x;
+                                const T ym2 = h ? col[i + 2].y : col[i + 2].x, yp2 = h ? col[i + 6].y : col[i + 6].x;
+                                const T ym1 = h ? col[i + 3].y : col[i + 3].x, yp1 = h ? col[i + 5].y : col[i + 5].x;
+                                const T sxx = (k.cx[3] * (xp4 + xm4) + k.cx[2] * (xp3 + xm3)) +
+                                              (k.cx[1] * (xp2 + xm2) + k.cx[0] * (xp1 + xm1));
+                                const T syy = (k.cy[3] * (yp4 + ym4) + k.cy[2] * (yp3 + ym3)) +
+                                              (k.cy[1] * (yp2 + ym2) + k.cy[0] * (yp1 + ym1));
+                                lxy[c][i][h] = sxx + syy;
+                                if (GRAD) {
+                                    const T gx_ = (k.ax[3] * (xp4 - xm4) + k.ax[2] * (xp3 - xm3)) +
+                                                  (k.ax[1] * (xp2 - xm2) + k.ax[0] * (xp1 - xm1));
+                                    const T gy_ = (k.ay[3] * (yp4 - ym4) + k.ay[2] * (yp3 - ym3)) +
+                                                  (k.ay[1] * (yp2 - ym2) + k.ay[0] * (yp1 - ym1));
+                                    gxy[c][i][h] = gx_ + gy_;
+                                }
+                            }
+                        }
+                    }
+                    if (MODE == 1) {
+#pragma unroll
+                        for (int i = 0; i < RY; ++i)
+                            ev[0][i] = *reinterpret_cast<const P2*>(cur + C::OFF_E + eoff + i * ZTX);
+                    }
+                }
+                if (MODE == 0 && j >= 2 * HW) {
+#pragma unroll
+                    for (int c = 0; c < NE; ++c)
+#pragma unroll
+                        for (int i = 0; i < RY; ++i)
+                            ev[c][i] = *reinterpret_cast<const P2*>(cur + C::OFF_E + c * C::EBOX + eoff + i * ZTX);
+                }
+                // every value of plane j is in registers: hand the stage back
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty[j % S]);
+
+                if (inner) {
+                    // centre, V and in-plane terms of output j (slot u)
+#pragma unroll
+                    for (int c = 0; c < NC; ++c)
+#pragma unroll
+                        for (int i = 0; i < RY; ++i)
+#pragma unroll
+                            for (int h = 0; h < 2; ++h) {
+                                const T p = PV(c, i, h);
+                                T r = k.c0 * p + lxy[c][i][h];
+                                if constexpr (sizeof(T) == 4) r = fmaf(k.c0lo, p, r);
+                                if (MODE == 1) r += (h ? ev[0][i].y : ev[0][i].x) * p;
+                                // out_re = L(re) - D(im), out_im = L(im) + D(re)
+                                if (CPLX && GRAD) r += c == 0 ? -gxy[NC - 1][i][h] : gxy[0][i][h];
+                                A[c][i][h][u] += r;
+                            }
+                }
+                // plane j enters outputs j -+ m (m = 1..3); output j-4 takes its last term
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+#pragma unroll
+                    for (int i = 0; i < RY; ++i)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const T p = PV(c, i, h);
+                            A[c][i][h][(u + 7) % 8] += k.cz[0] * p;
+                            A[c][i][h][(u + 1) % 8] += k.cz[0] * p;
+                            A[c][i][h][(u + 6) % 8] += k.cz[1] * p;
+                            A[c][i][h][(u + 2) % 8] += k.cz[1] * p;
+                            A[c][i][h][(u + 5) % 8] += k.cz[2] * p;
+                            A[c][i][h][(u + 3) % 8] += k.cz[2] * p;
+                            A[c][i][h][(u + 4) % 8] += k.cz[3] * p;
+                            if (CPLX && GRAD) {
+                                // D z-part: +a_m q[o+m] (o = j-m), -a_m q[o-m] (o = j+m)
+                                const T q = PV(NC - 1 - c, i, h);
+                                const T w = c == 0 ? -q : q;
+                                A[c][i][h][(u + 7) % 8] += k.az[0] * w;
+                                A[c][i][h][(u + 1) % 8] -= k.az[0] * w;
+                                A[c][i][h][(u + 6) % 8] += k.az[1] * w;
+                                A[c][i][h][(u + 2) % 8] -= k.az[1] * w;
+                                A[c][i][h][(u + 5) % 8] += k.az[2] * w;
+                                A[c][i][h][(u + 3) % 8] -= k.az[2] * w;
+                                A[c][i][h][(u + 4) % 8] += k.az[3] * w;
+                            }
+                        }
+                // output j-4 (z = z0 + j - 8) is complete
+                if (j >= 2 * HW) {
+                    const size_t zo = nxy * (size_t)(z0 + j - 2 * HW);
+#pragma unroll
+                    for (int i = 0; i < RY; ++i) {
+                        if (!own[i]) continue;
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) {
+                            P2 r;
+                            r.x = A[c][i][0][(u + 4) % 8];
+                            r.y = A[c][i][1][(u + 4) % 8];
+                            if (MODE == 0) {
+                                r.x += ev[c][i].x;
+                                r.y += ev[c][i].y;
+                            }
+                            *reinterpret_cast<P2*>(dst[c] + rowoff + (size_t)nx * i + zo) = r;
+                        }
+                    }
+                }
+                // the freed slot starts output j+4 with plane j's term
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+#pragma unroll
+                    for (int i = 0; i < RY; ++i)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            T a = k.cz[3] * PV(c, i, h);
+                            if (CPLX && GRAD) {
+                                const T q = PV(NC - 1 - c, i, h);
+                                a -= k.az[3] * (c == 0 ? -q : q);
+                            }
+                            A[c][i][h][(u + 4) % 8] = a;
+                        }
+#undef PV
+            }
+        }
+    }
+    if (failed && lane == 0) atomicOr(err, ERR_STENCIL_TIMEOUT);
+}
+
 // cuTensorMapEncodeTiled, looked up once through the runtime (no libcuda link)
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -675,6 +1406,106 @@ bool make_plane_map(CUtensorMap* map, const void* base, int nx, int ny, long lon
     return r == CUDA_SUCCESS;
 }
 
+// Stencil kernel choice: 0 fd8_ws_kernel (default; fd8_zacc_kernel where its tiling
+// does not apply), 1 fd8_tma_kernel, 2 fd8_kernel (register prefetch, no TMA),
+// 3 fd8_zacc_kernel; QSB_STENCIL=ws|tma|reg|zacc overrides it for A/B timing.
+int stencil_variant() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("QSB_STENCIL");
+        v = 0;
+        if (e && std::string(e) == "tma") v = 1;
+        if (e && std::string(e) == "reg") v = 2;
+        if (e && std::string(e) == "zacc") v = 3;
+    }
+    return v;
+}
+
+// 3-D map with a (bw, bh, 1) box over an array viewed as [zplanes][ny][nx]
+template <typename T>
+bool make_box_map(CUtensorMap* map, const void* base, int nx, int ny, long long zplanes, int bw, int bh) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)zplanes};
+    const cuuint64_t strides[2] = {(cuuint64_t)nx * sizeof(T), (cuuint64_t)nx * ny * sizeof(T)};
+    const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = fn(map, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                          const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+// A grid extent the box-fed kernel covers: one tile, or tiles (the last one
+// shifted back inside the grid) whose 4-wide halos never straddle the periodic
+// boundary.
+bool ws_dim_ok(int n, int tile) { return n == tile || (n >= tile + HW && (n % tile == 0 || n % tile >= HW)); }
+
+template <typename T, bool CPLX, int MODE, int RY, int S>
+bool launch_ws(const StencilLaunch& L, const FD8Coef& c, const KC<T>& k, cudaStream_t s) {
+    using C = WsCfg<T, CPLX, MODE, RY, S>;
+    if (!ws_dim_ok(L.nx, ZTX) || !ws_dim_ok(L.ny, C::TY) || L.nz < HW) return false;
+    const long long planes = (long long)L.nz * L.nb * (CPLX ? 2 : 1);
+    WsMaps m;
+    bool ok = make_box_map<T>(&m.full, L.in, L.nx, L.ny, planes, C::SW, C::TY + 2 * HW) &&
+              make_box_map<T>(&m.body, L.in, L.nx, L.ny, planes, C::SW, C::TY) &&
+              make_box_map<T>(&m.four, L.in, L.nx, L.ny, planes, C::SW, HW) &&
+              make_box_map<T>(&m.side, L.in, L.nx, L.ny, planes, HW, C::TY);
+    if (MODE == 1) ok = ok && make_box_map<T>(&m.e, L.V, L.nx, L.ny, L.nz, ZTX, C::TY);
+    else ok = ok && make_box_map<T>(&m.e, L.out, L.nx, L.ny, planes, ZTX, C::TY);
+    if (!ok) return false;
+    const int tiles = ((L.nx + ZTX - 1) / ZTX) * ((L.ny + C::TY - 1) / C::TY);
+    // enough CTAs for 148 SMs x 3 waves; split z only when tiles x bands is
+    // small, keeping chunks of >= 16 planes
+    int zsplit = 1;
+    while ((long long)tiles * L.nb * zsplit < 148LL * 3 && L.nz / (zsplit * 2) >= 16) zsplit *= 2;
+    const int zchunk = (L.nz + zsplit - 1) / zsplit;
+    dim3 grid(tiles, (L.nz + zchunk - 1) / zchunk, L.nb), block(ZX, WNT / ZX);
+    if (CPLX && c.has_grad) {
+        auto kern = fd8_ws_kernel<T, CPLX, MODE, CPLX, RY, S>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+        kern<<<grid, block, C::SMEM, s>>>(m, (T*)L.out, L.nx, L.ny, L.nz, zchunk, k, device_error_word());
+    } else {
+        auto kern = fd8_ws_kernel<T, CPLX, MODE, false, RY, S>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+        kern<<<grid, block, C::SMEM, s>>>(m, (T*)L.out, L.nx, L.ny, L.nz, zchunk, k, device_error_word());
+    }
+    return true;
+}
+
+template <typename T, bool CPLX, int MODE, int ZY, int RY, int SREQ, int MINB>
+bool launch_zacc(const StencilLaunch& L, const FD8Coef& c, const KC<T>& k, cudaStream_t s) {
+    // ring depth: SREQ stages, or as many as fit MINB CTAs per SM
+    constexpr int STAGE_B = (CPLX ? 2 : 1) * (ZY * RY + 2 * HW) * (ZTX + 2 * HW) * (int)sizeof(T);
+    constexpr int SFIT = (227 * 1024 / MINB - 256) / STAGE_B;
+    constexpr int S = SREQ < SFIT ? SREQ : SFIT;
+    static_assert(S >= 3, "ring too shallow");
+    using C = ZCfg<T, CPLX, ZY, RY, S, MINB>;
+    const int tiles = ((L.nx + ZTX - 1) / ZTX) * ((L.ny + C::TY - 1) / C::TY);
+    // enough CTAs for 148 SMs x MINB x 3 waves; split z only when tiles x bands
+    // is small, keeping chunks of >= 16 planes
+    int zsplit = 1;
+    while ((long long)tiles * L.nb * zsplit < 148LL * MINB * 3 && L.nz / (zsplit * 2) >= 16) zsplit *= 2;
+    const int zchunk = (L.nz + zsplit - 1) / zsplit;
+    dim3 grid(tiles, (L.nz + zchunk - 1) / zchunk, L.nb), block(ZX, ZY);
+    CUtensorMap map;
+    if (!make_plane_map<T>(&map, L.in, L.nx, L.ny, (long long)L.nz * L.nb * (CPLX ? 2 : 1), C::TY + 2 * HW))
+        return false;
+    if (CPLX && c.has_grad) {
+        auto kern = fd8_zacc_kernel<T, CPLX, MODE, CPLX, ZY, RY, S, MINB>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+        kern<<<grid, block, C::SMEM, s>>>(map, (T*)L.out, (const T*)L.in, (const T*)L.V, L.nx, L.ny, L.nz, zchunk, k,
+                                          device_error_word());
+    } else {
+        auto kern = fd8_zacc_kernel<T, CPLX, MODE, false, ZY, RY, S, MINB>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+        kern<<<grid, block, C::SMEM, s>>>(map, (T*)L.out, (const T*)L.in, (const T*)L.V, L.nx, L.ny, L.nz, zchunk, k,
+                                          device_error_word());
+    }
+    return true;
+}
+
 template <typename T, bool CPLX, int MODE>
 void launch_t(const StencilLaunch& L, const FD8Coef& c, cudaStream_t s) {
     // rows per thread: as many as fit 128 registers without spilling
@@ -695,7 +1526,26 @@ void launch_t(const StencilLaunch& L, const FD8Coef& c, cudaStream_t s) {
     const int vec = 16 / (int)sizeof(T);
     const bool aligned = (L.nx % vec == 0) && (((uintptr_t)L.in) % 16 == 0);
     CUtensorMap map;
-    if (aligned && L.tma_ok &&
+    const int variant = stencil_variant();
+    // the pending-output kernel also moves out / V / old values in 16-byte pairs
+    const bool pairs_ok = ((uintptr_t)L.out % 16 == 0) && (L.V == nullptr || (uintptr_t)L.V % 16 == 0);
+    if (aligned && pairs_ok && L.tma_ok && variant == 0) {
+        // rows per thread: 2 (fp64 complex: 1, within the register file at one CTA per SM)
+        constexpr int WRY = (CPLX && sizeof(T) == 8) ? 1 : 2;
+        constexpr int WS = sizeof(T) == 8 ? (CPLX ? 8 : 6) : (CPLX ? 8 : 12);
+        if (launch_ws<T, CPLX, MODE, WRY, WS>(L, c, k, s)) return;
+    }
+    if (aligned && pairs_ok && L.tma_ok && (variant == 0 || variant == 3)) {
+        // fp64 real 2 rows / 1 CTA per SM (212 registers), fp64 complex 1 row,
+        // fp32 real 2 rows / 2 CTAs per SM, fp32 complex 2 rows / 1 CTA
+        bool done;
+        if (sizeof(T) == 8) done = CPLX ? launch_zacc<T, CPLX, MODE, 16, 1, 8, 1>(L, c, k, s)
+                                        : launch_zacc<T, CPLX, MODE, 16, 2, 8, 1>(L, c, k, s);
+        else done = CPLX ? launch_zacc<T, CPLX, MODE, 16, 2, 8, 1>(L, c, k, s)
+                         : launch_zacc<T, CPLX, MODE, 16, 2, 8, 2>(L, c, k, s);
+        if (done) return;
+    }
+    if (aligned && L.tma_ok && variant <= 1 &&
         make_plane_map<T>(&map, L.in, L.nx, L.ny, (long long)L.nz * L.nb * (CPLX ? 2 : 1), TY + 2 * HW)) {
         using C = TmaCfg<T, CPLX, RY>;
         if (CPLX && c.has_grad) {
