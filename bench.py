@@ -475,7 +475,7 @@ def main():
     traffic = None
     tr_file = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tr_file):
-        traffic = json.load(open(tr_file)).get("fd8_tma_kernel_bytes_per_launch")
+        traffic = json.load(open(tr_file)).get("fd8_ws_kernel_bytes_per_launch")
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -491,7 +491,7 @@ def main():
         "breakdown_ms": {"nonlocal_projection": proj_ms / max(applies, 1), "stencil": sten_ms / max(applies, 1),
                          "nonlocal_expansion": exp_ms / max(applies, 1)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "fd8_tma_kernel (FD8 + V, MODE 1)",
+                     "traffic": traffic, "kernel": "fd8_ws_kernel (FD8 + V, MODE 1)",
                      "peak_source": f"{peak_kind} hbm_gbs"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": NB * N * 8, "d2h_bytes_per_step": NB * N * 8,
                 "ms_per_step": e2e_ms},
