@@ -21,6 +21,8 @@
 //    (mCreateNonoverlapList, :3410-3487), and the pull can be fused into the H
 //    stencil so Hpsi is written once.
 #include "qsb_internal.h"
+#include <cstdlib>
+#include <string>
 
 #include <cmath>
 #include <algorithm>
@@ -279,6 +281,137 @@ nl_apply_kernel(const int* __restrict__ cov_grid, int n_cov, const int* __restri
                 const int col = c0 + k;
                 if (col < ncol) hpsi[(size_t)col * N + g] = cur[k] + (T)acc[k];
             }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// expansion, v2: the pull of nl_apply_kernel with the coefficient rows of every
+// atom staged in shared memory one APPLY_CW-column slice at a time (threads
+// whose points share an atom read them as broadcasts instead of per-point L1
+// loads), up to MAXE entries of the point held in registers across all slices,
+// and SG columns of hpsi loaded before use.
+// ---------------------------------------------------------------------------
+constexpr int APPLY_CW = 32;
+
+template <typename T, bool CPLX, int WM>
+__global__ void __launch_bounds__(APPLY_THREADS, 2)
+nl_apply2_kernel(const int* __restrict__ cov_grid, int n_cov, const int* __restrict__ grid_ptr,
+                 const int* __restrict__ ent_atom, const int* __restrict__ ent_xyz, const T* __restrict__ ent_beta,
+                 int wmax, int n_atoms, const double* __restrict__ coef, int ncol, T* __restrict__ hpsi, size_t N,
+                 double gx_dx, double gy_dy, double gz_dz) {
+    extern __shared__ double csm[];                          // [atom][w][APPLY_CW]
+    constexpr int MAXE = CPLX ? 2 : (WM <= 4 ? 3 : 1);       // entries kept in registers
+    constexpr int SG = CPLX ? 8 : 16;                        // columns per pass
+    const int r = blockIdx.x * APPLY_THREADS + threadIdx.x;
+    const bool active = r < n_cov;
+    int g = 0, e0 = 0, e1 = 0;
+    if (active) {
+        g = __ldg(cov_grid + r);
+        e0 = __ldg(grid_ptr + g);
+        e1 = __ldg(grid_ptr + g + 1);
+    }
+    const int ne = min(MAXE, e1 - e0);
+    double b[MAXE][WM];
+    int ao[MAXE];
+    double cs[MAXE], sn[MAXE];
+    auto load_entry = [&](int e, double* bq, int& aq, double& cq, double& sq) {
+        aq = __ldg(ent_atom + e) * wmax * APPLY_CW;
+#pragma unroll
+        for (int w = 0; w < WM; ++w) bq[w] = w < wmax ? (double)__ldg(ent_beta + (size_t)e * wmax + w) : 0.0;
+        cq = 1.0;
+        sq = 0.0;
+        if (CPLX) {
+            const double kxx = gx_dx * (double)__ldg(ent_xyz + 3 * (size_t)e + 0);
+            const double kyy = gy_dy * (double)__ldg(ent_xyz + 3 * (size_t)e + 1);
+            const double kzz = gz_dz * (double)__ldg(ent_xyz + 3 * (size_t)e + 2);
+            sincos(kxx + kyy + kzz, &sq, &cq);
+        }
+    };
+#pragma unroll
+    for (int q = 0; q < MAXE; ++q) {
+        if (q < ne) {
+            load_entry(e0 + q, b[q], ao[q], cs[q], sn[q]);
+        } else {
+#pragma unroll
+            for (int w = 0; w < WM; ++w) b[q][w] = 0.0;
+            ao[q] = 0;
+            cs[q] = 1.0;
+            sn[q] = 0.0;
+        }
+    }
+    // adds entry (bq, aq, phase) times the staged slice to acc[SG]
+    auto contract = [&](const double* bq, int aq, double cq, double sq, int s0, double* acc) {
+        if constexpr (!CPLX) {
+            // real: no phase, accumulate in place
+#pragma unroll
+            for (int w = 0; w < WM; ++w) {
+                if (w < wmax) {
+                    const double* row = csm + aq + w * APPLY_CW + s0;
+#pragma unroll
+                    for (int k = 0; k < SG; k += 2) {
+                        const double2 v = *reinterpret_cast<const double2*>(row + k);
+                        acc[k] += bq[w] * v.x;
+                        acc[k + 1] += bq[w] * v.y;
+                    }
+                }
+            }
+        } else {
+        double tq[SG];
+#pragma unroll
+        for (int k = 0; k < SG; ++k) tq[k] = 0.0;
+#pragma unroll
+        for (int w = 0; w < WM; ++w) {
+            if (w < wmax) {
+                const double* row = csm + aq + w * APPLY_CW + s0;
+#pragma unroll
+                for (int k = 0; k < SG; k += 2) {
+                    const double2 v = *reinterpret_cast<const double2*>(row + k);
+                    tq[k] += bq[w] * v.x;
+                    tq[k + 1] += bq[w] * v.y;
+                }
+            }
+        }
+        {
+            // exp(-i k.r) (source/PseudoPotNonlocal_SvF2_kpoint.h:4026-4027)
+#pragma unroll
+            for (int j = 0; j < SG / 2; ++j) {
+                acc[2 * j] += cq * tq[2 * j] + sq * tq[2 * j + 1];
+                acc[2 * j + 1] += cq * tq[2 * j + 1] - sq * tq[2 * j];
+            }
+        }
+        }
+    };
+    const int slice = n_atoms * wmax * APPLY_CW;
+    for (int c0 = 0; c0 < ncol; c0 += APPLY_CW) {
+        const int cw = min(APPLY_CW, ncol - c0);
+        __syncthreads();   // the previous slice is no longer read
+        for (int i = threadIdx.x; i < slice; i += APPLY_THREADS) {
+            const int k = i % APPLY_CW, aw = i / APPLY_CW;
+            csm[i] = k < cw ? __ldg(coef + (size_t)aw * ncol + c0 + k) : 0.0;
+        }
+        __syncthreads();
+        if (!active) continue;
+        for (int s0 = 0; s0 < cw; s0 += SG) {
+            T cur[SG];
+#pragma unroll
+            for (int k = 0; k < SG; ++k) cur[k] = s0 + k < cw ? hpsi[(size_t)(c0 + s0 + k) * N + g] : T(0);
+            double acc[SG];
+#pragma unroll
+            for (int k = 0; k < SG; ++k) acc[k] = 0.0;
+#pragma unroll
+            for (int q = 0; q < MAXE; ++q)
+                if (q < ne) contract(b[q], ao[q], cs[q], sn[q], s0, acc);
+            // points covered by more than MAXE spheres
+            for (int e = e0 + MAXE; e < e1; ++e) {
+                double bx[WM], cx, sx;
+                int ax;
+                load_entry(e, bx, ax, cx, sx);
+                contract(bx, ax, cx, sx, s0, acc);
+            }
+#pragma unroll
+            for (int k = 0; k < SG; ++k)
+                if (s0 + k < cw) hpsi[(size_t)(c0 + s0 + k) * N + g] = cur[k] + (T)acc[k];
         }
     }
 }
@@ -588,10 +721,27 @@ qsb_status nl_apply(qsb_dtype dt, const NLDevice& d, int N, int nb, int is_compl
     if (d.n_points == 0 || d.n_cov == 0) return QSB_OK;
     const int ncol = is_complex ? 2 * nb : nb;
     const dim3 grid((d.n_cov + APPLY_THREADS - 1) / APPLY_THREADS);
-#define QSB_APPLY(T, C, W, B)                                                                                      \
-    nl_apply_kernel<T, C, W><<<grid, APPLY_THREADS, 0, s>>>(d.cov_grid, d.n_cov, d.grid_ptr, d.ent_atom, d.ent_xyz, \
-                                                            B, d.wmax, coef, ncol, (T*)hpsi, (size_t)N, nb, gx_dx,  \
-                                                            gy_dy, gz_dz)
+    // v2 (coefficients staged in shared memory) while one slice of every atom's
+    // rows fits; QSB_NLAPPLY=v1 keeps the L1 form for A/B timing
+    static const bool force_v1 = [] {
+        const char* e = std::getenv("QSB_NLAPPLY");
+        return e && std::string(e) == "v1";
+    }();
+    const size_t smem2 = (size_t)d.n_atoms * d.wmax * APPLY_CW * sizeof(double);
+    const bool v2 = !force_v1 && smem2 <= 96 * 1024;
+#define QSB_APPLY(T, C, W, B)                                                                                        \
+    do {                                                                                                             \
+        if (v2) {                                                                                                    \
+            cudaFuncSetAttribute(nl_apply2_kernel<T, C, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2); \
+            nl_apply2_kernel<T, C, W><<<grid, APPLY_THREADS, smem2, s>>>(d.cov_grid, d.n_cov, d.grid_ptr, d.ent_atom, \
+                                                                         d.ent_xyz, B, d.wmax, d.n_atoms, coef, ncol, \
+                                                                         (T*)hpsi, (size_t)N, gx_dx, gy_dy, gz_dz);   \
+        } else {                                                                                                     \
+            nl_apply_kernel<T, C, W><<<grid, APPLY_THREADS, 0, s>>>(d.cov_grid, d.n_cov, d.grid_ptr, d.ent_atom,      \
+                                                                    d.ent_xyz, B, d.wmax, coef, ncol, (T*)hpsi,      \
+                                                                    (size_t)N, nb, gx_dx, gy_dy, gz_dz);            \
+        }                                                                                                            \
+    } while (0)
 #define QSB_APPLY_W(T, C, B)                      \
     do {                                          \
         if (d.wmax <= 1) QSB_APPLY(T, C, 1, B);   \
