@@ -360,6 +360,52 @@ QSB_API qsb_status qsb_ham_set_timing(qsb_ham* ham, int enable);
 QSB_API qsb_status qsb_ham_get_timing(qsb_ham* ham, double* project_ms, double* stencil_ms, double* expand_ms,
                                       int* applies, int* kernel_launches);
 
+/* ---------------------------------------------------------------------------
+ * Self-consistent field on the device (Gamma point, spin-unpolarised, LDA).
+ *
+ * Building blocks:
+ *   qsb_density  rho = sum_n occ_n psi_n^2 over a real bundle (n x N, device;
+ *                occupations on the host).  Replaces mSetDensityByPsi /
+ *                SetDensityOne (source/qumasun_base1.density.h:19-105,
+ *                source/qumasun_SetDensityOne.h).
+ *   qsb_lda_pz   Perdew-Zunger LDA per point: exc = rho eps_xc (may be NULL),
+ *                vxc = V_x + V_c; zero below rho = 1e-8.  Replaces Calc_XC_LDA
+ *                (source/Vxc.h:43-75) as mSetPotentialVxc uses it.
+ *
+ * Driver (the loop of QUMASUN_KPOINT::Execute, source/qumasun_kpoint.scfloop.h:61-230,
+ * with LOBPCG as the solver): per step V_eff = V_loc + V_H[rho_in] + V_xc[rho_in]
+ * goes into the qsb_ham, qsb_lobpcg_d runs lobpcg_iters iterations on X (the
+ * solver's precision decides FP64 or mixed), FP64 Rayleigh quotients of X give
+ * the Fermi-Dirac occupations (bisection of mSetOccupancyTemperature,
+ * source/qumasun_base1.occupancy.h:76-170, kbT set by qsb_scf_set_smearing,
+ * default 0.01 Ha) and the output density, the Kohn-Sham energy of the output
+ * density E = sum occ e - int (V_H + V_xc)[rho_in] rho_out + E_H + E_xc [rho_out]
+ * (ion-ion term excluded: a constant) is recorded, and the run stops when
+ * |dE| / atom < tol_per_atom; otherwise Kerker-preconditioned DIIS (depth, A,
+ * q0 of qsb_scf_set_mixing; default 6, 0.5, 0.8 bohr^-1) gives the next rho_in.
+ * The first density is that of the input X with the lowest bands doubly
+ * filled (mSetOccupancyZero's filling).  V_loc: analytic GTH local parts,
+ * qsb_scf_set_gth_local (per-species arrays indexed by species[atom]).
+ * energies: host, max_steps values; eigen_values / occupations: host, nb
+ * values (may be NULL).  qsb_scf_get_field copies rho_out (0), V_loc (1),
+ * V_eff (2) or the mixed input density (3) to a device buffer of N doubles.
+ * --------------------------------------------------------------------------- */
+typedef struct qsb_scf qsb_scf;
+QSB_API qsb_status qsb_density(int64_t N, int nb, const double* X, const double* occupations, double* rho,
+                               void* stream);
+QSB_API qsb_status qsb_lda_pz(int64_t n, const double* rho, double* exc, double* vxc, void* stream);
+QSB_API qsb_status qsb_scf_create(qsb_scf** scf, qsb_ham* ham, qsb_eigensolver* es, int nb, double num_electrons);
+QSB_API qsb_status qsb_scf_destroy(qsb_scf* scf);
+QSB_API qsb_status qsb_scf_set_gth_local(qsb_scf* scf, int n_atoms, const double* pos, const int* species,
+                                         int n_species, const double* zion, const double* rloc, const double* c1,
+                                         const double* c2);
+QSB_API qsb_status qsb_scf_set_mixing(qsb_scf* scf, double amplitude, double q0, int depth);
+QSB_API qsb_status qsb_scf_set_smearing(qsb_scf* scf, double kbt);
+QSB_API qsb_status qsb_scf_run(qsb_scf* scf, double* X, double* keep, int lobpcg_iters, int max_steps,
+                               double tol_per_atom, double* energies, int* steps, double* eigen_values,
+                               double* occupations, void* stream);
+QSB_API qsb_status qsb_scf_get_field(qsb_scf* scf, int which, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,6 +24,8 @@
  *                             (qumasun_base1.matrix.h:263-317): H = V.psi + NL + FD8(-1/2)
  *   qsref_lobpcg_d            EigenLOBPCG_d_multi           lobpcg_d_multi.h:23-545
  *   qsref_lobpcg_z            LOBPCG::Eigen_z_multi_mpi     lobpcg_z_multi_mpi.h:1732-2852
+ *   qsref_lda_pz              Calc_XC_LDA (Perdew-Zunger)   Vxc.h:43-75
+ *   qsref_set_occupancy       SetOccupancy (Fermi-Dirac)    SetOccupancy.h:7-18
  *
  * The nonlocal class itself (projector construction from UPF via SvF) is not
  * compiled: the projector values are supplied by the caller on the block
@@ -61,6 +63,8 @@ inline int lapack_DSYGVX(double* A, double* B, double* w, double* Z, double* /*t
 #include "lobpcg_d_multi.h"
 #ifdef QSREF_WITH_Z
 #include "lobpcg_z_multi_mpi.h"
+#include "Vxc.h"
+#include "SetOccupancy.h"
 #endif
 
 namespace {
@@ -453,5 +457,19 @@ void qsref_lobpcg_z(int nx, int ny, int nz, double dx, double dy, double dz, con
                               [&](SoAComplex* Ax, SoAComplex* x, int nb) { apply_h_complex(H, Ax, x, nb); }, watch);
 }
 #endif
+
+/* exc[i] = rho eps_xc (exchange + correlation energy density), vxc[i] = V_x + V_c. */
+void qsref_lda_pz(int n, const double* rho, double* exc, double* vxc) {
+    for (int i = 0; i < n; ++i) {
+        const Return_XC r = Calc_XC_LDA(rho[i]);
+        exc[i] = r.rho_E_den_x + r.rho_E_den_c;
+        vxc[i] = r.V_x + r.V_c;
+    }
+}
+
+/* Fermi-Dirac occupations at chemical potential mu; returns their sum. */
+double qsref_set_occupancy(double coef, double kbT, int n, const double* eig, double mu, double* occ) {
+    return SetOccupancy(coef, kbT, n, eig, mu, occ);
+}
 
 } // extern "C"

@@ -1,0 +1,302 @@
+"""CPU oracle of the self-consistent-field loop (test infrastructure only).
+
+Gamma point, spin-unpolarised, LDA (Perdew-Zunger), analytic GTH local part,
+Fermi-Dirac occupations, Kerker-preconditioned DIIS density mixing, and the
+reference's own real LOBPCG (EigenLOBPCG_d_multi through oracle/_ref) as the
+eigensolver.  The step order is QUMASUN_KPOINT::Execute's
+(source/qumasun_kpoint.scfloop.h:61-230): eigensolver -> occupations ->
+density -> mixing -> potentials -> energy -> |dE| test.
+
+Pinned pieces: lda_pz against the reference's Calc_XC_LDA (source/Vxc.h:43-75)
+and fermi_occupations against its SetOccupancy (source/SetOccupancy.h:7-18)
+with the bisection of mSetOccupancyTemperature
+(source/qumasun_base1.occupancy.h:76-170), both compiled from the reference
+sources into oracle/_ref.  Restated from the mathematics (no reference
+counterpart on this path): the GTH local potential in G space, the FFT Poisson
+solve, the Kerker-preconditioned DIIS mixer and the Kohn-Sham energy of the
+output density; SCF-level parity with the reference is therefore unpinned
+(its local potential goes through core charges and a Poisson solve on a finer
+grid, source/qumasun_base1.core.h), and the device SCF is checked against
+this oracle.
+"""
+import contextlib
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+import oracle as O
+
+_C2 = (3.0 / (4.0 * np.pi)) ** (1.0 / 3.0)
+_C3 = -(3.0 / (4.0 * np.pi)) * (9.0 * np.pi / 4.0) ** (1.0 / 3.0)
+
+
+def lda_pz(rho):
+    """(rho * eps_xc, v_xc) of the Perdew-Zunger LDA, zero below rho = 1e-8
+    (Calc_XC_LDA, source/Vxc.h:43-75; PZ81 parameters of calc_LSDA_ge1/_lt1)."""
+    rho = np.asarray(rho, np.float64)
+    exc = np.zeros_like(rho)
+    vxc = np.zeros_like(rho)
+    m = rho >= 1.0e-8
+    r = rho[m]
+    rs = _C2 / np.cbrt(r)
+    ex = _C3 / rs
+    ec = np.empty_like(rs)
+    ndec = np.empty_like(rs)
+    ge = rs >= 1.0
+    s = np.sqrt(rs[ge])
+    g, b1, b2 = -0.1423, 1.0529, 0.3334
+    ec[ge] = g / (1.0 + b1 * s + b2 * rs[ge])
+    ndec[ge] = ec[ge] * ec[ge] * (b1 * 0.5 * s + b2 * rs[ge]) / (3.0 * g)
+    lt = ~ge
+    A, B, C, D = 0.0311, -0.0480, 0.0020, -0.0116
+    lr = np.log(rs[lt])
+    ec[lt] = B + A * lr + D * rs[lt] + C * rs[lt] * lr
+    ndec[lt] = -(A + (D + C) * rs[lt] + C * rs[lt] * lr) / 3.0
+    exc[m] = r * ex + r * ec
+    vxc[m] = (ex + ex / 3.0) + (ec + ndec)
+    return exc, vxc
+
+
+def ref_lda_pz(rho):
+    """The reference's Calc_XC_LDA, compiled from its sources."""
+    lib = O.ref_lib()
+    rho = np.ascontiguousarray(rho, np.float64)
+    exc = np.zeros_like(rho)
+    vxc = np.zeros_like(rho)
+    lib.qsref_lda_pz(rho.size, O._d(rho), O._d(exc), O._d(vxc))
+    return exc, vxc
+
+
+def _occupancy(eig, mu, kbt, weight):
+    # SetOccupancy (source/SetOccupancy.h:7-18): coef / (exp(min(beta (e - mu), 80)) + 1)
+    p = np.minimum((eig - mu) / kbt, 80.0)
+    return weight / (np.exp(p) + 1.0)
+
+
+def fermi_occupations(eig, n_el, kbt, weight=2.0, occupancy=_occupancy):
+    """Occupations at the chemical potential found by the bisection of
+    mSetOccupancyTemperature (source/qumasun_base1.occupancy.h:76-170): mu in
+    [min eig, max eig], halved until the bracket is below 1e-9 or the electron
+    count is met exactly."""
+    eig = np.asarray(eig, np.float64)
+    mu_min, mu_max = float(eig.min()), float(eig.max())
+    mu = 0.5 * (mu_min + mu_max)
+    go = abs(mu_max - mu_min) > 1.0e-9
+    occ = occupancy(eig, mu, kbt, weight)
+    mu_occ = mu
+    while go:
+        occ = occupancy(eig, mu, kbt, weight)
+        mu_occ = mu
+        ne = float(np.sum(occ))
+        if ne < n_el:
+            mu_min = mu
+        elif ne > n_el:
+            mu_max = mu
+        else:
+            break
+        mu = 0.5 * (mu_min + mu_max)
+        go = abs(mu_max - mu_min) > 1.0e-9
+    # the occupations are those of the last evaluated mu (as the reference leaves them)
+    return occ, mu_occ
+
+
+def ref_occupancy(eig, mu, kbt, weight):
+    lib = O.ref_lib()
+    lib.qsref_set_occupancy.restype = ctypes.c_double
+    eig = np.ascontiguousarray(eig, np.float64)
+    occ = np.zeros_like(eig)
+    lib.qsref_set_occupancy(ctypes.c_double(weight), ctypes.c_double(kbt), eig.size, O._d(eig), ctypes.c_double(mu),
+                            O._d(occ))
+    return occ
+
+
+def zero_temperature_occupations(nb, n_el, weight=2.0):
+    """Lowest bands filled with `weight` electrons each (mSetOccupancyZero's
+    filling, source/qumasun_base1.occupancy.h:35-66), used for the initial density."""
+    occ = np.zeros(nb)
+    left = float(n_el)
+    for n in range(nb):
+        occ[n] = min(weight, left)
+        left -= occ[n]
+        if left <= 0.0:
+            break
+    return occ
+
+
+def g_squared(nx, ny, nz, dx, dy, dz):
+    """|G|^2 on the FFT grid, array [z][y][x] (x fastest, as the grid layout)."""
+    gx = 2.0 * np.pi * np.fft.fftfreq(nx, dx)
+    gy = 2.0 * np.pi * np.fft.fftfreq(ny, dy)
+    gz = 2.0 * np.pi * np.fft.fftfreq(nz, dz)
+    return gz[:, None, None] ** 2 + gy[None, :, None] ** 2 + gx[None, None, :] ** 2, (gx, gy, gz)
+
+
+def gth_local_potential(grid, pos, species_params):
+    """V_loc(r) = sum over atoms and periodic images of the GTH local part
+    v(r) = -Z/r erf(r / (sqrt(2) r_loc)) + exp(-(r/r_loc)^2 / 2) (C1 + C2 (r/r_loc)^2)
+    through its Fourier series: v(G) = -4 pi Z exp(-G^2 r^2 / 2) / G^2 + (2 pi)^(3/2)
+    r^3 exp(-G^2 r^2 / 2) (C1 + C2 (3 - G^2 r^2)); at G = 0 the Coulomb tail is
+    neutralised by the electrons' Hartree G = 0 term and the finite remainder
+    2 pi Z r^2 + (2 pi)^(3/2) r^3 (C1 + 3 C2) is kept."""
+    nx, ny, nz, dx, dy, dz = grid
+    omega = nx * ny * nz * dx * dy * dz
+    G2, (gx, gy, gz) = g_squared(nx, ny, nz, dx, dy, dz)
+    VG = np.zeros((nz, ny, nx), np.complex128)
+    nz0 = G2 > 0
+    safe = np.where(nz0, G2, 1.0)
+    for (X, Y, Z), sp in zip(np.asarray(pos, np.float64), species_params):
+        r, zion, c1, c2 = sp["rloc"], sp["zion"], sp["c1"], sp["c2"]
+        e = np.exp(-0.5 * G2 * r * r)
+        coul = np.where(nz0, -4.0 * np.pi * zion * e / safe, 2.0 * np.pi * zion * r * r)
+        short = (2.0 * np.pi) ** 1.5 * r ** 3 * e * (c1 + c2 * (3.0 - G2 * r * r))
+        phase = np.exp(-1j * (gz[:, None, None] * Z + gy[None, :, None] * Y + gx[None, None, :] * X))
+        VG += (coul + short) * phase
+    VG /= omega
+    return (np.fft.ifftn(VG) * (nx * ny * nz)).real.reshape(-1)
+
+
+def hartree(rho, grid):
+    """V_H solving lap V_H = -4 pi rho (G = 0 removed) through the FFT, and
+    E_H = 1/2 int V_H rho."""
+    nx, ny, nz, dx, dy, dz = grid
+    G2, _ = g_squared(nx, ny, nz, dx, dy, dz)
+    rg = np.fft.fftn(np.asarray(rho, np.float64).reshape(nz, ny, nx))
+    vg = np.where(G2 > 0, 4.0 * np.pi * rg / np.where(G2 > 0, G2, 1.0), 0.0)
+    vh = np.fft.ifftn(vg).real.reshape(-1)
+    return vh, 0.5 * float(np.dot(vh, rho)) * dx * dy * dz
+
+
+def kerker(res, grid, amplitude, q0):
+    """A G^2 / (G^2 + q0^2) applied to a density residual (G = 0 removed)."""
+    nx, ny, nz, dx, dy, dz = grid
+    G2, _ = g_squared(nx, ny, nz, dx, dy, dz)
+    rg = np.fft.fftn(np.asarray(res, np.float64).reshape(nz, ny, nx))
+    rg *= amplitude * G2 / (G2 + q0 * q0)
+    return np.fft.ifftn(rg).real.reshape(-1)
+
+
+class KerkerDIIS:
+    """Pulay (DIIS) density mixing with a Kerker preconditioner.
+
+    History of (rho_in_i, R_i = rho_out_i - rho_in_i) over the last `depth`
+    steps; coefficients a (sum a = 1) minimise |sum a_i R_i|^2 (grid inner
+    product), solved as the bordered system [B 1; 1 0][a; l] = [0; 1] with B
+    scaled by its largest diagonal; the next input density is
+    sum a_i rho_in_i + P[sum a_i R_i], P = Kerker(amplitude, q0).  The
+    reference's MixingDIIS (source/mixing_DIIS.h) is the unpreconditioned form
+    of the same bordered system."""
+
+    def __init__(self, grid, amplitude, q0, depth):
+        self.grid, self.A, self.q0, self.depth = grid, amplitude, q0, depth
+        self.rin, self.res = [], []
+
+    def coefficients(self):
+        m = len(self.res)
+        B = np.array([[float(np.dot(a, b)) for b in self.res] for a in self.res])
+        s = max(float(np.max(np.diag(B))), 1e-300)
+        M = np.zeros((m + 1, m + 1))
+        M[:m, :m] = B / s
+        M[:m, m] = 1.0
+        M[m, :m] = 1.0
+        rhs = np.zeros(m + 1)
+        rhs[m] = 1.0
+        return solve_bordered(M, rhs)[:m]
+
+    def next(self, rho_in, rho_out):
+        self.rin.append(np.array(rho_in, np.float64))
+        self.res.append(np.asarray(rho_out, np.float64) - rho_in)
+        if len(self.res) > self.depth:
+            self.rin.pop(0)
+            self.res.pop(0)
+        a = self.coefficients()
+        rin = sum(ai * r for ai, r in zip(a, self.rin))
+        res = sum(ai * r for ai, r in zip(a, self.res))
+        return rin + kerker(res, self.grid, self.A, self.q0)
+
+
+def solve_bordered(M, rhs):
+    """Gaussian elimination with partial pivoting (the device driver's host
+    solve, restated so both sides take the same steps)."""
+    M = np.array(M, np.float64)
+    b = np.array(rhs, np.float64)
+    n = len(b)
+    for k in range(n):
+        p = k + int(np.argmax(np.abs(M[k:, k])))
+        if p != k:
+            M[[k, p]] = M[[p, k]]
+            b[[k, p]] = b[[p, k]]
+        if M[k, k] == 0.0:
+            continue
+        for i in range(k + 1, n):
+            f = M[i, k] / M[k, k]
+            M[i, k:] -= f * M[k, k:]
+            b[i] -= f * b[k]
+    x = np.zeros(n)
+    for i in range(n - 1, -1, -1):
+        x[i] = (b[i] - np.dot(M[i, i + 1:], x[i + 1:])) / M[i, i] if M[i, i] != 0.0 else 0.0
+    return x
+
+
+@contextlib.contextmanager
+def _quiet_stdout():
+    """The reference's LOBPCG prints per band and iteration (printf); route the
+    process's stdout to /dev/null meanwhile."""
+    sys.stdout.flush()
+    saved = os.dup(1)
+    null = os.open(os.devnull, os.O_WRONLY)
+    try:
+        os.dup2(null, 1)
+        yield
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(null)
+
+
+def density(X, occ, N):
+    """rho = sum_n occ_n psi_n^2 (SetDensityOne, source/qumasun_SetDensityOne.h),
+    psi normalised as int |psi|^2 dV = 1."""
+    X = np.asarray(X).reshape(len(occ), N)
+    return np.einsum("n,ni->i", np.asarray(occ, np.float64), X * X)
+
+
+def scf(grid, pos, species_params, nb, n_el, X0, kbt=0.01, lobpcg_iters=4, max_steps=60, tol_per_atom=1e-6,
+        amplitude=0.5, q0=0.8, depth=6, rcut_factor=O.RCUT_FACTOR):
+    """The oracle SCF.  Returns a dict with the per-step total energies,
+    final Rayleigh quotients, occupations, density and wavefunctions."""
+    nx, ny, nz, dx, dy, dz = grid
+    N = nx * ny * nz
+    dV = dx * dy * dz
+    n_atoms = len(pos)
+    tables = O.gth_tables(pos, species_params, dx, dy, dz, rcut_factor=rcut_factor)
+    cube = O.gth_cube_tables(pos, species_params, nx, ny, nz, dx, dy, dz, rcut_factor=rcut_factor)
+    vloc = gth_local_potential(grid, pos, species_params)
+    X = np.array(X0, np.float64).reshape(nb, N).copy()
+    keep = np.zeros_like(X)
+    ev = np.zeros(nb)
+    rho_in = density(X, zero_temperature_occupations(nb, n_el), N)
+    mixer = KerkerDIIS(grid, amplitude, q0, depth)
+    energies, e_prev = [], None
+    for step in range(max_steps):
+        vh, _ = hartree(rho_in, grid)
+        _, vxc = lda_pz(rho_in)
+        veff = vloc + vh + vxc
+        with _quiet_stdout():
+            O.ref_lobpcg_d(grid, veff, cube, X, keep, nb, lobpcg_iters, ev, step == 0)
+        HX = O.hamiltonian(grid, veff, tables, X, nb).reshape(nb, N)
+        rq = np.einsum("ni,ni->n", X, HX) / np.einsum("ni,ni->n", X, X)
+        occ, mu = fermi_occupations(rq, n_el, kbt)
+        rho_out = density(X, occ, N)
+        vh_out, eh = hartree(rho_out, grid)
+        exc_out, _ = lda_pz(rho_out)
+        etot = float(np.dot(occ, rq)) - float(np.dot(vh + vxc, rho_out)) * dV + eh + float(np.sum(exc_out)) * dV
+        energies.append(etot)
+        done = e_prev is not None and abs(etot - e_prev) / n_atoms < tol_per_atom
+        e_prev = etot
+        if done:
+            break
+        rho_in = mixer.next(rho_in, rho_out)
+    return dict(energies=np.array(energies), rq=rq, occ=occ, mu=mu, rho=rho_out, X=X, vloc=vloc, steps=len(energies),
+                converged=done)

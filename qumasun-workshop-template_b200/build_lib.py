@@ -44,7 +44,7 @@ def build(verbose=False, force=False):
     if (force or not os.path.exists(LIB)
             or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs)):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + [
-            "-L/usr/local/cuda/lib64", "-lcublas", "-lcusolver",
+            "-L/usr/local/cuda/lib64", "-lcublas", "-lcusolver", "-lcufft",
             "-Xlinker", "-rpath,/usr/local/cuda/lib64"]
         if verbose:
             print(" ".join(cmd))

@@ -181,16 +181,43 @@ qsb_status qsb_ham_destroy(qsb_ham* h) {
     return QSB_OK;
 }
 
+// V64 = V, V32 = (float)V, flag = 1 on a non-finite value
+static __global__ void potential_copy_kernel(size_t N, const double* __restrict__ V, double* __restrict__ V64,
+                                      float* __restrict__ V32, int* __restrict__ flag) {
+    bool bad = false;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+        const double v = V[i];
+        bad |= !isfinite(v);
+        V64[i] = v;
+        V32[i] = (float)v;
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) *flag = 1;
+}
+
 qsb_status qsb_ham_set_potential(qsb_ham* h, const double* V, int on_device) {
     if (!h || !V) return fail(QSB_ERR_INVALID, "set_potential: null argument");
+    if (!h->V64) QSB_CUDA_TRY(cudaMalloc((void**)&h->V64, h->N * sizeof(double)));
+    if (!h->V32) QSB_CUDA_TRY(cudaMalloc((void**)&h->V32, h->N * sizeof(float)));
+    if (on_device) {
+        // stays on the device: copy, FP32 copy and a non-finite flag (4 bytes back)
+        int* flag = nullptr;
+        QSB_CUDA_TRY(cudaMalloc((void**)&flag, sizeof(int)));
+        QSB_CUDA_TRY(cudaMemset(flag, 0, sizeof(int)));
+        potential_copy_kernel<<<(unsigned)std::min<size_t>((h->N + 255) / 256, 148 * 8), 256>>>(h->N, V, h->V64,
+                                                                                              h->V32, flag);
+        int hf = 0;
+        const cudaError_t e = cudaGetLastError();
+        QSB_CUDA_TRY(cudaMemcpy(&hf, flag, sizeof(int), cudaMemcpyDeviceToHost));
+        cudaFree(flag);
+        if (e != cudaSuccess) return cuda_fail(e, "potential_copy_kernel");
+        if (hf) return fail(QSB_ERR_NUMERIC, "set_potential: non-finite value");
+        return QSB_OK;
+    }
     std::vector<double> hv(h->N);
-    if (on_device) QSB_CUDA_TRY(cudaMemcpy(hv.data(), V, h->N * sizeof(double), cudaMemcpyDeviceToHost));
-    else std::memcpy(hv.data(), V, h->N * sizeof(double));
+    std::memcpy(hv.data(), V, h->N * sizeof(double));
     for (size_t i = 0; i < h->N; ++i)
         if (!std::isfinite(hv[i])) return fail(QSB_ERR_NUMERIC, "set_potential: non-finite value");
     std::vector<float> hf(hv.begin(), hv.end());
-    if (!h->V64) QSB_CUDA_TRY(cudaMalloc((void**)&h->V64, h->N * sizeof(double)));
-    if (!h->V32) QSB_CUDA_TRY(cudaMalloc((void**)&h->V32, h->N * sizeof(float)));
     QSB_CUDA_TRY(cudaMemcpy(h->V64, hv.data(), h->N * sizeof(double), cudaMemcpyHostToDevice));
     QSB_CUDA_TRY(cudaMemcpy(h->V32, hf.data(), h->N * sizeof(float), cudaMemcpyHostToDevice));
     return QSB_OK;

@@ -1,0 +1,652 @@
+// Self-consistent-field driver on the device: Gamma point, spin-unpolarised,
+// LDA (Perdew-Zunger), analytic GTH local part, Fermi-Dirac occupations,
+// Kerker-preconditioned DIIS density mixing, the real LOBPCG of lobpcg.cu.
+//
+// Step order of QUMASUN_KPOINT::Execute (source/qumasun_kpoint.scfloop.h:61-230):
+// eigensolver -> occupations -> density -> mixing -> potentials -> energy ->
+// |dE| / atom test.  The wavefunctions, densities, potentials, the Poisson and
+// XC steps and the mixing history stay on the device; per step only the band
+// energies (nb values), a handful of inner products and the DIIS matrix cross
+// to the host.
+//
+// Pieces and their sources:
+//   * density: SetDensityOne (source/qumasun_SetDensityOne.h), rho = sum occ psi^2;
+//   * LDA: Calc_XC_LDA (source/Vxc.h:43-75);
+//   * occupations: SetOccupancy (source/SetOccupancy.h:7-18) with the bisection
+//     of mSetOccupancyTemperature (source/qumasun_base1.occupancy.h:76-170);
+//   * Hartree: lap V = -4 pi rho by the FFT (cuFFT), G = 0 removed;
+//   * GTH local part in G space (published GTH form), Kerker-preconditioned
+//     DIIS and the Kohn-Sham energy of the output density: restated from the
+//     mathematics (the reference forms its local potential from core charges on
+//     a finer grid, source/qumasun_base1.core.h, and mixes with DIIS or Kerker
+//     separately, source/mixing_DIIS.h, source/mixing_kerker.h).
+#include "qsb_internal.h"
+#include <cufft.h>
+#include <cmath>
+#include <vector>
+#include <algorithm>
+
+namespace qsb {
+namespace {
+
+constexpr int RB = 256;          // reduction block
+constexpr int RBLOCKS = 592;     // partial sums (4 x 148 SMs), fixed: deterministic order
+
+// ---------------- pointwise kernels ----------------
+
+// rho[i] = sum_n occ[n] X[n][i]^2, bands in order (deterministic)
+__global__ void density_kernel(size_t N, int nb, const double* __restrict__ X, const double* __restrict__ occ,
+                               double* __restrict__ rho) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+        double r = 0.0;
+        for (int n = 0; n < nb; ++n) {
+            const double x = X[(size_t)n * N + i];
+            r += occ[n] * (x * x);
+        }
+        rho[i] = r;
+    }
+}
+
+// Perdew-Zunger LDA (Calc_XC_LDA, source/Vxc.h:43-75): exc = rho eps_xc, vxc = V_x + V_c
+__device__ __forceinline__ void lda_pz_point(double rho, double& exc, double& vxc) {
+    if (rho < 1.0e-8) {
+        exc = 0.0;
+        vxc = 0.0;
+        return;
+    }
+    const double c2 = 0.62035049089940001667;            // cbrt(3 / (4 pi))
+    const double c3 = -0.45816529328314287;               // -(3 / (4 pi)) cbrt(9 pi / 4)
+    const double rs = c2 / cbrt(rho);
+    const double ex = c3 / rs;
+    double ec, ndec;
+    if (rs >= 1.0) {
+        const double g = -0.1423, b1 = 1.0529, b2 = 0.3334;
+        const double s = sqrt(rs);
+        ec = g / (1.0 + b1 * s + b2 * rs);
+        ndec = ec * ec * (b1 * 0.5 * s + b2 * rs) / (3.0 * g);
+    } else {
+        const double A = 0.0311, B = -0.0480, C = 0.0020, D = -0.0116;
+        const double lr = log(rs);
+        ec = B + A * lr + D * rs + C * rs * lr;
+        ndec = -(A + (D + C) * rs + C * rs * lr) / 3.0;
+    }
+    exc = rho * ex + rho * ec;
+    vxc = (ex + ex / 3.0) + (ec + ndec);
+}
+
+__global__ void lda_kernel(size_t N, const double* __restrict__ rho, double* __restrict__ exc,
+                           double* __restrict__ vxc) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+        double e, v;
+        lda_pz_point(rho[i], e, v);
+        if (exc) exc[i] = e;
+        vxc[i] = v;
+    }
+}
+
+// out = a + b + c
+__global__ void sum3_kernel(size_t N, const double* __restrict__ a, const double* __restrict__ b,
+                            const double* __restrict__ c, double* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = a[i] + b[i] + c[i];
+}
+
+// out = a - b
+__global__ void sub_kernel(size_t N, const double* __restrict__ a, const double* __restrict__ b,
+                           double* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = a[i] - b[i];
+}
+
+// out = sum_k coef[k] in[k], m <= 8 arrays, in the given order
+struct Combo {
+    const double* in[8];
+    double coef[8];
+    int m;
+};
+__global__ void combo_kernel(size_t N, Combo c, double* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+        double r = 0.0;
+        for (int k = 0; k < c.m; ++k) r += c.coef[k] * c.in[k][i];
+        out[i] = r;
+    }
+}
+
+// out += in
+__global__ void add_kernel(size_t N, const double* __restrict__ in, double* __restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x)
+        out[i] += in[i];
+}
+
+// ---------------- deterministic reductions ----------------
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < RB / 32; ++w) r += sh[w];
+    __syncthreads();
+    return r;
+}
+
+// partial[j * gridDim.x + blockIdx.x] = sum over this block's points of a_j b (j < na; b null: of a_j)
+__global__ void __launch_bounds__(RB) dot_partial_kernel(size_t N, int na, const double* const* __restrict__ a,
+                                                         const double* __restrict__ b, double* __restrict__ partial) {
+    __shared__ double sh[RB / 32];
+    for (int j = 0; j < na; ++j) {
+        double v = 0.0;
+        for (size_t i = blockIdx.x * (size_t)RB + threadIdx.x; i < N; i += (size_t)gridDim.x * RB)
+            v += b ? a[j][i] * b[i] : a[j][i];
+        const double s = block_sum(v, sh);
+        if (threadIdx.x == 0) partial[(size_t)j * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// per band n: partial[n][blk] = sum x_n y_n and sum x_n x_n over this block's points
+__global__ void __launch_bounds__(RB) band_dot_kernel(size_t N, const double* __restrict__ X,
+                                                      const double* __restrict__ Y, double* __restrict__ pxy,
+                                                      double* __restrict__ pxx) {
+    __shared__ double sh[RB / 32];
+    const int n = blockIdx.y;
+    const double* x = X + (size_t)n * N;
+    const double* y = Y + (size_t)n * N;
+    double vxy = 0.0, vxx = 0.0;
+    for (size_t i = blockIdx.x * (size_t)RB + threadIdx.x; i < N; i += (size_t)gridDim.x * RB) {
+        const double xi = x[i];
+        vxy += xi * y[i];
+        vxx += xi * xi;
+    }
+    const double s1 = block_sum(vxy, sh);
+    const double s2 = block_sum(vxx, sh);
+    if (threadIdx.x == 0) {
+        pxy[(size_t)n * gridDim.x + blockIdx.x] = s1;
+        pxx[(size_t)n * gridDim.x + blockIdx.x] = s2;
+    }
+}
+
+// out[j] = sum over blk of partial[j][blk], fixed order (one warp per row)
+__global__ void row_sum_kernel(int rows, int cols, const double* __restrict__ partial, double* __restrict__ out) {
+    const int j = blockIdx.x;
+    if (j >= rows) return;
+    double v = 0.0;
+    for (int k = threadIdx.x; k < cols; k += 32) v += partial[(size_t)j * cols + k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) out[j] = v;
+}
+
+// ---------------- reciprocal space (half-complex grid [nz][ny][nx/2+1]) ----------------
+
+__device__ __forceinline__ double freq(int k, int n, double d) {
+    // numpy fftfreq convention: k < n/2 -> k, else k - n (the Nyquist bin is -n/2)
+    return 2.0 * M_PI * (double)(k < (n + 1) / 2 ? k : k - n) / ((double)n * d);
+}
+
+struct KGrid {
+    int nx, ny, nz, nxh;
+    double dx, dy, dz;
+};
+
+__device__ __forceinline__ void kvec(const KGrid& g, size_t idx, double& gx, double& gy, double& gz) {
+    const int kx = (int)(idx % g.nxh);
+    const size_t r = idx / g.nxh;
+    const int ky = (int)(r % g.ny);
+    const int kz = (int)(r / g.ny);
+    gx = freq(kx, g.nx, g.dx);
+    gy = freq(ky, g.ny, g.dy);
+    gz = freq(kz, g.nz, g.dz);
+}
+
+// f *= 4 pi / G^2 / N (G != 0), 0 at G = 0
+__global__ void hartree_k_kernel(KGrid g, size_t M, double inv_n, cufftDoubleComplex* __restrict__ f) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < M; i += (size_t)gridDim.x * blockDim.x) {
+        double gx, gy, gz;
+        kvec(g, i, gx, gy, gz);
+        const double g2 = gx * gx + gy * gy + gz * gz;
+        const double s = g2 > 0.0 ? 4.0 * M_PI / g2 * inv_n : 0.0;
+        f[i].x *= s;
+        f[i].y *= s;
+    }
+}
+
+// f *= A G^2 / (G^2 + q0^2) / N, 0 at G = 0
+__global__ void kerker_k_kernel(KGrid g, size_t M, double inv_n, double amp, double q02,
+                                cufftDoubleComplex* __restrict__ f) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < M; i += (size_t)gridDim.x * blockDim.x) {
+        double gx, gy, gz;
+        kvec(g, i, gx, gy, gz);
+        const double g2 = gx * gx + gy * gy + gz * gz;
+        const double s = g2 > 0.0 ? amp * g2 / (g2 + q02) * inv_n : 0.0;
+        f[i].x *= s;
+        f[i].y *= s;
+    }
+}
+
+// GTH local part: V(G) = (1/Omega) sum_a v_a(G) exp(-i G.R_a),
+// v(G) = -4 pi Z exp(-G^2 r^2 / 2) / G^2 + (2 pi)^(3/2) r^3 exp(-G^2 r^2 / 2) (C1 + C2 (3 - G^2 r^2)),
+// G = 0: 2 pi Z r^2 + (2 pi)^(3/2) r^3 (C1 + 3 C2)  (Coulomb tail neutralised by the Hartree G = 0 term)
+struct GthAtom {
+    double x, y, z, zion, rloc, c1, c2;
+};
+__global__ void vloc_k_kernel(KGrid g, size_t M, double inv_omega, int na, const GthAtom* __restrict__ atoms,
+                              cufftDoubleComplex* __restrict__ f) {
+    const double tp32 = 15.749609945722419;   // (2 pi)^(3/2)
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < M; i += (size_t)gridDim.x * blockDim.x) {
+        double gx, gy, gz;
+        kvec(g, i, gx, gy, gz);
+        const double g2 = gx * gx + gy * gy + gz * gz;
+        double re = 0.0, im = 0.0;
+        for (int a = 0; a < na; ++a) {
+            const GthAtom at = atoms[a];
+            const double r2 = at.rloc * at.rloc;
+            const double e = exp(-0.5 * g2 * r2);
+            const double coul = g2 > 0.0 ? -4.0 * M_PI * at.zion * e / g2 : 2.0 * M_PI * at.zion * r2;
+            const double v = coul + tp32 * r2 * at.rloc * e * (at.c1 + at.c2 * (3.0 - g2 * r2));
+            double sn, cs;
+            sincos(gx * at.x + gy * at.y + gz * at.z, &sn, &cs);
+            re += v * cs;
+            im -= v * sn;
+        }
+        f[i].x = re * inv_omega;
+        f[i].y = im * inv_omega;
+    }
+}
+
+inline int pw_blocks(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
+
+}  // namespace
+}  // namespace qsb
+
+struct qsb_scf {
+    qsb_ham* ham = nullptr;
+    qsb_eigensolver* es = nullptr;
+    int nx = 0, ny = 0, nz = 0, nb = 0;
+    size_t N = 0, M = 0;          // grid points, half-complex points
+    double dx = 0, dy = 0, dz = 0, dV = 0;
+    double n_el = 0, kbt = 0.01;
+    double amp = 0.5, q0 = 0.8;
+    int depth = 6;
+    int n_atoms = 0;
+    // device fields
+    double *vloc = nullptr, *rho_in = nullptr, *rho_out = nullptr, *vh = nullptr, *vxc = nullptr, *veff = nullptr;
+    double *exc = nullptr, *tmp = nullptr, *hx = nullptr, *hist = nullptr;   // hist: depth x (rho_in, R)
+    double *partial = nullptr, *sums = nullptr, *occ_dev = nullptr;
+    const double** ptrs = nullptr;
+    cufftDoubleComplex* fk = nullptr;
+    cufftHandle plan_f = 0, plan_b = 0;
+    bool have_plans = false;
+    // host
+    std::vector<int> slots;       // history slots, oldest first
+    std::vector<double> B;        // depth x depth residual inner products (by slot)
+};
+
+namespace qsb {
+namespace {
+
+#define QSB_CUFFT_TRY(expr)                                                                          \
+    do {                                                                                             \
+        const cufftResult r_ = (expr);                                                               \
+        if (r_ != CUFFT_SUCCESS) return fail(QSB_ERR_CUDA, std::string("cuFFT call failed: ") + #expr); \
+    } while (0)
+
+KGrid kgrid(const qsb_scf* c) { return KGrid{c->nx, c->ny, c->nz, c->nx / 2 + 1, c->dx, c->dy, c->dz}; }
+
+// dots[j] = int a_j b dV (b null: int a_j dV), na <= 8, deterministic
+qsb_status dots(qsb_scf* c, int na, const double* const* a, const double* b, double* out, cudaStream_t s) {
+    QSB_CUDA_TRY(cudaMemcpyAsync((void*)c->ptrs, a, na * sizeof(double*), cudaMemcpyHostToDevice, s));
+    dot_partial_kernel<<<RBLOCKS, RB, 0, s>>>(c->N, na, c->ptrs, b, c->partial);
+    row_sum_kernel<<<na, 32, 0, s>>>(na, RBLOCKS, c->partial, c->sums);
+    QSB_CUDA_TRY(cudaMemcpyAsync(out, c->sums, na * sizeof(double), cudaMemcpyDeviceToHost, s));
+    QSB_CUDA_TRY(cudaStreamSynchronize(s));
+    for (int j = 0; j < na; ++j) out[j] *= c->dV;
+    return QSB_OK;
+}
+
+// out = FFT^-1 [ factor(G) FFT[in] ]  (factor kernels divide by N)
+enum class KOp { hartree, kerker };
+qsb_status kspace(qsb_scf* c, KOp op, const double* in, double* out, cudaStream_t s) {
+    QSB_CUFFT_TRY(cufftSetStream(c->plan_f, s));
+    QSB_CUFFT_TRY(cufftSetStream(c->plan_b, s));
+    QSB_CUFFT_TRY(cufftExecD2Z(c->plan_f, const_cast<double*>(in), c->fk));
+    const double inv_n = 1.0 / (double)c->N;
+    if (op == KOp::hartree) hartree_k_kernel<<<pw_blocks(c->M), 256, 0, s>>>(kgrid(c), c->M, inv_n, c->fk);
+    else kerker_k_kernel<<<pw_blocks(c->M), 256, 0, s>>>(kgrid(c), c->M, inv_n, c->amp, c->q0 * c->q0, c->fk);
+    QSB_CUFFT_TRY(cufftExecZ2D(c->plan_b, c->fk, out));
+    QSB_CUDA_TRY(cudaGetLastError());
+    return QSB_OK;
+}
+
+// veff = vloc + V_H[rho_in] + V_xc[rho_in]
+qsb_status potentials(qsb_scf* c, cudaStream_t s) {
+    QSB_TRY(kspace(c, KOp::hartree, c->rho_in, c->vh, s));
+    lda_kernel<<<pw_blocks(c->N), 256, 0, s>>>(c->N, c->rho_in, nullptr, c->vxc);
+    sum3_kernel<<<pw_blocks(c->N), 256, 0, s>>>(c->N, c->vloc, c->vh, c->vxc, c->veff);
+    QSB_CUDA_TRY(cudaGetLastError());
+    return qsb_ham_set_potential(c->ham, c->veff, 1);
+}
+
+// Fermi-Dirac occupations (SetOccupancy, source/SetOccupancy.h:7-18) at the mu of
+// the bisection of mSetOccupancyTemperature (source/qumasun_base1.occupancy.h:76-170)
+void fermi(const std::vector<double>& eig, double n_el, double kbt, std::vector<double>& occ) {
+    const int n = (int)eig.size();
+    auto fill = [&](double mu) {
+        double sum = 0.0;
+        for (int k = 0; k < n; ++k) {
+            const double p = std::min((eig[k] - mu) / kbt, 80.0);
+            occ[k] = 2.0 / (std::exp(p) + 1.0);
+            sum += occ[k];
+        }
+        return sum;
+    };
+    double mu_min = *std::min_element(eig.begin(), eig.end()), mu_max = *std::max_element(eig.begin(), eig.end());
+    double mu = 0.5 * (mu_min + mu_max);
+    bool go = std::fabs(mu_max - mu_min) > 1.0e-9;
+    fill(mu);
+    while (go) {
+        const double ne = fill(mu);
+        if (ne < n_el) mu_min = mu;
+        else if (ne > n_el) mu_max = mu;
+        else break;
+        mu = 0.5 * (mu_min + mu_max);
+        go = std::fabs(mu_max - mu_min) > 1.0e-9;
+    }
+}
+
+// Gaussian elimination with partial pivoting of the bordered DIIS system
+void solve_bordered(std::vector<double> M, std::vector<double> b, std::vector<double>& x) {
+    const int n = (int)b.size();
+    for (int k = 0; k < n; ++k) {
+        int p = k;
+        for (int i = k + 1; i < n; ++i)
+            if (std::fabs(M[i * n + k]) > std::fabs(M[p * n + k])) p = i;
+        if (p != k) {
+            for (int j = 0; j < n; ++j) std::swap(M[k * n + j], M[p * n + j]);
+            std::swap(b[k], b[p]);
+        }
+        if (M[k * n + k] == 0.0) continue;
+        for (int i = k + 1; i < n; ++i) {
+            const double f = M[i * n + k] / M[k * n + k];
+            for (int j = k; j < n; ++j) M[i * n + j] -= f * M[k * n + j];
+            b[i] -= f * b[k];
+        }
+    }
+    x.assign(n, 0.0);
+    for (int i = n - 1; i >= 0; --i) {
+        double r = b[i];
+        for (int j = i + 1; j < n; ++j) r -= M[i * n + j] * x[j];
+        x[i] = M[i * n + i] != 0.0 ? r / M[i * n + i] : 0.0;
+    }
+}
+
+double* hist_rin(qsb_scf* c, int slot) { return c->hist + (size_t)(2 * slot) * c->N; }
+double* hist_res(qsb_scf* c, int slot) { return c->hist + (size_t)(2 * slot + 1) * c->N; }
+
+// Kerker-preconditioned DIIS: rho_in <- sum a_i rho_in_i + P[sum a_i R_i]
+qsb_status mix(qsb_scf* c, cudaStream_t s) {
+    const int D = c->depth;
+    int slot;
+    if ((int)c->slots.size() < D) {
+        slot = (int)c->slots.size();
+    } else {
+        slot = c->slots.front();
+        c->slots.erase(c->slots.begin());
+    }
+    c->slots.push_back(slot);
+    const size_t bytes = c->N * sizeof(double);
+    QSB_CUDA_TRY(cudaMemcpyAsync(hist_rin(c, slot), c->rho_in, bytes, cudaMemcpyDeviceToDevice, s));
+    sub_kernel<<<pw_blocks(c->N), 256, 0, s>>>(c->N, c->rho_out, c->rho_in, hist_res(c, slot));
+    QSB_CUDA_TRY(cudaGetLastError());
+    // inner products of the new residual with every stored one
+    const int m = (int)c->slots.size();
+    const double* a[8];
+    for (int k = 0; k < m; ++k) a[k] = hist_res(c, c->slots[k]);
+    double d[8];
+    QSB_TRY(dots(c, m, a, hist_res(c, slot), d, s));
+    for (int k = 0; k < m; ++k) {
+        c->B[slot * D + c->slots[k]] = d[k];
+        c->B[c->slots[k] * D + slot] = d[k];
+    }
+    // bordered system in history order, B scaled by its largest diagonal
+    double sc = 0.0;
+    for (int k = 0; k < m; ++k) sc = std::max(sc, c->B[c->slots[k] * D + c->slots[k]]);
+    sc = std::max(sc, 1e-300);
+    const int n = m + 1;
+    std::vector<double> Mt(n * n, 0.0), rhs(n, 0.0), x;
+    for (int i = 0; i < m; ++i) {
+        for (int j = 0; j < m; ++j) Mt[i * n + j] = c->B[c->slots[i] * D + c->slots[j]] / sc;
+        Mt[i * n + m] = 1.0;
+        Mt[m * n + i] = 1.0;
+    }
+    rhs[m] = 1.0;
+    solve_bordered(Mt, rhs, x);
+    Combo cr{}, cq{};
+    cr.m = cq.m = m;
+    for (int k = 0; k < m; ++k) {
+        cr.in[k] = hist_rin(c, c->slots[k]);
+        cq.in[k] = hist_res(c, c->slots[k]);
+        cr.coef[k] = cq.coef[k] = x[k];
+    }
+    combo_kernel<<<pw_blocks(c->N), 256, 0, s>>>(c->N, cr, c->rho_in);
+    combo_kernel<<<pw_blocks(c->N), 256, 0, s>>>(c->N, cq, c->tmp);
+    QSB_CUDA_TRY(cudaGetLastError());
+    QSB_TRY(kspace(c, KOp::kerker, c->tmp, c->tmp, s));
+    add_kernel<<<pw_blocks(c->N), 256, 0, s>>>(c->N, c->tmp, c->rho_in);
+    QSB_CUDA_TRY(cudaGetLastError());
+    return QSB_OK;
+}
+
+}  // namespace
+}  // namespace qsb
+
+using namespace qsb;
+
+extern "C" {
+
+qsb_status qsb_density(int64_t N, int nb, const double* X, const double* occupations, double* rho, void* stream) {
+    if (N <= 0 || nb < 0 || !X || !occupations || !rho) return fail(QSB_ERR_INVALID, "density: bad argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    double* occ = nullptr;
+    QSB_CUDA_TRY(cudaMallocAsync((void**)&occ, std::max(nb, 1) * sizeof(double), s));
+    QSB_CUDA_TRY(cudaMemcpyAsync(occ, occupations, nb * sizeof(double), cudaMemcpyHostToDevice, s));
+    density_kernel<<<pw_blocks((size_t)N), 256, 0, s>>>((size_t)N, nb, X, occ, rho);
+    QSB_CUDA_TRY(cudaGetLastError());
+    QSB_CUDA_TRY(cudaFreeAsync(occ, s));
+    return QSB_OK;
+}
+
+qsb_status qsb_lda_pz(int64_t n, const double* rho, double* exc, double* vxc, void* stream) {
+    if (n <= 0 || !rho || !vxc) return fail(QSB_ERR_INVALID, "lda_pz: bad argument");
+    lda_kernel<<<pw_blocks((size_t)n), 256, 0, (cudaStream_t)stream>>>((size_t)n, rho, exc, vxc);
+    QSB_CUDA_TRY(cudaGetLastError());
+    return QSB_OK;
+}
+
+qsb_status qsb_scf_create(qsb_scf** out, qsb_ham* ham, qsb_eigensolver* es, int nb, double num_electrons) {
+    if (!out || !ham || !es || nb <= 0 || !(num_electrons > 0.0) || num_electrons > 2.0 * nb)
+        return fail(QSB_ERR_INVALID, "scf_create: bad argument (need ham, solver, nb > 0, 0 < electrons <= 2 nb)");
+    if (ham->nx < 2 || ham->ny < 2 || ham->nz < 2) return fail(QSB_ERR_INVALID, "scf_create: grid too small");
+    auto* c = new qsb_scf;
+    c->ham = ham;
+    c->es = es;
+    c->nx = ham->nx; c->ny = ham->ny; c->nz = ham->nz;
+    c->dx = ham->dx; c->dy = ham->dy; c->dz = ham->dz;
+    c->N = (size_t)c->nx * c->ny * c->nz;
+    c->M = (size_t)c->nz * c->ny * (c->nx / 2 + 1);
+    c->dV = c->dx * c->dy * c->dz;
+    c->nb = nb;
+    c->n_el = num_electrons;
+    *out = c;
+    auto cleanup = [&](qsb_status st) {
+        qsb_scf_destroy(c);
+        *out = nullptr;
+        return st;
+    };
+    const size_t fb = c->N * sizeof(double);
+    double** fields[] = {&c->vloc, &c->rho_in, &c->rho_out, &c->vh, &c->vxc, &c->veff, &c->exc, &c->tmp};
+    for (double** f : fields) {
+        if (cudaMalloc((void**)f, fb) != cudaSuccess) return cleanup(fail(QSB_ERR_NOMEM, "scf_create: device allocation"));
+        cudaMemset(*f, 0, fb);
+    }
+    if (cudaMalloc((void**)&c->hist, 2 * (size_t)c->depth * fb) != cudaSuccess ||
+        cudaMalloc((void**)&c->hx, (size_t)nb * fb) != cudaSuccess ||
+        cudaMalloc((void**)&c->partial, (size_t)std::max(8, nb) * RBLOCKS * 2 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc((void**)&c->sums, (size_t)std::max(8, 2 * nb) * sizeof(double)) != cudaSuccess ||
+        cudaMalloc((void**)&c->occ_dev, (size_t)nb * sizeof(double)) != cudaSuccess ||
+        cudaMalloc((void**)&c->ptrs, 8 * sizeof(double*)) != cudaSuccess ||
+        cudaMalloc((void**)&c->fk, c->M * sizeof(cufftDoubleComplex)) != cudaSuccess)
+        return cleanup(fail(QSB_ERR_NOMEM, "scf_create: device allocation"));
+    if (cufftPlan3d(&c->plan_f, c->nz, c->ny, c->nx, CUFFT_D2Z) != CUFFT_SUCCESS ||
+        cufftPlan3d(&c->plan_b, c->nz, c->ny, c->nx, CUFFT_Z2D) != CUFFT_SUCCESS)
+        return cleanup(fail(QSB_ERR_CUDA, "scf_create: cuFFT plan"));
+    c->have_plans = true;
+    c->B.assign((size_t)c->depth * c->depth, 0.0);
+    return QSB_OK;
+}
+
+qsb_status qsb_scf_destroy(qsb_scf* c) {
+    if (!c) return QSB_OK;
+    double* fields[] = {c->vloc, c->rho_in, c->rho_out, c->vh, c->vxc, c->veff, c->exc, c->tmp, c->hist, c->hx,
+                        c->partial, c->sums, c->occ_dev};
+    for (double* f : fields)
+        if (f) cudaFree(f);
+    if (c->ptrs) cudaFree((void*)c->ptrs);
+    if (c->fk) cudaFree(c->fk);
+    if (c->have_plans) {
+        cufftDestroy(c->plan_f);
+        cufftDestroy(c->plan_b);
+    }
+    delete c;
+    return QSB_OK;
+}
+
+qsb_status qsb_scf_set_mixing(qsb_scf* c, double amplitude, double q0, int depth) {
+    if (!c || !(amplitude > 0.0) || !(q0 >= 0.0) || depth < 1 || depth > 8)
+        return fail(QSB_ERR_INVALID, "scf_set_mixing: need amplitude > 0, q0 >= 0, 1 <= depth <= 8");
+    if (depth != c->depth) {
+        double* h = nullptr;
+        if (cudaMalloc((void**)&h, 2 * (size_t)depth * c->N * sizeof(double)) != cudaSuccess)
+            return fail(QSB_ERR_NOMEM, "scf_set_mixing: device allocation");
+        cudaFree(c->hist);
+        c->hist = h;
+        c->depth = depth;
+    }
+    c->amp = amplitude;
+    c->q0 = q0;
+    c->B.assign((size_t)depth * depth, 0.0);
+    c->slots.clear();
+    return QSB_OK;
+}
+
+qsb_status qsb_scf_set_smearing(qsb_scf* c, double kbt) {
+    if (!c || !(kbt > 0.0)) return fail(QSB_ERR_INVALID, "scf_set_smearing: need kbT > 0");
+    c->kbt = kbt;
+    return QSB_OK;
+}
+
+qsb_status qsb_scf_set_gth_local(qsb_scf* c, int n_atoms, const double* pos, const int* species, int n_species,
+                                 const double* zion, const double* rloc, const double* c1, const double* c2) {
+    if (!c || n_atoms <= 0 || !pos || !species || n_species <= 0 || !zion || !rloc || !c1 || !c2)
+        return fail(QSB_ERR_INVALID, "scf_set_gth_local: bad argument");
+    std::vector<GthAtom> at(n_atoms);
+    for (int a = 0; a < n_atoms; ++a) {
+        const int sp = species[a];
+        if (sp < 0 || sp >= n_species || !(rloc[sp] > 0.0)) return fail(QSB_ERR_INVALID, "scf_set_gth_local: bad species");
+        at[a] = GthAtom{pos[3 * a], pos[3 * a + 1], pos[3 * a + 2], zion[sp], rloc[sp], c1[sp], c2[sp]};
+    }
+    GthAtom* d = nullptr;
+    QSB_CUDA_TRY(cudaMalloc((void**)&d, n_atoms * sizeof(GthAtom)));
+    QSB_CUDA_TRY(cudaMemcpy(d, at.data(), n_atoms * sizeof(GthAtom), cudaMemcpyHostToDevice));
+    const double omega = (double)c->N * c->dV;
+    vloc_k_kernel<<<pw_blocks(c->M), 256>>>(kgrid(c), c->M, 1.0 / omega, n_atoms, d, c->fk);
+    const cudaError_t e = cudaGetLastError();
+    QSB_CUFFT_TRY(cufftSetStream(c->plan_b, 0));
+    QSB_CUFFT_TRY(cufftExecZ2D(c->plan_b, c->fk, c->vloc));
+    QSB_CUDA_TRY(cudaDeviceSynchronize());
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "vloc_k_kernel");
+    c->n_atoms = n_atoms;
+    return QSB_OK;
+}
+
+qsb_status qsb_scf_get_field(qsb_scf* c, int which, double* out_dev) {
+    if (!c || !out_dev) return fail(QSB_ERR_INVALID, "scf_get_field: bad argument");
+    const double* f = which == 0 ? c->rho_out : which == 1 ? c->vloc : which == 2 ? c->veff : which == 3 ? c->rho_in
+                                                                                                        : nullptr;
+    if (!f) return fail(QSB_ERR_INVALID, "scf_get_field: which is 0 (rho), 1 (V_loc), 2 (V_eff) or 3 (mixed rho)");
+    QSB_CUDA_TRY(cudaMemcpy(out_dev, f, c->N * sizeof(double), cudaMemcpyDeviceToDevice));
+    return QSB_OK;
+}
+
+qsb_status qsb_scf_run(qsb_scf* c, double* X, double* keep, int lobpcg_iters, int max_steps, double tol_per_atom,
+                       double* energies, int* steps, double* eigen_values, double* occupations, void* stream) {
+    if (!c || !X || !keep || lobpcg_iters <= 0 || max_steps <= 0 || !(tol_per_atom > 0.0) || !energies || !steps)
+        return fail(QSB_ERR_INVALID, "scf_run: bad argument");
+    if (c->n_atoms <= 0) return fail(QSB_ERR_STATE, "scf_run: no local potential (qsb_scf_set_gth_local)");
+    QSB_TRY(qsb_eigensolver_set_hamiltonian(c->es, c->ham, 0.0, 0.0, 0.0));
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nb = c->nb;
+    const size_t N = c->N;
+    std::vector<double> ev(nb, 0.0), rq(nb), occ(nb), pxy(nb), pxx(nb);
+    // initial density: the input states with the zero-temperature filling
+    // (mSetOccupancyZero, source/qumasun_base1.occupancy.h:35-66)
+    {
+        double left = c->n_el;
+        for (int n = 0; n < nb; ++n) {
+            occ[n] = std::min(2.0, std::max(left, 0.0));
+            left -= occ[n];
+        }
+    }
+    QSB_CUDA_TRY(cudaMemcpyAsync(c->occ_dev, occ.data(), nb * sizeof(double), cudaMemcpyHostToDevice, s));
+    density_kernel<<<pw_blocks(N), 256, 0, s>>>(N, nb, X, c->occ_dev, c->rho_in);
+    QSB_CUDA_TRY(cudaGetLastError());
+    c->slots.clear();
+    std::fill(c->B.begin(), c->B.end(), 0.0);
+    double e_prev = 0.0;
+    *steps = 0;
+    for (int step = 0; step < max_steps; ++step) {
+        QSB_TRY(potentials(c, s));
+        QSB_TRY(qsb_lobpcg_d(c->es, c->dV, nb, lobpcg_iters, ev.data(), X, keep, step == 0 ? 1 : 0, stream));
+        // FP64 Rayleigh quotients of the states (the energy and the occupations use these)
+        QSB_TRY(qsb_ham_apply(c->ham, QSB_F64, 0, nb, X, c->hx, 0.0, 0.0, 0.0, stream));
+        band_dot_kernel<<<dim3(RBLOCKS / 4, nb), RB, 0, s>>>(N, X, c->hx, c->partial, c->partial + (size_t)nb * (RBLOCKS / 4));
+        row_sum_kernel<<<2 * nb, 32, 0, s>>>(2 * nb, RBLOCKS / 4, c->partial, c->sums);
+        QSB_CUDA_TRY(cudaGetLastError());
+        std::vector<double> sums(2 * nb);
+        QSB_CUDA_TRY(cudaMemcpyAsync(sums.data(), c->sums, 2 * nb * sizeof(double), cudaMemcpyDeviceToHost, s));
+        QSB_CUDA_TRY(cudaStreamSynchronize(s));
+        for (int n = 0; n < nb; ++n) {
+            if (!(sums[nb + n] > 0.0) || !std::isfinite(sums[n])) return fail(QSB_ERR_NUMERIC, "scf_run: bad band norm");
+            rq[n] = sums[n] / sums[nb + n];
+        }
+        fermi(rq, c->n_el, c->kbt, occ);
+        QSB_CUDA_TRY(cudaMemcpyAsync(c->occ_dev, occ.data(), nb * sizeof(double), cudaMemcpyHostToDevice, s));
+        density_kernel<<<pw_blocks(N), 256, 0, s>>>(N, nb, X, c->occ_dev, c->rho_out);
+        // energy of the output density: sum occ rq - int (V_H + V_xc)[rho_in] rho_out + E_H + E_xc [rho_out]
+        sub_kernel<<<pw_blocks(N), 256, 0, s>>>(N, c->veff, c->vloc, c->tmp);
+        QSB_TRY(kspace(c, KOp::hartree, c->rho_out, c->vh, s));
+        lda_kernel<<<pw_blocks(N), 256, 0, s>>>(N, c->rho_out, c->exc, c->vxc);
+        QSB_CUDA_TRY(cudaGetLastError());
+        double d2[2], exc_int;
+        {
+            const double* a[2] = {c->tmp, c->vh};
+            QSB_TRY(dots(c, 2, a, c->rho_out, d2, s));
+            const double* e[1] = {c->exc};
+            QSB_TRY(dots(c, 1, e, nullptr, &exc_int, s));
+        }
+        double eband = 0.0;
+        for (int n = 0; n < nb; ++n) eband += occ[n] * rq[n];
+        const double etot = eband - d2[0] + 0.5 * d2[1] + exc_int;
+        energies[step] = etot;
+        *steps = step + 1;
+        const bool done = step > 0 && std::fabs(etot - e_prev) / c->n_atoms < tol_per_atom;
+        e_prev = etot;
+        if (done) break;
+        QSB_TRY(mix(c, s));
+    }
+    if (eigen_values) std::copy(rq.begin(), rq.end(), eigen_values);
+    if (occupations) std::copy(occ.begin(), occ.end(), occupations);
+    return QSB_OK;
+}
+
+}  // extern "C"

@@ -258,7 +258,7 @@ class EigenSolver:
 
     def __init__(self, N, n, is_complex, precision="fp64"):
         """precision "fp64" (the reference's arithmetic) or "mixed" (fp32 bundles
-        and operator, split-BF16x3 tensor-core Gram products, fp64 pencil)."""
+        and operator, tensor-core Gram / rotation products, fp64 pencil)."""
         h = ctypes.c_void_p()
         _check(lib.qsb_eigensolver_create_ex(ctypes.byref(h), ctypes.c_int64(N), n, int(bool(is_complex)),
                                              self.PRECISIONS[precision]))
@@ -343,3 +343,74 @@ class EigenSolver:
         _check(lib.qsb_lobpcg_d(self._h, _c_d(dV), n, iter_max,
                                 eigen_values.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _dev_ptr(X),
                                 _dev_ptr(keep), int(bool(is_first_time)), _stream_ptr(X)))
+
+
+def density(X, occupations, N):
+    """rho = sum_n occ_n X_n^2 (qsb_density ~ SetDensityOne); X: [nb, N] fp64 CUDA."""
+    torch = _torch()
+    occ, occ_p = _f64(occupations)
+    rho = torch.empty(N, dtype=torch.float64, device=X.device)
+    _check(lib.qsb_density(ctypes.c_int64(N), len(occ), _dev_ptr(X), occ_p, _dev_ptr(rho), _stream_ptr(X)))
+    return rho
+
+
+def lda_pz(rho):
+    """(rho eps_xc, v_xc) of the Perdew-Zunger LDA (qsb_lda_pz ~ Calc_XC_LDA)."""
+    torch = _torch()
+    exc, vxc = torch.empty_like(rho), torch.empty_like(rho)
+    _check(lib.qsb_lda_pz(ctypes.c_int64(rho.numel()), _dev_ptr(rho), _dev_ptr(exc), _dev_ptr(vxc),
+                          _stream_ptr(rho)))
+    return exc, vxc
+
+
+class SCF:
+    """Device SCF loop (qsb_scf_* ~ QUMASUN_KPOINT::Execute with the LOBPCG
+    solver): Gamma point, LDA, GTH local part, Fermi smearing, Kerker-DIIS."""
+
+    def __init__(self, ham, solver, nb, num_electrons):
+        h = ctypes.c_void_p()
+        _check(lib.qsb_scf_create(ctypes.byref(h), ham._h, solver._h, nb, _c_d(num_electrons)))
+        self._h, self._ham, self._es, self.nb = h, ham, solver, nb
+        self.N = solver.N
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.qsb_scf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_gth_local(self, pos, species, zion, rloc, c1, c2):
+        pos, pos_p = _f64(np.asarray(pos, np.float64).reshape(-1, 3))
+        sp, sp_p = _i32(species)
+        arrs = [_f64(v) for v in (zion, rloc, c1, c2)]
+        _check(lib.qsb_scf_set_gth_local(self._h, len(pos), pos_p, sp_p, len(arrs[0][0]),
+                                         *[p for _, p in arrs]))
+
+    def set_mixing(self, amplitude=0.5, q0=0.8, depth=6):
+        _check(lib.qsb_scf_set_mixing(self._h, _c_d(amplitude), _c_d(q0), depth))
+
+    def set_smearing(self, kbt):
+        _check(lib.qsb_scf_set_smearing(self._h, _c_d(kbt)))
+
+    def run(self, X, keep, lobpcg_iters=4, max_steps=60, tol_per_atom=1e-6):
+        """Runs to |dE|/atom < tol; X, keep: [nb, N] fp64 CUDA (updated in place).
+        Returns (energies per step, final Rayleigh quotients, occupations)."""
+        e, e_p = _f64(np.zeros(max_steps))
+        ev, ev_p = _f64(np.zeros(self.nb))
+        occ, occ_p = _f64(np.zeros(self.nb))
+        steps = ctypes.c_int()
+        _check(lib.qsb_scf_run(self._h, _dev_ptr(X), _dev_ptr(keep), lobpcg_iters, max_steps, _c_d(tol_per_atom),
+                               e_p, ctypes.byref(steps), ev_p, occ_p, _stream_ptr(X)))
+        return e[:steps.value].copy(), ev, occ
+
+    def field(self, which):
+        """0: output density, 1: V_loc, 2: V_eff, 3: mixed input density."""
+        torch = _torch()
+        out = torch.empty(self.N, dtype=torch.float64, device="cuda")
+        _check(lib.qsb_scf_get_field(self._h, which, _dev_ptr(out)))
+        return out

@@ -152,3 +152,22 @@ CASES.update({
     "eig_exact_z": dict(inputs=lambda: eig_inputs(0, True), reference=lambda i: eig_exact(i, True), oracle=None),
     "eig_exact_d": dict(inputs=lambda: eig_inputs(0, False), reference=lambda i: eig_exact(i, False), oracle=None),
 })
+
+
+# SCF of config 0: 2-atom bcc (a = 6 bohr), 32^3 grid (h = 0.1875), GTH
+# (Z 6, r_loc 0.45, C1 -4, C2 0.6; s + p projectors), LDA, 16 bands, 12
+# electrons, Fermi 0.01 Ha, 4 LOBPCG iterations per step, Kerker (q0 0.8
+# bohr^-1, A 0.5) + DIIS depth 6, |dE| < 1e-6 Ha / atom.
+SCF_C0 = dict(n=32, a=A_BCC, nb=16, n_el=12.0, seed=0,
+              params=dict(kbt=0.01, lobpcg_iters=4, max_steps=60, tol_per_atom=1e-6, amplitude=0.5, q0=0.8,
+                          depth=6))
+
+
+def scf_inputs():
+    n, a = SCF_C0["n"], SCF_C0["a"]
+    h = a / n
+    grid = (n, n, n, h, h, h)
+    pos = O.bcc_positions(a, 1)
+    sp = [dict(O.GTH_BCC)] * len(pos)
+    X = O.orthonormal_psi(SCF_C0["seed"], SCF_C0["nb"], n ** 3, h ** 3)
+    return dict(grid=grid, pos=pos, sp=sp, X=X, checked=[X, pos])

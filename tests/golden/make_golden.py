@@ -17,7 +17,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
 import oracle as O  # noqa: E402
 
-from cases import CASES  # noqa: E402
+from cases import CASES, SCF_C0, scf_inputs  # noqa: E402
+import scf_oracle as S  # noqa: E402
 
 
 def main():
@@ -28,6 +29,13 @@ def main():
         np.savez_compressed(os.path.join(HERE, name + ".npz"), out=out,
                             checksum=np.array([float(np.sum(v)) for v in inp["checked"]]))
         print(name, out.shape, float(np.linalg.norm(out)))
+    # SCF of config 0: the oracle loop (reference LOBPCG + restated SCF pieces)
+    inp = scf_inputs()
+    r = S.scf(inp["grid"], inp["pos"], inp["sp"], SCF_C0["nb"], SCF_C0["n_el"], inp["X"], **SCF_C0["params"])
+    np.savez_compressed(os.path.join(HERE, "scf_c0.npz"), energies=r["energies"], rq=r["rq"], occ=r["occ"],
+                        rho=r["rho"], vloc=r["vloc"], converged=np.array(r["converged"]),
+                        checksum=np.array([float(np.sum(v)) for v in inp["checked"]]))
+    print("scf_c0", r["steps"], r["energies"][-1])
 
 
 if __name__ == "__main__":
