@@ -357,6 +357,101 @@ def lobpcg_section(H, psi, N, NB, dV, n_occ, stream, max_calls=60):
     return out
 
 
+# SCF workloads: bcc cells of the a = 6 bohr cell (GTH Z 6, r_loc 0.45, C1 -4,
+# C2 0.6; s + p projectors), h = 0.125 bohr, LDA, Fermi 0.01 Ha, 4 LOBPCG
+# iterations per step, Kerker (q0 0.8) + DIIS depth 6, |dE| < 1e-6 Ha / atom.
+SCF_CONFIGS = {
+    "c2": dict(reps=2, n=96, bands=128, jitter=0.0, seed=2),     # 16 atoms, 96 electrons
+    "c3": dict(reps=3, n=144, bands=384, jitter=0.1, seed=3),    # 54 atoms, 324 electrons, displaced
+}
+GTH_LOCAL = dict(zion=6.0, rloc=0.45, c1=-4.0, c2=0.6)
+
+
+def scf_positions(reps, jitter, seed):
+    pos = []
+    for i in range(reps):
+        for j in range(reps):
+            for k in range(reps):
+                base = np.array([i, j, k], float) * A_CELL
+                pos.append(base)
+                pos.append(base + 0.5 * A_CELL)
+    pos = np.array(pos)
+    if jitter > 0.0:
+        pos = pos + np.random.default_rng(seed).normal(0.0, jitter, pos.shape)
+    return pos
+
+
+def scf_section(name, tol_ref=1e-8, max_steps=None):
+    """SCF wall time to 1e-6 Ha / atom, FP64 drop-in vs mixed precision, from one
+    dV-orthonormal seeded start with the same mixer.  Both runs continue to
+    |dE| < tol_ref per atom (or the step cap); the FP64 run's final energy is
+    the reference E*.  Time to tolerance = summed wall seconds of the steps up
+    to the first step after which |E - E*| / atom stays below 1e-6 (steps timed
+    by the driver's host clock; each step ends with its energy on the host).
+    Also reported: the stopping-rule point |dE| / atom < 1e-6 of each run."""
+    import torch
+    import qsb
+    cfg = SCF_CONFIGS[name]
+    n, nb = cfg["n"], cfg["bands"]
+    cap = max_steps or (100 if name == "c2" else 80)
+    h = A_CELL * cfg["reps"] / n
+    N, dV = n ** 3, h ** 3
+    pos = scf_positions(cfg["reps"], cfg["jitter"], cfg["seed"])
+    na = len(pos)
+    n_el = GTH_LOCAL["zion"] * na
+    H = qsb.Hamiltonian(n, n, n, h, h, h)
+    H.set_gth_projectors(pos, [0] * na, [GTH["nl"]], [GTH["r"]], [GTH["h"]], RCUT)
+    H.set_potential(np.zeros(N))
+    gen = torch.Generator(device="cuda").manual_seed(cfg["seed"])
+    psi = torch.rand(nb, N, dtype=torch.float64, device="cuda", generator=gen) - 0.5
+    X0 = torch.linalg.qr(psi.t())[0].t().contiguous() / math.sqrt(dV)
+    del psi
+    out = {"config": name, "atoms": na, "grid": [n, n, n], "bands": nb, "electrons": n_el,
+           "lobpcg_iterations_per_step": 4, "tolerance_ha_per_atom": 1e-6, "reference_tolerance_ha_per_atom": tol_ref,
+           "step_cap": cap, "mixing": "Kerker q0 0.8 A 0.5 + DIIS depth 6", "smearing_ha": 0.01}
+    runs = {}
+    for prec in ("fp64", "mixed"):
+        es = qsb.EigenSolver(N, nb, False, prec)
+        scf = qsb.SCF(H, es, nb, n_el)
+        scf.set_gth_local(pos, [0] * na, [GTH_LOCAL["zion"]], [GTH_LOCAL["rloc"]], [GTH_LOCAL["c1"]],
+                          [GTH_LOCAL["c2"]])
+        X = X0.clone()
+        keep = torch.zeros_like(X)
+        scf.run(X, keep, 4, 1, 1e-6)           # one step: sizes the solver's workspaces
+        X.copy_(X0)
+        keep.zero_()
+        torch.cuda.synchronize()
+        e, ev, occ = scf.run(X, keep, 4, cap, tol_ref)
+        runs[prec] = (e, scf.step_seconds())
+        scf.close()
+        es.close()
+        del X, keep
+        torch.cuda.empty_cache()
+    e_ref = runs["fp64"][0][-1]
+    for prec, (e, t) in runs.items():
+        err = np.abs(e - e_ref) / na
+        ok = np.nonzero(err >= 1e-6)[0]
+        k = 0 if len(ok) == 0 else int(ok[-1]) + 1          # first step after which all stay within
+        hit = k < len(e)
+        de = np.abs(np.diff(e)) / na
+        stop = np.nonzero(de < 1e-6)[0]
+        ks = int(stop[0]) + 1 if len(stop) else None          # stopping rule |dE| / atom < 1e-6
+        out[prec] = {"steps_run": len(e), "seconds_run": float(np.sum(t)),
+                     "steps_to_tolerance": k + 1 if hit else None,
+                     "seconds_to_tolerance": float(np.sum(t[:k + 1])) if hit else None,
+                     "final_error_ha_per_atom": float(err[-1]),
+                     "stopping_rule_step": ks + 1 if ks is not None else None,
+                     "stopping_rule_seconds": float(np.sum(t[:ks + 1])) if ks is not None else None,
+                     "stopping_rule_error_ha_per_atom": float(err[ks]) if ks is not None else None,
+                     "final_energy_ha": float(e[-1])}
+    if out["fp64"]["seconds_to_tolerance"] and out["mixed"]["seconds_to_tolerance"]:
+        out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds_to_tolerance"] / out["mixed"]["seconds_to_tolerance"]
+    out["note"] = ("E excludes the constant ion-ion term; E* = FP64 run's final energy; the mixed run's "
+                   "final_error_ha_per_atom is its error against it (bar 1e-6)")
+    H.close()
+    return out
+
+
 def main():
     global NB
     ap = argparse.ArgumentParser()
@@ -366,6 +461,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-lobpcg", action="store_true")
+    ap.add_argument("--no-scf", action="store_true")
+    ap.add_argument("--scf-config", default="c2", choices=sorted(SCF_CONFIGS),
+                    help="SCF workload: c2 (16 atoms, 96^3, 128 bands; default) or c3 (54 atoms, 144^3, 384 bands)")
     ap.add_argument("--bands", type=int, default=NB,
                     help="bands per GPU (default 128, the benchmark workload; smaller only for profiler captures)")
     args = ap.parse_args()
@@ -460,6 +558,10 @@ def main():
     gram = gram_section(N, 3 * NB, stream)
     if not args.no_lobpcg:
         lob = lobpcg_section(H, psi, N, NB, H_GRID ** 3, n_occ=min(NB_OCC, NB), stream=stream)
+    # ---- whole SCF to 1e-6 Ha/atom: FP64 drop-in vs mixed precision (one system, N = 1 only)
+    scf = None
+    if not args.no_scf and world == 1:
+        scf = scf_section(args.scf_config)
     clk = clocks.stop()
 
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist, "cuda")
@@ -497,6 +599,7 @@ def main():
                 "ms_per_step": e2e_ms},
         "gpu_launches": launches,
         "lobpcg": lob,
+        "scf": scf,
         "gram": gram,
         "clocks": clk,
     }

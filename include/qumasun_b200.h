@@ -405,6 +405,9 @@ QSB_API qsb_status qsb_scf_run(qsb_scf* scf, double* X, double* keep, int lobpcg
                                double tol_per_atom, double* energies, int* steps, double* eigen_values,
                                double* occupations, void* stream);
 QSB_API qsb_status qsb_scf_get_field(qsb_scf* scf, int which, double* out);
+/* Wall seconds of each step of the last qsb_scf_run (host clock; a step ends
+ * when its energy is on the host): up to max values, *n = steps recorded. */
+QSB_API qsb_status qsb_scf_step_seconds(qsb_scf* scf, double* seconds, int max, int* n);
 
 #ifdef __cplusplus
 }

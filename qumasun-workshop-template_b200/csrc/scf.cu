@@ -25,6 +25,7 @@
 #include <cmath>
 #include <vector>
 #include <algorithm>
+#include <chrono>
 
 namespace qsb {
 namespace {
@@ -279,6 +280,7 @@ struct qsb_scf {
     // host
     std::vector<int> slots;       // history slots, oldest first
     std::vector<double> B;        // depth x depth residual inner products (by slot)
+    std::vector<double> step_s;   // wall seconds of each step of the last run
 };
 
 namespace qsb {
@@ -569,6 +571,13 @@ qsb_status qsb_scf_set_gth_local(qsb_scf* c, int n_atoms, const double* pos, con
     return QSB_OK;
 }
 
+qsb_status qsb_scf_step_seconds(qsb_scf* c, double* seconds, int max, int* n) {
+    if (!c || !n || (max > 0 && !seconds)) return fail(QSB_ERR_INVALID, "scf_step_seconds: bad argument");
+    *n = (int)c->step_s.size();
+    for (int k = 0; k < std::min(max, *n); ++k) seconds[k] = c->step_s[k];
+    return QSB_OK;
+}
+
 qsb_status qsb_scf_get_field(qsb_scf* c, int which, double* out_dev) {
     if (!c || !out_dev) return fail(QSB_ERR_INVALID, "scf_get_field: bad argument");
     const double* f = which == 0 ? c->rho_out : which == 1 ? c->vloc : which == 2 ? c->veff : which == 3 ? c->rho_in
@@ -604,6 +613,9 @@ qsb_status qsb_scf_run(qsb_scf* c, double* X, double* keep, int lobpcg_iters, in
     std::fill(c->B.begin(), c->B.end(), 0.0);
     double e_prev = 0.0;
     *steps = 0;
+    c->step_s.clear();
+    QSB_CUDA_TRY(cudaStreamSynchronize(s));
+    auto t_prev = std::chrono::steady_clock::now();
     for (int step = 0; step < max_steps; ++step) {
         QSB_TRY(potentials(c, s));
         QSB_TRY(qsb_lobpcg_d(c->es, c->dV, nb, lobpcg_iters, ev.data(), X, keep, step == 0 ? 1 : 0, stream));
@@ -639,6 +651,10 @@ qsb_status qsb_scf_run(qsb_scf* c, double* X, double* keep, int lobpcg_iters, in
         const double etot = eband - d2[0] + 0.5 * d2[1] + exc_int;
         energies[step] = etot;
         *steps = step + 1;
+        // the step ends with the energy on the host (the inner products synchronized the stream)
+        const auto t_now = std::chrono::steady_clock::now();
+        c->step_s.push_back(std::chrono::duration<double>(t_now - t_prev).count());
+        t_prev = t_now;
         const bool done = step > 0 && std::fabs(etot - e_prev) / c->n_atoms < tol_per_atom;
         e_prev = etot;
         if (done) break;

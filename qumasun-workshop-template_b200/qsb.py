@@ -408,6 +408,13 @@ class SCF:
                                e_p, ctypes.byref(steps), ev_p, occ_p, _stream_ptr(X)))
         return e[:steps.value].copy(), ev, occ
 
+    def step_seconds(self):
+        """Wall seconds of each step of the last run."""
+        buf, buf_p = _f64(np.zeros(1024))
+        n = ctypes.c_int()
+        _check(lib.qsb_scf_step_seconds(self._h, buf_p, len(buf), ctypes.byref(n)))
+        return buf[:n.value].copy()
+
     def field(self, which):
         """0: output density, 1: V_loc, 2: V_eff, 3: mixed input density."""
         torch = _torch()

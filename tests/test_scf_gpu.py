@@ -72,6 +72,8 @@ def test_fp64_scf_follows_the_oracle(qsb):
     assert abs(r["e"][-1] - ge[-1]) / n_atoms < 1e-6, (r["e"][-1], ge[-1])
     assert abs(len(r["e"]) - len(ge)) <= 4, (len(r["e"]), len(ge))
     assert abs(r["occ"].sum() - SCF_C0["n_el"]) < 1e-6
+    t = r["scf"].step_seconds()
+    assert len(t) == len(r["e"]) and np.all(t > 0)
     rho = r["scf"].field(0).cpu().numpy()
     dV = (SCF_C0["a"] / SCF_C0["n"]) ** 3
     assert np.abs(rho - gold["rho"]).sum() * dV / SCF_C0["n_el"] < 1e-3
