@@ -416,12 +416,6 @@ __device__ __forceinline__ double2 lds2<double>(uint32_t a) {
     asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(a));
     return v;
 }
-template <>
-__device__ __forceinline__ float2 lds2<float>(uint32_t a) {
-    float2 v;
-    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
-    return v;
-}
 
 template <typename T, bool CPLX, int ZY, int RY, int S, int MINB>
 struct ZCfg {
@@ -537,6 +531,19 @@ fd8_zacc_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ out, c
     // pending outputs: slot o % 8 holds output plane o (local index; plane j is
     // z = z0 - 4 + j, output o is stored at step o + 4)
     T A[NC][RY][2][8];
+    // FP32, MODE 1: V psi of the last four outputs, added when the output is
+    // stored, after its stencil sum has cancelled the ~|c0| centre term (added
+    // earlier it would be resolved only to 2^-24 |c0|)
+    constexpr bool VQ = sizeof(T) == 4 && MODE == 1;
+    T vq[NC][RY][2][VQ ? 4 : 1];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int i = 0; i < RY; ++i)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int s4 = 0; s4 < (VQ ? 4 : 1); ++s4) vq[c][i][h][s4] = T(0);
 #pragma unroll
     for (int c = 0; c < NC; ++c)
 #pragma unroll
@@ -609,6 +616,14 @@ fd8_zacc_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ out, c
                     for (int i = 0; i < RY; ++i)
                         pc[c][i] = *reinterpret_cast<const P2*>(cur + c * C::COMP + soff + i * SW);
 #define PV(c, i, h) ((h) ? pc[c][i].y : pc[c][i].x)
+                // V psi of output j-4 (stored this step) before slot u % 4 takes output j's
+                T vs[NC][RY][2];
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+#pragma unroll
+                    for (int i = 0; i < RY; ++i)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) vs[c][i][h] = vq[c][i][h][VQ ? (u % 4) : 0];
 
                 if (inner) {
                     T lxy[NC][RY][2];
@@ -665,7 +680,11 @@ fd8_zacc_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ out, c
                                 const T p = PV(c, i, h);
                                 T r = k.c0 * p + lxy[c][i][h];
                                 if constexpr (sizeof(T) == 4) r = fmaf(k.c0lo, p, r);
-                                if (MODE == 1) r += (h ? ep[u % 2][0][i].y : ep[u % 2][0][i].x) * p;
+                                if (MODE == 1) {
+                                    const T vp = (h ? ep[u % 2][0][i].y : ep[u % 2][0][i].x) * p;
+                                    if constexpr (VQ) vq[c][i][h][u % 4] = vp;
+                                    else r += vp;
+                                }
                                 // out_re = L(re) - D(im), out_im = L(im) + D(re)
                                 if (CPLX && GRAD) r += c == 0 ? -gxy[NC - 1][i][h] : gxy[0][i][h];
                                 A[c][i][h][u] += r;
@@ -711,6 +730,10 @@ fd8_zacc_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ out, c
                             P2 r;
                             r.x = A[c][i][0][(u + 4) % 8];
                             r.y = A[c][i][1][(u + 4) % 8];
+                            if constexpr (VQ) {
+                                r.x += vs[c][i][0];
+                                r.y += vs[c][i][1];
+                            }
                             if (MODE == 0) {
                                 r.x += ep[u % 2][c][i].x;
                                 r.y += ep[u % 2][c][i].y;
@@ -972,6 +995,19 @@ fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, 
     }
 
     T A[NC][RY][2][8];
+    // FP32, MODE 1: V psi of the last four outputs, added when the output is
+    // stored, after its stencil sum has cancelled the ~|c0| centre term (added
+    // earlier it would be resolved only to 2^-24 |c0|)
+    constexpr bool VQ = sizeof(T) == 4 && MODE == 1;
+    T vq[NC][RY][2][VQ ? 4 : 1];
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int i = 0; i < RY; ++i)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int s4 = 0; s4 < (VQ ? 4 : 1); ++s4) vq[c][i][h][s4] = T(0);
 #pragma unroll
     for (int c = 0; c < NC; ++c)
 #pragma unroll
@@ -999,6 +1035,14 @@ fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, 
 #pragma unroll
                     for (int i = 0; i < RY; ++i) pc[c][i] = lds2<T>(cur + c * C::MAIN * TB + soff + i * SW * TB);
 #define PV(c, i, h) ((h) ? pc[c][i].y : pc[c][i].x)
+                // V psi of output j-4 (stored this step) before slot u % 4 takes output j's
+                T vs[NC][RY][2];
+#pragma unroll
+                for (int c = 0; c < NC; ++c)
+#pragma unroll
+                    for (int i = 0; i < RY; ++i)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) vs[c][i][h] = vq[c][i][h][VQ ? (u % 4) : 0];
                 // in-plane sums per point: ISO, (x+y) pairs per offset m; else x and y apart
                 T sm[NC][RY][2][4];
                 T syy[NC][RY][2];
@@ -1081,9 +1125,16 @@ fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, 
 #pragma unroll
                             for (int h = 0; h < 2; ++h) {
                                 const T p = PV(c, i, h);
-                                const T c0v = MODE == 1 ? k.c0 + (h ? ev[0][i].y : ev[0][i].x) : k.c0;
-                                T r1 = c0v * p;
-                                if constexpr (sizeof(T) == 4) r1 = fmaf(k.c0lo, p, r1);
+                                const T v = MODE == 1 ? (h ? ev[0][i].y : ev[0][i].x) : T(0);
+                                T r1;
+                                if constexpr (sizeof(T) == 4) {
+                                    // the centre weight stays the exact pair c0 + c0lo; V psi waits
+                                    // for the store (vq)
+                                    r1 = fmaf(k.c0lo, p, k.c0 * p);
+                                    if constexpr (VQ) vq[c][i][h][u % 4] = v * p;
+                                } else {
+                                    r1 = (k.c0 + v) * p;
+                                }
                                 r1 += k.cx[0] * sm[c][i][h][0];
                                 r1 += k.cx[1] * sm[c][i][h][1];
                                 T r2 = k.cx[3] * sm[c][i][h][3];
@@ -1133,6 +1184,10 @@ fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, 
                             P2 r;
                             r.x = A[c][i][0][(u + 4) % 8];
                             r.y = A[c][i][1][(u + 4) % 8];
+                            if constexpr (VQ) {
+                                r.x += vs[c][i][0];
+                                r.y += vs[c][i][1];
+                            }
                             if (MODE == 0) {
                                 r.x += ev[c][i].x;
                                 r.y += ev[c][i].y;
@@ -1199,7 +1254,7 @@ bool make_plane_map(CUtensorMap* map, const void* base, int nx, int ny, long lon
     return r == CUDA_SUCCESS;
 }
 
-// Stencil kernel choice: 0 fd8_ws_kernel (default; fd8_zacc_kernel where its tiling
+// Stencil kernel choice (FP64): 0 fd8_ws_kernel (default; fd8_zacc_kernel where its tiling
 // does not apply, fd8_kernel without 16-byte alignment), 2 fd8_kernel (register
 // prefetch, no TMA), 3 fd8_zacc_kernel; QSB_STENCIL=ws|reg|zacc overrides it for
 // A/B timing.
@@ -1334,21 +1389,23 @@ void launch_t(const StencilLaunch& L, const FD8Coef& c, cudaStream_t s) {
     const int variant = stencil_variant();
     // the pending-output kernel also moves out / V / old values in 16-byte pairs
     const bool pairs_ok = ((uintptr_t)L.out % 16 == 0) && (L.V == nullptr || (uintptr_t)L.V % 16 == 0);
-    if (aligned && pairs_ok && L.tma_ok && variant == 0) {
-        // rows per thread: 2 (fp64 complex: 1, within the register file at one CTA per SM)
-        constexpr int WRY = (CPLX && sizeof(T) == 8) ? 1 : 2;
-        constexpr int WS = sizeof(T) == 8 ? (CPLX ? 8 : 6) : (CPLX ? 8 : 12);
-        if (launch_ws<T, CPLX, MODE, WRY, WS>(L, c, k, s)) return;
-    }
-    if (aligned && pairs_ok && L.tma_ok && (variant == 0 || variant == 3)) {
-        // fp64 real 2 rows / 1 CTA per SM (212 registers), fp64 complex 1 row,
-        // fp32 real 2 rows / 2 CTAs per SM, fp32 complex 2 rows / 1 CTA
-        bool done;
-        if (sizeof(T) == 8) done = CPLX ? launch_zacc<T, CPLX, MODE, 16, 1, 8, 1>(L, c, k, s)
-                                        : launch_zacc<T, CPLX, MODE, 16, 2, 8, 1>(L, c, k, s);
-        else done = CPLX ? launch_zacc<T, CPLX, MODE, 16, 2, 8, 1>(L, c, k, s)
-                         : launch_zacc<T, CPLX, MODE, 16, 2, 8, 2>(L, c, k, s);
-        if (done) return;
+    // FP64 only: the pending-output z sums round at 2^-24 of the ~|c0| partial
+    // sums in FP32, which measured as a 4e-6..6e-6 Ha eigenvalue floor of the
+    // mixed solver at h = 0.125 bohr against 8e-7 with fd8_kernel's order
+    // (centre + (x + y neighbours + z neighbours), each completed first)
+    if constexpr (sizeof(T) == 8) {
+        if (aligned && pairs_ok && L.tma_ok && variant == 0) {
+            // rows per thread: 2 (complex: 1, within the register file at one CTA per SM)
+            constexpr int WRY = CPLX ? 1 : 2;
+            constexpr int WS = CPLX ? 8 : 6;
+            if (launch_ws<T, CPLX, MODE, WRY, WS>(L, c, k, s)) return;
+        }
+        if (aligned && pairs_ok && L.tma_ok && (variant == 0 || variant == 3)) {
+            // real 2 rows / 1 CTA per SM (212 registers), complex 1 row
+            const bool done = CPLX ? launch_zacc<T, CPLX, MODE, 16, 1, 8, 1>(L, c, k, s)
+                                   : launch_zacc<T, CPLX, MODE, 16, 2, 8, 1>(L, c, k, s);
+            if (done) return;
+        }
     }
     if (CPLX && c.has_grad)
         fd8_kernel<T, CPLX, MODE, CPLX, RY><<<grid, block, 0, s>>>((const T*)L.in, (T*)L.out, (const T*)L.V, L.nx,
