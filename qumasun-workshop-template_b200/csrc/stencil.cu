@@ -531,19 +531,7 @@ fd8_zacc_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ out, c
     // pending outputs: slot o % 8 holds output plane o (local index; plane j is
     // z = z0 - 4 + j, output o is stored at step o + 4)
     T A[NC][RY][2][8];
-    // FP32, MODE 1: V psi of the last four outputs, added when the output is
-    // stored, after its stencil sum has cancelled the ~|c0| centre term (added
-    // earlier it would be resolved only to 2^-24 |c0|)
-    constexpr bool VQ = sizeof(T) == 4 && MODE == 1;
-    T vq[NC][RY][2][VQ ? 4 : 1];
-#pragma unroll
-    for (int c = 0; c < NC; ++c)
-#pragma unroll
-        for (int i = 0; i < RY; ++i)
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-#pragma unroll
-                for (int s4 = 0; s4 < (VQ ? 4 : 1); ++s4) vq[c][i][h][s4] = T(0);
+    static_assert(sizeof(T) == 8, "pending-output z sums are FP64 only (FP32 uses fd8_kernel's order)");
 #pragma unroll
     for (int c = 0; c < NC; ++c)
 #pragma unroll
@@ -616,14 +604,6 @@ fd8_zacc_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ out, c
                     for (int i = 0; i < RY; ++i)
                         pc[c][i] = *reinterpret_cast<const P2*>(cur + c * C::COMP + soff + i * SW);
 #define PV(c, i, h) ((h) ? pc[c][i].y : pc[c][i].x)
-                // V psi of output j-4 (stored this step) before slot u % 4 takes output j's
-                T vs[NC][RY][2];
-#pragma unroll
-                for (int c = 0; c < NC; ++c)
-#pragma unroll
-                    for (int i = 0; i < RY; ++i)
-#pragma unroll
-                        for (int h = 0; h < 2; ++h) vs[c][i][h] = vq[c][i][h][VQ ? (u % 4) : 0];
 
                 if (inner) {
                     T lxy[NC][RY][2];
@@ -679,12 +659,7 @@ fd8_zacc_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ out, c
                             for (int h = 0; h < 2; ++h) {
                                 const T p = PV(c, i, h);
                                 T r = k.c0 * p + lxy[c][i][h];
-                                if constexpr (sizeof(T) == 4) r = fmaf(k.c0lo, p, r);
-                                if (MODE == 1) {
-                                    const T vp = (h ? ep[u % 2][0][i].y : ep[u % 2][0][i].x) * p;
-                                    if constexpr (VQ) vq[c][i][h][u % 4] = vp;
-                                    else r += vp;
-                                }
+                                if (MODE == 1) r += (h ? ep[u % 2][0][i].y : ep[u % 2][0][i].x) * p;
                                 // out_re = L(re) - D(im), out_im = L(im) + D(re)
                                 if (CPLX && GRAD) r += c == 0 ? -gxy[NC - 1][i][h] : gxy[0][i][h];
                                 A[c][i][h][u] += r;
@@ -730,10 +705,6 @@ fd8_zacc_kernel(const __grid_constant__ CUtensorMap tmap, T* __restrict__ out, c
                             P2 r;
                             r.x = A[c][i][0][(u + 4) % 8];
                             r.y = A[c][i][1][(u + 4) % 8];
-                            if constexpr (VQ) {
-                                r.x += vs[c][i][0];
-                                r.y += vs[c][i][1];
-                            }
                             if (MODE == 0) {
                                 r.x += ep[u % 2][c][i].x;
                                 r.y += ep[u % 2][c][i].y;
@@ -995,19 +966,7 @@ fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, 
     }
 
     T A[NC][RY][2][8];
-    // FP32, MODE 1: V psi of the last four outputs, added when the output is
-    // stored, after its stencil sum has cancelled the ~|c0| centre term (added
-    // earlier it would be resolved only to 2^-24 |c0|)
-    constexpr bool VQ = sizeof(T) == 4 && MODE == 1;
-    T vq[NC][RY][2][VQ ? 4 : 1];
-#pragma unroll
-    for (int c = 0; c < NC; ++c)
-#pragma unroll
-        for (int i = 0; i < RY; ++i)
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-#pragma unroll
-                for (int s4 = 0; s4 < (VQ ? 4 : 1); ++s4) vq[c][i][h][s4] = T(0);
+    static_assert(sizeof(T) == 8, "pending-output z sums are FP64 only (FP32 uses fd8_kernel's order)");
 #pragma unroll
     for (int c = 0; c < NC; ++c)
 #pragma unroll
@@ -1035,14 +994,6 @@ fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, 
 #pragma unroll
                     for (int i = 0; i < RY; ++i) pc[c][i] = lds2<T>(cur + c * C::MAIN * TB + soff + i * SW * TB);
 #define PV(c, i, h) ((h) ? pc[c][i].y : pc[c][i].x)
-                // V psi of output j-4 (stored this step) before slot u % 4 takes output j's
-                T vs[NC][RY][2];
-#pragma unroll
-                for (int c = 0; c < NC; ++c)
-#pragma unroll
-                    for (int i = 0; i < RY; ++i)
-#pragma unroll
-                        for (int h = 0; h < 2; ++h) vs[c][i][h] = vq[c][i][h][VQ ? (u % 4) : 0];
                 // in-plane sums per point: ISO, (x+y) pairs per offset m; else x and y apart
                 T sm[NC][RY][2][4];
                 T syy[NC][RY][2];
@@ -1126,15 +1077,7 @@ fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, 
                             for (int h = 0; h < 2; ++h) {
                                 const T p = PV(c, i, h);
                                 const T v = MODE == 1 ? (h ? ev[0][i].y : ev[0][i].x) : T(0);
-                                T r1;
-                                if constexpr (sizeof(T) == 4) {
-                                    // the centre weight stays the exact pair c0 + c0lo; V psi waits
-                                    // for the store (vq)
-                                    r1 = fmaf(k.c0lo, p, k.c0 * p);
-                                    if constexpr (VQ) vq[c][i][h][u % 4] = v * p;
-                                } else {
-                                    r1 = (k.c0 + v) * p;
-                                }
+                                T r1 = (k.c0 + v) * p;
                                 r1 += k.cx[0] * sm[c][i][h][0];
                                 r1 += k.cx[1] * sm[c][i][h][1];
                                 T r2 = k.cx[3] * sm[c][i][h][3];
@@ -1184,10 +1127,6 @@ fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, 
                             P2 r;
                             r.x = A[c][i][0][(u + 4) % 8];
                             r.y = A[c][i][1][(u + 4) % 8];
-                            if constexpr (VQ) {
-                                r.x += vs[c][i][0];
-                                r.y += vs[c][i][1];
-                            }
                             if (MODE == 0) {
                                 r.x += ev[c][i].x;
                                 r.y += ev[c][i].y;
