@@ -401,10 +401,22 @@ QSB_API qsb_status qsb_scf_set_gth_local(qsb_scf* scf, int n_atoms, const double
                                          const double* c2);
 QSB_API qsb_status qsb_scf_set_mixing(qsb_scf* scf, double amplitude, double q0, int depth);
 QSB_API qsb_status qsb_scf_set_smearing(qsb_scf* scf, double kbt);
+/* Also require int |rho_out - rho_in| dV / N_e < rho_tol to stop (the
+ * reference's RHO_ETOT convergence mode, source/qumasun_kpoint.scfloop.h:182-213);
+ * 0 (default) stops on the energy alone. */
+QSB_API qsb_status qsb_scf_set_density_tolerance(qsb_scf* scf, double rho_tol);
 QSB_API qsb_status qsb_scf_run(qsb_scf* scf, double* X, double* keep, int lobpcg_iters, int max_steps,
                                double tol_per_atom, double* energies, int* steps, double* eigen_values,
                                double* occupations, void* stream);
 QSB_API qsb_status qsb_scf_get_field(qsb_scf* scf, int which, double* out);
+/* Force of the GTH local parts on every atom, -d/dR_a int rho V_loc, from the
+ * last output density (rho_dev = NULL) or a given device density: forces
+ * (host, 3 x n_atoms) accumulate ("+="), so the nonlocal part
+ * (qsb_ham_nonlocal_energy_force) adds on.  Exact derivative of the grid sum
+ * dV sum rho V_loc (V_loc's Fourier series).  Replaces the local-potential
+ * terms of the reference's mGetForce (source/qumasun_base1.force.h:23-205;
+ * mGetForceOnNuclRho_HR :247-284 on its core-charge form of V_loc). */
+QSB_API qsb_status qsb_scf_local_forces(qsb_scf* scf, const double* rho_dev, double* forces);
 /* Wall seconds of each step of the last qsb_scf_run (host clock; a step ends
  * when its energy is on the host): up to max values, *n = steps recorded. */
 QSB_API qsb_status qsb_scf_step_seconds(qsb_scf* scf, double* seconds, int max, int* n);

@@ -11,7 +11,8 @@ Pinned pieces: lda_pz against the reference's Calc_XC_LDA (source/Vxc.h:43-75)
 and fermi_occupations against its SetOccupancy (source/SetOccupancy.h:7-18)
 with the bisection of mSetOccupancyTemperature
 (source/qumasun_base1.occupancy.h:76-170), both compiled from the reference
-sources into oracle/_ref.  Restated from the mathematics (no reference
+sources into oracle/_ref; the loop refines the bisection's mu by Newton steps
+to the exact electron count (fermi_occupations_exact).  Restated from the mathematics (no reference
 counterpart on this path): the GTH local potential in G space, the FFT Poisson
 solve, the Kerker-preconditioned DIIS mixer and the Kohn-Sham energy of the
 output density; SCF-level parity with the reference is therefore unpinned
@@ -102,6 +103,22 @@ def fermi_occupations(eig, n_el, kbt, weight=2.0, occupancy=_occupancy):
     return occ, mu_occ
 
 
+def fermi_occupations_exact(eig, n_el, kbt, weight=2.0):
+    """fermi_occupations refined by Newton steps on sum f(mu) = N_e (the
+    bisection's 1e-9 bracket leaves the count off by dN/dmu 1e-9, ~1e-7
+    electrons at a partly filled Fermi level); the device driver's form."""
+    occ, mu = fermi_occupations(eig, n_el, kbt, weight)
+    eig = np.asarray(eig, np.float64)
+    for _ in range(8):
+        occ = _occupancy(eig, mu, kbt, weight)
+        r = float(np.sum(occ)) - n_el
+        dn = float(np.sum(occ * (1.0 - occ / weight))) / kbt
+        if abs(r) <= 1e-14 * n_el or not dn > 1e-300:
+            break
+        mu -= r / dn
+    return _occupancy(eig, mu, kbt, weight), mu
+
+
 def ref_occupancy(eig, mu, kbt, weight):
     lib = O.ref_lib()
     lib.qsref_set_occupancy.restype = ctypes.c_double
@@ -125,6 +142,18 @@ def zero_temperature_occupations(nb, n_el, weight=2.0):
     return occ
 
 
+def nyquist_mask(nx, ny, nz):
+    """True off the Nyquist planes (k = n/2 of an even n): there G and -G are the
+    same grid point and a structure-factor phase exp(-i G.R) has no real-field
+    representation, so the local part leaves them out."""
+    def ok(n):
+        m = np.ones(n, bool)
+        if n % 2 == 0:
+            m[n // 2] = False
+        return m
+    return ok(nz)[:, None, None] & ok(ny)[None, :, None] & ok(nx)[None, None, :]
+
+
 def g_squared(nx, ny, nz, dx, dy, dz):
     """|G|^2 on the FFT grid, array [z][y][x] (x fastest, as the grid layout)."""
     gx = 2.0 * np.pi * np.fft.fftfreq(nx, dx)
@@ -139,7 +168,8 @@ def gth_local_potential(grid, pos, species_params):
     through its Fourier series: v(G) = -4 pi Z exp(-G^2 r^2 / 2) / G^2 + (2 pi)^(3/2)
     r^3 exp(-G^2 r^2 / 2) (C1 + C2 (3 - G^2 r^2)); at G = 0 the Coulomb tail is
     neutralised by the electrons' Hartree G = 0 term and the finite remainder
-    2 pi Z r^2 + (2 pi)^(3/2) r^3 (C1 + 3 C2) is kept."""
+    2 pi Z r^2 + (2 pi)^(3/2) r^3 (C1 + 3 C2) is kept; Nyquist planes left out
+    (nyquist_mask)."""
     nx, ny, nz, dx, dy, dz = grid
     omega = nx * ny * nz * dx * dy * dz
     G2, (gx, gy, gz) = g_squared(nx, ny, nz, dx, dy, dz)
@@ -153,8 +183,31 @@ def gth_local_potential(grid, pos, species_params):
         short = (2.0 * np.pi) ** 1.5 * r ** 3 * e * (c1 + c2 * (3.0 - G2 * r * r))
         phase = np.exp(-1j * (gz[:, None, None] * Z + gy[None, :, None] * Y + gx[None, None, :] * X))
         VG += (coul + short) * phase
-    VG /= omega
+    VG *= nyquist_mask(nx, ny, nz) / omega
     return (np.fft.ifftn(VG) * (nx * ny * nz)).real.reshape(-1)
+
+
+def gth_local_forces(rho, grid, pos, species_params):
+    """F_a = -d/dR_a (dV sum_r rho(r) V_loc(r)) for V_loc = gth_local_potential:
+    sum over G of G v_a(G) [sin(G.R_a) Re rho_G + cos(G.R_a) Im rho_G],
+    rho_G = FFT(rho) / N (the G = 0 term carries no force; Nyquist planes out
+    as in gth_local_potential)."""
+    nx, ny, nz, dx, dy, dz = grid
+    G2, (gx, gy, gz) = g_squared(nx, ny, nz, dx, dy, dz)
+    rg = np.fft.fftn(np.asarray(rho, np.float64).reshape(nz, ny, nx)) / (nx * ny * nz)
+    safe = np.where(G2 > 0, G2, 1.0)
+    out = np.zeros((len(pos), 3))
+    for a, ((X, Y, Z), sp) in enumerate(zip(np.asarray(pos, np.float64), species_params)):
+        r, zion, c1, c2 = sp["rloc"], sp["zion"], sp["c1"], sp["c2"]
+        e = np.exp(-0.5 * G2 * r * r)
+        v = np.where(G2 > 0, -4.0 * np.pi * zion * e / safe, 0.0) + (2.0 * np.pi) ** 1.5 * r ** 3 * e * (
+            c1 + c2 * (3.0 - G2 * r * r))
+        v = np.where((G2 > 0) & nyquist_mask(nx, ny, nz), v, 0.0)
+        th = gz[:, None, None] * Z + gy[None, :, None] * Y + gx[None, None, :] * X
+        t = v * (np.sin(th) * rg.real + np.cos(th) * rg.imag)
+        out[a] = [float(np.sum(gx[None, None, :] * t)), float(np.sum(gy[None, :, None] * t)),
+                  float(np.sum(gz[:, None, None] * t))]
+    return out
 
 
 def hartree(rho, grid):
@@ -287,7 +340,7 @@ def scf(grid, pos, species_params, nb, n_el, X0, kbt=0.01, lobpcg_iters=4, max_s
             O.ref_lobpcg_d(grid, veff, cube, X, keep, nb, lobpcg_iters, ev, step == 0)
         HX = O.hamiltonian(grid, veff, tables, X, nb).reshape(nb, N)
         rq = np.einsum("ni,ni->n", X, HX) / np.einsum("ni,ni->n", X, X)
-        occ, mu = fermi_occupations(rq, n_el, kbt)
+        occ, mu = fermi_occupations_exact(rq, n_el, kbt)
         rho_out = density(X, occ, N)
         vh_out, eh = hartree(rho_out, grid)
         exc_out, _ = lda_pz(rho_out)

@@ -145,6 +145,17 @@ __global__ void __launch_bounds__(RB) dot_partial_kernel(size_t N, int na, const
     }
 }
 
+// partial[blockIdx.x] = sum over this block's points of |a - b|
+__global__ void __launch_bounds__(RB) l1_diff_partial_kernel(size_t N, const double* __restrict__ a,
+                                                             const double* __restrict__ b,
+                                                             double* __restrict__ partial) {
+    __shared__ double sh[RB / 32];
+    double v = 0.0;
+    for (size_t i = blockIdx.x * (size_t)RB + threadIdx.x; i < N; i += (size_t)gridDim.x * RB) v += fabs(a[i] - b[i]);
+    const double s = block_sum(v, sh);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
 // per band n: partial[n][blk] = sum x_n y_n and sum x_n x_n over this block's points
 __global__ void __launch_bounds__(RB) band_dot_kernel(size_t N, const double* __restrict__ X,
                                                       const double* __restrict__ Y, double* __restrict__ pxy,
@@ -188,6 +199,18 @@ struct KGrid {
     int nx, ny, nz, nxh;
     double dx, dy, dz;
 };
+
+// a Nyquist plane (k = n/2 of an even n): there G and -G are the same grid
+// point, so a structure-factor phase exp(-i G.R) has no real-field
+// representation; the local part leaves these planes out (energy and force alike)
+__device__ __forceinline__ bool on_nyquist(const KGrid& g, size_t idx) {
+    const int kx = (int)(idx % g.nxh);
+    const size_t r = idx / g.nxh;
+    const int ky = (int)(r % g.ny);
+    const int kz = (int)(r / g.ny);
+    return (g.nx % 2 == 0 && kx == g.nx / 2) || (g.ny % 2 == 0 && ky == g.ny / 2) ||
+           (g.nz % 2 == 0 && kz == g.nz / 2);
+}
 
 __device__ __forceinline__ void kvec(const KGrid& g, size_t idx, double& gx, double& gy, double& gz) {
     const int kx = (int)(idx % g.nxh);
@@ -238,6 +261,11 @@ __global__ void vloc_k_kernel(KGrid g, size_t M, double inv_omega, int na, const
         kvec(g, i, gx, gy, gz);
         const double g2 = gx * gx + gy * gy + gz * gz;
         double re = 0.0, im = 0.0;
+        if (on_nyquist(g, i)) {
+            f[i].x = 0.0;
+            f[i].y = 0.0;
+            continue;
+        }
         for (int a = 0; a < na; ++a) {
             const GthAtom at = atoms[a];
             const double r2 = at.rloc * at.rloc;
@@ -254,6 +282,47 @@ __global__ void vloc_k_kernel(KGrid g, size_t M, double inv_omega, int na, const
     }
 }
 
+// Force of the local part on every atom from a density's half-complex transform
+// f (f = D2Z(rho), rho_G = f / N): F_a = -d/dR_a int rho V_loc
+//   = sum_G G v_a(G) [sin(G.R_a) Re rho_G + cos(G.R_a) Im rho_G],
+// the exact derivative of dV sum_r rho(r) V_loc(r) with V_loc the Fourier
+// series above (Nyquist planes left out as there).  The half grid counts the
+// kx = 0 plane once and the others twice.  partial[(a * 3 + d) * gridDim.x + blockIdx.x].
+__global__ void __launch_bounds__(RB) local_force_kernel(KGrid g, size_t M, double inv_n, int na,
+                                                         const GthAtom* __restrict__ atoms,
+                                                         const cufftDoubleComplex* __restrict__ f,
+                                                         double* __restrict__ partial) {
+    __shared__ double sh[RB / 32];
+    const double tp32 = 15.749609945722419;   // (2 pi)^(3/2)
+    for (int a = 0; a < na; ++a) {
+        const GthAtom at = atoms[a];
+        const double r2 = at.rloc * at.rloc;
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        for (size_t i = blockIdx.x * (size_t)RB + threadIdx.x; i < M; i += (size_t)gridDim.x * RB) {
+            double gx, gy, gz;
+            kvec(g, i, gx, gy, gz);
+            const double g2 = gx * gx + gy * gy + gz * gz;
+            if (g2 == 0.0 || on_nyquist(g, i)) continue;
+            const int kx = (int)(i % g.nxh);
+            const double w = kx == 0 ? 1.0 : 2.0;   // +-G pairs: kx and nx - kx
+            const double e = exp(-0.5 * g2 * r2);
+            const double v = -4.0 * M_PI * at.zion * e / g2 + tp32 * r2 * at.rloc * e * (at.c1 + at.c2 * (3.0 - g2 * r2));
+            double sn, cs;
+            sincos(gx * at.x + gy * at.y + gz * at.z, &sn, &cs);
+            const double t = w * v * (sn * f[i].x + cs * f[i].y) * inv_n;
+            fx += gx * t;
+            fy += gy * t;
+            fz += gz * t;
+        }
+        const double sx = block_sum(fx, sh), sy = block_sum(fy, sh), sz = block_sum(fz, sh);
+        if (threadIdx.x == 0) {
+            partial[(size_t)(a * 3 + 0) * gridDim.x + blockIdx.x] = sx;
+            partial[(size_t)(a * 3 + 1) * gridDim.x + blockIdx.x] = sy;
+            partial[(size_t)(a * 3 + 2) * gridDim.x + blockIdx.x] = sz;
+        }
+    }
+}
+
 inline int pw_blocks(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
 
 }  // namespace
@@ -267,6 +336,7 @@ struct qsb_scf {
     double dx = 0, dy = 0, dz = 0, dV = 0;
     double n_el = 0, kbt = 0.01;
     double amp = 0.5, q0 = 0.8;
+    double rho_tol = 0.0;         // int |rho_out - rho_in| / N_e bound of the stop (0: off)
     int depth = 6;
     int n_atoms = 0;
     // device fields
@@ -275,6 +345,7 @@ struct qsb_scf {
     double *partial = nullptr, *sums = nullptr, *occ_dev = nullptr;
     const double** ptrs = nullptr;
     cufftDoubleComplex* fk = nullptr;
+    qsb::GthAtom* atoms = nullptr;     // GTH local parts (device), set_gth_local
     cufftHandle plan_f = 0, plan_b = 0;
     bool have_plans = false;
     // host
@@ -329,7 +400,8 @@ qsb_status potentials(qsb_scf* c, cudaStream_t s) {
 }
 
 // Fermi-Dirac occupations (SetOccupancy, source/SetOccupancy.h:7-18) at the mu of
-// the bisection of mSetOccupancyTemperature (source/qumasun_base1.occupancy.h:76-170)
+// the bisection of mSetOccupancyTemperature (source/qumasun_base1.occupancy.h:76-170),
+// refined by Newton steps to the exact electron count
 void fermi(const std::vector<double>& eig, double n_el, double kbt, std::vector<double>& occ) {
     const int n = (int)eig.size();
     auto fill = [&](double mu) {
@@ -345,14 +417,29 @@ void fermi(const std::vector<double>& eig, double n_el, double kbt, std::vector<
     double mu = 0.5 * (mu_min + mu_max);
     bool go = std::fabs(mu_max - mu_min) > 1.0e-9;
     fill(mu);
+    double mu_last = mu;
     while (go) {
         const double ne = fill(mu);
+        mu_last = mu;
         if (ne < n_el) mu_min = mu;
         else if (ne > n_el) mu_max = mu;
         else break;
         mu = 0.5 * (mu_min + mu_max);
         go = std::fabs(mu_max - mu_min) > 1.0e-9;
     }
+    // the bisection leaves the electron count off by dN/dmu x ~1e-9 (1e-7 electrons
+    // with a partly filled level at the Fermi energy), which moves the energy by
+    // ~mu 1e-7: Newton steps on sum f(mu) = N_e from the last bisection point
+    mu = mu_last;
+    for (int it = 0; it < 8; ++it) {
+        const double ne = fill(mu);
+        double dn = 0.0;
+        for (int k = 0; k < n; ++k) dn += occ[k] * (1.0 - 0.5 * occ[k]) / kbt;
+        const double r = ne - n_el;
+        if (std::fabs(r) <= 1e-14 * n_el || !(dn > 1e-300)) break;
+        mu -= r / dn;
+    }
+    fill(mu);
 }
 
 // Gaussian elimination with partial pivoting of the bordered DIIS system
@@ -514,6 +601,7 @@ qsb_status qsb_scf_destroy(qsb_scf* c) {
         if (f) cudaFree(f);
     if (c->ptrs) cudaFree((void*)c->ptrs);
     if (c->fk) cudaFree(c->fk);
+    if (c->atoms) cudaFree(c->atoms);
     if (c->have_plans) {
         cufftDestroy(c->plan_f);
         cufftDestroy(c->plan_b);
@@ -540,6 +628,12 @@ qsb_status qsb_scf_set_mixing(qsb_scf* c, double amplitude, double q0, int depth
     return QSB_OK;
 }
 
+qsb_status qsb_scf_set_density_tolerance(qsb_scf* c, double rho_tol) {
+    if (!c || !(rho_tol >= 0.0)) return fail(QSB_ERR_INVALID, "scf_set_density_tolerance: need rho_tol >= 0");
+    c->rho_tol = rho_tol;
+    return QSB_OK;
+}
+
 qsb_status qsb_scf_set_smearing(qsb_scf* c, double kbt) {
     if (!c || !(kbt > 0.0)) return fail(QSB_ERR_INVALID, "scf_set_smearing: need kbT > 0");
     c->kbt = kbt;
@@ -556,6 +650,9 @@ qsb_status qsb_scf_set_gth_local(qsb_scf* c, int n_atoms, const double* pos, con
         if (sp < 0 || sp >= n_species || !(rloc[sp] > 0.0)) return fail(QSB_ERR_INVALID, "scf_set_gth_local: bad species");
         at[a] = GthAtom{pos[3 * a], pos[3 * a + 1], pos[3 * a + 2], zion[sp], rloc[sp], c1[sp], c2[sp]};
     }
+    if (c->atoms) cudaFree(c->atoms);
+    c->atoms = nullptr;
+    c->n_atoms = 0;
     GthAtom* d = nullptr;
     QSB_CUDA_TRY(cudaMalloc((void**)&d, n_atoms * sizeof(GthAtom)));
     QSB_CUDA_TRY(cudaMemcpy(d, at.data(), n_atoms * sizeof(GthAtom), cudaMemcpyHostToDevice));
@@ -565,9 +662,41 @@ qsb_status qsb_scf_set_gth_local(qsb_scf* c, int n_atoms, const double* pos, con
     QSB_CUFFT_TRY(cufftSetStream(c->plan_b, 0));
     QSB_CUFFT_TRY(cufftExecZ2D(c->plan_b, c->fk, c->vloc));
     QSB_CUDA_TRY(cudaDeviceSynchronize());
-    cudaFree(d);
-    if (e != cudaSuccess) return cuda_fail(e, "vloc_k_kernel");
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        return cuda_fail(e, "vloc_k_kernel");
+    }
+    c->atoms = d;
     c->n_atoms = n_atoms;
+    return QSB_OK;
+}
+
+qsb_status qsb_scf_local_forces(qsb_scf* c, const double* rho_dev, double* forces) {
+    if (!c || !forces) return fail(QSB_ERR_INVALID, "scf_local_forces: bad argument");
+    if (c->n_atoms <= 0) return fail(QSB_ERR_STATE, "scf_local_forces: no local potential (qsb_scf_set_gth_local)");
+    const double* rho = rho_dev ? rho_dev : c->rho_out;
+    QSB_CUFFT_TRY(cufftSetStream(c->plan_f, 0));
+    QSB_CUFFT_TRY(cufftExecD2Z(c->plan_f, const_cast<double*>(rho), c->fk));
+    const int blocks = RBLOCKS / 4;
+    const int rows = 3 * c->n_atoms;
+    double* part = nullptr;
+    double* sums = nullptr;
+    QSB_CUDA_TRY(cudaMalloc((void**)&part, (size_t)rows * blocks * sizeof(double)));
+    if (cudaMalloc((void**)&sums, (size_t)rows * sizeof(double)) != cudaSuccess) {
+        cudaFree(part);
+        return fail(QSB_ERR_NOMEM, "scf_local_forces: device allocation");
+    }
+    local_force_kernel<<<blocks, RB>>>(kgrid(c), c->M, 1.0 / (double)c->N, c->n_atoms, c->atoms, c->fk, part);
+    row_sum_kernel<<<rows, 32>>>(rows, blocks, part, sums);
+    std::vector<double> h(rows);
+    const cudaError_t e = cudaMemcpy(h.data(), sums, rows * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(part);
+    cudaFree(sums);
+    if (e != cudaSuccess) return cuda_fail(e, "scf_local_forces");
+    for (int k = 0; k < rows; ++k) {
+        if (!std::isfinite(h[k])) return fail(QSB_ERR_NUMERIC, "scf_local_forces: non-finite value");
+        forces[k] += h[k];
+    }
     return QSB_OK;
 }
 
@@ -655,7 +784,16 @@ qsb_status qsb_scf_run(qsb_scf* c, double* X, double* keep, int lobpcg_iters, in
         const auto t_now = std::chrono::steady_clock::now();
         c->step_s.push_back(std::chrono::duration<double>(t_now - t_prev).count());
         t_prev = t_now;
-        const bool done = step > 0 && std::fabs(etot - e_prev) / c->n_atoms < tol_per_atom;
+        bool done = step > 0 && std::fabs(etot - e_prev) / c->n_atoms < tol_per_atom;
+        if (done && c->rho_tol > 0.0) {
+            // and the density residual (CONVERGENCE_MODE::RHO_ETOT of the reference's loop)
+            l1_diff_partial_kernel<<<RBLOCKS, RB, 0, s>>>(N, c->rho_out, c->rho_in, c->partial);
+            row_sum_kernel<<<1, 32, 0, s>>>(1, RBLOCKS, c->partial, c->sums);
+            double l1 = 0.0;
+            QSB_CUDA_TRY(cudaMemcpyAsync(&l1, c->sums, sizeof(double), cudaMemcpyDeviceToHost, s));
+            QSB_CUDA_TRY(cudaStreamSynchronize(s));
+            done = l1 * c->dV / c->n_el < c->rho_tol;
+        }
         e_prev = etot;
         if (done) break;
         QSB_TRY(mix(c, s));

@@ -386,6 +386,7 @@ class SCF:
 
     def set_gth_local(self, pos, species, zion, rloc, c1, c2):
         pos, pos_p = _f64(np.asarray(pos, np.float64).reshape(-1, 3))
+        self._n_atoms = len(pos)
         sp, sp_p = _i32(species)
         arrs = [_f64(v) for v in (zion, rloc, c1, c2)]
         _check(lib.qsb_scf_set_gth_local(self._h, len(pos), pos_p, sp_p, len(arrs[0][0]),
@@ -393,6 +394,9 @@ class SCF:
 
     def set_mixing(self, amplitude=0.5, q0=0.8, depth=6):
         _check(lib.qsb_scf_set_mixing(self._h, _c_d(amplitude), _c_d(q0), depth))
+
+    def set_density_tolerance(self, rho_tol):
+        _check(lib.qsb_scf_set_density_tolerance(self._h, _c_d(rho_tol)))
 
     def set_smearing(self, kbt):
         _check(lib.qsb_scf_set_smearing(self._h, _c_d(kbt)))
@@ -407,6 +411,14 @@ class SCF:
         _check(lib.qsb_scf_run(self._h, _dev_ptr(X), _dev_ptr(keep), lobpcg_iters, max_steps, _c_d(tol_per_atom),
                                e_p, ctypes.byref(steps), ev_p, occ_p, _stream_ptr(X)))
         return e[:steps.value].copy(), ev, occ
+
+    def local_forces(self, rho=None, n_atoms=None):
+        """Forces of the GTH local parts, [n_atoms, 3], from the last output
+        density (or a given fp64 CUDA density)."""
+        na = n_atoms if n_atoms is not None else self._n_atoms
+        f, f_p = _f64(np.zeros(3 * na))
+        _check(lib.qsb_scf_local_forces(self._h, _dev_ptr(rho) if rho is not None else None, f_p))
+        return f.reshape(na, 3)
 
     def step_seconds(self):
         """Wall seconds of each step of the last run."""

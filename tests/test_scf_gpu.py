@@ -94,3 +94,89 @@ def test_mixed_scf_reaches_the_fp64_energy(qsb):
     occ_n = int(SCF_C0["n_el"] // 2)
     np.testing.assert_allclose(r32["ev"][:occ_n], r64["ev"][:occ_n], rtol=0, atol=5e-5)
     assert qsb.device_status() == 0
+
+
+def _bcc(qsb, pos, X0=None):
+    """Config 0's cell (2-atom bcc, 32^3, 16 bands, 12 electrons, Fermi 0.01 Ha)
+    with displaced atoms, converged to |dE| < 1e-11 Ha / atom and
+    int |rho_out - rho_in| / N_e < 1e-10; projector cutoff 9 r_l so that no
+    projector value jumps at the sphere edge when an atom moves."""
+    import torch
+    n, a = SCF_C0["n"], SCF_C0["a"]
+    h = a / n
+    N = n ** 3
+    sp = O.GTH_BCC
+    H = qsb.Hamiltonian(n, n, n, h, h, h)
+    H.set_gth_projectors(pos, [0, 0], [sp["nl"]], [sp["r"]], [sp["h"]], 9.0)
+    H.set_potential(np.zeros(N))
+    es = qsb.EigenSolver(N, 16, False, "fp64")
+    scf = qsb.SCF(H, es, 16, 12.0)
+    scf.set_gth_local(pos, [0, 0], [sp["zion"]], [sp["rloc"]], [sp["c1"]], [sp["c2"]])
+    scf.set_density_tolerance(1e-10)
+    X = torch.from_numpy(O.orthonormal_psi(0, 16, N, h ** 3)).cuda() if X0 is None else X0.clone()
+    keep = torch.zeros_like(X)
+    e, ev, occ = scf.run(X, keep, 4, 300, 1e-11)
+    return dict(H=H, es=es, scf=scf, e=e, ev=ev, occ=occ, X=X)
+
+
+def _ts(occ, kbt=0.01):
+    """kBT S of spin-paired Fermi-Dirac occupations (S = -2 sum f ln f + (1-f) ln(1-f), f = occ / 2)."""
+    f = np.clip(np.asarray(occ) / 2.0, 1e-300, 1.0 - 1e-16)
+    return kbt * 2.0 * float(np.sum(-(f * np.log(f) + (1.0 - f) * np.log1p(-f))))
+
+
+def test_forces_are_minus_the_free_energy_gradient(qsb):
+    """Adjoint forces (local part from the output density, qsb_scf_local_forces;
+    nonlocal part from the projections on the analytic projector gradients,
+    qsb_ham_nonlocal_energy_force) against central differences (delta = 1e-3
+    bohr) of the converged SCF free energy F = E - kBT S (the variational
+    functional with Fermi smearing; the cell's Fermi level sits in a partly
+    filled triplet): every component within 1e-6 Ha / bohr (the stated bar is
+    1e-5), and within 1e-8 after Richardson extrapolation from delta / 2."""
+    pos = O.bcc_positions(SCF_C0["a"], 1) + np.array([[0.13, -0.07, 0.21], [-0.11, 0.05, 0.02]])
+    r0 = _bcc(qsb, pos)
+    assert 0.01 < _ts(r0["occ"])                                # smearing matters here (kBT S ~ 0.04 Ha)
+    f = r0["scf"].local_forces() + np.asarray(r0["H"].nonlocal_energy_force(r0["X"], r0["occ"], 2)[1]).reshape(2, 3)
+    assert np.abs(f).max() > 0.05
+    for at in range(2):
+        for k in range(3):
+            fds = []
+            for d in (1e-3, 5e-4):
+                fe = []
+                for sgn in (1.0, -1.0):
+                    p = pos.copy()
+                    p[at, k] += sgn * d
+                    r = _bcc(qsb, p, r0["X"])
+                    fe.append(r["e"][-1] - _ts(r["occ"]))
+                fds.append(-(fe[0] - fe[1]) / (2 * d))
+            assert abs(f[at, k] - fds[0]) < 1e-6, (at, k, f[at, k], fds[0])
+            assert abs(f[at, k] - (4 * fds[1] - fds[0]) / 3) < 1e-8, (at, k, f[at, k], fds)
+    assert qsb.device_status() == 0
+
+
+def test_local_forces_match_the_oracle_on_a_molecule(qsb):
+    """Config 1 (O + 2 H in a 20 bohr box, 112^3): the device local force on the
+    converged SCF density equals the oracle's to 1e-10 relative (Nyquist planes
+    left out by both)."""
+    import torch
+    n, L = 112, 20.0
+    h = L / n
+    N = n ** 3
+    pos = np.array([[0.0, 0.0, 0.0], [1.43, 1.11, 0.0], [-1.43, 1.11, 0.0]])
+    pos = pos + np.random.default_rng(1).normal(0.0, 0.05, pos.shape)
+    H = qsb.Hamiltonian(n, n, n, h, h, h)
+    H.set_gth_projectors(pos, [0, 1, 1], [1, 0], [[O.GTH_O["r"][0], 0.0], [0.0, 0.0]],
+                         [[O.GTH_O["h"][0], 0.0], [0.0, 0.0]], 9.0)
+    H.set_potential(np.zeros(N))
+    es = qsb.EigenSolver(N, 8, False, "fp64")
+    scf = qsb.SCF(H, es, 8, 8.0)
+    sps = [O.GTH_O, O.GTH_H]
+    scf.set_gth_local(pos, [0, 1, 1], [s["zion"] for s in sps], [s["rloc"] for s in sps], [s["c1"] for s in sps],
+                      [s["c2"] for s in sps])
+    X = torch.from_numpy(O.orthonormal_psi(1, 8, N, h ** 3)).cuda()
+    e, ev, occ = scf.run(X, torch.zeros_like(X), 4, 200, 1e-8)
+    rho = scf.field(0)
+    f = scf.local_forces()
+    f_o = S.gth_local_forces(rho.cpu().numpy(), (n, n, n, h, h, h), pos, [O.GTH_O, O.GTH_H, O.GTH_H])
+    np.testing.assert_allclose(f, f_o, rtol=0, atol=1e-10 * np.abs(f_o).max())
+    assert np.abs(f).max() > 0.1

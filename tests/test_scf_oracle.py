@@ -83,3 +83,29 @@ def test_scf_fixture_matches_its_inputs():
     assert abs(e[-1] - e[-2]) / 2 < SCF_C0["params"]["tol_per_atom"]
     assert abs(f["occ"].sum() - SCF_C0["n_el"]) < 1e-6
     assert abs(f["rho"].sum() * (SCF_C0["a"] / SCF_C0["n"]) ** 3 - SCF_C0["n_el"]) < 1e-6
+
+
+def test_local_forces_are_minus_the_local_energy_gradient():
+    """gth_local_forces against central differences (delta 1e-4 bohr) of
+    E_loc(R) = dV sum rho V_loc(R) with the density frozen: 1e-7 of the largest
+    component (the Fourier series is smooth in R; error O(delta^2))."""
+    n, a = 24, 6.0
+    h = a / n
+    grid = (n, n, n, h, h, h)
+    pos = O.bcc_positions(a, 1) + np.array([[0.13, -0.07, 0.21], [-0.11, 0.05, 0.02]])
+    sps = [dict(O.GTH_BCC)] * 2
+    rng = np.random.default_rng(9)
+    rho = 0.05 + 0.02 * rng.uniform(size=n ** 3)
+    f = S.gth_local_forces(rho, grid, pos, sps)
+    d = 1e-4
+    fd = np.zeros_like(f)
+    for at in range(2):
+        for k in range(3):
+            p1, p2 = pos.copy(), pos.copy()
+            p1[at, k] += d
+            p2[at, k] -= d
+            e1 = float(np.dot(rho, S.gth_local_potential(grid, p1, sps))) * h ** 3
+            e2 = float(np.dot(rho, S.gth_local_potential(grid, p2, sps))) * h ** 3
+            fd[at, k] = -(e1 - e2) / (2 * d)
+    assert np.abs(f).max() > 1e-3
+    np.testing.assert_allclose(f, fd, rtol=0, atol=1e-7 * np.abs(f).max())
