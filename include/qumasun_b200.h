@@ -417,6 +417,36 @@ QSB_API qsb_status qsb_scf_get_field(qsb_scf* scf, int which, double* out);
  * terms of the reference's mGetForce (source/qumasun_base1.force.h:23-205;
  * mGetForceOnNuclRho_HR :247-284 on its core-charge form of V_loc). */
 QSB_API qsb_status qsb_scf_local_forces(qsb_scf* scf, const double* rho_dev, double* forces);
+/* Ion-ion energy of point charges (the GTH Z_ion, host arrays) in the
+ * orthorhombic cell cell[3] (bohr) with a neutralising background, by Ewald
+ * summation (alpha = 5 / min(L), sums cut at 1e-16); forces (host, 3 x n_atoms,
+ * may be NULL) accumulate ("+=").  Host code, no device work.  The ion-ion
+ * term of the reference's total energy and force (mGetForce's nuclear part,
+ * source/qumasun_base1.force.h:23-205). */
+QSB_API qsb_status qsb_ewald(int n_atoms, const double* pos, const double* charge, const double* cell,
+                             double* energy, double* forces);
+/* Geometry relaxation by LBFGS on the free energy E - kBT S + E_ewald, forces
+ * local + nonlocal + Ewald.  Replaces the relaxation drivers
+ * glips::Relaxation1Q..4Q::Evolve (source/Relaxation1.h:45-190) as the
+ * reference's SCF/relax loop uses them.  Each evaluation moves the projectors
+ * (qsb_ham_set_gth_projectors with nl, r_l, h_l, rcut_factor) and the local
+ * parts (qsb_scf_set_gth_local with zion, rloc, c1, c2) to the positions and
+ * runs qsb_scf_run(X, keep, lobpcg_iters, scf_max_steps, scf_tol) warm from
+ * the previous states.  Steps: two-loop recursion over the last `history`
+ * pairs (initial scale s.y / y.y; 1 bohr^2/Ha before any pair), capped at
+ * max_step bohr per atom, halved (up to 5 times) while the energy rises by
+ * more than 10 scf_tol per atom (the SCF energies' own error).
+ * fixed (may be NULL): atoms with fixed[a] != 0 do not move.  Stops at
+ * max_a |F_a| < fmax or after max_iter steps.  pos (host) returns the last
+ * geometry, energies (host, max_iter + 1 values) the energy after each
+ * step (index 0: the start), *iters the steps taken, forces (host, may be
+ * NULL) the last forces. */
+QSB_API qsb_status qsb_relax_lbfgs(qsb_scf* scf, int n_atoms, double* pos, const int* species, int n_species,
+                                   const int* nl, const double* r_l, const double* h_l, double rcut_factor,
+                                   const double* zion, const double* rloc, const double* c1, const double* c2,
+                                   const int* fixed, double* X, double* keep, int lobpcg_iters, int scf_max_steps,
+                                   double scf_tol, int max_iter, double fmax, double max_step, int history,
+                                   double* energies, int* iters, double* forces, void* stream);
 /* Wall seconds of each step of the last qsb_scf_run (host clock; a step ends
  * when its energy is on the host): up to max values, *n = steps recorded. */
 QSB_API qsb_status qsb_scf_step_seconds(qsb_scf* scf, double* seconds, int max, int* n);

@@ -353,3 +353,58 @@ def scf(grid, pos, species_params, nb, n_el, X0, kbt=0.01, lobpcg_iters=4, max_s
         rho_in = mixer.next(rho_in, rho_out)
     return dict(energies=np.array(energies), rq=rq, occ=occ, mu=mu, rho=rho_out, X=X, vloc=vloc, steps=len(energies),
                 converged=done)
+
+
+def ewald(pos, charge, cell, alpha=None, tol=1e-16):
+    """Ewald energy and forces of point charges in an orthorhombic periodic cell
+    with a neutralising background (the ion-ion term that goes with the G-space
+    GTH local part, whose Coulomb tail -Z/r is that of a point charge):
+    E = 1/2 sum' Z_a Z_b erfc(alpha r)/r + (2 pi/Omega) sum_{G!=0} exp(-G^2/4alpha^2)/G^2 |S(G)|^2
+        - alpha/sqrt(pi) sum Z^2 - pi/(2 Omega alpha^2) (sum Z)^2,  S(G) = sum Z e^{iG.R}.
+    Restated from the mathematics (the reference forms nucleus-nucleus terms from
+    core charges on its finer grid, source/qumasun_base1.energy.h)."""
+    from math import erfc, sqrt, pi, exp
+    pos = np.asarray(pos, np.float64)
+    Z = np.asarray(charge, np.float64)
+    L = np.asarray(cell, np.float64)
+    omega = float(np.prod(L))
+    if alpha is None:
+        alpha = 5.0 / float(L.min())
+    rc = sqrt(-np.log(tol)) / alpha
+    gc = 2.0 * alpha * sqrt(-np.log(tol))
+    na = len(pos)
+    E = 0.0
+    F = np.zeros((na, 3))
+    nimg = [int(np.ceil(rc / L[d])) + 1 for d in range(3)]
+    for a in range(na):
+        for b in range(na):
+            d0 = pos[a] - pos[b]
+            for i in range(-nimg[0], nimg[0] + 1):
+                for j in range(-nimg[1], nimg[1] + 1):
+                    for k in range(-nimg[2], nimg[2] + 1):
+                        if a == b and i == 0 and j == 0 and k == 0:
+                            continue
+                        d = d0 + np.array([i, j, k]) * L
+                        r = sqrt(float(d @ d))
+                        if r > rc:
+                            continue
+                        E += 0.5 * Z[a] * Z[b] * erfc(alpha * r) / r
+                        g = Z[a] * Z[b] * (erfc(alpha * r) / r + 2 * alpha / sqrt(pi) * exp(-alpha * alpha * r * r)) / (r * r)
+                        F[a] += g * d
+    m = [int(np.ceil(gc * L[d] / (2 * pi))) for d in range(3)]
+    for i in range(-m[0], m[0] + 1):
+        for j in range(-m[1], m[1] + 1):
+            for k in range(-m[2], m[2] + 1):
+                if i == 0 and j == 0 and k == 0:
+                    continue
+                G = 2 * pi * np.array([i / L[0], j / L[1], k / L[2]])
+                g2 = float(G @ G)
+                if g2 > gc * gc:
+                    continue
+                w = exp(-g2 / (4 * alpha * alpha)) / g2
+                ph = pos @ G
+                S = np.sum(Z * np.exp(1j * ph))
+                E += 2 * pi / omega * w * abs(S) ** 2
+                F += (4 * pi / omega * w * Z * np.imag(np.conj(S) * np.exp(1j * ph)))[:, None] * G[None, :]
+    E += -alpha / sqrt(pi) * float(np.sum(Z * Z)) - pi / (2 * omega * alpha * alpha) * float(np.sum(Z)) ** 2
+    return E, F

@@ -804,3 +804,223 @@ qsb_status qsb_scf_run(qsb_scf* c, double* X, double* keep, int lobpcg_iters, in
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Ion-ion (Ewald) energy and forces, and LBFGS geometry relaxation.
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+// Point charges in an orthorhombic cell with a neutralising background: the
+// ion-ion term that goes with the G-space GTH local part (whose Coulomb tail is
+// that of a point charge Z_ion).  Splitting alpha = 5 / min(L), real and
+// reciprocal sums cut where erfc / the Gaussian fall below 1e-16.
+qsb_status qsb_ewald(int n_atoms, const double* pos, const double* charge, const double* cell, double* energy,
+                     double* forces) {
+    if (n_atoms <= 0 || !pos || !charge || !cell || !energy) return fail(QSB_ERR_INVALID, "ewald: bad argument");
+    const double L[3] = {cell[0], cell[1], cell[2]};
+    if (!(L[0] > 0) || !(L[1] > 0) || !(L[2] > 0)) return fail(QSB_ERR_INVALID, "ewald: cell edges must be > 0");
+    const double omega = L[0] * L[1] * L[2];
+    const double alpha = 5.0 / std::min(L[0], std::min(L[1], L[2]));
+    const double lt = std::sqrt(-std::log(1e-16));
+    const double rc = lt / alpha, gc = 2.0 * alpha * lt;
+    const double spi = std::sqrt(M_PI);
+    double E = 0.0;
+    std::vector<double> F(3 * (size_t)n_atoms, 0.0);
+    int nimg[3];
+    for (int d = 0; d < 3; ++d) nimg[d] = (int)std::ceil(rc / L[d]) + 1;
+    for (int a = 0; a < n_atoms; ++a)
+        for (int b = 0; b < n_atoms; ++b)
+            for (int i = -nimg[0]; i <= nimg[0]; ++i)
+                for (int j = -nimg[1]; j <= nimg[1]; ++j)
+                    for (int k = -nimg[2]; k <= nimg[2]; ++k) {
+                        if (a == b && i == 0 && j == 0 && k == 0) continue;
+                        const double d[3] = {pos[3 * a] - pos[3 * b] + i * L[0], pos[3 * a + 1] - pos[3 * b + 1] + j * L[1],
+                                             pos[3 * a + 2] - pos[3 * b + 2] + k * L[2]};
+                        const double r = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+                        if (r > rc) continue;
+                        const double zz = charge[a] * charge[b];
+                        E += 0.5 * zz * std::erfc(alpha * r) / r;
+                        const double g = zz * (std::erfc(alpha * r) / r + 2.0 * alpha / spi * std::exp(-alpha * alpha * r * r)) /
+                                         (r * r);
+                        for (int c = 0; c < 3; ++c) F[3 * a + c] += g * d[c];
+                    }
+    int m[3];
+    for (int d = 0; d < 3; ++d) m[d] = (int)std::ceil(gc * L[d] / (2.0 * M_PI));
+    for (int i = -m[0]; i <= m[0]; ++i)
+        for (int j = -m[1]; j <= m[1]; ++j)
+            for (int k = -m[2]; k <= m[2]; ++k) {
+                if (i == 0 && j == 0 && k == 0) continue;
+                const double G[3] = {2.0 * M_PI * i / L[0], 2.0 * M_PI * j / L[1], 2.0 * M_PI * k / L[2]};
+                const double g2 = G[0] * G[0] + G[1] * G[1] + G[2] * G[2];
+                if (g2 > gc * gc) continue;
+                const double w = std::exp(-g2 / (4.0 * alpha * alpha)) / g2;
+                double sr = 0.0, si = 0.0;
+                for (int a = 0; a < n_atoms; ++a) {
+                    const double ph = G[0] * pos[3 * a] + G[1] * pos[3 * a + 1] + G[2] * pos[3 * a + 2];
+                    sr += charge[a] * std::cos(ph);
+                    si += charge[a] * std::sin(ph);
+                }
+                E += 2.0 * M_PI / omega * w * (sr * sr + si * si);
+                for (int a = 0; a < n_atoms; ++a) {
+                    const double ph = G[0] * pos[3 * a] + G[1] * pos[3 * a + 1] + G[2] * pos[3 * a + 2];
+                    // Im(conj(S) e^{i ph}) = sr sin(ph) - si cos(ph)
+                    const double t = 4.0 * M_PI / omega * w * charge[a] * (sr * std::sin(ph) - si * std::cos(ph));
+                    for (int c = 0; c < 3; ++c) F[3 * a + c] += t * G[c];
+                }
+            }
+    double z2 = 0.0, zs = 0.0;
+    for (int a = 0; a < n_atoms; ++a) {
+        z2 += charge[a] * charge[a];
+        zs += charge[a];
+    }
+    E += -alpha / spi * z2 - M_PI / (2.0 * omega * alpha * alpha) * zs * zs;
+    *energy = E;
+    if (forces)
+        for (size_t q = 0; q < F.size(); ++q) forces[q] += F[q];
+    return QSB_OK;
+}
+
+// LBFGS on the free energy E - kBT S + E_ewald with the forces local + nonlocal
+// + Ewald (the relaxation the reference drives with damped dynamics,
+// glips::Relaxation1Q..4Q::Evolve, source/Relaxation1.h:45-190): per iteration
+// the projectors and the local part move to the new positions, the SCF runs
+// warm from the previous states, the two-loop recursion (history `history`,
+// initial scale s.y / y.y) proposes a step, capped at max_step bohr per atom
+// (the reference's upper move limit); a step that raises the energy is halved
+// (up to 5 times, rises under 10 scf_tol per atom count as noise) before
+// the history is updated.  Fixed atoms (fixed[a] != 0)
+// feel no force.  Stops at max |F| < fmax.
+qsb_status qsb_relax_lbfgs(qsb_scf* c, int n_atoms, double* pos, const int* species, int n_species, const int* nl,
+                           const double* r_l, const double* h_l, double rcut_factor, const double* zion,
+                           const double* rloc, const double* c1, const double* c2, const int* fixed, double* X,
+                           double* keep, int lobpcg_iters, int scf_max_steps, double scf_tol, int max_iter,
+                           double fmax, double max_step, int history, double* energies, int* iters, double* forces,
+                           void* stream) {
+    if (!c || n_atoms <= 0 || !pos || !species || !X || !keep || max_iter <= 0 || !(fmax > 0) || !(max_step > 0) ||
+        history < 1 || !energies || !iters || scf_max_steps <= 0)
+        return fail(QSB_ERR_INVALID, "relax_lbfgs: bad argument");
+    const int n3 = 3 * n_atoms;
+    std::vector<double> q(n_atoms);
+    for (int a = 0; a < n_atoms; ++a) {
+        if (species[a] < 0 || species[a] >= n_species) return fail(QSB_ERR_INVALID, "relax_lbfgs: bad species");
+        q[a] = zion[species[a]];
+    }
+    const double cell[3] = {c->nx * c->dx, c->ny * c->dy, c->nz * c->dz};
+    std::vector<double> e_scf(scf_max_steps), occ(c->nb), ev(c->nb);
+    // free energy and gradient (g = -F) at x
+    auto evaluate = [&](const double* x, double& E, std::vector<double>& g) -> qsb_status {
+        QSB_TRY(qsb_ham_set_gth_projectors(c->ham, n_atoms, x, species, n_species, nl, r_l, h_l, rcut_factor));
+        QSB_TRY(qsb_scf_set_gth_local(c, n_atoms, x, species, n_species, zion, rloc, c1, c2));
+        int steps = 0;
+        QSB_TRY(qsb_scf_run(c, X, keep, lobpcg_iters, scf_max_steps, scf_tol, e_scf.data(), &steps, ev.data(),
+                            occ.data(), stream));
+        double ts = 0.0;
+        for (int n = 0; n < c->nb; ++n) {
+            const double f = std::min(std::max(occ[n] / 2.0, 1e-300), 1.0 - 1e-16);
+            ts -= c->kbt * 2.0 * (f * std::log(f) + (1.0 - f) * std::log1p(-f));
+        }
+        std::vector<double> F(n3, 0.0);
+        double ee = 0.0, enl = 0.0;
+        QSB_TRY(qsb_ewald(n_atoms, x, q.data(), cell, &ee, F.data()));
+        QSB_TRY(qsb_scf_local_forces(c, nullptr, F.data()));
+        QSB_TRY(qsb_ham_nonlocal_energy_force(c->ham, QSB_F64, 0, c->nb, X, occ.data(), 0.0, 0.0, 0.0, &enl,
+                                              F.data(), stream));
+        E = e_scf[steps - 1] - ts + ee;
+        g.assign(n3, 0.0);
+        for (int a = 0; a < n_atoms; ++a)
+            for (int k = 0; k < 3; ++k) g[3 * a + k] = (fixed && fixed[a]) ? 0.0 : -F[3 * a + k];
+        return QSB_OK;
+    };
+    auto fmax_of = [&](const std::vector<double>& g) {
+        double m = 0.0;
+        for (int a = 0; a < n_atoms; ++a)
+            m = std::max(m, std::sqrt(g[3 * a] * g[3 * a] + g[3 * a + 1] * g[3 * a + 1] + g[3 * a + 2] * g[3 * a + 2]));
+        return m;
+    };
+    std::vector<double> x(pos, pos + n3), g, xn(n3), gn;
+    std::vector<std::vector<double>> S, Y;
+    double E = 0.0, En = 0.0;
+    QSB_TRY(evaluate(x.data(), E, g));
+    *iters = 0;
+    energies[0] = E;
+    for (int it = 1; it <= max_iter && fmax_of(g) >= fmax; ++it) {
+        // two-loop recursion: d = -H g
+        std::vector<double> d(g);
+        const int m = (int)S.size();
+        std::vector<double> al(m), rho(m);
+        for (int i = m - 1; i >= 0; --i) {
+            double sy = 0.0, sd = 0.0;
+            for (int k = 0; k < n3; ++k) {
+                sy += S[i][k] * Y[i][k];
+                sd += S[i][k] * d[k];
+            }
+            rho[i] = 1.0 / sy;
+            al[i] = rho[i] * sd;
+            for (int k = 0; k < n3; ++k) d[k] -= al[i] * Y[i][k];
+        }
+        double h0 = 1.0;   // bohr^2 / Ha without history
+        if (m > 0) {
+            double sy = 0.0, yy = 0.0;
+            for (int k = 0; k < n3; ++k) {
+                sy += S[m - 1][k] * Y[m - 1][k];
+                yy += Y[m - 1][k] * Y[m - 1][k];
+            }
+            h0 = sy / yy;
+        }
+        for (int k = 0; k < n3; ++k) d[k] *= h0;
+        for (int i = 0; i < m; ++i) {
+            double yd = 0.0;
+            for (int k = 0; k < n3; ++k) yd += Y[i][k] * d[k];
+            const double b = rho[i] * yd;
+            for (int k = 0; k < n3; ++k) d[k] += S[i][k] * (al[i] - b);
+        }
+        for (int k = 0; k < n3; ++k) d[k] = -d[k];
+        // cap the displacement per atom
+        double dm = 0.0;
+        for (int a = 0; a < n_atoms; ++a)
+            dm = std::max(dm, std::sqrt(d[3 * a] * d[3 * a] + d[3 * a + 1] * d[3 * a + 1] + d[3 * a + 2] * d[3 * a + 2]));
+        const double sc = dm > max_step ? max_step / dm : 1.0;
+        double step = sc;
+        bool ok = false;
+        // energies carry the SCF stop's error (|dE| < scf_tol per atom per
+        // step, a few steps' worth from the fixed point): rises below that are noise
+        const double slack = 10.0 * scf_tol * n_atoms;
+        for (int tries = 0; tries < 6; ++tries) {
+            for (int k = 0; k < n3; ++k) xn[k] = x[k] + step * d[k];
+            QSB_TRY(evaluate(xn.data(), En, gn));
+            if (En <= E + slack || tries == 5) {
+                ok = true;
+                break;
+            }
+            step *= 0.5;
+        }
+        if (!ok) break;
+        std::vector<double> s(n3), y(n3);
+        double sy = 0.0;
+        for (int k = 0; k < n3; ++k) {
+            s[k] = xn[k] - x[k];
+            y[k] = gn[k] - g[k];
+            sy += s[k] * y[k];
+        }
+        if (sy > 1e-12) {
+            S.push_back(s);
+            Y.push_back(y);
+            if ((int)S.size() > history) {
+                S.erase(S.begin());
+                Y.erase(Y.begin());
+            }
+        }
+        x = xn;
+        g = gn;
+        E = En;
+        energies[it] = E;
+        *iters = it;
+    }
+    std::copy(x.begin(), x.end(), pos);
+    if (forces)
+        for (int k = 0; k < n3; ++k) forces[k] = -g[k];
+    return QSB_OK;
+}
+
+}  // extern "C"

@@ -354,6 +354,19 @@ def density(X, occupations, N):
     return rho
 
 
+def ewald(pos, charge, cell):
+    """(energy, forces [n_atoms, 3]) of point charges in an orthorhombic cell
+    with a neutralising background (qsb_ewald; host code)."""
+    p, p_p = _f64(np.asarray(pos, np.float64).reshape(-1, 3))
+    q, q_p = _f64(np.asarray(charge, np.float64).ravel())
+    c, c_p = _f64(np.asarray(cell, np.float64).ravel())
+    assert len(q) == len(p) and len(c) == 3
+    f, f_p = _f64(np.zeros(3 * len(p)))
+    e = ctypes.c_double()
+    _check(lib.qsb_ewald(len(p), p_p, q_p, c_p, ctypes.byref(e), f_p))
+    return e.value, f.reshape(len(p), 3)
+
+
 def lda_pz(rho):
     """(rho eps_xc, v_xc) of the Perdew-Zunger LDA (qsb_lda_pz ~ Calc_XC_LDA)."""
     torch = _torch()
@@ -426,6 +439,33 @@ class SCF:
         n = ctypes.c_int()
         _check(lib.qsb_scf_step_seconds(self._h, buf_p, len(buf), ctypes.byref(n)))
         return buf[:n.value].copy()
+
+    def relax(self, X, keep, pos, species, projectors, local, fixed=None, lobpcg_iters=4, scf_max_steps=60,
+              scf_tol=1e-8, max_iter=50, fmax=1e-4, max_step=0.2, history=5):
+        """LBFGS relaxation (qsb_relax_lbfgs) of the atoms at pos [n_atoms, 3];
+        projectors = (nl, r_l, h_l, rcut_factor) as set_gth_projectors takes
+        them, local = (zion, rloc, c1, c2) as set_gth_local.  X, keep: [nb, N]
+        fp64 CUDA, warm states (updated).  Returns (positions, energies per
+        step, forces [n_atoms, 3])."""
+        p, p_p = _f64(np.asarray(pos, np.float64).reshape(-1, 3).copy())
+        na = len(p)
+        self._n_atoms = na
+        sp, sp_p = _i32(species)
+        nl, r_l, h_l, rcut = projectors
+        n, n_p = _i32(nl)
+        r, r_p = _f64(np.asarray(r_l, np.float64).ravel())
+        hh, h_p = _f64(np.asarray(h_l, np.float64).ravel())
+        loc = [_f64(v) for v in local]
+        fx, fx_p = _i32(np.asarray(fixed, np.int32).ravel()) if fixed is not None else (None, None)
+        assert fx is None or len(fx) == na
+        e, e_p = _f64(np.zeros(max_iter + 1))
+        f, f_p = _f64(np.zeros(3 * na))
+        it = ctypes.c_int()
+        _check(lib.qsb_relax_lbfgs(self._h, na, p_p, sp_p, len(n), n_p, r_p, h_p, _c_d(rcut),
+                                   *[q for _, q in loc], fx_p, _dev_ptr(X), _dev_ptr(keep), lobpcg_iters,
+                                   scf_max_steps, _c_d(scf_tol), max_iter, _c_d(fmax), _c_d(max_step), history, e_p,
+                                   ctypes.byref(it), f_p, _stream_ptr(X)))
+        return p.reshape(na, 3).copy(), e[:it.value + 1].copy(), f.reshape(na, 3)
 
     def field(self, which):
         """0: output density, 1: V_loc, 2: V_eff, 3: mixed input density."""

@@ -180,3 +180,43 @@ def test_local_forces_match_the_oracle_on_a_molecule(qsb):
     f_o = S.gth_local_forces(rho.cpu().numpy(), (n, n, n, h, h, h), pos, [O.GTH_O, O.GTH_H, O.GTH_H])
     np.testing.assert_allclose(f, f_o, rtol=0, atol=1e-10 * np.abs(f_o).max())
     assert np.abs(f).max() > 0.1
+
+
+def test_lbfgs_relaxes_the_molecule(qsb):
+    """Config 1 relaxed by qsb_relax_lbfgs (free energy E - kBT S + Ewald; forces
+    local + nonlocal + Ewald) to max |F| < 1e-4 Ha / bohr: the energy never
+    rises by more than the SCF noise, the returned forces equal the ones
+    assembled afresh at the returned geometry from the parts (1e-6), and the
+    two O-H bonds come out equal (the molecule's mirror symmetry; the grid
+    breaks it only by its egg-box ripple, 1e-2 bohr)."""
+    import torch
+    n, L = 112, 20.0
+    h = L / n
+    N = n ** 3
+    pos = np.array([[0.0, 0.0, 0.0], [1.43, 1.11, 0.0], [-1.43, 1.11, 0.0]])
+    pos = pos + np.random.default_rng(1).normal(0.0, 0.05, pos.shape) + L / 2
+    sps = [O.GTH_O, O.GTH_H]
+    species = [0, 1, 1]
+    proj = ([1, 0], [[O.GTH_O["r"][0], 0.0], [0.0, 0.0]], [[O.GTH_O["h"][0], 0.0], [0.0, 0.0]], 9.0)
+    local = ([s["zion"] for s in sps], [s["rloc"] for s in sps], [s["c1"] for s in sps], [s["c2"] for s in sps])
+    H = qsb.Hamiltonian(n, n, n, h, h, h)
+    H.set_gth_projectors(pos, species, *proj)
+    H.set_potential(np.zeros(N))
+    es = qsb.EigenSolver(N, 8, False, "fp64")
+    scf = qsb.SCF(H, es, 8, 8.0)
+    scf.set_gth_local(pos, species, *local)
+    scf.set_density_tolerance(1e-7)
+    X = torch.from_numpy(O.orthonormal_psi(1, 8, N, h ** 3)).cuda()
+    keep = torch.zeros_like(X)
+    p, e, f = scf.relax(X, keep, pos, species, proj, local, scf_tol=1e-9, max_iter=40, fmax=1e-4)
+    assert np.linalg.norm(f, axis=1).max() < 1e-4, f
+    assert len(e) >= 3 and e[-1] < e[0] - 1e-3
+    assert np.all(np.diff(e) < 10 * 1e-9 * 3 + 1e-12), np.diff(e)
+    # forces afresh from the parts at the returned geometry (states and density of the last evaluation)
+    e_run, ev, occ = scf.run(X, keep, 4, 200, 1e-9)
+    f2 = scf.local_forces() + np.asarray(H.nonlocal_energy_force(X, occ, 3)[1]).reshape(3, 3)
+    f2 += qsb.ewald(p, [6.0, 1.0, 1.0], (L, L, L))[1]
+    np.testing.assert_allclose(f2, f, rtol=0, atol=1e-6)
+    b1, b2 = np.linalg.norm(p[1] - p[0]), np.linalg.norm(p[2] - p[0])
+    assert abs(b1 - b2) < 1e-2, (b1, b2)
+    assert qsb.device_status() == 0

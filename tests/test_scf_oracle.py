@@ -109,3 +109,50 @@ def test_local_forces_are_minus_the_local_energy_gradient():
             fd[at, k] = -(e1 - e2) / (2 * d)
     assert np.abs(f).max() > 1e-3
     np.testing.assert_allclose(f, fd, rtol=0, atol=1e-7 * np.abs(f).max())
+
+
+def test_ewald_is_independent_of_the_splitting_and_its_forces_are_exact():
+    """The Ewald energy does not depend on the splitting alpha (1e-10
+    relative); the forces equal central differences of the energy (delta 1e-4,
+    1e-7 relative); the NaCl-like check: a rocksalt cell's energy per ion pair
+    gives the Madelung constant 1.7475646 (1e-7)."""
+    rng = np.random.default_rng(2)
+    cell = (7.0, 8.0, 9.0)
+    pos = rng.uniform(0, 7, (3, 3))
+    Z = np.array([6.0, 1.0, 1.0])
+    e1, f1 = S.ewald(pos, Z, cell, alpha=0.5)
+    e2, f2 = S.ewald(pos, Z, cell, alpha=0.9)
+    assert abs(e1 - e2) < 1e-10 * abs(e1)
+    np.testing.assert_allclose(f1, f2, rtol=0, atol=1e-9 * np.abs(f1).max())
+    d = 1e-4
+    for a in range(3):
+        for k in range(3):
+            p1, p2 = pos.copy(), pos.copy()
+            p1[a, k] += d
+            p2[a, k] -= d
+            fd = -(S.ewald(p1, Z, cell)[0] - S.ewald(p2, Z, cell)[0]) / (2 * d)
+            assert abs(fd - f1[a, k]) < 1e-7 * np.abs(f1).max()
+    # rocksalt: conventional cell of edge 2 (nearest neighbour 1), 4 Na+ and 4 Cl-
+    fcc = np.array([[0, 0, 0], [0, 1, 1], [1, 0, 1], [1, 1, 0]], float)
+    pos = np.vstack([fcc, fcc + np.array([1.0, 0, 0])])
+    Z = np.array([1.0] * 4 + [-1.0] * 4)
+    e, _ = S.ewald(pos, Z, (2.0, 2.0, 2.0), alpha=2.0)
+    assert abs(-e / 4 - 1.74756459463) < 1e-7
+
+
+def test_library_ewald_matches_the_oracle():
+    """qsb_ewald (host code in the C-ABI library) against the oracle's Ewald sum:
+    energy 1e-12 relative, forces 1e-10 of the largest; the rocksalt Madelung
+    constant to 1e-9."""
+    import qsb
+    rng = np.random.default_rng(5)
+    for cell, Z in (((7.0, 8.0, 9.0), [6.0, 1.0, 1.0]), ((20.0, 20.0, 20.0), [6.0, 1.0, 1.0]),
+                    ((12.0, 12.0, 12.0), [6.0] * 16)):
+        pos = rng.uniform(0, min(cell), (len(Z), 3))
+        e, f = qsb.ewald(pos, Z, cell)
+        eo, fo = S.ewald(pos, np.array(Z), cell)
+        assert abs(e - eo) <= 1e-12 * abs(eo)
+        np.testing.assert_allclose(f, fo, rtol=0, atol=1e-10 * np.abs(fo).max())
+    fcc = np.array([[0, 0, 0], [0, 1, 1], [1, 0, 1], [1, 1, 0]], float)
+    e, _ = qsb.ewald(np.vstack([fcc, fcc + np.array([1.0, 0, 0])]), [1.0] * 4 + [-1.0] * 4, (2.0, 2.0, 2.0))
+    assert abs(-e / 4 - 1.74756459463) < 1e-9
