@@ -381,14 +381,19 @@ def scf_positions(reps, jitter, seed):
     return pos
 
 
-def scf_section(name, tol_ref=1e-8, max_steps=None):
+def scf_section(name, tol_ref=1e-8, max_steps=None, rho_tol=0.0):
     """SCF wall time to 1e-6 Ha / atom, FP64 drop-in vs mixed precision, from one
     dV-orthonormal seeded start with the same mixer.  Both runs continue to
     |dE| < tol_ref per atom (or the step cap); the FP64 run's final energy is
     the reference E*.  Time to tolerance = summed wall seconds of the steps up
     to the first step after which |E - E*| / atom stays below 1e-6 (steps timed
     by the driver's host clock; each step ends with its energy on the host).
-    Also reported: the stopping-rule point |dE| / atom < 1e-6 of each run."""
+    Also reported: the stopping-rule point |dE| / atom < 1e-6 of each run, and
+    at both end points the forces on every atom (local + nonlocal + Ewald)
+    and the occupied Rayleigh quotients.  rho_tol > 0 also requires
+    int |rho_out - rho_in| / N_e < rho_tol of both runs, so that the end
+    points differ by the precision, not by where the stopping rule left each
+    run."""
     import torch
     import qsb
     cfg = SCF_CONFIGS[name]
@@ -408,13 +413,15 @@ def scf_section(name, tol_ref=1e-8, max_steps=None):
     del psi
     out = {"config": name, "atoms": na, "grid": [n, n, n], "bands": nb, "electrons": n_el,
            "lobpcg_iterations_per_step": 4, "tolerance_ha_per_atom": 1e-6, "reference_tolerance_ha_per_atom": tol_ref,
-           "step_cap": cap, "mixing": "Kerker q0 0.8 A 0.5 + DIIS depth 6", "smearing_ha": 0.01}
-    runs = {}
+           "step_cap": cap, "density_residual_tolerance": rho_tol,
+           "mixing": "Kerker q0 0.8 A 0.5 + DIIS depth 6", "smearing_ha": 0.01}
+    runs, forces, rq = {}, {}, {}
     for prec in ("fp64", "mixed"):
         es = qsb.EigenSolver(N, nb, False, prec)
         scf = qsb.SCF(H, es, nb, n_el)
         scf.set_gth_local(pos, [0] * na, [GTH_LOCAL["zion"]], [GTH_LOCAL["rloc"]], [GTH_LOCAL["c1"]],
                           [GTH_LOCAL["c2"]])
+        scf.set_density_tolerance(rho_tol)
         X = X0.clone()
         keep = torch.zeros_like(X)
         scf.run(X, keep, 4, 1, 1e-6)           # one step: sizes the solver's workspaces
@@ -422,6 +429,17 @@ def scf_section(name, tol_ref=1e-8, max_steps=None):
         keep.zero_()
         torch.cuda.synchronize()
         e, ev, occ = scf.run(X, keep, 4, cap, tol_ref)
+        # adjoint forces on every atom at the end point, local + nonlocal
+        # device-timed, + Ewald (host)
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0.record()
+        f = scf.local_forces() + np.asarray(H.nonlocal_energy_force(X, occ, na)[1]).reshape(na, 3)
+        t1.record()
+        torch.cuda.synchronize()
+        f = f + qsb.ewald(pos, [GTH_LOCAL["zion"]] * na, [A_CELL * cfg["reps"]] * 3)[1]
+        forces[prec] = (f, t0.elapsed_time(t1))
+        rq[prec] = (ev, occ)
         runs[prec] = (e, scf.step_seconds())
         scf.close()
         es.close()
@@ -436,7 +454,7 @@ def scf_section(name, tol_ref=1e-8, max_steps=None):
         de = np.abs(np.diff(e)) / na
         stop = np.nonzero(de < 1e-6)[0]
         ks = int(stop[0]) + 1 if len(stop) else None          # stopping rule |dE| / atom < 1e-6
-        out[prec] = {"steps_run": len(e), "seconds_run": float(np.sum(t)),
+        out[prec] = {"steps_run": len(e), "stopped_before_cap": len(e) < cap, "seconds_run": float(np.sum(t)),
                      "steps_to_tolerance": k + 1 if hit else None,
                      "seconds_to_tolerance": float(np.sum(t[:k + 1])) if hit else None,
                      "final_error_ha_per_atom": float(err[-1]),
@@ -446,8 +464,16 @@ def scf_section(name, tol_ref=1e-8, max_steps=None):
                      "final_energy_ha": float(e[-1])}
     if out["fp64"]["seconds_to_tolerance"] and out["mixed"]["seconds_to_tolerance"]:
         out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds_to_tolerance"] / out["mixed"]["seconds_to_tolerance"]
+    occupied = rq["fp64"][1] > 1e-6
+    out["mixed_vs_fp64_end_point"] = {
+        "max_force_error_ha_per_bohr": float(np.abs(forces["mixed"][0] - forces["fp64"][0]).max()),
+        "max_force_ha_per_bohr": float(np.abs(forces["fp64"][0]).max()),
+        "max_occupied_eigenvalue_error_ha": float(np.abs(rq["mixed"][0] - rq["fp64"][0])[occupied].max()),
+        "force_ms": {k: v[1] for k, v in forces.items()}}
     out["note"] = ("E excludes the constant ion-ion term; E* = FP64 run's final energy; the mixed run's "
-                   "final_error_ha_per_atom is its error against it (bar 1e-6)")
+                   "final_error_ha_per_atom is its error against it (bar 1e-6); end-point errors compare "
+                   "the two runs' end points: forces local + nonlocal + Ewald on every atom, Rayleigh "
+                   "quotients of the bands with occupation > 1e-6")
     H.close()
     return out
 
@@ -464,6 +490,11 @@ def main():
     ap.add_argument("--no-scf", action="store_true")
     ap.add_argument("--scf-config", default="c2", choices=sorted(SCF_CONFIGS),
                     help="SCF workload: c2 (16 atoms, 96^3, 128 bands; default) or c3 (54 atoms, 144^3, 384 bands)")
+    ap.add_argument("--scf-tol-ref", type=float, default=1e-8,
+                    help="|dE| / atom both SCF runs continue to (the FP64 end point is E*)")
+    ap.add_argument("--scf-rho-tol", type=float, default=0.0,
+                    help="also require int |rho_out - rho_in| / N_e below this in both SCF runs (0: off)")
+    ap.add_argument("--scf-max-steps", type=int, default=None, help="SCF step cap (default 100 for c2, 80 for c3)")
     ap.add_argument("--bands", type=int, default=NB,
                     help="bands per GPU (default 128, the benchmark workload; smaller only for profiler captures)")
     args = ap.parse_args()
@@ -561,7 +592,7 @@ def main():
     # ---- whole SCF to 1e-6 Ha/atom: FP64 drop-in vs mixed precision (one system, N = 1 only)
     scf = None
     if not args.no_scf and world == 1:
-        scf = scf_section(args.scf_config)
+        scf = scf_section(args.scf_config, args.scf_tol_ref, args.scf_max_steps, args.scf_rho_tol)
     clk = clocks.stop()
 
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist, "cuda")
