@@ -9,8 +9,9 @@ psi ~ U[-0.5, 0.5] (seed 2) and a seeded synthetic local potential.
 
 value  = algorithmic H.psi bytes / device time (GB/s), all ranks, inputs resident in HBM;
          algorithmic bytes per apply = nb*N*(8 read + 8 write) + 8*N (V) + projector tables.
-e2e    = the same bytes / time of the public-API call with pinned HOST psi in and H.psi out
-         (host->device and device->host copies inside the timed region).
+e2e    = the same bytes / time of the public-API call on pinned HOST psi in and H.psi out
+         (qsb_ham_apply_host: host->device and device->host copies inside the timed region,
+         band chunks pipelined so that both copy directions and the apply overlap).
 N > 1  : each rank applies H to its own 128-band slice of a 128*N-band set (band
          decomposition, no data-path collective): weak scaling.
 --impl reference: the reference's own CPU operators (oracle/_ref, compiled from the
@@ -567,18 +568,14 @@ def main():
     # ---- end to end through the public API with host buffers -------------------
     e2e_steps = max(3, min(args.steps, 10))
     for _ in range(2):
-        psi.copy_(psi_host, non_blocking=True)
-        H.apply(psi, hpsi)
-        hpsi_host.copy_(hpsi, non_blocking=True)
+        H.apply_host(psi_host, hpsi_host)
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     for _ in range(e2e_steps):
-        psi.copy_(psi_host, non_blocking=True)
-        H.apply(psi, hpsi)
-        hpsi_host.copy_(hpsi, non_blocking=True)
+        H.apply_host(psi_host, hpsi_host)      # qsb_ham_apply_host: chunked, copies both ways overlapped
     f1.record(stream)
     torch.cuda.synchronize()
     barrier()

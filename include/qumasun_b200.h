@@ -132,6 +132,21 @@ QSB_API qsb_status qsb_ham_apply(qsb_ham* ham, qsb_dtype dtype, int is_complex, 
                          const void* psi_dev, void* hpsi_dev,
                          double gx, double gy, double gz, void* stream);
 
+/* The same H psi for bundles in HOST memory, the call shape of the reference's
+ * CPU build of mHamiltonianMatrix_ddm (source/qumasun_base1.matrix.h:263-291,
+ * psi and hpsi in host arrays): the bands go through the device in chunks of
+ * chunk_bands (0: nb / 16 rounded up), the host-to-device copy of the next
+ * chunk, the apply of this one (on `stream`) and the device-to-host copy of the
+ * previous one overlapping (two device staging slots of 2 chunks each, kept in
+ * the context and grown with cudaMalloc; two copy streams of the context).
+ * Asynchronous like cudaMemcpyAsync: hpsi_host is complete once `stream` has
+ * reached this point.  Page-locked host buffers (cudaHostAlloc /
+ * cudaHostRegister) let the copies overlap; pageable ones work but serialize.
+ * Calls on one context must not overlap (they share the staging slots). */
+QSB_API qsb_status qsb_ham_apply_host(qsb_ham* ham, qsb_dtype dtype, int is_complex, int nb,
+                                      const void* psi_host, void* hpsi_host,
+                                      double gx, double gy, double gz, int chunk_bands, void* stream);
+
 /* hpsi += V_NL psi.  Replaces PseudoPotNonlocal_SvF2_kpoint::ProjectionPP_bundle
  * (source/PseudoPotNonlocal_SvF2_kpoint.h:4239-4247, CPU :3911-4046, GPU :4053-4236). */
 QSB_API qsb_status qsb_ham_nonlocal_apply(qsb_ham* ham, qsb_dtype dtype, int is_complex, int nb,

@@ -174,6 +174,11 @@ qsb_status qsb_ham_destroy(qsb_ham* h) {
     if (h->V64) cudaFree(h->V64);
     if (h->V32) cudaFree(h->V32);
     if (h->ws) cudaFree(h->ws);
+    if (h->stage) cudaFree(h->stage);
+    for (cudaEvent_t e : h->pev)
+        if (e) cudaEventDestroy(e);
+    if (h->up) cudaStreamDestroy(h->up);
+    if (h->down) cudaStreamDestroy(h->down);
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : h->ev_rec) cudaEventDestroy(e);
     nl_free(h->nl);
@@ -348,6 +353,64 @@ qsb_status qsb_ham_apply(qsb_ham* h, qsb_dtype dtype, int is_complex, int nb, co
         h->launches += 1;
     }
     if (h->timing) QSB_TRY(timing_event(h, s));
+    return QSB_OK;
+}
+
+// H psi of host bundles: band chunks go through two device staging slots, the
+// host-to-device copy of chunk k + 1 (stream up), the apply of chunk k (the
+// caller's stream) and the device-to-host copy of chunk k - 1 (stream down)
+// overlapping, so that both copy directions of the host link run at once.
+qsb_status qsb_ham_apply_host(qsb_ham* h, qsb_dtype dtype, int is_complex, int nb, const void* psi_host,
+                              void* hpsi_host, double gx, double gy, double gz, int chunk_bands, void* stream) {
+    QSB_TRY(check_apply(h, dtype, nb, psi_host, hpsi_host));
+    if (!h->V64) return fail(QSB_ERR_STATE, "ham_apply_host: potential not set");
+    if (chunk_bands < 0) return fail(QSB_ERR_INVALID, "ham_apply_host: chunk_bands must be >= 0");
+    if (nb == 0) return QSB_OK;
+    const int chunk = std::min(nb, chunk_bands > 0 ? chunk_bands : std::max(1, (nb + 15) / 16));
+    const size_t band_bytes = (is_complex ? 2 : 1) * h->N * (dtype == QSB_F64 ? 8 : 4);
+    const size_t slot = (size_t)chunk * band_bytes;      // one psi or hpsi chunk
+    if (h->stage_bytes < 4 * slot) {
+        if (h->stage) QSB_CUDA_TRY(cudaFree(h->stage));
+        h->stage = nullptr;
+        h->stage_bytes = 0;
+        QSB_CUDA_TRY(cudaMalloc(&h->stage, 4 * slot));
+        h->stage_bytes = 4 * slot;
+    }
+    if (!h->up) QSB_CUDA_TRY(cudaStreamCreateWithFlags(&h->up, cudaStreamNonBlocking));
+    if (!h->down) QSB_CUDA_TRY(cudaStreamCreateWithFlags(&h->down, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : h->pev)
+        if (!e) QSB_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t start = h->pev[0], *in_ready = h->pev + 1, *done = h->pev + 3, *out_free = h->pev + 5;
+    char* d_in[2] = {(char*)h->stage, (char*)h->stage + slot};
+    char* d_out[2] = {(char*)h->stage + 2 * slot, (char*)h->stage + 3 * slot};
+    const char* src = (const char*)psi_host;
+    char* dst = (char*)hpsi_host;
+    // the staging slots are free once everything before this call on the caller's stream is done
+    QSB_CUDA_TRY(cudaEventRecord(start, s));
+    QSB_CUDA_TRY(cudaStreamWaitEvent(h->up, start, 0));
+    QSB_CUDA_TRY(cudaStreamWaitEvent(h->down, start, 0));
+    const int n_chunks = (nb + chunk - 1) / chunk;
+    for (int k = 0; k < n_chunks; ++k) {
+        const int j = k & 1;
+        const int b0 = k * chunk, nbk = std::min(chunk, nb - b0);
+        const size_t bytes = (size_t)nbk * band_bytes, off = (size_t)b0 * band_bytes;
+        if (k >= 2) QSB_CUDA_TRY(cudaStreamWaitEvent(h->up, done[j], 0));        // apply k - 2 read slot j
+        QSB_CUDA_TRY(cudaMemcpyAsync(d_in[j], src + off, bytes, cudaMemcpyHostToDevice, h->up));
+        QSB_CUDA_TRY(cudaEventRecord(in_ready[j], h->up));
+        QSB_CUDA_TRY(cudaStreamWaitEvent(s, in_ready[j], 0));
+        if (k >= 2) QSB_CUDA_TRY(cudaStreamWaitEvent(s, out_free[j], 0));        // copy-out k - 2 left slot j
+        QSB_TRY(qsb_ham_apply(h, dtype, is_complex, nbk, d_in[j], d_out[j], gx, gy, gz, s));
+        QSB_CUDA_TRY(cudaEventRecord(done[j], s));
+        QSB_CUDA_TRY(cudaStreamWaitEvent(h->down, done[j], 0));
+        QSB_CUDA_TRY(cudaMemcpyAsync(dst + off, d_out[j], bytes, cudaMemcpyDeviceToHost, h->down));
+        QSB_CUDA_TRY(cudaEventRecord(out_free[j], h->down));
+    }
+    // the caller's stream sees the last copies out (and the copy streams' work ends there)
+    QSB_CUDA_TRY(cudaStreamWaitEvent(s, out_free[(n_chunks - 1) & 1], 0));
+    if (n_chunks > 1) QSB_CUDA_TRY(cudaStreamWaitEvent(s, out_free[n_chunks & 1], 0));
+    QSB_CUDA_TRY(cudaEventRecord(start, h->up));
+    QSB_CUDA_TRY(cudaStreamWaitEvent(s, start, 0));
     return QSB_OK;
 }
 

@@ -205,4 +205,10 @@ struct qsb_ham {
     std::vector<cudaEvent_t> ev_pool;      // free events
     std::vector<cudaEvent_t> ev_rec;       // recorded triples: start, after projection, after stencil
     int launches = 0;
+    // qsb_ham_apply_host: two device staging slots (psi chunk, hpsi chunk) and
+    // the copy streams / events of the pipeline (created on first use)
+    void* stage = nullptr;
+    size_t stage_bytes = 0;
+    cudaStream_t up = nullptr, down = nullptr;
+    cudaEvent_t pev[7] = {};               // start, in_ready[2], done[2], out_free[2]
 };

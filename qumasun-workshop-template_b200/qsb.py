@@ -228,6 +228,20 @@ class Hamiltonian:
                                  _c_d(g[0]), _c_d(g[1]), _c_d(g[2]), _stream_ptr(psi)))
         return hpsi
 
+    def apply_host(self, psi, hpsi, is_complex=False, g=(0.0, 0.0, 0.0), chunk_bands=0):
+        """hpsi = H psi for contiguous CPU tensors (pinned ones let the copies
+        overlap), chunked through the device on the current CUDA stream;
+        hpsi is complete once that stream is synchronized."""
+        torch = _torch()
+        if psi.is_cuda or hpsi.is_cuda or not (psi.is_contiguous() and hpsi.is_contiguous()):
+            raise ValueError("expected contiguous CPU tensors")
+        assert hpsi.dtype == psi.dtype and hpsi.numel() == psi.numel()
+        nb = self._nb(psi, is_complex)
+        _check(lib.qsb_ham_apply_host(self._h, _dtype_code(psi), int(is_complex), nb, _vp(psi.data_ptr()),
+                                      _vp(hpsi.data_ptr()), _c_d(g[0]), _c_d(g[1]), _c_d(g[2]), int(chunk_bands),
+                                      _vp(torch.cuda.current_stream().cuda_stream)))
+        return hpsi
+
     def nonlocal_apply(self, psi, hpsi, is_complex=False, g=(0.0, 0.0, 0.0)):
         """hpsi += V_NL psi."""
         nb = self._nb(psi, is_complex)

@@ -145,6 +145,33 @@ def test_hamiltonian_complex_vs_oracle(qsb, g):
     assert rel(host(hp), ref) < TOL64
 
 
+@pytest.mark.parametrize("cplx,nb,chunk,prec", [(False, 16, 0, "f64"), (False, 16, 3, "f64"), (False, 16, 16, "f64"),
+                                                (True, 3, 2, "f64"), (False, 5, 2, "f32")])
+def test_apply_host_matches_apply(qsb, cplx, nb, chunk, prec):
+    """qsb_ham_apply_host (pinned host bundles, chunked through the device with
+    the copies overlapping) gives the device apply's result (1e-15 relative: the
+    same kernels per band) and the oracle's (the H.psi bar); twice in a row,
+    so the second call reuses the staging slots; a ragged last chunk."""
+    import torch
+    grid = (32, 32, 32, 0.1875, 0.1875, 0.1875) if not cplx else (24, 20, 16, 0.25, 0.3, 0.375)
+    g = (0.3, -0.2, 0.7) if cplx else (0.0, 0.0, 0.0)
+    H, tab, V, psi = _setup(qsb, grid, nb, cplx, 23)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    ref = O.hamiltonian(grid, V, tab, psi, nb, cplx, g)
+    p = dev(psi, dt)
+    hp = torch.empty_like(p)
+    H.apply(p, hp, cplx, g)
+    d = host(hp)
+    ph = torch.from_numpy(np.ascontiguousarray(psi)).to(dt).pin_memory()
+    for it in range(2):
+        hh = torch.full_like(ph, float("nan")).pin_memory()
+        H.apply_host(ph, hh, cplx, g, chunk)
+        torch.cuda.synchronize()
+        out = hh.double().numpy()
+        assert rel(out, d) < 1e-15, it
+        assert rel(out, ref) < (TOL64 if prec == "f64" else TOL32), it
+
+
 @pytest.mark.parametrize("cplx", [False, True])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 def test_nonlocal_apply_and_project_vs_oracle(qsb, cplx, prec):
