@@ -82,14 +82,21 @@ nl_proj_kernel(const int* __restrict__ chunk_begin, const int* __restrict__ chun
     // UP points per thread per pass: their index and psi loads are all issued
     // before the first use, so UP x CB (x2 complex) gathers are in flight
     constexpr int UP = (WM <= 4 && !CPLX) ? 2 : 1;
+    // the grid indices of the next pass are loaded while this pass's psi
+    // gathers are in flight (one dependent load latency per pass, not two)
+    int idx_next[UP];
+#pragma unroll
+    for (int u = 0; u < UP; ++u) {
+        const int p = p0 + threadIdx.x + u * PROJ_THREADS;
+        idx_next[u] = p < p1 ? __ldg(pt_idx + p) : 0;
+    }
     for (int pb = p0 + threadIdx.x; pb < p1; pb += PROJ_THREADS * UP) {
         int idx[UP];
         bool live[UP];
 #pragma unroll
         for (int u = 0; u < UP; ++u) {
-            const int p = pb + u * PROJ_THREADS;
-            live[u] = p < p1;
-            idx[u] = live[u] ? __ldg(pt_idx + p) : 0;
+            live[u] = pb + u * PROJ_THREADS < p1;
+            idx[u] = idx_next[u];
         }
         double vals[UP][CPLX ? 2 * CB : CB];
 #pragma unroll
@@ -105,6 +112,11 @@ nl_proj_kernel(const int* __restrict__ chunk_begin, const int* __restrict__ chun
                     vals[u][j] = ok ? (double)__ldg(psi + (size_t)(band0 + j) * N + idx[u]) : 0.0;
                 }
             }
+#pragma unroll
+        for (int u = 0; u < UP; ++u) {
+            const int p = pb + PROJ_THREADS * UP + u * PROJ_THREADS;
+            idx_next[u] = p < p1 ? __ldg(pt_idx + p) : 0;
+        }
 #pragma unroll
         for (int u = 0; u < UP; ++u) {
             if (!live[u]) continue;
