@@ -62,8 +62,8 @@ inline int fold(int v, int n) {
 // projection: partial[chunk][w][col] = sum_{p in chunk} beta[p][w] * phi_col[idx_p]
 // phi = psi (real) or psi*exp(+i k.r) (complex; columns 2b = re, 2b+1 = im)
 // ---------------------------------------------------------------------------
-template <typename T, bool CPLX, int WM, int CB>
-__global__ void __launch_bounds__(PROJ_THREADS)
+template <typename T, bool CPLX, int WM, int CB, int UP, int MINB>
+__global__ void __launch_bounds__(PROJ_THREADS, MINB)
 nl_proj_kernel(const int* __restrict__ chunk_begin, const int* __restrict__ chunk_end,
                const int* __restrict__ pt_idx, const int* __restrict__ pt_xyz, const T* __restrict__ pt_beta,
                int wmax, const T* __restrict__ psi, size_t N, int nb, double gx_dx, double gy_dy, double gz_dz,
@@ -80,8 +80,9 @@ nl_proj_kernel(const int* __restrict__ chunk_begin, const int* __restrict__ chun
     for (int i = 0; i < NV; ++i) acc[i] = 0.0;
 
     // UP points per thread per pass: their index and psi loads are all issued
-    // before the first use, so UP x CB (x2 complex) gathers are in flight
-    constexpr int UP = (WM <= 4 && !CPLX) ? 2 : 1;
+    // before the first use, so UP x CB (x2 complex) gathers are in flight.
+    // Thread t takes the points t + 256 m in increasing m whatever UP is, so
+    // the summation order does not depend on UP.
     // the grid indices of the next pass are loaded while this pass's psi
     // gathers are in flight (one dependent load latency per pass, not two)
     int idx_next[UP];
@@ -432,15 +433,21 @@ nl_apply2_kernel(const int* __restrict__ cov_grid, int n_cov, const int* __restr
 template <typename T, bool CPLX, int WM>
 void launch_proj(const NLDevice& d, int table, int nb, const void* psi, size_t N, double gx_dx, double gy_dy,
                  double gz_dz, double* partial, int ncol, cudaStream_t s) {
-    constexpr int CB = CPLX ? 4 : 8;
-    dim3 grid(d.n_chunks, (nb + CB - 1) / CB);
     const size_t toff = table < 0 ? 0 : (size_t)table * d.n_points * d.wmax;
     const T* beta = table < 0 ? (std::is_same<T, double>::value ? (const T*)d.pt_beta64 : (const T*)d.pt_beta32)
                               : (std::is_same<T, double>::value ? (const T*)d.pt_dbeta64 + toff
                                                                 : (const T*)d.pt_dbeta32 + toff);
-    nl_proj_kernel<T, CPLX, WM, CB><<<grid, PROJ_THREADS, 0, s>>>(d.chunk_begin, d.chunk_end, d.pt_idx, d.pt_xyz, beta,
-                                                                  d.wmax, (const T*)psi, N, nb, gx_dx, gy_dy, gz_dz,
-                                                                  partial, ncol);
+    // up to 4 projectors: 8 real bands (4 complex) x 2 (1) points per thread
+    // in at most 128 registers, two CTAs per SM (at 136 registers, one CTA:
+    // 0.50 ms instead of 0.34 at the 96^3 x 128-band workload; 4 bands x 3
+    // points at 80 registers and three CTAs: 0.35 ms)
+    constexpr int CB = CPLX ? 4 : 8;
+    constexpr int UP = (WM <= 4 && !CPLX) ? 2 : 1;
+    constexpr int MINB = WM <= 4 ? 2 : 1;
+    dim3 grid(d.n_chunks, (nb + CB - 1) / CB);
+    nl_proj_kernel<T, CPLX, WM, CB, UP, MINB><<<grid, PROJ_THREADS, 0, s>>>(d.chunk_begin, d.chunk_end, d.pt_idx, d.pt_xyz,
+                                                                        beta, d.wmax, (const T*)psi, N, nb, gx_dx,
+                                                                        gy_dy, gz_dz, partial, ncol);
 }
 
 template <typename T, bool CPLX>
