@@ -479,6 +479,35 @@ def scf_section(name, tol_ref=1e-8, max_steps=None, rho_tol=0.0):
     return out
 
 
+def fft_kinetic_section(H, psi, hpsi, stream, alg_bytes, steps=20):
+    """Device time of one H.psi with the FFT kinetic (qsb_ham_set_kinetic(1):
+    batched cuFFT D2Z / Z2D in 32-band chunks, |G|^2 / 2, 1/N + V psi fused,
+    the same nonlocal kernels) on the bench workload; the same algorithmic bytes
+    as the FD8 apply for comparison (an FFT re-reads each band several times)."""
+    import torch
+    H.set_kinetic(1)
+    try:
+        for _ in range(3):
+            H.apply(psi, hpsi)
+        torch.cuda.synchronize()
+        H.get_timing()
+        H.set_timing(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            H.apply(psi, hpsi)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        H.set_timing(False)
+        ms = e0.elapsed_time(e1) / steps
+        pm, km, em, applies, _ = H.get_timing()
+    finally:
+        H.set_kinetic(0)
+    return {"ms_per_apply": ms, "algorithmic_gbs": alg_bytes / ms / 1e6,
+            "breakdown_ms": {"nonlocal_projection": pm / applies, "fft_kinetic_plus_v": km / applies,
+                             "nonlocal_expansion": em / applies}}
+
+
 def main():
     global NB
     ap = argparse.ArgumentParser()
@@ -581,6 +610,9 @@ def main():
     barrier()
     e2e_ms = f0.elapsed_time(f1) / e2e_steps
 
+    # ---- the same H.psi with the FFT kinetic (the reference's default operator) --
+    fft = fft_kinetic_section(H, psi, hpsi, stream, algorithmic_bytes(NB, N, n_pts, 4))
+
     # ---- block LOBPCG on the same H: FP64 drop-in vs mixed precision ----------
     lob = None
     gram = gram_section(N, 3 * NB, stream)
@@ -626,6 +658,7 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": NB * N * 8, "d2h_bytes_per_step": NB * N * 8,
                 "ms_per_step": e2e_ms},
         "gpu_launches": launches,
+        "fft_kinetic": fft,
         "lobpcg": lob,
         "scf": scf,
         "gram": gram,

@@ -132,6 +132,19 @@ QSB_API qsb_status qsb_ham_apply(qsb_ham* ham, qsb_dtype dtype, int is_complex, 
                          const void* psi_dev, void* hpsi_dev,
                          double gx, double gy, double gz, void* stream);
 
+/* Kinetic operator of qsb_ham_apply (and of everything built on it: the
+ * eigensolvers given this context, the SCF driver, qsb_ham_apply_host):
+ *   0  FD8 Laplacian (default; mKineticMatrixAdd_ddm_kpint, the stencil path);
+ *   1  FFT kinetic, the reference's default (m_algorithm_Laplacian = 1,
+ *      source/qumasun_base1.h:243; mHamiltonianMatrix_ddm_bundle,
+ *      source/qumasun_base1.matrix.h:171-228): forward 3-D FFT of each band,
+ *      times |G + k|^2 / 2 with the Nyquist index of an even grid taken as
+ *      +n/2 (OperateKineticInKspace_bundle :96-123), inverse FFT, times 1/N,
+ *      + V psi, + the nonlocal part.  Batched cuFFT plans and a spectrum
+ *      buffer for 32 bands are made on first use and kept in the context.
+ *      FP64 and FP32 (the mixed solver's operator). */
+QSB_API qsb_status qsb_ham_set_kinetic(qsb_ham* ham, int algorithm);
+
 /* The same H psi for bundles in HOST memory, the call shape of the reference's
  * CPU build of mHamiltonianMatrix_ddm (source/qumasun_base1.matrix.h:263-291,
  * psi and hpsi in host arrays): the bands go through the device in chunks of

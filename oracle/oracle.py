@@ -310,6 +310,10 @@ def laplacian_kpoint8th(nx, ny, nz, out, src, coef, dx, dy, dz, g):
 
 def hamiltonian(grid, V, tables, psi, nb, is_complex=False, g=(0.0, 0.0, 0.0)):
     """H psi (restatement of mHamiltonianMatrix_ddm), FP64."""
+    return _hamiltonian_fd8(grid, V, tables, psi, nb, is_complex, g)
+
+
+def _hamiltonian_fd8(grid, V, tables, psi, nb, is_complex=False, g=(0.0, 0.0, 0.0)):
     lib = oracle_lib()
     nx, ny, nz, dx, dy, dz = grid
     npts, widths, coords, beta, energy = tables
@@ -458,8 +462,10 @@ def ref_lobpcg_d(grid, V, cube, X, keep, n, iter_max, eigen_values, is_first_tim
                        _d(eigen_values), _d(X), _d(keep), _d(work), int(is_first_time))
 
 
-def dense_eigenvalues(grid, V, tables, k, is_complex=False, g=(0.0, 0.0, 0.0)):
-    """Lowest k eigenvalues of H built column by column with the C restatement (small grids only)."""
+def dense_eigenvalues(grid, V, tables, k, is_complex=False, g=(0.0, 0.0, 0.0), fft=False):
+    """Lowest k eigenvalues of H built column by column with the C restatement
+    (fft: with the FFT kinetic of hamiltonian_fft; small grids only)."""
+    hamiltonian = hamiltonian_fft if fft else _hamiltonian_fd8
     nx, ny, nz = grid[:3]
     N = nx * ny * nz
     if is_complex:
@@ -480,3 +486,45 @@ def dense_eigenvalues(grid, V, tables, k, is_complex=False, g=(0.0, 0.0, 0.0)):
             M[:, j] = hamiltonian(grid, V, tables, e, 1)[0]
         M = 0.5 * (M + M.T)
     return np.linalg.eigvalsh(M)[:k]
+
+
+def kinetic_fft(grid, psi, nb, is_complex=False, g=(0.0, 0.0, 0.0)):
+    """-1/2 (grad + i k)^2 psi by FFT, FP64: the FFT kinetic of the reference's
+    default Hamiltonian (mHamiltonianMatrix_ddm_bundle, algorithm 1,
+    source/qumasun_base1.matrix.h:171-228, multiplier of
+    OperateKineticInKspace_bundle :96-123): forward 3-D FFT of each band,
+    times |G + k|^2 / 2 with G_d = 2 pi m / (n_d h_d) and m folded as
+    (2m > n ? m - n : m) -- the Nyquist index of an even grid stays +n/2 --
+    inverse FFT, times 1/N.  Real bands (k = 0): the same operator on psi as a
+    complex field with zero imaginary part, real part returned."""
+    nx, ny, nz, dx, dy, dz = grid
+    psi = np.asarray(psi, np.float64)
+
+    def axis(n, h, gk):
+        m = np.arange(n)
+        m = np.where(2 * m > n, m - n, m)
+        return 2.0 * math.pi * m / (n * h) + gk
+
+    kx, ky, kz = axis(nx, dx, g[0]), axis(ny, dy, g[1]), axis(nz, dz, g[2])
+    mult = 0.5 * (kz[:, None, None] ** 2 + ky[None, :, None] ** 2 + kx[None, None, :] ** 2)
+    if is_complex:
+        f = psi.reshape(nb, 2, nz, ny, nx)
+        c = f[:, 0] + 1j * f[:, 1]
+    else:
+        c = psi.reshape(nb, nz, ny, nx).astype(np.complex128)
+    out = np.fft.ifftn(np.fft.fftn(c, axes=(-3, -2, -1)) * mult, axes=(-3, -2, -1))
+    if is_complex:
+        return np.stack([out.real, out.imag], axis=1).reshape(psi.shape)
+    return out.real.reshape(psi.shape)
+
+
+def hamiltonian_fft(grid, V, tables, psi, nb, is_complex=False, g=(0.0, 0.0, 0.0)):
+    """H psi with the FFT kinetic (mHamiltonianMatrix_ddm_bundle, algorithm 1):
+    FFT kinetic + V psi (mPotentialMatrixAdd_ddm_bundle) + nonlocal
+    (ProjectionPP_bundle), FP64."""
+    nx, ny, nz = grid[:3]
+    N = nx * ny * nz
+    psi = np.ascontiguousarray(psi, np.float64)
+    hp = kinetic_fft(grid, psi, nb, is_complex, g)
+    hp = hp + (psi.reshape(-1, N) * np.asarray(V, np.float64)[None, :]).reshape(psi.shape)
+    return nonlocal_apply(grid, tables, psi, nb, is_complex, g, np.ascontiguousarray(hp))

@@ -175,6 +175,7 @@ qsb_status qsb_ham_destroy(qsb_ham* h) {
     if (h->V32) cudaFree(h->V32);
     if (h->ws) cudaFree(h->ws);
     if (h->stage) cudaFree(h->stage);
+    kinetic_fft_free(h);
     for (cudaEvent_t e : h->pev)
         if (e) cudaEventDestroy(e);
     if (h->up) cudaStreamDestroy(h->up);
@@ -341,11 +342,16 @@ qsb_status qsb_ham_apply(qsb_ham* h, qsb_dtype dtype, int is_complex, int nb, co
         h->launches += 2;
     }
     if (h->timing) QSB_TRY(timing_event(h, s));
-    // 2) hpsi = V psi - 1/2 FD8(psi)   (mPotentialMatrix_ddm + mKineticMatrixAdd_ddm_kpint)
-    StencilLaunch L{h->nx, h->ny, h->nz, nb, is_complex ? 1 : 0, 1, psi_dev, hpsi_dev,
-                    dtype == QSB_F64 ? (const void*)h->V64 : (const void*)h->V32};
-    QSB_TRY(launch_stencil(dtype, L, make_fd8_coef(-0.5, h->dx, h->dy, h->dz, gx, gy, gz), s));
-    h->launches += 1;
+    if (h->kinetic == 1) {
+        // 2') hpsi = V psi + FFT kinetic   (mHamiltonianMatrix_ddm_bundle, algorithm 1)
+        QSB_TRY(kinetic_fft_apply(h, dtype, is_complex, nb, psi_dev, hpsi_dev, gx, gy, gz, s, &h->launches));
+    } else {
+        // 2) hpsi = V psi - 1/2 FD8(psi)   (mPotentialMatrix_ddm + mKineticMatrixAdd_ddm_kpint)
+        StencilLaunch L{h->nx, h->ny, h->nz, nb, is_complex ? 1 : 0, 1, psi_dev, hpsi_dev,
+                        dtype == QSB_F64 ? (const void*)h->V64 : (const void*)h->V32};
+        QSB_TRY(launch_stencil(dtype, L, make_fd8_coef(-0.5, h->dx, h->dy, h->dz, gx, gy, gz), s));
+        h->launches += 1;
+    }
     if (h->timing) QSB_TRY(timing_event(h, s));
     // 3) hpsi += sum |beta> E <beta|psi>   (ProjectionPP_bundle expansion, pull form)
     if (has_nl) {
@@ -411,6 +417,13 @@ qsb_status qsb_ham_apply_host(qsb_ham* h, qsb_dtype dtype, int is_complex, int n
     if (n_chunks > 1) QSB_CUDA_TRY(cudaStreamWaitEvent(s, out_free[n_chunks & 1], 0));
     QSB_CUDA_TRY(cudaEventRecord(start, h->up));
     QSB_CUDA_TRY(cudaStreamWaitEvent(s, start, 0));
+    return QSB_OK;
+}
+
+qsb_status qsb_ham_set_kinetic(qsb_ham* h, int algorithm) {
+    if (!h) return fail(QSB_ERR_INVALID, "set_kinetic: null context");
+    if (algorithm != 0 && algorithm != 1) return fail(QSB_ERR_INVALID, "set_kinetic: algorithm must be 0 (FD8) or 1 (FFT)");
+    h->kinetic = algorithm;
     return QSB_OK;
 }
 

@@ -211,4 +211,21 @@ struct qsb_ham {
     size_t stage_bytes = 0;
     cudaStream_t up = nullptr, down = nullptr;
     cudaEvent_t pev[7] = {};               // start, in_ready[2], done[2], out_free[2]
+    // kinetic operator of qsb_ham_apply: 0 FD8 stencil, 1 FFT (qsb_ham_set_kinetic)
+    int kinetic = 0;
+    struct FftPlan {
+        int dtype, cplx, batch;
+        int forward, backward;             // cufftHandle values
+    };
+    std::vector<FftPlan> fft_plans;        // by (dtype, complex, batch)
+    void* fft_buf = nullptr;               // spectra of one band chunk
+    size_t fft_buf_bytes = 0;
 };
+
+namespace qsb {
+// FFT kinetic term of qsb_ham_apply (kinetic_fft.cu): hpsi = -1/2 (grad + i g)^2 psi
+// + V psi ("=" semantics; the nonlocal part is added by the caller).
+qsb_status kinetic_fft_apply(qsb_ham* h, qsb_dtype dtype, int is_complex, int nb, const void* psi, void* hpsi,
+                             double gx, double gy, double gz, cudaStream_t s, int* launches);
+void kinetic_fft_free(qsb_ham* h);
+}  // namespace qsb

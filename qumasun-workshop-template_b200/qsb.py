@@ -228,6 +228,10 @@ class Hamiltonian:
                                  _c_d(g[0]), _c_d(g[1]), _c_d(g[2]), _stream_ptr(psi)))
         return hpsi
 
+    def set_kinetic(self, algorithm):
+        """0: FD8 Laplacian (default); 1: FFT kinetic (the reference's default operator)."""
+        _check(lib.qsb_ham_set_kinetic(self._h, int(algorithm)))
+
     def apply_host(self, psi, hpsi, is_complex=False, g=(0.0, 0.0, 0.0), chunk_bands=0):
         """hpsi = H psi for contiguous CPU tensors (pinned ones let the copies
         overlap), chunked through the device on the current CUDA stream;
