@@ -479,6 +479,29 @@ QSB_API qsb_status qsb_relax_lbfgs(qsb_scf* scf, int n_atoms, double* pos, const
  * when its energy is on the host): up to max values, *n = steps recorded. */
 QSB_API qsb_status qsb_scf_step_seconds(qsb_scf* scf, double* seconds, int max, int* n);
 
+/* ---------------------------------------------------------------------------
+ * Cube files (host code; no device work).  The reference's state and density
+ * exchange format: files written by qsb_cube_write are byte-identical to those
+ * of CubeWriter::SaveCube (source/cube_writer.h:27-90; title "Generated by
+ * QUMASUN", the same printf formats, values z fastest, 6 per line, each z row
+ * ending its line), and qsb_cube_read returns the values CubeReader3::LoadCube
+ * + GetMeshData (source/cube_reader3.h:38-124) return, in this library's grid
+ * layout (x fastest).  Where the reference reader silently stops on a short or
+ * malformed file, these return QSB_ERR_INVALID with the counts found.
+ *   axis[9]    the three box edge vectors (grid count x voxel vector), bohr
+ *   origin[3]  the volume origin, bohr
+ *   Z, pos     n_atoms atomic numbers and positions (3 per atom)
+ *   field      nx*ny*nz doubles, host memory, x fastest
+ * The comment is one line.  Rows are formatted / parsed by up to 16 host
+ * threads. */
+QSB_API qsb_status qsb_cube_write(const char* path, const char* comment, int nx, int ny, int nz,
+                                  const double* axis, const double* origin, int n_atoms, const int* Z,
+                                  const double* pos, const double* field);
+/* grid[3] out; axis, origin, n_atoms may be NULL. */
+QSB_API qsb_status qsb_cube_read_header(const char* path, int* grid, double* axis, double* origin, int* n_atoms);
+/* field (grid product doubles) out; Z (n_atoms ints) and pos (3 n_atoms) may be NULL. */
+QSB_API qsb_status qsb_cube_read(const char* path, double* field, int* Z, double* pos);
+
 #ifdef __cplusplus
 }
 #endif

@@ -528,3 +528,27 @@ def hamiltonian_fft(grid, V, tables, psi, nb, is_complex=False, g=(0.0, 0.0, 0.0
     hp = kinetic_fft(grid, psi, nb, is_complex, g)
     hp = hp + (psi.reshape(-1, N) * np.asarray(V, np.float64)[None, :]).reshape(psi.shape)
     return nonlocal_apply(grid, tables, psi, nb, is_complex, g, np.ascontiguousarray(hp))
+
+
+def ref_cube_write(path, field, grid, axis, origin, Z, pos, comment=""):
+    """The reference's CubeWriter::SaveCube (cube_writer.h:27-90) through oracle/_ref."""
+    lib = ref_lib()
+    nx, ny, nz = grid
+    f = np.ascontiguousarray(field, np.float64).ravel()
+    z = np.ascontiguousarray(Z, np.int32).ravel()
+    p = np.ascontiguousarray(pos, np.float64).ravel()
+    ax = np.ascontiguousarray(axis, np.float64).ravel()
+    org = np.ascontiguousarray(origin, np.float64).ravel()
+    lib.qsref_cube_write(os.fsencode(path), comment.encode(), nx, ny, nz, _d(ax), _d(org), int(z.size),
+                         z.ctypes.data_as(_ip), _d(p), _d(f))
+
+
+def ref_cube_read(path):
+    """The reference's CubeReader3::LoadCube + GetMeshData (cube_reader3.h:38-124)."""
+    lib = ref_lib()
+    grid = np.zeros(3, np.int32)
+    ax, org = np.zeros(9), np.zeros(3)
+    lib.qsref_cube_read(os.fsencode(path), grid.ctypes.data_as(_ip), _d(ax), _d(org), None)
+    f = np.zeros(int(np.prod(grid)))
+    lib.qsref_cube_read(os.fsencode(path), grid.ctypes.data_as(_ip), _d(ax), _d(org), _d(f))
+    return f, {"grid": tuple(int(v) for v in grid), "axis": ax.reshape(3, 3), "origin": org}

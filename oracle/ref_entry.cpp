@@ -26,6 +26,8 @@
  *   qsref_lobpcg_z            LOBPCG::Eigen_z_multi_mpi     lobpcg_z_multi_mpi.h:1732-2852
  *   qsref_lda_pz              Calc_XC_LDA (Perdew-Zunger)   Vxc.h:43-75
  *   qsref_set_occupancy       SetOccupancy (Fermi-Dirac)    SetOccupancy.h:7-18
+ *   qsref_cube_write          CubeWriter::SaveCube          cube_writer.h:27-90
+ *   qsref_cube_read           CubeReader3::LoadCube + GetMeshData  cube_reader3.h:38-124
  *
  * The nonlocal class itself (projector construction from UPF via SvF) is not
  * compiled: the projector values are supplied by the caller on the block
@@ -66,6 +68,8 @@ inline int lapack_DSYGVX(double* A, double* B, double* w, double* Z, double* /*t
 #include "Vxc.h"
 #include "SetOccupancy.h"
 #endif
+#include "cube_reader3.h"
+#include "cube_writer.h"
 
 namespace {
 
@@ -470,6 +474,29 @@ void qsref_lda_pz(int n, const double* rho, double* exc, double* vxc) {
 /* Fermi-Dirac occupations at chemical potential mu; returns their sum. */
 double qsref_set_occupancy(double coef, double kbT, int n, const double* eig, double mu, double* occ) {
     return SetOccupancy(coef, kbT, n, eig, mu, occ);
+}
+
+/* axis: the three box edge vectors (grid_x * voxel_x, ...), as the frames hold them */
+int qsref_cube_write(const char* path, const char* comment, int nx, int ny, int nz, const double* axis,
+                     const double* org, int n_atoms, const int* Z, const double* pos, double* field) {
+    CubeWriter::Frame f{};
+    f.grid_x = nx; f.grid_y = ny; f.grid_z = nz;
+    for (int i = 0; i < 9; ++i) f.boxaxis[i] = axis[i];
+    for (int i = 0; i < 3; ++i) f.boxorg[i] = org[i];
+    std::snprintf(f.comment, sizeof(f.comment), "%s", comment);
+    std::vector<Nucleus> nuc(n_atoms);
+    for (int a = 0; a < n_atoms; ++a) nuc[a] = Nucleus{Z[a], pos[3 * a], pos[3 * a + 1], pos[3 * a + 2]};
+    return CubeWriter::SaveCube(path, f, n_atoms, nuc.data(), field);
+}
+
+/* grid[3] and axis[9], org[3] out; field (x fastest) out when not NULL */
+void qsref_cube_read(const char* path, int* grid, double* axis, double* org, double* field) {
+    CubeReader3 r;
+    const CubeReader3::Frame f = r.LoadCube(path);
+    grid[0] = f.grid_x; grid[1] = f.grid_y; grid[2] = f.grid_z;
+    for (int i = 0; i < 9; ++i) axis[i] = f.boxaxis[i];
+    for (int i = 0; i < 3; ++i) org[i] = f.boxorg[i];
+    if (field) r.GetMeshData(field);
 }
 
 } // extern "C"

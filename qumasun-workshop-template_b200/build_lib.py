@@ -2,7 +2,8 @@
 
     python qumasun-workshop-template_b200/build_lib.py
 
-compiles every csrc/*.cu with nvcc for sm_100a only and links one shared
+compiles every csrc/*.cu with nvcc for sm_100a only (csrc/*.cpp, host-only
+code, with the host compiler) and links one shared
 library next to this file.  The library exports exactly the C ABI declared in
 include/qumasun_b200.h.
 """
@@ -21,8 +22,13 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hid
          "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]
 
 
+CXX = os.environ.get("CXX", "g++")
+CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-pthread", "-I", os.path.join(ROOT, "include")]
+
+
 def sources():
-    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
+    """csrc/*.cu (device code, nvcc) and csrc/*.cpp (host-only code, the host compiler)."""
+    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
 
 
 def build(verbose=False, force=False):
@@ -37,7 +43,10 @@ def build(verbose=False, force=False):
         if (not force and os.path.exists(obj)
                 and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr_mtime)):
             continue
-        cmd = [NVCC] + ARCH + FLAGS + ["-c", src, "-o", obj]
+        if src.endswith(".cpp"):
+            cmd = [CXX] + CXXFLAGS + ["-c", src, "-o", obj]
+        else:
+            cmd = [NVCC] + ARCH + FLAGS + ["-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
@@ -45,7 +54,7 @@ def build(verbose=False, force=False):
             or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs)):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + [
             "-L/usr/local/cuda/lib64", "-lcublas", "-lcusolver", "-lcufft",
-            "-Xlinker", "-rpath,/usr/local/cuda/lib64"]
+            "-Xlinker", "-rpath,/usr/local/cuda/lib64", "-Xcompiler", "-pthread"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

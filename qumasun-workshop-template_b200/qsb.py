@@ -372,6 +372,37 @@ def density(X, occupations, N):
     return rho
 
 
+def cube_write(path, field, grid, axis, origin=(0.0, 0.0, 0.0), Z=(), pos=(), comment=""):
+    """Writes field (nx*ny*nz values, x fastest) as a cube file in the
+    reference's dialect (qsb_cube_write).  axis: the three box edge vectors."""
+    nx, ny, nz = (int(v) for v in grid)
+    f, f_p = _f64(np.asarray(field, np.float64).ravel())
+    assert f.size == nx * ny * nz
+    ax, ax_p = _f64(np.asarray(axis, np.float64).ravel())
+    org, org_p = _f64(np.asarray(origin, np.float64).ravel())
+    z, z_p = _i32(np.asarray(Z, np.int32).ravel())
+    p, p_p = _f64(np.asarray(pos, np.float64).ravel())
+    assert ax.size == 9 and org.size == 3 and p.size == 3 * z.size
+    _check(lib.qsb_cube_write(os.fsencode(path), comment.encode(), nx, ny, nz, ax_p, org_p, int(z.size),
+                              z_p if z.size else None, p_p if z.size else None, f_p))
+
+
+def cube_read(path):
+    """(field [nx*ny*nz], x fastest; dict with grid, axis [3, 3], origin, Z, pos [n, 3])."""
+    grid = (ctypes.c_int * 3)()
+    ax, ax_p = _f64(np.zeros(9))
+    org, org_p = _f64(np.zeros(3))
+    na = ctypes.c_int()
+    _check(lib.qsb_cube_read_header(os.fsencode(path), grid, ax_p, org_p, ctypes.byref(na)))
+    g = tuple(grid)
+    f, f_p = _f64(np.zeros(g[0] * g[1] * g[2]))
+    z, z_p = _i32(np.zeros(max(na.value, 1), np.int32))
+    p, p_p = _f64(np.zeros(3 * max(na.value, 1)))
+    _check(lib.qsb_cube_read(os.fsencode(path), f_p, z_p, p_p))
+    n = na.value
+    return f, {"grid": g, "axis": ax.reshape(3, 3), "origin": org, "Z": z[:n].copy(), "pos": p[:3 * n].reshape(n, 3)}
+
+
 def ewald(pos, charge, cell):
     """(energy, forces [n_atoms, 3]) of point charges in an orthorhombic cell
     with a neutralising background (qsb_ewald; host code)."""

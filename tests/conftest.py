@@ -22,3 +22,10 @@ def qsb():
         pytest.skip("no CUDA device")
     import qsb as mod
     return mod
+
+
+@pytest.fixture(scope="session")
+def qsb_host():
+    """The product binding for host-only entry points (no device needed)."""
+    import qsb as mod
+    return mod
