@@ -12,7 +12,9 @@
 // real plane (im == re + N) and bands of a bundle are consecutive.
 #pragma once
 
+#include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -87,11 +89,93 @@ public:
         check(qsb_ham_nonlocal_apply(h_, QSB_F64, 1, end_n - begin_n, p[begin_n].re, Hp[begin_n].re, gx, gy, gz,
                                      stream));
     }
+    // m_algorithm_Laplacian (source/qumasun_base1.h:243): 1 makes Apply the FFT
+    // kinetic of mHamiltonianMatrix_ddm_bundle (source/qumasun_base1.matrix.h:171-228),
+    // 0 the FD8 form of mHamiltonianMatrix_ddm
+    void SetKineticAlgorithm(int algorithm) { check(qsb_ham_set_kinetic(h_, algorithm)); }
+    // Apply on bundles in host memory (the reference's CPU build), chunked
+    // through the device; complete when `stream` is
+    template <class SoA>
+    void ApplyHost(SoA* Hp, const SoA* p, int num_bundle, double gx, double gy, double gz, void* stream = nullptr,
+                   int chunk_bands = 0) {
+        if (num_bundle <= 0) return;
+        if (Hp[0].im != Hp[0].re + N_ || p[0].im != p[0].re + N_)
+            throw std::invalid_argument("Hamiltonian::ApplyHost: im plane must follow re plane (WaveSet layout)");
+        check(qsb_ham_apply_host(h_, QSB_F64, 1, num_bundle, p[0].re, Hp[0].re, gx, gy, gz, chunk_bands, stream));
+    }
     qsb_ham* handle() const { return h_; }
 
 private:
     qsb_ham* h_ = nullptr;
     size_t N_;
+};
+
+// CubeWriter::SaveCube(filename, frame, num_nuclei, nuclei, field)
+// (source/cube_writer.h:27-90): the same Frame (box edge vectors in boxaxis),
+// any Nucleus type with Z, Rx, Ry, Rz; byte-identical files.  Returns 1 like
+// the reference; failures (unwritable path) throw instead of crashing.
+struct CubeWriter {
+    struct Frame {
+        int grid_x;
+        int grid_y;
+        int grid_z;
+        double boxaxis[9];
+        double boxorg[3];
+        char comment[256]{0};
+    };
+    template <class Nucleus>
+    static int SaveCube(const char* filename, const Frame& frame, int num_nuclei, const Nucleus* nuclei,
+                        const double* field) {
+        std::vector<int> Z(num_nuclei > 0 ? num_nuclei : 0);
+        std::vector<double> pos(3 * Z.size());
+        for (size_t a = 0; a < Z.size(); ++a) {
+            Z[a] = nuclei[a].Z;
+            pos[3 * a] = nuclei[a].Rx;
+            pos[3 * a + 1] = nuclei[a].Ry;
+            pos[3 * a + 2] = nuclei[a].Rz;
+        }
+        check(qsb_cube_write(filename, frame.comment, frame.grid_x, frame.grid_y, frame.grid_z, frame.boxaxis,
+                             frame.boxorg, num_nuclei, Z.empty() ? nullptr : Z.data(),
+                             pos.empty() ? nullptr : pos.data(), field));
+        return 1;
+    }
+};
+
+// CubeReader3 (source/cube_reader3.h:11-124): LoadCube reads header and values
+// (boxaxis = grid count x voxel vector, as there), GetMeshData copies the
+// values in the x-fastest grid layout.  Where the reference returns a zeroed
+// frame or leaves a short file's tail unread, these throw.
+class CubeReader3 {
+public:
+    struct Frame {
+        int grid_x;
+        int grid_y;
+        int grid_z;
+        double boxaxis[9];
+        double boxorg[3];
+        char comment[1024];
+    };
+    Frame LoadCube(const char* filename) {
+        Frame f{};
+        int grid[3];
+        check(qsb_cube_read_header(filename, grid, f.boxaxis, f.boxorg, nullptr));
+        f.grid_x = grid[0];
+        f.grid_y = grid[1];
+        f.grid_z = grid[2];
+        if (std::FILE* fp = std::fopen(filename, "r")) {      // the comment line, kept with its newline as there
+            char line[1024];
+            if (std::fgets(line, sizeof line, fp) && std::fgets(line, sizeof line, fp))
+                std::snprintf(f.comment, sizeof f.comment, "%s", line);
+            std::fclose(fp);
+        }
+        values_.resize((size_t)grid[0] * grid[1] * grid[2]);
+        check(qsb_cube_read(filename, values_.data(), nullptr, nullptr));
+        return f;
+    }
+    void GetMeshData(double* dest) const { std::copy(values_.begin(), values_.end(), dest); }
+
+private:
+    std::vector<double> values_;
 };
 
 // LOBPCG::Eigen_z_multi_mpi(l_grid, dVol, num_solution, iter_max, eigen_values,

@@ -88,3 +88,60 @@ def test_malformed_files_are_rejected(qsb_host, tmp_path):
         qsb_host.cube_read(tmp_path / "missing.cube")
     with pytest.raises(qsb_host.QsbError, match="one line"):
         qsb_host.cube_write(tmp_path / "c.cube", field, (6, 6, 6), axis, origin, comment="two\nlines")
+
+
+CUBE_DROPIN_PROGRAM = r"""
+#include <cstdio>
+#include <cstring>
+#include <vector>
+struct GridRange { int begin_x, begin_y, begin_z, end_x, end_y, end_z;
+  int SizeX() const { return end_x - begin_x; } int SizeY() const { return end_y - begin_y; }
+  int SizeZ() const { return end_z - begin_z; } };
+struct Nucleus { int Z; double Rx; double Ry; double Rz; };
+#include "qumasun_dropin.hpp"
+int main(int argc, char** argv) {
+  const int nx = 5, ny = 4, nz = 7;
+  std::vector<double> f(nx * ny * nz);
+  for (size_t i = 0; i < f.size(); ++i) f[i] = 0.001 * (double)i - 0.05;
+  qsb_dropin::CubeWriter::Frame frame{};
+  frame.grid_x = nx; frame.grid_y = ny; frame.grid_z = nz;
+  const double ax[9] = {2.5, 0, 0, 0, 2.0, 0, 0, 0, 3.5};
+  std::memcpy(frame.boxaxis, ax, sizeof ax);
+  std::strcpy(frame.comment, "density");
+  Nucleus nuc[2] = {{8, 0.1, 0.2, 0.3}, {1, 1.5, -0.5, 2.0}};
+  if (qsb_dropin::CubeWriter::SaveCube(argv[1], frame, 2, nuc, f.data()) != 1) return 2;
+  qsb_dropin::CubeReader3 r;
+  const auto g = r.LoadCube(argv[1]);
+  std::vector<double> back(f.size());
+  r.GetMeshData(back.data());
+  double err = 0;
+  for (size_t i = 0; i < f.size(); ++i) err = std::max(err, std::fabs(back[i] - f[i]));
+  std::printf("%d %d %d %.17g %s", g.grid_x, g.grid_y, g.grid_z, err, g.comment);
+  return 0;
+}
+"""
+
+
+@needs_ref
+def test_dropin_cube_classes_match_the_reference(tmp_path):
+    """The reference-shaped CubeWriter / CubeReader3 of qumasun_dropin.hpp compile
+    against a caller's own Nucleus type, write the reference writer's bytes and
+    read them back."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.join(root, "qumasun-workshop-template_b200")
+    src = tmp_path / "cube.cpp"
+    src.write_text(CUBE_DROPIN_PROGRAM)
+    exe = tmp_path / "cube"
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(root, "include"), str(src), "-o", str(exe), "-L", libdir,
+                    "-lqumasun_b200", f"-Wl,-rpath,{libdir}"], check=True, capture_output=True)
+    ours = tmp_path / "ours.cube"
+    out = subprocess.run([str(exe), str(ours)], capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
+    nx, ny, nz, err, comment = out.stdout.split()
+    assert (int(nx), int(ny), int(nz)) == (5, 4, 7) and float(err) <= 5e-13 and comment == "density"
+    f = 0.001 * np.arange(5 * 4 * 7) - 0.05
+    ref = tmp_path / "ref.cube"
+    O.ref_cube_write(str(ref), f, (5, 4, 7), [[2.5, 0, 0], [0, 2.0, 0], [0, 0, 3.5]], np.zeros(3), [8, 1],
+                     [[0.1, 0.2, 0.3], [1.5, -0.5, 2.0]], "density")
+    assert ours.read_bytes() == ref.read_bytes()
