@@ -480,6 +480,44 @@ QSB_API qsb_status qsb_relax_lbfgs(qsb_scf* scf, int n_atoms, double* pos, const
 QSB_API qsb_status qsb_scf_step_seconds(qsb_scf* scf, double* seconds, int max, int* n);
 
 /* ---------------------------------------------------------------------------
+ * UPF (v2, ONCV norm-conserving) pseudopotentials (host code; no device work).
+ * qsb_upf_load reads the radial data LoadUPF_ONCV keeps
+ * (source/upf_oncv_loader.h:353-520): per radial projector k its l_k, E_k =
+ * D_kk / 2 (Ha) and beta_k(r) = (r beta_k)(r) / r resampled onto the log grid
+ * r_i = exp(xi_min + i xi_delta), i < n_grid (xi_min = -9, 1000 points up to
+ * the UPF mesh's end) with the reference's quintic uniform-grid interpolant;
+ * cutoff_l[l] = the largest cutoff_radius of channel l; v_local: the UPF's
+ * PP_LOCAL resampled the same way (Ha), BEFORE the tail correction the
+ * reference then applies to it (ONCV_CORRECT_VLOCAL, upf_oncv_loader.h:641-1025),
+ * which is not restated here.
+ * qsb_upf_grid_tables builds the tables qsb_ham_set_projectors and
+ * qsb_ham_set_projector_gradients take: beta_k(|r - R|) Y_lm(r - R) (real
+ * harmonics, m = -l..l) on the grid points within the atom's largest cutoff,
+ * E_k per column, and the analytic gradient tables.  (The reference's own
+ * grid construction, the SvF2 filter of PseudoPotNonlocal_SvF2_kpoint.h:911-1180,
+ * goes through FFTW; this one samples directly.)  Atoms with more than 16
+ * projector columns are split into table entries of whole radial projectors at
+ * the same position; entry_atom[e] is the atom of entry e (H psi is a sum over
+ * entries; per-entry nonlocal forces add up to the atom's).
+ * Call once with entry_atom (or any output array) NULL for the sizes:
+ * n_entries, n_points (sum of npts), n_values (sum of npts * widths); then with
+ * entry_atom / npts / widths [n_entries], coords [3 n_points], beta [n_values],
+ * energy [sum of widths <= 16 n_entries], dbeta [3 n_values] (may be NULL). */
+typedef struct qsb_upf qsb_upf;
+QSB_API qsb_status qsb_upf_load(qsb_upf** upf, const char* path);
+QSB_API qsb_status qsb_upf_destroy(qsb_upf* upf);
+/* cutoff_l[4]; xi_min_delta[2]; any output may be NULL */
+QSB_API qsb_status qsb_upf_info(const qsb_upf* upf, int* n_projectors, double* z_valence, int* n_grid,
+                                double* cutoff_l, double* xi_min_delta);
+/* radius, v_local [n_grid]; l, energy [n_projectors]; projectors [n_projectors x n_grid]; any may be NULL */
+QSB_API qsb_status qsb_upf_radial(const qsb_upf* upf, double* radius, double* v_local, int* l, double* energy,
+                                  double* projectors);
+QSB_API qsb_status qsb_upf_grid_tables(const qsb_upf* const* upf, int n_species, int n_atoms, const double* pos,
+                                       const int* species, double dx, double dy, double dz, int* n_entries,
+                                       int64_t* n_points, int64_t* n_values, int* entry_atom, int* npts,
+                                       int* widths, int* coords, double* beta, double* energy, double* dbeta);
+
+/* ---------------------------------------------------------------------------
  * Cube files (host code; no device work).  The reference's state and density
  * exchange format: files written by qsb_cube_write are byte-identical to those
  * of CubeWriter::SaveCube (source/cube_writer.h:27-90; title "Generated by

@@ -552,3 +552,21 @@ def ref_cube_read(path):
     f = np.zeros(int(np.prod(grid)))
     lib.qsref_cube_read(os.fsencode(path), grid.ctypes.data_as(_ip), _d(ax), _d(org), _d(f))
     return f, {"grid": tuple(int(v) for v in grid), "axis": ax.reshape(3, 3), "origin": org}
+
+
+def ref_upf_load(path):
+    """The reference's LoadUPF_ONCV (upf_oncv_loader.h:353-1050) through oracle/_ref:
+    dict of its radial data (projectors are the up-spin copies)."""
+    lib = ref_lib()
+    info = np.zeros(3, np.int32)
+    if not lib.qsref_upf_load(os.fsencode(path), info.ctypes.data_as(_ip), None, None, None, None, None, None, None):
+        raise OSError(path)
+    n, zv, ng = (int(v) for v in info)
+    cut, xi = np.zeros(4), np.zeros(2)
+    r, v = np.zeros(ng), np.zeros(ng)
+    l, e = np.zeros(max(n, 1), np.int32), np.zeros(max(n, 1))
+    pr = np.zeros(max(n, 1) * ng)
+    lib.qsref_upf_load(os.fsencode(path), info.ctypes.data_as(_ip), _d(cut), _d(xi), _d(r), _d(v),
+                       l.ctypes.data_as(_ip), _d(e), _d(pr))
+    return {"n_projectors": n, "z_valence": zv, "n_grid": ng, "cutoff_l": cut, "xi": xi, "radius": r,
+            "v_local": v, "l": l[:n], "energy": e[:n], "projectors": pr[: n * ng].reshape(n, ng)}

@@ -28,6 +28,7 @@
  *   qsref_set_occupancy       SetOccupancy (Fermi-Dirac)    SetOccupancy.h:7-18
  *   qsref_cube_write          CubeWriter::SaveCube          cube_writer.h:27-90
  *   qsref_cube_read           CubeReader3::LoadCube + GetMeshData  cube_reader3.h:38-124
+ *   qsref_upf_load            LoadUPF_ONCV                  upf_oncv_loader.h:353-1050
  *
  * The nonlocal class itself (projector construction from UPF via SvF) is not
  * compiled: the projector values are supplied by the caller on the block
@@ -70,6 +71,7 @@ inline int lapack_DSYGVX(double* A, double* B, double* w, double* Z, double* /*t
 #endif
 #include "cube_reader3.h"
 #include "cube_writer.h"
+#include "upf_oncv_loader.h"
 
 namespace {
 
@@ -487,6 +489,30 @@ int qsref_cube_write(const char* path, const char* comment, int nx, int ny, int 
     std::vector<Nucleus> nuc(n_atoms);
     for (int a = 0; a < n_atoms; ++a) nuc[a] = Nucleus{Z[a], pos[3 * a], pos[3 * a + 1], pos[3 * a + 2]};
     return CubeWriter::SaveCube(path, f, n_atoms, nuc.data(), field);
+}
+
+/* LoadUPF_ONCV's radial data: info = {n_proj, valence, n_grid}; cutoff[4];
+ * xi[2] = {xi_min, xi_delta}; radius, v_local [n_grid]; l, energy [n_proj];
+ * proj [n_proj x n_grid] (the up-spin copies).  Outputs after info may be NULL
+ * (first call for the sizes).  Returns 0 when the file did not load. */
+int qsref_upf_load(const char* path, int* info, double* cutoff, double* xi, double* radius, double* v_local, int* l,
+                   double* energy, double* proj) {
+    PseudoPot_MBK* p = LoadUPF_ONCV(path);
+    if (!p) return 0;
+    info[0] = p->num_radial_projectors;
+    info[1] = (int)p->valence_electron;
+    info[2] = p->num_radial_grids;
+    if (cutoff) for (int i = 0; i < 4; ++i) cutoff[i] = p->cutoff_r[i];
+    if (xi) { xi[0] = p->xi_min; xi[1] = p->xi_delta; }
+    const int n = p->num_radial_grids;
+    if (radius) for (int i = 0; i < n; ++i) radius[i] = p->radius[i];
+    if (v_local) for (int i = 0; i < n; ++i) v_local[i] = p->V_local[i];
+    for (int k = 0; k < p->num_radial_projectors; ++k) {
+        if (l) l[k] = p->projector_quantum_l[k];
+        if (energy) energy[k] = p->projector_energy_up[k];
+        if (proj) for (int i = 0; i < n; ++i) proj[(size_t)k * n + i] = p->projector[2 * k][i];
+    }
+    return 1;
 }
 
 /* grid[3] and axis[9], org[3] out; field (x fastest) out when not NULL */

@@ -372,6 +372,69 @@ def density(X, occupations, N):
     return rho
 
 
+class Upf:
+    """A UPF (v2, ONCV) pseudopotential's radial data (qsb_upf_load)."""
+
+    def __init__(self, path):
+        h = ctypes.c_void_p()
+        _check(lib.qsb_upf_load(ctypes.byref(h), os.fsencode(path)))
+        self._h = h
+        n, ng = ctypes.c_int(), ctypes.c_int()
+        zv = ctypes.c_double()
+        cut, cut_p = _f64(np.zeros(4))
+        xi, xi_p = _f64(np.zeros(2))
+        _check(lib.qsb_upf_info(h, ctypes.byref(n), ctypes.byref(zv), ctypes.byref(ng), cut_p, xi_p))
+        self.n_projectors, self.z_valence, self.n_grid = n.value, zv.value, ng.value
+        self.cutoff_l, self.xi = cut, xi
+        r, r_p = _f64(np.zeros(ng.value))
+        v, v_p = _f64(np.zeros(ng.value))
+        l, l_p = _i32(np.zeros(max(n.value, 1), np.int32))
+        e, e_p = _f64(np.zeros(max(n.value, 1)))
+        pr, pr_p = _f64(np.zeros(max(n.value, 1) * ng.value))
+        _check(lib.qsb_upf_radial(h, r_p, v_p, l_p, e_p, pr_p))
+        self.radius, self.v_local = r, v
+        self.l, self.energy = l[:n.value].copy(), e[:n.value].copy()
+        self.projectors = pr[: n.value * ng.value].reshape(n.value, ng.value)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.qsb_upf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def upf_grid_tables(upfs, pos, species, spacing, gradients=True):
+    """Projector tables of atoms at pos [n, 3] (species index into upfs) on a grid
+    of the given spacing (qsb_upf_grid_tables): (entry_atom, (npts, widths,
+    coords, beta, energy), dbeta or None) -- the tables as
+    Hamiltonian.set_projectors takes them."""
+    arr = (ctypes.c_void_p * len(upfs))(*[u._h.value for u in upfs])
+    p, p_p = _f64(np.asarray(pos, np.float64).reshape(-1, 3))
+    sp, sp_p = _i32(np.asarray(species, np.int32).ravel())
+    ne, npt, nv = ctypes.c_int(), ctypes.c_int64(), ctypes.c_int64()
+    dx, dy, dz = spacing
+    args = (arr, len(upfs), len(p), p_p, sp_p, _c_d(dx), _c_d(dy), _c_d(dz), ctypes.byref(ne), ctypes.byref(npt),
+            ctypes.byref(nv))
+    _check(lib.qsb_upf_grid_tables(*args, None, None, None, None, None, None, None))
+    ea, ea_p = _i32(np.zeros(max(ne.value, 1), np.int32))
+    npts, npts_p = _i32(np.zeros(max(ne.value, 1), np.int32))
+    w, w_p = _i32(np.zeros(max(ne.value, 1), np.int32))
+    c, c_p = _i32(np.zeros(max(3 * npt.value, 1), np.int32))
+    b, b_p = _f64(np.zeros(max(nv.value, 1)))
+    e, e_p = _f64(np.zeros(max(16 * ne.value, 1)))
+    g, g_p = (_f64(np.zeros(max(3 * nv.value, 1))) if gradients else (None, None))
+    _check(lib.qsb_upf_grid_tables(*args, ea_p, npts_p, w_p, c_p, b_p, e_p, g_p))
+    n = ne.value
+    tables = (npts[:n].copy(), w[:n].copy(), c[: 3 * npt.value].copy(), b[: nv.value].copy(),
+              e[: int(w[:n].sum())].copy())
+    return ea[:n].copy(), tables, (g[: 3 * nv.value].copy() if gradients else None)
+
+
 def cube_write(path, field, grid, axis, origin=(0.0, 0.0, 0.0), Z=(), pos=(), comment=""):
     """Writes field (nx*ny*nz values, x fastest) as a cube file in the
     reference's dialect (qsb_cube_write).  axis: the three box edge vectors."""
