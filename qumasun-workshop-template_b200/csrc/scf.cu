@@ -915,6 +915,7 @@ qsb_status qsb_relax_lbfgs(qsb_scf* c, int n_atoms, double* pos, const int* spec
         int steps = 0;
         QSB_TRY(qsb_scf_run(c, X, keep, lobpcg_iters, scf_max_steps, scf_tol, e_scf.data(), &steps, ev.data(),
                             occ.data(), stream));
+        if (steps < 1 || steps > scf_max_steps) return fail(QSB_ERR_STATE, "relax_lbfgs: the SCF ran no step");
         double ts = 0.0;
         for (int n = 0; n < c->nb; ++n) {
             const double f = std::min(std::max(occ[n] / 2.0, 1e-300), 1.0 - 1e-16);
