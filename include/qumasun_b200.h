@@ -487,9 +487,9 @@ QSB_API qsb_status qsb_scf_step_seconds(qsb_scf* scf, double* seconds, int max, 
  * r_i = exp(xi_min + i xi_delta), i < n_grid (xi_min = -9, 1000 points up to
  * the UPF mesh's end) with the reference's quintic uniform-grid interpolant;
  * cutoff_l[l] = the largest cutoff_radius of channel l; v_local: the UPF's
- * PP_LOCAL resampled the same way (Ha), BEFORE the tail correction the
- * reference then applies to it (ONCV_CORRECT_VLOCAL, upf_oncv_loader.h:641-1025),
- * which is not restated here.
+ * PP_LOCAL with its tail blended into -2 Z_v / r past the local cutoff, as the
+ * reference corrects it (ONCV_CORRECT_VLOCAL 11, upf_oncv_loader.h:803-921,
+ * 1022-1026), resampled the same way (Ha).
  * qsb_upf_grid_tables builds the tables qsb_ham_set_projectors and
  * qsb_ham_set_projector_gradients take: beta_k(|r - R|) Y_lm(r - R) (real
  * harmonics, m = -l..l) on the grid points within the atom's largest cutoff,

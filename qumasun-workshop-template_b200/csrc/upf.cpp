@@ -10,7 +10,10 @@
 //     beta_k(r) = (r beta_k)(r) / r from the UPF's uniform mesh (its first
 //     point replaced by the second for l = 0 and by 0 otherwise), resampled on
 //     the log grid; cutoff_r[l] = the largest cutoff_radius of channel l;
-//   * V_local(r) resampled the same way, / 2 (Ry -> Ha).
+//   * V_local(r): the UPF's local potential with its tail blended into
+//     -2 Z_v / r beyond the local cutoff (the reference's correction of it),
+//     resampled the same way, / 2 (Ry -> Ha); the cutoff it reports is the
+//     corrected one.
 // Resampling is the reference's uniform-grid interpolant (UniformGrid::GetValue,
 // source/UniformGrid.h:38-89): on each mesh interval a quintic Hermite
 // polynomial matching values, first and second derivatives at both ends, the
@@ -236,6 +239,7 @@ qsb_status qsb_upf_load(qsb_upf** out, const char* path) {
     u->n_proj = std::atoi(a.c_str());
     if (!attribute(s, hdr, "z_valence", a)) return bad("no z_valence");
     u->z_valence = std::strtod(a.c_str(), nullptr);
+    const std::string a_zval = a;
     const Span r = find_path(s, {"UPF", "PP_MESH", "PP_R"});
     if (!r.ok() || !attribute(s, r, "size", a)) return bad("no PP_MESH/PP_R size");
     const int nu = std::atoi(a.c_str());
@@ -269,16 +273,64 @@ qsb_status qsb_upf_load(qsb_upf** out, const char* path) {
         const std::vector<double> d = numbers(s, dij, u->n_proj * u->n_proj);
         for (int k = 0; k < u->n_proj; ++k) u->energy[k] = d[k + u->n_proj * k] / 2.0;
     }
-    // local potential (Ry -> Ha)
+    // local potential (Ry), tail-corrected to -2 Z_v / r as the reference does
+    // (ONCV_CORRECT_VLOCAL 11, source/upf_oncv_loader.h:803-921), then Ry -> Ha
     const Span loc = find_path(s, {"UPF", "PP_LOCAL"});
     if (!loc.ok()) return bad("no PP_LOCAL");
     const std::vector<double> vl = numbers(s, loc, nu);
-    u->v_local.resize(u->n_grid);
-    const Quintic qv{vl.data(), nu, mesh[0], h, 1};
-    for (int i = 0; i < u->n_grid; ++i) {
-        double v;
-        qv.eval(u->radius[i], v, nullptr);
-        u->v_local[i] = v / 2.0;
+    {
+        // the reference keeps the valence as an integer (std::stol of the attribute)
+        const double zv = (double)std::strtol(a_zval.c_str(), nullptr, 10);
+        // nuclear-charge density of the UPF's V_local: -(1 / 8 pi) (v'' + 2 v' / r),
+        // 4th-order differences on the uniform mesh
+        std::vector<double> rho(nu, 0.0);
+        for (int i = 2; i < nu - 2; ++i) {
+            const double d1 = (8.0 * (vl[i + 1] - vl[i - 1]) - (vl[i + 2] - vl[i - 2])) / (12.0 * h);
+            const double d2 =
+                (-30.0 * vl[i] + 16.0 * (vl[i + 1] + vl[i - 1]) - (vl[i + 2] + vl[i - 2])) / (12.0 * h * h);
+            rho[i] = -(1.0 / (8.0 * M_PI)) * (d2 + (2.0 / mesh[i]) * d1);
+        }
+        rho[0] = rho[1] = rho[2];
+        rho[nu - 2] = rho[nu - 1] = 0.0;
+        int i_cut = (int)std::floor(u->cutoff_vlocal / h);
+        // sign changes of rho and the most negative r^2 rho
+        int nodes = 0, node2 = 0, i_peak = 0;
+        double r2rho_min = 0.0;
+        for (int i = 1; i < nu - 1; ++i) {
+            if (rho[i] * rho[i + 1] < 0.0 && ++nodes == 2) node2 = i;
+            const double r2rho = mesh[i] * mesh[i] * rho[i];
+            if (r2rho_min > r2rho) {
+                r2rho_min = r2rho;
+                i_peak = i;
+            }
+        }
+        if (node2 > i_cut) {   // the density's second node lies outside: extend the cutoff
+            i_cut = std::min(node2, (int)(i_cut * 1.5));
+            u->cutoff_vlocal = mesh[i_cut];
+        }
+        // blend start: where r^2 rho climbs back above half its minimum
+        int i_in = 0;
+        for (int i = i_peak + 1; i < i_cut - 1; ++i)
+            if (r2rho_min * 0.5 < mesh[i] * mesh[i] * rho[i]) {
+                i_in = i;
+                break;
+            }
+        std::vector<double> vc(nu);
+        for (int i = i_cut; i < nu; ++i) vc[i] = -2.0 * zv / mesh[i];
+        for (int i = 0; i < i_in; ++i) vc[i] = vl[i];
+        const double width = mesh[i_cut] - mesh[i_in];
+        for (int i = i_in; i < i_cut; ++i) {
+            const double x = (mesh[i] - mesh[i_in]) / width;
+            const double f = x * x * x * x * (-20.0 * x * x * x + 70.0 * x * x - 84.0 * x + 35.0);
+            vc[i] = f * (-2.0 * zv / mesh[i]) + (1.0 - f) * vl[i];
+        }
+        u->v_local.resize(u->n_grid);
+        const Quintic qv{vc.data(), nu, mesh[0], h, 1};
+        for (int i = 0; i < u->n_grid; ++i) {
+            double v;
+            qv.eval(u->radius[i], v, nullptr);
+            u->v_local[i] = v / 2.0;
+        }
     }
     // projectors: (r beta)(r) / r, resampled
     u->proj.resize((size_t)u->n_proj * u->n_grid);

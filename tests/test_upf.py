@@ -4,8 +4,8 @@ on the pseudopotentials the reference ships, and properties of the grid
 projector tables qsb_upf_grid_tables builds from them.
 
 Bars: log grid, channels, KB energies (D_kk / 2) and cutoffs equal the
-reference's exactly; resampled projectors equal its values to 1e-14 relative
-(the same interpolant); on the grid, each column's norm sum beta^2 dV matches
+reference's exactly; resampled projectors and the tail-corrected local
+potential equal its values to 1e-14 relative (the same interpolant); on the grid, each column's norm sum beta^2 dV matches
 the radial integral to 2e-3 at h = 0.15 bohr, different m of a channel are
 orthogonal to 1e-3, and the gradient tables equal central differences of the
 tables under an atom shift to 1e-6."""
@@ -42,6 +42,8 @@ def test_radial_data_equals_the_reference_loader(qsb_host, el):
     assert np.array_equal(u.radius, r["radius"])
     scale = np.abs(r["projectors"]).max()
     assert np.abs(u.projectors - r["projectors"]).max() <= 1e-14 * scale
+    # the local potential after the reference's tail correction
+    assert np.abs(u.v_local - r["v_local"]).max() <= 1e-14 * np.abs(r["v_local"]).max()
 
 
 def _load(qsb_host, el):
