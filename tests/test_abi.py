@@ -83,3 +83,30 @@ def test_dropin_header_compiles_and_reports_errors(tmp_path):
     out = subprocess.run([str(exe)], capture_output=True, text=True)
     assert out.returncode == 0, out.stdout + out.stderr
     assert "grid dimensions" in out.stdout
+
+
+def test_host_side_argument_errors_of_the_newer_entry_points():
+    """Argument and state errors are reported before any device work, so they
+    are checked without a GPU: the kinetic switch, the host-buffer apply, the
+    Ewald sum and the relaxation driver."""
+    lib = ctypes.CDLL(LIB)
+    lib.qsb_last_error.restype = ctypes.c_char_p
+    d = ctypes.c_double
+    h = ctypes.c_void_p()
+    assert lib.qsb_ham_create(ctypes.byref(h), 8, 8, 8, d(0.5), d(0.5), d(0.5)) == 0
+    try:
+        assert lib.qsb_ham_set_kinetic(h, 2) == 1 and b"FD8" in lib.qsb_last_error()
+        assert lib.qsb_ham_set_kinetic(h, 1) == 0 and lib.qsb_ham_set_kinetic(h, 0) == 0
+        buf = ctypes.create_string_buffer(8 * 512)
+        assert lib.qsb_ham_apply_host(h, 0, 0, 1, buf, buf, d(0), d(0), d(0), 0, None) == 4   # no potential
+        assert b"potential" in lib.qsb_last_error()
+        assert lib.qsb_ham_apply_host(h, 0, 0, 1, None, buf, d(0), d(0), d(0), 0, None) == 1  # null psi
+    finally:
+        assert lib.qsb_ham_destroy(h) == 0
+    pos = (ctypes.c_double * 3)(0, 0, 0)
+    q = (ctypes.c_double * 1)(1.0)
+    bad_cell = (ctypes.c_double * 3)(5.0, 0.0, 5.0)
+    e = ctypes.c_double()
+    assert lib.qsb_ewald(1, pos, q, bad_cell, ctypes.byref(e), None) == 1 and b"cell" in lib.qsb_last_error()
+    assert lib.qsb_relax_lbfgs(None, 1, pos, None, 1, None, None, None, d(9.0), None, None, None, None, None,
+                               None, None, 4, 10, d(1e-8), 10, d(1e-4), d(0.2), 5, None, None, None, None) == 1
