@@ -479,6 +479,53 @@ def scf_section(name, tol_ref=1e-8, max_steps=None, rho_tol=0.0):
     return out
 
 
+# config 1: O + 2 H in a 20 bohr box, 112^3, GTH-form species (O: one s
+# projector; H: local only), 4 occupied + 4 empty bands
+WATER_O = dict(zion=6.0, rloc=0.247, c1=-16.58, c2=2.40, r=0.222, h=18.27)
+WATER_H = dict(zion=1.0, rloc=0.2, c1=-4.18, c2=0.725)
+
+
+def relax_section(fmax=1e-4):
+    """Wall time of the LBFGS relaxation of config 1 (qsb_relax_lbfgs: SCF warm
+    from the previous geometry's states, local + nonlocal + Ewald forces) from
+    its jittered start to max |F| < fmax, FP64."""
+    import torch
+    import qsb
+    n, L = 112, 20.0
+    h = L / n
+    N = n ** 3
+    pos = np.array([[0.0, 0.0, 0.0], [1.43, 1.11, 0.0], [-1.43, 1.11, 0.0]])
+    pos = pos + np.random.default_rng(1).normal(0.0, 0.05, pos.shape) + L / 2
+    species = [0, 1, 1]
+    proj = ([1, 0], [[WATER_O["r"], 0.0], [0.0, 0.0]], [[WATER_O["h"], 0.0], [0.0, 0.0]], 9.0)
+    sps = (WATER_O, WATER_H)
+    local = tuple([sp[k] for sp in sps] for k in ("zion", "rloc", "c1", "c2"))
+    H = qsb.Hamiltonian(n, n, n, h, h, h)
+    H.set_gth_projectors(pos, species, *proj)
+    H.set_potential(np.zeros(N))
+    es = qsb.EigenSolver(N, 8, False, "fp64")
+    scf = qsb.SCF(H, es, 8, 8.0)
+    scf.set_gth_local(pos, species, *local)
+    scf.set_density_tolerance(1e-7)
+    gen = torch.Generator(device="cuda").manual_seed(1)
+    psi = torch.rand(8, N, dtype=torch.float64, device="cuda", generator=gen) - 0.5
+    X = torch.linalg.qr(psi.t())[0].t().contiguous() / math.sqrt(h ** 3)
+    keep = torch.zeros_like(X)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    p, e, f = scf.relax(X, keep, pos, species, proj, local, scf_tol=1e-9, max_iter=40, fmax=fmax)
+    torch.cuda.synchronize()
+    seconds = time.time() - t0
+    out = {"config": "water, 20 bohr box, 112^3, 8 bands", "lbfgs_steps": int(len(e) - 1), "seconds": seconds,
+           "max_force_ha_per_bohr": float(np.linalg.norm(f, axis=1).max()), "fmax": fmax,
+           "energy_drop_ha": float(e[0] - e[-1]),
+           "oh_bonds_bohr": [float(np.linalg.norm(p[1] - p[0])), float(np.linalg.norm(p[2] - p[0]))]}
+    scf.close()
+    es.close()
+    H.close()
+    return out
+
+
 def fft_kinetic_section(H, psi, hpsi, stream, alg_bytes, steps=20):
     """Device time of one H.psi with the FFT kinetic (qsb_ham_set_kinetic(1):
     batched cuFFT D2Z / Z2D in 32-band chunks, |G|^2 / 2, 1/N + V psi fused,
@@ -520,6 +567,8 @@ def main():
     ap.add_argument("--no-scf", action="store_true")
     ap.add_argument("--scf-config", default="c2", choices=sorted(SCF_CONFIGS),
                     help="SCF workload: c2 (16 atoms, 96^3, 128 bands; default) or c3 (54 atoms, 144^3, 384 bands)")
+    ap.add_argument("--relax", action="store_true",
+                    help="also time the LBFGS relaxation of config 1 (water, 112^3) to max |F| < 1e-4 Ha/bohr")
     ap.add_argument("--scf-tol-ref", type=float, default=1e-8,
                     help="|dE| / atom both SCF runs continue to (the FP64 end point is E*)")
     ap.add_argument("--scf-rho-tol", type=float, default=0.0,
@@ -622,6 +671,7 @@ def main():
     scf = None
     if not args.no_scf and world == 1:
         scf = scf_section(args.scf_config, args.scf_tol_ref, args.scf_max_steps, args.scf_rho_tol)
+    relax = relax_section() if args.relax and world == 1 else None
     clk = clocks.stop()
 
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist, "cuda")
@@ -659,6 +709,7 @@ def main():
                 "ms_per_step": e2e_ms},
         "gpu_launches": launches,
         "fft_kinetic": fft,
+        "relax": relax,
         "lobpcg": lob,
         "scf": scf,
         "gram": gram,
