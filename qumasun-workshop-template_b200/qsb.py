@@ -466,6 +466,71 @@ def cube_read(path):
     return f, {"grid": g, "axis": ax.reshape(3, 3), "origin": org, "Z": z[:n].copy(), "pos": p[:3 * n].reshape(n, 3)}
 
 
+def write_states(directory, header, bundle, eigen_values, grid, box, Z=(), pos=(), is_complex=True, sk=0,
+                 n_kpoints=1, kpoint=(0, 1, 0, 1, 0, 1), list_name=None):
+    """Writes a band bundle (host array: complex SoA [n, 2, N] or real [n, N])
+    as the reference's state files (its Output.StateVector writer,
+    source/qumasun_base1.output.h:250-365): per band n the cube files
+    {header}_{up|down}_k{k}_n{n}_re.cube and _im.cube with the comment
+    "eigenvalue=..., kpoint=kx/nx,ky/ny,kz/nz", box axes on the diagonal, origin
+    0; sk < n_kpoints is spin up.  Real bands get a zero imaginary file.  With
+    list_name, also the list of file names (re, im per band) the reference's
+    Initial.State reads.  Returns the file names."""
+    nx, ny, nz = (int(v) for v in grid)
+    N = nx * ny * nz
+    b = np.asarray(bundle, np.float64).reshape(-1, 2, N) if is_complex else \
+        np.asarray(bundle, np.float64).reshape(-1, N)
+    axis = np.diag(np.asarray(box, np.float64))
+    tag = ("_up" if sk < n_kpoints else "_down") + "_k%d" % (sk % n_kpoints)
+    names = []
+    for n in range(b.shape[0]):
+        comment = "eigenvalue=%.10f, kpoint=%d/%d,%d/%d,%d/%d" % ((float(eigen_values[n]),) + tuple(kpoint))
+        re = b[n, 0] if is_complex else b[n]
+        im = b[n, 1] if is_complex else np.zeros(N)
+        for part, field in (("_re", re), ("_im", im)):
+            name = "%s%s_n%d%s.cube" % (header, tag, n, part)
+            cube_write(os.path.join(directory, name), field, (nx, ny, nz), axis, (0.0, 0.0, 0.0), Z, pos, comment)
+            names.append(name)
+    if list_name:
+        with open(os.path.join(directory, list_name), "w") as f:
+            f.writelines(n + "\n" for n in names)
+    return names
+
+
+def read_states(list_path, directory=None):
+    """Reads the state files a list names (re, im per band, the order of the
+    reference's Initial.State lists, source/qumasun_base1.initialize.h:455-540):
+    returns (bundle [n, 2, N] complex SoA, eigen_values [n] from each re file's
+    "eigenvalue=" comment, header of the first file).  Relative names resolve
+    against directory (default: the list's folder)."""
+    base = directory if directory is not None else os.path.dirname(os.path.abspath(list_path))
+    with open(list_path) as f:
+        names = [l.strip() for l in f if l.strip()]
+    if len(names) % 2:
+        raise ValueError("state list: re and im files come in pairs")
+    bands, evs, hdr0 = [], [], None
+    for i in range(0, len(names), 2):
+        pair = []
+        for name in names[i:i + 2]:
+            if name.startswith("["):
+                raise ValueError("state list: operation keys ([...]) are not supported: " + name)
+            path = name if os.path.isabs(name) else os.path.join(base, name)
+            field, hdr = cube_read(path)
+            if hdr0 is None:
+                hdr0 = hdr
+            elif hdr["grid"] != hdr0["grid"]:
+                raise ValueError("state list: grids differ between files")
+            pair.append(field)
+            if len(pair) == 1:
+                with open(path) as f:
+                    f.readline()
+                    comment = f.readline()
+                k = comment.find("eigenvalue=")
+                evs.append(float(comment[k + 11:].split(",")[0]) if k >= 0 else 0.0)
+        bands.append(np.stack(pair))
+    return np.stack(bands), np.array(evs), hdr0
+
+
 def ewald(pos, charge, cell):
     """(energy, forces [n_atoms, 3]) of point charges in an orthorhombic cell
     with a neutralising background (qsb_ewald; host code)."""

@@ -145,3 +145,28 @@ def test_dropin_cube_classes_match_the_reference(tmp_path):
     O.ref_cube_write(str(ref), f, (5, 4, 7), [[2.5, 0, 0], [0, 2.0, 0], [0, 0, 3.5]], np.zeros(3), [8, 1],
                      [[0.1, 0.2, 0.3], [1.5, -0.5, 2.0]], "density")
     assert ours.read_bytes() == ref.read_bytes()
+
+
+@needs_ref
+def test_state_files_follow_the_reference_naming_and_round_trip(qsb_host, tmp_path):
+    """write_states / read_states: the reference's state file names, list
+    order and comment; its own CubeReader3 reads the values; the round trip
+    keeps the bundle to the %.12f rounding and the eigenvalues to 1e-10."""
+    grid = (6, 5, 7)
+    N = 6 * 5 * 7
+    rng = np.random.default_rng(8)
+    X = rng.uniform(-1, 1, (3, 2, N))
+    ev = np.array([-0.512345678912, -0.25, 0.125])
+    names = qsb_host.write_states(str(tmp_path), "state", X, ev, grid, (3.0, 2.5, 3.5), [6], [[0.1, 0.2, 0.3]],
+                                  sk=1, n_kpoints=4, kpoint=(1, 4, 0, 1, 0, 1), list_name="states.txt")
+    assert names[:2] == ["state_up_k1_n0_re.cube", "state_up_k1_n0_im.cube"] and len(names) == 6
+    f_ref, _ = O.ref_cube_read(str(tmp_path / names[3]))
+    assert np.abs(f_ref - X[1, 1]).max() <= 5e-13
+    line2 = (tmp_path / names[0]).read_text().splitlines()[1]
+    assert line2 == "eigenvalue=-0.5123456789, kpoint=1/4,0/1,0/1"
+    Y, ev2, hdr = qsb_host.read_states(str(tmp_path / "states.txt"))
+    assert Y.shape == X.shape and np.abs(Y - X).max() <= 5e-13
+    assert np.abs(ev2 - ev).max() <= 1e-10 and hdr["grid"] == grid
+    # spin down: k index past the spin-up set
+    assert qsb_host.write_states(str(tmp_path), "s", X[:1], ev, grid, (3.0, 2.5, 3.5), sk=5, n_kpoints=4)[0] == \
+        "s_down_k1_n0_re.cube"
