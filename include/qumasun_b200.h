@@ -512,6 +512,19 @@ QSB_API qsb_status qsb_upf_info(const qsb_upf* upf, int* n_projectors, double* z
 /* radius, v_local [n_grid]; l, energy [n_projectors]; projectors [n_projectors x n_grid]; any may be NULL */
 QSB_API qsb_status qsb_upf_radial(const qsb_upf* upf, double* radius, double* v_local, int* l, double* energy,
                                   double* projectors);
+/* Fourier transform of a radial local potential (Ha) with Coulomb tail -z/r,
+ * v(G) = int V(r) exp(-i G.r) d^3r, on G = j dg, j < n_g, in the convention of
+ * the SCF driver's GTH local part: for G > 0 the full transform (its
+ * -4 pi z / G^2 included), at G = 0 the finite part lim (v(G) + 4 pi z / G^2).
+ * Computed as 4 pi int r^2 [V + z erf(r / (sqrt2 sigma)) / r] j0(G r) dr
+ * (Simpson in ln r on the log grid radius[n_r]) minus the Gaussian charge's
+ * 4 pi z exp(-G^2 sigma^2 / 2) / G^2 (2 pi z sigma^2 at G = 0); the result
+ * does not depend on sigma.  For a UPF: radius and v_local of qsb_upf_radial,
+ * z = z_valence.  (The reference forms its local potential from core charges
+ * by a Poisson solve on a finer grid, source/qumasun_base1.core.h; this table
+ * is the G-space route the SCF driver takes.) */
+QSB_API qsb_status qsb_radial_local_table(int n_r, const double* radius, const double* v, double z, double sigma,
+                                          int n_g, double dg, double* table);
 QSB_API qsb_status qsb_upf_grid_tables(const qsb_upf* const* upf, int n_species, int n_atoms, const double* pos,
                                        const int* species, double dx, double dy, double dz, int* n_entries,
                                        int64_t* n_points, int64_t* n_values, int* entry_atom, int* npts,

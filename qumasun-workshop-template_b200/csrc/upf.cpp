@@ -377,6 +377,44 @@ qsb_status qsb_upf_radial(const qsb_upf* u, double* radius, double* v_local, int
     return QSB_OK;
 }
 
+qsb_status qsb_radial_local_table(int n_r, const double* radius, const double* v, double z, double sigma,
+                                 int n_g, double dg, double* table) {
+    if (n_r < 5 || !radius || !v || !table || n_g <= 0 || !(dg > 0) || !(sigma > 0))
+        return fail(QSB_ERR_INVALID, "radial_local_table: bad argument");
+    // log grid: r_i = r_0 exp(i dxi); integrals in xi with dr = r dxi (Simpson,
+    // trapezoid on a last odd interval)
+    const double dxi = std::log(radius[1] / radius[0]);
+    for (int i = 2; i < n_r; ++i)
+        if (std::fabs(std::log(radius[i] / radius[i - 1]) - dxi) > 1e-9 * std::fabs(dxi) + 1e-12)
+            return fail(QSB_ERR_INVALID, "radial_local_table: radius is not a logarithmic grid");
+    const double s2 = std::sqrt(2.0) * sigma;
+    std::vector<double> sr(n_r);   // r^3 (V + z erf(r / (sqrt2 sigma)) / r), the short-range part times r^3
+    for (int i = 0; i < n_r; ++i) {
+        const double r = radius[i];
+        sr[i] = r * r * r * (v[i] + z * std::erf(r / s2) / r);
+    }
+    auto simpson = [&](auto f) {
+        const int m = (n_r - 1) % 2 ? n_r - 1 : n_r;   // odd point count for Simpson
+        double acc = f(0) + f(m - 1);
+        for (int i = 1; i < m - 1; ++i) acc += (i % 2 ? 4.0 : 2.0) * f(i);
+        acc *= dxi / 3.0;
+        if (m < n_r) acc += 0.5 * dxi * (f(n_r - 2) + f(n_r - 1));
+        return acc;
+    };
+    for (int j = 0; j < n_g; ++j) {
+        const double G = j * dg;
+        // 4 pi int r^2 V_sr j0(G r) dr = 4 pi int r^3 V_sr j0(G r) dxi
+        const double vs = 4.0 * M_PI * simpson([&](int i) {
+            const double x = G * radius[i];
+            return sr[i] * (x > 1e-8 ? std::sin(x) / x : 1.0 - x * x / 6.0);
+        });
+        const double coul = j == 0 ? 2.0 * M_PI * z * sigma * sigma
+                                   : -4.0 * M_PI * z * std::exp(-0.5 * G * G * sigma * sigma) / (G * G);
+        table[j] = vs + coul;
+    }
+    return QSB_OK;
+}
+
 qsb_status qsb_upf_grid_tables(const qsb_upf* const* upf, int n_species, int n_atoms, const double* pos,
                                const int* species, double dx, double dy, double dz, int* n_entries,
                                int64_t* n_points, int64_t* n_values, int* entry_atom, int* npts, int* widths,

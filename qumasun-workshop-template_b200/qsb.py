@@ -408,6 +408,16 @@ class Upf:
             pass
 
 
+def radial_local_table(radius, v, z, n_g, dg, sigma=0.5):
+    """v(G) on G = j dg of a radial local potential with tail -z/r (qsb_radial_local_table)."""
+    r, r_p = _f64(np.asarray(radius, np.float64).ravel())
+    vv, v_p = _f64(np.asarray(v, np.float64).ravel())
+    assert r.size == vv.size
+    t, t_p = _f64(np.zeros(int(n_g)))
+    _check(lib.qsb_radial_local_table(r.size, r_p, v_p, _c_d(z), _c_d(sigma), int(n_g), _c_d(dg), t_p))
+    return t
+
+
 def upf_grid_tables(upfs, pos, species, spacing, gradients=True):
     """Projector tables of atoms at pos [n, 3] (species index into upfs) on a grid
     of the given spacing (qsb_upf_grid_tables): (entry_atom, (npts, widths,

@@ -131,3 +131,34 @@ def test_missing_file_is_reported(qsb_host, tmp_path):
     bad.write_text("<UPF version=\"2.0.1\"><PP_INFO/></UPF>")
     with pytest.raises(qsb_host.QsbError, match="PP_HEADER"):
         qsb_host.Upf(str(bad))
+
+
+def test_local_table_equals_the_analytic_gth_transform(qsb_host):
+    """qsb_radial_local_table on a GTH-form local potential (Z 6, r_loc 0.45,
+    C1 -4, C2 0.6) tabulated on a log grid equals the analytic GTH transform the
+    SCF driver uses (-4 pi Z e^{-G^2 r^2/2} / G^2 + (2 pi)^{3/2} r^3 e^{-G^2 r^2/2}
+    (C1 + C2 (3 - G^2 r^2)); 2 pi Z r^2 + ... at G = 0) to 1e-9 absolute for
+    G < 20 bohr^-1, whatever the splitting width sigma."""
+    import math
+    from scipy.special import erf
+    Z, rl, c1, c2 = 6.0, 0.45, -4.0, 0.6
+    r = np.exp(-9 + np.arange(2000) * (math.log(15.0) + 9) / 2000)
+    x = r / rl
+    V = -Z * erf(r / (math.sqrt(2) * rl)) / r + np.exp(-0.5 * x * x) * (c1 + c2 * x * x)
+    G = np.arange(400) * 0.05
+    g2 = G * G
+    e = np.exp(-0.5 * g2 * rl * rl)
+    coul = np.where(G > 0, -4 * math.pi * Z * e / np.where(G > 0, g2, 1.0), 2 * math.pi * Z * rl * rl)
+    ana = coul + (2 * math.pi) ** 1.5 * rl ** 3 * e * (c1 + c2 * (3 - g2 * rl * rl))
+    for sigma in (0.3, 0.45, 0.8):
+        t = qsb_host.radial_local_table(r, V, Z, 400, 0.05, sigma)
+        assert np.abs(t - ana).max() <= 1e-9, sigma
+
+
+@needs_pp
+@pytest.mark.parametrize("el", ["C", "Al"])
+def test_local_table_of_a_upf_does_not_depend_on_the_splitting(qsb_host, el):
+    u = _load(qsb_host, el)
+    t1 = qsb_host.radial_local_table(u.radius, u.v_local, float(int(u.z_valence)), 300, 0.05, 0.4)
+    t2 = qsb_host.radial_local_table(u.radius, u.v_local, float(int(u.z_valence)), 300, 0.05, 0.7)
+    assert np.abs(t1 - t2).max() <= 1e-6 * np.abs(t1[1:]).max()
