@@ -19,6 +19,10 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# Checkout of the reference project (its source/ and PP/ trees), read by the
+# oracle/_ref build and by the CPU tests that compare with its shipped files.
+# Set QSB_REFERENCE_ROOT where it lives elsewhere; absent, those tests skip.
+REFERENCE_ROOT = os.environ.get("QSB_REFERENCE_ROOT", "/root/reference")
 LIB_ORACLE = os.path.join(HERE, "_build", "libqsoracle.so")
 LIB_REF = os.path.join(HERE, "_ref", "libqsref.so")
 

@@ -161,7 +161,14 @@ qsb_status qsb_ham_create(qsb_ham** ham, int nx, int ny, int nz, double dx, doub
     *ham = nullptr;
     QSB_TRY(check_grid(nx, ny, nz));
     if (dx <= 0 || dy <= 0 || dz <= 0) return fail(QSB_ERR_INVALID, "ham_create: spacing must be > 0");
+    // the device the tables will live on (host-only checks also work without one)
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        dev = -1;
+        cudaGetLastError();
+    }
     qsb_ham* h = new qsb_ham();
+    h->device = dev;
     h->nx = nx; h->ny = ny; h->nz = nz;
     h->N = (size_t)nx * ny * nz;
     h->dx = dx; h->dy = dy; h->dz = dz;
@@ -315,12 +322,16 @@ static qsb_status timing_event(qsb_ham* h, cudaStream_t s) {
     return QSB_OK;
 }
 
-static qsb_status check_apply(qsb_ham* h, qsb_dtype dtype, int nb, const void* a, const void* b) {
+}  // extern "C"
+
+qsb_status qsb::check_apply(qsb_ham* h, qsb_dtype dtype, int nb, const void* a, const void* b) {
     if (!h) return fail(QSB_ERR_INVALID, "null context");
     if (dtype != QSB_F64 && dtype != QSB_F32) return fail(QSB_ERR_INVALID, "bad dtype");
     if (nb < 0 || (nb > 0 && (!a || !b))) return fail(QSB_ERR_INVALID, "bad bands/pointers");
     return QSB_OK;
 }
+
+extern "C" {
 
 qsb_status qsb_ham_apply(qsb_ham* h, qsb_dtype dtype, int is_complex, int nb, const void* psi_dev, void* hpsi_dev,
                          double gx, double gy, double gz, void* stream) {

@@ -30,10 +30,9 @@ constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mutex;
 void* g_scratch_addr[kMaxDevices] = {nullptr};
 
-// Device address of the scratch on the current device, looked up once per device.
-qsb_status static_scratch(void** out) {
-    int dev = -1;
-    QSB_CUDA_TRY(cudaGetDevice(&dev));
+// Device address of the scratch on device `dev` (the current one), looked up
+// once per device.
+qsb_status static_scratch(int dev, void** out) {
     if (dev < 0 || dev >= kMaxDevices) return qsb::fail(QSB_ERR_INVALID, "nonlocal_apply_static: device index out of range");
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
     if (!g_scratch_addr[dev]) {
@@ -51,10 +50,14 @@ qsb_status static_scratch(void** out) {
 extern "C" qsb_status qsb_ham_nonlocal_apply_static(qsb_ham* h, qsb_dtype dtype, int is_complex, int nb,
                                                     const void* psi_dev, void* hpsi_dev, double gx, double gy,
                                                     double gz, void* stream) {
-    if (!h) return qsb::fail(QSB_ERR_INVALID, "nonlocal_apply_static: null context");
-    if (dtype != QSB_F64 && dtype != QSB_F32) return qsb::fail(QSB_ERR_INVALID, "nonlocal_apply_static: bad dtype");
-    if (nb < 0 || (nb > 0 && (!psi_dev || !hpsi_dev)))
-        return qsb::fail(QSB_ERR_INVALID, "nonlocal_apply_static: bad bands/pointers");
+    QSB_TRY(qsb::check_apply(h, dtype, nb, psi_dev, hpsi_dev));
+    // the projector tables live on the device the context was created on; the
+    // scratch must be that device's copy of the array
+    int dev = -1;
+    QSB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != h->device)
+        return qsb::fail(QSB_ERR_STATE, "nonlocal_apply_static: current device " + std::to_string(dev) +
+                                            " is not the context's device " + std::to_string(h->device));
     if (nb == 0 || h->nl.n_points == 0) return QSB_OK;
     if (!is_complex) gx = gy = gz = 0.0;
     const int ncol = is_complex ? 2 * nb : nb;
@@ -65,7 +68,7 @@ extern "C" qsb_status qsb_ham_nonlocal_apply_static(qsb_ham* h, qsb_dtype dtype,
                                               std::to_string((size_t)QSB_NL_STATIC_SCRATCH_BYTES) +
                                               " (use fewer bands per call, or qsb_ham_nonlocal_apply)");
     void* ws = nullptr;
-    QSB_TRY(static_scratch(&ws));
+    QSB_TRY(static_scratch(dev, &ws));
     cudaStream_t s = (cudaStream_t)stream;
     double* coef = nullptr;
     QSB_TRY(qsb::nl_project(dtype, h->nl, h->nx, h->ny, h->nz, nb, is_complex, psi_dev, h->dx * h->dy * h->dz,

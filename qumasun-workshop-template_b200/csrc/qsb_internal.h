@@ -57,6 +57,10 @@ int* device_error_word();
 
 qsb_status launch_stencil(qsb_dtype dt, const StencilLaunch& L, const FD8Coef& c, cudaStream_t s);
 
+// Argument checks shared by the apply entry points (context, dtype, band count
+// and the two bundle pointers).
+qsb_status check_apply(qsb_ham* h, qsb_dtype dtype, int nb, const void* a, const void* b);
+
 // Device-side nonlocal tables (owned by qsb_ham).
 struct NLDevice {
     int n_atoms = 0;
@@ -192,6 +196,7 @@ qsb_status gram_bf16x3(qsb_dtype dt, int64_t N, int p, int q, const void* U, con
 }  // namespace qsb
 
 struct qsb_ham {
+    int device = -1;                       // CUDA device current at qsb_ham_create (holds the tables)
     int nx = 0, ny = 0, nz = 0;
     size_t N = 0;
     double dx = 0, dy = 0, dz = 0;

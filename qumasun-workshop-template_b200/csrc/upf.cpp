@@ -381,6 +381,8 @@ qsb_status qsb_radial_local_table(int n_r, const double* radius, const double* v
                                  int n_g, double dg, double* table) {
     if (n_r < 5 || !radius || !v || !table || n_g <= 0 || !(dg > 0) || !(sigma > 0))
         return fail(QSB_ERR_INVALID, "radial_local_table: bad argument");
+    if (!(radius[0] > 0.0) || !(radius[1] > radius[0]))
+        return fail(QSB_ERR_INVALID, "radial_local_table: radius must start above 0 and increase");
     // log grid: r_i = r_0 exp(i dxi); integrals in xi with dr = r dxi (Simpson,
     // trapezoid on a last odd interval)
     const double dxi = std::log(radius[1] / radius[0]);

@@ -16,7 +16,7 @@ import pytest
 
 import oracle as O
 
-PP_DIR = "/root/reference/PP/nc-sr-05_pbe_standard_upf"
+PP_DIR = os.path.join(O.REFERENCE_ROOT, "PP", "nc-sr-05_pbe_standard_upf")
 needs_pp = pytest.mark.skipif(not (O.ref_available() and os.path.isdir(PP_DIR)),
                               reason="needs the reference's UPF files and oracle/_ref")
 SPECIES = ["C", "Al", "Au", "Bi", "Ba", "O", "Si"]
@@ -153,6 +153,22 @@ def test_local_table_equals_the_analytic_gth_transform(qsb_host):
     for sigma in (0.3, 0.45, 0.8):
         t = qsb_host.radial_local_table(r, V, Z, 400, 0.05, sigma)
         assert np.abs(t - ana).max() <= 1e-9, sigma
+
+
+def test_local_table_rejects_a_grid_that_does_not_start_above_zero_and_increase(qsb_host):
+    """A decreasing radius would flip the sign of the Simpson sums and a
+    radius <= 0 has no logarithm: both are argument errors."""
+    r = np.exp(-9 + np.arange(200) * 0.05)
+    V = -1.0 / r
+    with pytest.raises(qsb_host.QsbError, match="increase"):
+        qsb_host.radial_local_table(r[::-1].copy(), V[::-1].copy(), 1.0, 10, 0.1, 0.5)
+    r0 = r.copy()
+    r0[0] = 0.0
+    with pytest.raises(qsb_host.QsbError, match="increase"):
+        qsb_host.radial_local_table(r0, V, 1.0, 10, 0.1, 0.5)
+    r0[0] = -r[0]
+    with pytest.raises(qsb_host.QsbError, match="increase"):
+        qsb_host.radial_local_table(r0, V, 1.0, 10, 0.1, 0.5)
 
 
 @needs_pp

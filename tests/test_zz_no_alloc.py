@@ -60,10 +60,15 @@ def test_static_scratch_rejects_oversized_requests(qsb):
     H.set_potential(O.seeded_potential(4, n ** 3))
     H.set_gth_projectors(O.bcc_positions(6.0, 1), [0, 0], [2], [O.GTH_BCC["r"]], [O.GTH_BCC["h"]], O.RCUT_FACTOR)
     # 2 atoms of one chunk each, 4 projectors: 128 B of scratch per column, so
-    # 40000 real bands need 5 MB > 4 MiB (the buffers are real, 1.3 GB each)
+    # 40000 real bands need 5 MB > 4 MiB.  The size check comes before any
+    # device access, so one small buffer stands in for both bundles.
     nb = 40000
-    psi = torch.empty(nb, n ** 3, dtype=torch.float64, device="cuda")
-    with pytest.raises(qsb.QsbError, match="static scratch holds"):
-        _call(qsb, qsb.lib.qsb_ham_nonlocal_apply_static, H, psi, torch.empty_like(psi), False, (0.0, 0.0, 0.0))
-    del psi
-    torch.cuda.empty_cache()
+    buf = torch.zeros(16, dtype=torch.float64, device="cuda")
+    ptr = ctypes.c_void_p(buf.data_ptr())
+    st = qsb.lib.qsb_ham_nonlocal_apply_static(H._h, 0, 0, nb, ptr, ptr, ctypes.c_double(0.0), ctypes.c_double(0.0),
+                                               ctypes.c_double(0.0),
+                                               ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert st == 1                                   # QSB_ERR_INVALID
+    assert "static scratch holds" in qsb.lib.qsb_last_error().decode()
+    torch.cuda.synchronize()
+    assert buf.abs().sum().item() == 0.0             # nothing was touched
