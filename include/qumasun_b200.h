@@ -273,13 +273,17 @@ typedef int (*qsb_apply_f32_fn)(void* user, int nb, const float* x_dev, float* a
 QSB_API qsb_status qsb_eigensolver_set_operator_f32(qsb_eigensolver* es, qsb_apply_f32_fn op, void* user);
 /* Iterations done by the last solve, and whether it ended with the norm-check rollback. */
 QSB_API qsb_status qsb_eigensolver_last_stats(const qsb_eigensolver* es, int* iterations, int* rolled_back);
-/* QSB_PREC_MIXED only.  The Rayleigh-Ritz step scales the pencil to a unit
+/* Overlap-basis fallback of the Rayleigh-Ritz step.  When the Cholesky of
+ * ZHEGVD / DSYGVD finds the overlap matrix not positive definite (mixed
+ * precision: on the unit-diagonal-scaled pencil, where the tensor-core Gram
+ * errors, ~2^-17 / sqrt(N) of the diagonal for split-BF16x3, make it fail once
+ * the basis [X R P] turns ill-conditioned near convergence; FP64: a search
+ * basis that has become numerically dependent, as when a run is continued
+ * from states of another precision), the step scales the pencil to a unit
  * diagonal, eigendecomposes the overlap matrix and drops the directions whose
  * overlap eigenvalue is below tol * (largest); the Ritz pairs are taken in the
  * rest (Stathopoulos-Wu's SVQB basis, as Hetmaniuk-Lehoucq use it in LOBPCG).
- * This replaces the Cholesky of ZHEGVD, which the split-BF16x3 overlap errors
- * (~2^-17 / sqrt(N) of the diagonal) make fail once the basis [X R P] turns
- * ill-conditioned near convergence.  Default: 1e-5 / sqrt(N) within [1e-8, 1e-5]. */
+ * Default: mixed 1e-5 / sqrt(N) within [1e-8, 1e-5]; FP64 1e-12. */
 QSB_API qsb_status qsb_eigensolver_set_drop_tolerance(qsb_eigensolver* es, double tol);
 /* QSB_PREC_MIXED: how the Gram / Rayleigh-Ritz products are formed.
  *   QSB_GRAM_BF16X3     split-BF16x3 on the tensor cores (qsb_gram_bf16x3)
@@ -293,10 +297,10 @@ QSB_API qsb_status qsb_eigensolver_set_drop_tolerance(qsb_eigensolver* es, doubl
  * BF16 solvers diverge, the INT8 one converges. */
 typedef enum qsb_gram_kind { QSB_GRAM_BF16X3 = 3, QSB_GRAM_BF16X4 = 4, QSB_GRAM_INT8_OZAKI = 8 } qsb_gram_kind;
 QSB_API qsb_status qsb_eigensolver_set_gram_kind(qsb_eigensolver* es, qsb_gram_kind kind);
-/* Of the last call (mixed precision): how many Rayleigh-Ritz steps were solved
- * by the Cholesky route (?hegvd on the unit-diagonal-scaled pencil, tried
- * first) and how many fell back to the overlap-basis solve because that
- * Cholesky found the overlap not positive definite. */
+/* Of the last call: how many Rayleigh-Ritz steps were solved by the Cholesky
+ * route (?hegvd / ?sygvd; mixed precision: on the unit-diagonal-scaled pencil)
+ * and how many fell back to the overlap-basis solve because that Cholesky found
+ * the overlap not positive definite. */
 QSB_API qsb_status qsb_eigensolver_solve_stats(const qsb_eigensolver* es, int* cholesky_solves,
                                                int* overlap_basis_solves);
 /* Of the last call (mixed precision): most directions dropped in one
@@ -433,6 +437,24 @@ QSB_API qsb_status qsb_scf_set_smearing(qsb_scf* scf, double kbt);
  * reference's RHO_ETOT convergence mode, source/qumasun_kpoint.scfloop.h:182-213);
  * 0 (default) stops on the energy alone. */
 QSB_API qsb_status qsb_scf_set_density_tolerance(qsb_scf* scf, double rho_tol);
+/* FP64 polish of a mixed-precision run: once the run meets its own stop
+ * (|dE| / atom below qsb_scf_run's tol and, if set, the density tolerance) the
+ * loop goes on with es_fp64 -- a real QSB_PREC_FP64 solver context of the
+ * SCF's grid and at least its bands -- from the mixed run's states and mixed
+ * density, for at most max_steps further steps (counted within qsb_scf_run's
+ * max_steps), until |dE| / atom < tol_per_atom (0: the run's tol) and
+ * int |rho_out - rho_in| dV / N_e < rho_tol (0: the energy alone).  The first
+ * FP64 call starts without the kept search directions (P = 0, the [X R]
+ * pencil), as at an SCF's first step.  FP32 rounding in the mixed solver's
+ * states sets a floor under its density residual (~1e-8 N_e) and so under its
+ * force error; the polish takes the end point to the FP64 one.  es_fp64 = NULL
+ * or max_steps = 0 switches the polish off (the default).  No counterpart in
+ * the reference (its solver has one precision). */
+QSB_API qsb_status qsb_scf_set_polish(qsb_scf* scf, qsb_eigensolver* es_fp64, int max_steps, double tol_per_atom,
+                                      double rho_tol);
+/* Of the last qsb_scf_run: index of the first FP64 polish step (-1: none) and
+ * how many polish steps ran. */
+QSB_API qsb_status qsb_scf_polish_stats(const qsb_scf* scf, int* first_step, int* steps);
 QSB_API qsb_status qsb_scf_run(qsb_scf* scf, double* X, double* keep, int lobpcg_iters, int max_steps,
                                double tol_per_atom, double* energies, int* steps, double* eigen_values,
                                double* occupations, void* stream);

@@ -655,6 +655,32 @@ qsb_status solve_pencil_overlap_basis(qsb_eigensolver* es, int m, int nout, cuda
     return QSB_OK;
 }
 
+// The FP64 solvers' Rayleigh-Ritz step: ZHEGVD / DSYGVD (the reference's
+// lapack_ZHEGVD / lapack_DSYGVX route) on the pencil as formed.  If its Cholesky
+// finds the overlap not positive definite (a search basis [X R P] that has
+// turned numerically dependent, e.g. when a run is continued from states of
+// another precision), the same pencil is solved on its well-conditioned part
+// by the overlap-basis route instead of failing the call.  The reference prints
+// the LAPACK info and carries on with the garbage; here the step stays defined.
+qsb_status solve_pencil_fp64(qsb_eigensolver* es, int m, int nout, cudaStream_t s) {
+    const size_t mm = (size_t)m * m * (es->cplx ? 2 : 1);
+    double* Sa0 = es->svq;
+    double* Sb0 = Sa0 + mm;
+    QSB_CUDA_TRY(cudaMemcpyAsync(Sa0, es->Sa, sizeof(double) * mm, cudaMemcpyDeviceToDevice, s));
+    QSB_CUDA_TRY(cudaMemcpyAsync(Sb0, es->Sb, sizeof(double) * mm, cudaMemcpyDeviceToDevice, s));
+    const std::string saved_error = qsb_last_error();
+    const qsb_status st = solve_pencil(es, m, s);
+    if (st == QSB_OK) {
+        ++es->last_chol;
+        return QSB_OK;
+    }
+    if (st != QSB_ERR_SOLVER) return st;
+    set_last_error(saved_error);
+    QSB_CUDA_TRY(cudaMemcpyAsync(es->Sa, Sa0, sizeof(double) * mm, cudaMemcpyDeviceToDevice, s));
+    QSB_CUDA_TRY(cudaMemcpyAsync(es->Sb, Sb0, sizeof(double) * mm, cudaMemcpyDeviceToDevice, s));
+    return solve_pencil_overlap_basis(es, m, nout, s);
+}
+
 // a[i] /= b[i]
 __global__ void divide_by(double* __restrict__ a, const double* __restrict__ b, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1000,6 +1026,13 @@ qsb_status lobpcg_z_mixed(qsb_eigensolver* es, double dVol, int n, int iter_max,
 }  // namespace
 }  // namespace qsb
 
+void qsb::eigensolver_shape(const qsb_eigensolver* es, int64_t* N, int* nmax, int* cplx, int* mixed) {
+    *N = es->N;
+    *nmax = es->nmax;
+    *cplx = es->cplx;
+    *mixed = es->mixed;
+}
+
 extern "C" {
 
 qsb_status qsb_eigensolver_create(qsb_eigensolver** out, int64_t N, int n, int is_complex) {
@@ -1052,14 +1085,19 @@ qsb_status qsb_eigensolver_create_ex(qsb_eigensolver** out, int64_t N, int n, in
             cudaMalloc(&es->gpart, es->gpart_bytes) != cudaSuccess ||
             cudaMalloc((void**)&es->T2, sizeof(double) * (size_t)pmax * pmax) != cudaSuccess ||
             cudaMalloc((void**)&es->rc32, sizeof(float) * (size_t)6 * 2 * n * n) != cudaSuccess ||
-            cudaMalloc((void**)&es->svq, sizeof(double) * ((size_t)3 * (3 * n) * (3 * n) * c2 + 2 * (3 * n))) !=
-                cudaSuccess ||
             cudaMalloc((void**)&es->rotw, sizeof(double) * ((size_t)(3 * n) * (3 * n) * c2 +
                                                             (size_t)2 * (3 * n * c2) * (2 * n * c2) + 2 * n * c2)) !=
                 cudaSuccess ||
             cudaMalloc(&es->rotc, es->rotc_bytes = ozaki_rot_coef_bytes(3 * n * c2, 2 * n * c2)) != cudaSuccess)
             return cleanup(fail(QSB_ERR_NOMEM, "eigensolver: mixed-precision workspace allocation"));
     }
+    // overlap-basis pencil solve (both precisions: the mixed solver's route, the
+    // FP64 solvers' fallback); FP64 Gram entries are exact to ~1e-16 of the
+    // diagonal, so only directions below 1e-12 of the largest are dropped there
+    if (cudaMalloc((void**)&es->svq, sizeof(double) * ((size_t)3 * (3 * n) * (3 * n) * c2 + 2 * (3 * n))) !=
+        cudaSuccess)
+        return cleanup(fail(QSB_ERR_NOMEM, "eigensolver: pencil workspace allocation"));
+    if (!es->mixed) es->drop_tol = 1e-12;
     const int m = 3 * n;
     const size_t cm = (size_t)m * m * (is_complex ? 2 : 1);
     const size_t tsz = (size_t)(2 * n) * (2 * n);
@@ -1135,7 +1173,6 @@ qsb_status qsb_eigensolver_set_operator_f32(qsb_eigensolver* es, qsb_apply_f32_f
 
 qsb_status qsb_eigensolver_set_drop_tolerance(qsb_eigensolver* es, double tol) {
     if (!es) return fail(QSB_ERR_INVALID, "set_drop_tolerance: null solver");
-    if (!es->mixed) return fail(QSB_ERR_STATE, "set_drop_tolerance: only mixed-precision contexts drop directions");
     if (!(tol > 0.0 && tol < 1.0)) return fail(QSB_ERR_INVALID, "set_drop_tolerance: needs 0 < tol < 1");
     es->drop_tol = tol;
     return QSB_OK;
@@ -1271,7 +1308,7 @@ qsb_status qsb_lobpcg_z(qsb_eigensolver* es, double dVol, int n, int iter_max, d
                     QSB_TRY(gram_block(es, U[I], AU[J], N_, es->Sa, m, I, J, 1.0, s));
                     QSB_TRY(gram_block(es, U[I], U[J], N_, es->Sb, m, I, J, 1.0, s));
                 }
-            QSB_TRY(solve_pencil(es, m, s));   // ZHEGVD (:2254-2263 / :2492-2511)
+            QSB_TRY(solve_pencil_fp64(es, m, N_, s));   // ZHEGVD (:2254-2263 / :2492-2511)
             QSB_TRY(make_coefficients(es, N_, m, nblk, s));
             // P' = R Cr + P Cp (into TMP), P = TMP; TMP += X Cx  (NextVector_z2)
             QSB_TRY(rotate_complex(es, N_, es->TMP, U[1], 1, 0.0, s));
@@ -1407,7 +1444,7 @@ qsb_status qsb_lobpcg_d(qsb_eigensolver* es, double dVol, int n, int iter_max, d
                 QSB_TRY(gram_block(es, U[I], AU[J], n, es->Sa, m, I, J, dVol, s));
                 QSB_TRY(gram_block(es, U[I], U[J], n, es->Sb, m, I, J, dVol, s));
             }
-        QSB_TRY(solve_pencil(es, m, s));   // DSYGVX, lowest n (:209, :284)
+        QSB_TRY(solve_pencil_fp64(es, m, n, s));   // DSYGVX, lowest n (:209, :284)
         QSB_TRY(make_coefficients(es, n, m, nblk, s));
         // P = R Cr (+ P Cp); X = X Cx + P; same for A-bundles (:226-365)
         QSB_TRY(rotate_real(es, n, es->TMP, es->R, 1, 0.0, s));

@@ -228,6 +228,8 @@ struct qsb_ham {
 };
 
 namespace qsb {
+// Shape of a solver context (lobpcg.cu): grid points, bands, complex, mixed precision.
+void eigensolver_shape(const qsb_eigensolver* es, int64_t* N, int* nmax, int* cplx, int* mixed);
 // FFT kinetic term of qsb_ham_apply (kinetic_fft.cu): hpsi = -1/2 (grad + i g)^2 psi
 // + V psi ("=" semantics; the nonlocal part is added by the caller).
 qsb_status kinetic_fft_apply(qsb_ham* h, qsb_dtype dtype, int is_complex, int nb, const void* psi, void* hpsi,

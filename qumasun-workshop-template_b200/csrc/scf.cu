@@ -337,6 +337,12 @@ struct qsb_scf {
     double n_el = 0, kbt = 0.01;
     double amp = 0.5, q0 = 0.8;
     double rho_tol = 0.0;         // int |rho_out - rho_in| / N_e bound of the stop (0: off)
+    // FP64 polish of a mixed-precision run (qsb_scf_set_polish)
+    qsb_eigensolver* polish_es = nullptr;
+    int polish_max = 0;
+    double polish_tol = 0.0;      // |dE| / atom of the polish's stop (0: the run's)
+    double polish_rho_tol = 0.0;
+    int last_polish_first = -1, last_polish_steps = 0;
     int depth = 6;
     int n_atoms = 0;
     // device fields
@@ -634,6 +640,35 @@ qsb_status qsb_scf_set_density_tolerance(qsb_scf* c, double rho_tol) {
     return QSB_OK;
 }
 
+qsb_status qsb_scf_set_polish(qsb_scf* c, qsb_eigensolver* es_fp64, int max_steps, double tol_per_atom,
+                              double rho_tol) {
+    if (!c) return fail(QSB_ERR_INVALID, "scf_set_polish: null context");
+    if (!es_fp64 || max_steps <= 0) {
+        c->polish_es = nullptr;
+        c->polish_max = 0;
+        return QSB_OK;
+    }
+    if (!(rho_tol >= 0.0) || !(tol_per_atom >= 0.0))
+        return fail(QSB_ERR_INVALID, "scf_set_polish: need tol_per_atom >= 0 and rho_tol >= 0");
+    int64_t N = 0;
+    int nmax = 0, cplx = 0, mixed = 0;
+    eigensolver_shape(es_fp64, &N, &nmax, &cplx, &mixed);
+    if (mixed || cplx || (size_t)N != c->N || nmax < c->nb)
+        return fail(QSB_ERR_INVALID, "scf_set_polish: needs a real FP64 solver context of the SCF's grid and bands");
+    c->polish_es = es_fp64;
+    c->polish_max = max_steps;
+    c->polish_tol = tol_per_atom;
+    c->polish_rho_tol = rho_tol;
+    return QSB_OK;
+}
+
+qsb_status qsb_scf_polish_stats(const qsb_scf* c, int* first_step, int* steps) {
+    if (!c) return fail(QSB_ERR_INVALID, "scf_polish_stats: null context");
+    if (first_step) *first_step = c->last_polish_first;
+    if (steps) *steps = c->last_polish_steps;
+    return QSB_OK;
+}
+
 qsb_status qsb_scf_set_smearing(qsb_scf* c, double kbt) {
     if (!c || !(kbt > 0.0)) return fail(QSB_ERR_INVALID, "scf_set_smearing: need kbT > 0");
     c->kbt = kbt;
@@ -722,6 +757,10 @@ qsb_status qsb_scf_run(qsb_scf* c, double* X, double* keep, int lobpcg_iters, in
         return fail(QSB_ERR_INVALID, "scf_run: bad argument");
     if (c->n_atoms <= 0) return fail(QSB_ERR_STATE, "scf_run: no local potential (qsb_scf_set_gth_local)");
     QSB_TRY(qsb_eigensolver_set_hamiltonian(c->es, c->ham, 0.0, 0.0, 0.0));
+    if (c->polish_es) QSB_TRY(qsb_eigensolver_set_hamiltonian(c->polish_es, c->ham, 0.0, 0.0, 0.0));
+    c->last_polish_first = -1;
+    c->last_polish_steps = 0;
+    bool polishing = false;
     cudaStream_t s = (cudaStream_t)stream;
     const int nb = c->nb;
     const size_t N = c->N;
@@ -747,7 +786,12 @@ qsb_status qsb_scf_run(qsb_scf* c, double* X, double* keep, int lobpcg_iters, in
     auto t_prev = std::chrono::steady_clock::now();
     for (int step = 0; step < max_steps; ++step) {
         QSB_TRY(potentials(c, s));
-        QSB_TRY(qsb_lobpcg_d(c->es, c->dV, nb, lobpcg_iters, ev.data(), X, keep, step == 0 ? 1 : 0, stream));
+        // the polish's first FP64 call starts without search directions: the kept
+        // P of the mixed solver is a direction of its FP32 iterations
+        const bool fresh = step == 0 || (polishing && c->last_polish_steps == 0);
+        QSB_TRY(qsb_lobpcg_d(polishing ? c->polish_es : c->es, c->dV, nb, lobpcg_iters, ev.data(), X, keep,
+                             fresh ? 1 : 0, stream));
+        if (polishing) ++c->last_polish_steps;
         // FP64 Rayleigh quotients of the states (the energy and the occupations use these)
         QSB_TRY(qsb_ham_apply(c->ham, QSB_F64, 0, nb, X, c->hx, 0.0, 0.0, 0.0, stream));
         band_dot_kernel<<<dim3(RBLOCKS / 4, nb), RB, 0, s>>>(N, X, c->hx, c->partial, c->partial + (size_t)nb * (RBLOCKS / 4));
@@ -784,17 +828,26 @@ qsb_status qsb_scf_run(qsb_scf* c, double* X, double* keep, int lobpcg_iters, in
         const auto t_now = std::chrono::steady_clock::now();
         c->step_s.push_back(std::chrono::duration<double>(t_now - t_prev).count());
         t_prev = t_now;
-        bool done = step > 0 && std::fabs(etot - e_prev) / c->n_atoms < tol_per_atom;
-        if (done && c->rho_tol > 0.0) {
+        const double etol = polishing && c->polish_tol > 0.0 ? c->polish_tol : tol_per_atom;
+        bool done = step > 0 && std::fabs(etot - e_prev) / c->n_atoms < etol;
+        const double rho_tol = polishing ? c->polish_rho_tol : c->rho_tol;
+        if (done && rho_tol > 0.0) {
             // and the density residual (CONVERGENCE_MODE::RHO_ETOT of the reference's loop)
             l1_diff_partial_kernel<<<RBLOCKS, RB, 0, s>>>(N, c->rho_out, c->rho_in, c->partial);
             row_sum_kernel<<<1, 32, 0, s>>>(1, RBLOCKS, c->partial, c->sums);
             double l1 = 0.0;
             QSB_CUDA_TRY(cudaMemcpyAsync(&l1, c->sums, sizeof(double), cudaMemcpyDeviceToHost, s));
             QSB_CUDA_TRY(cudaStreamSynchronize(s));
-            done = l1 * c->dV / c->n_el < c->rho_tol;
+            done = l1 * c->dV / c->n_el < rho_tol;
         }
         e_prev = etot;
+        if (polishing && c->last_polish_steps >= c->polish_max) done = true;
+        if (done && !polishing && c->polish_es && step + 1 < max_steps) {
+            // the mixed run has met its stop: go on in FP64 from its states and density
+            polishing = true;
+            c->last_polish_first = step + 1;
+            done = false;
+        }
         if (done) break;
         QSB_TRY(mix(c, s));
     }

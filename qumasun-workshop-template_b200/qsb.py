@@ -601,6 +601,19 @@ class SCF:
     def set_smearing(self, kbt):
         _check(lib.qsb_scf_set_smearing(self._h, _c_d(kbt)))
 
+    def set_polish(self, solver_fp64, max_steps=10, tol_per_atom=0.0, rho_tol=0.0):
+        """FP64 polish of a mixed run (qsb_scf_set_polish); solver_fp64=None switches it off."""
+        self._polish = solver_fp64
+        _check(lib.qsb_scf_set_polish(self._h, solver_fp64._h if solver_fp64 is not None else None,
+                                      max_steps if solver_fp64 is not None else 0, _c_d(tol_per_atom),
+                                      _c_d(rho_tol)))
+
+    def polish_stats(self):
+        """(first polish step or -1, polish steps) of the last run."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        _check(lib.qsb_scf_polish_stats(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def run(self, X, keep, lobpcg_iters=4, max_steps=60, tol_per_atom=1e-6):
         """Runs to |dE|/atom < tol; X, keep: [nb, N] fp64 CUDA (updated in place).
         Returns (energies per step, final Rayleigh quotients, occupations)."""
