@@ -433,6 +433,17 @@ QSB_API qsb_status qsb_scf_set_gth_local(qsb_scf* scf, int n_atoms, const double
                                          const double* c2);
 QSB_API qsb_status qsb_scf_set_mixing(qsb_scf* scf, double amplitude, double q0, int depth);
 QSB_API qsb_status qsb_scf_set_smearing(qsb_scf* scf, double kbt);
+/* The SCF's LDA.  pz_variant 0 (default): Perdew-Zunger with the published
+ * constants, as Calc_XC_LDA (source/Vxc.h:43-75) has them; its two correlation
+ * branches miss each other at rs = 1 by 3.2e-5 Ha in eps_c, so the energy
+ * jumps by (3 / 4 pi) dV 3.2e-5 Ha whenever a grid point's density crosses
+ * 3 / (4 pi) -- as atoms move, central differences of the energy see these
+ * steps.  pz_variant 1: the high-density branch's C and D solved from value
+ * and slope continuity at rs = 1 (C = 0.0020191519, D = -0.0116320664; A, B
+ * and the low-density branch unchanged), which leaves the energy a smooth
+ * function of the positions.  rho_min (default 1e-8, Calc_XC_LDA's cut,
+ * >= 1e-30): exc = vxc = 0 below it. */
+QSB_API qsb_status qsb_scf_set_xc(qsb_scf* scf, int pz_variant, double rho_min);
 /* Also require int |rho_out - rho_in| dV / N_e < rho_tol to stop (the
  * reference's RHO_ETOT convergence mode, source/qumasun_kpoint.scfloop.h:182-213);
  * 0 (default) stops on the energy alone. */
@@ -500,6 +511,10 @@ QSB_API qsb_status qsb_relax_lbfgs(qsb_scf* scf, int n_atoms, double* pos, const
 /* Wall seconds of each step of the last qsb_scf_run (host clock; a step ends
  * when its energy is on the host): up to max values, *n = steps recorded. */
 QSB_API qsb_status qsb_scf_step_seconds(qsb_scf* scf, double* seconds, int max, int* n);
+/* Density residual int |rho_out - rho_in| dV / N_e of each step of the last
+ * qsb_scf_run (the quantity of qsb_scf_set_density_tolerance), up to max
+ * values; *n = steps recorded. */
+QSB_API qsb_status qsb_scf_step_residuals(qsb_scf* scf, double* residuals, int max, int* n);
 
 /* ---------------------------------------------------------------------------
  * UPF (v2, ONCV norm-conserving) pseudopotentials (host code; no device work).

@@ -49,8 +49,14 @@ __global__ void density_kernel(size_t N, int nb, const double* __restrict__ X, c
 }
 
 // Perdew-Zunger LDA (Calc_XC_LDA, source/Vxc.h:43-75): exc = rho eps_xc, vxc = V_x + V_c
-__device__ __forceinline__ void lda_pz_point(double rho, double& exc, double& vxc) {
-    if (rho < 1.0e-8) {
+// continuous = true: the high-density correlation branch with C and D solved
+// from value and slope continuity at rs = 1 (A, B kept); with the published
+// C = 0.0020, D = -0.0116 the two branches miss each other there by 3.2e-5 Ha
+// in eps_c, so E_xc jumps by rho dV 3.2e-5 whenever a grid point's density
+// crosses 3 / (4 pi).
+__device__ __forceinline__ void lda_pz_point(double rho, double& exc, double& vxc, double rho_min = 1.0e-8,
+                                             bool continuous = false) {
+    if (rho < rho_min) {
         exc = 0.0;
         vxc = 0.0;
         return;
@@ -66,7 +72,9 @@ __device__ __forceinline__ void lda_pz_point(double rho, double& exc, double& vx
         ec = g / (1.0 + b1 * s + b2 * rs);
         ndec = ec * ec * (b1 * 0.5 * s + b2 * rs) / (3.0 * g);
     } else {
-        const double A = 0.0311, B = -0.0480, C = 0.0020, D = -0.0116;
+        const double A = 0.0311, B = -0.0480;
+        const double C = continuous ? 0.0020191519406228 : 0.0020;
+        const double D = continuous ? -0.0116320663789130 : -0.0116;
         const double lr = log(rs);
         ec = B + A * lr + D * rs + C * rs * lr;
         ndec = -(A + (D + C) * rs + C * rs * lr) / 3.0;
@@ -76,10 +84,10 @@ __device__ __forceinline__ void lda_pz_point(double rho, double& exc, double& vx
 }
 
 __global__ void lda_kernel(size_t N, const double* __restrict__ rho, double* __restrict__ exc,
-                           double* __restrict__ vxc) {
+                           double* __restrict__ vxc, double rho_min = 1.0e-8, bool continuous = false) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
         double e, v;
-        lda_pz_point(rho[i], e, v);
+        lda_pz_point(rho[i], e, v, rho_min, continuous);
         if (exc) exc[i] = e;
         vxc[i] = v;
     }
@@ -337,6 +345,8 @@ struct qsb_scf {
     double n_el = 0, kbt = 0.01;
     double amp = 0.5, q0 = 0.8;
     double rho_tol = 0.0;         // int |rho_out - rho_in| / N_e bound of the stop (0: off)
+    double xc_rho_min = 1.0e-8;   // LDA: exc = vxc = 0 below this density (Calc_XC_LDA's cut)
+    bool xc_continuous = false;   // PZ correlation made continuous at rs = 1 (qsb_scf_set_xc)
     // FP64 polish of a mixed-precision run (qsb_scf_set_polish)
     qsb_eigensolver* polish_es = nullptr;
     int polish_max = 0;
@@ -358,6 +368,7 @@ struct qsb_scf {
     std::vector<int> slots;       // history slots, oldest first
     std::vector<double> B;        // depth x depth residual inner products (by slot)
     std::vector<double> step_s;   // wall seconds of each step of the last run
+    std::vector<double> step_res; // int |rho_out - rho_in| dV / N_e of each step of the last run
 };
 
 namespace qsb {
@@ -399,7 +410,8 @@ qsb_status kspace(qsb_scf* c, KOp op, const double* in, double* out, cudaStream_
 // veff = vloc + V_H[rho_in] + V_xc[rho_in]
 qsb_status potentials(qsb_scf* c, cudaStream_t s) {
     QSB_TRY(kspace(c, KOp::hartree, c->rho_in, c->vh, s));
-    lda_kernel<<<pw_blocks(c->N), 256, 0, s>>>(c->N, c->rho_in, nullptr, c->vxc);
+    lda_kernel<<<pw_blocks(c->N), 256, 0, s>>>(c->N, c->rho_in, nullptr, c->vxc, c->xc_rho_min,
+                                                c->xc_continuous);
     sum3_kernel<<<pw_blocks(c->N), 256, 0, s>>>(c->N, c->vloc, c->vh, c->vxc, c->veff);
     QSB_CUDA_TRY(cudaGetLastError());
     return qsb_ham_set_potential(c->ham, c->veff, 1);
@@ -669,6 +681,14 @@ qsb_status qsb_scf_polish_stats(const qsb_scf* c, int* first_step, int* steps) {
     return QSB_OK;
 }
 
+qsb_status qsb_scf_set_xc(qsb_scf* c, int pz_variant, double rho_min) {
+    if (!c || (pz_variant != 0 && pz_variant != 1) || !(rho_min >= 1e-30))
+        return fail(QSB_ERR_INVALID, "scf_set_xc: need pz_variant 0 or 1 and rho_min >= 1e-30");
+    c->xc_continuous = pz_variant == 1;
+    c->xc_rho_min = rho_min;
+    return QSB_OK;
+}
+
 qsb_status qsb_scf_set_smearing(qsb_scf* c, double kbt) {
     if (!c || !(kbt > 0.0)) return fail(QSB_ERR_INVALID, "scf_set_smearing: need kbT > 0");
     c->kbt = kbt;
@@ -735,6 +755,13 @@ qsb_status qsb_scf_local_forces(qsb_scf* c, const double* rho_dev, double* force
     return QSB_OK;
 }
 
+qsb_status qsb_scf_step_residuals(qsb_scf* c, double* residuals, int max, int* n) {
+    if (!c || !n || (max > 0 && !residuals)) return fail(QSB_ERR_INVALID, "scf_step_residuals: bad argument");
+    *n = (int)c->step_res.size();
+    for (int k = 0; k < std::min(max, *n); ++k) residuals[k] = c->step_res[k];
+    return QSB_OK;
+}
+
 qsb_status qsb_scf_step_seconds(qsb_scf* c, double* seconds, int max, int* n) {
     if (!c || !n || (max > 0 && !seconds)) return fail(QSB_ERR_INVALID, "scf_step_seconds: bad argument");
     *n = (int)c->step_s.size();
@@ -782,6 +809,7 @@ qsb_status qsb_scf_run(qsb_scf* c, double* X, double* keep, int lobpcg_iters, in
     double e_prev = 0.0;
     *steps = 0;
     c->step_s.clear();
+    c->step_res.clear();
     QSB_CUDA_TRY(cudaStreamSynchronize(s));
     auto t_prev = std::chrono::steady_clock::now();
     for (int step = 0; step < max_steps; ++step) {
@@ -810,7 +838,8 @@ qsb_status qsb_scf_run(qsb_scf* c, double* X, double* keep, int lobpcg_iters, in
         // energy of the output density: sum occ rq - int (V_H + V_xc)[rho_in] rho_out + E_H + E_xc [rho_out]
         sub_kernel<<<pw_blocks(N), 256, 0, s>>>(N, c->veff, c->vloc, c->tmp);
         QSB_TRY(kspace(c, KOp::hartree, c->rho_out, c->vh, s));
-        lda_kernel<<<pw_blocks(N), 256, 0, s>>>(N, c->rho_out, c->exc, c->vxc);
+        lda_kernel<<<pw_blocks(N), 256, 0, s>>>(N, c->rho_out, c->exc, c->vxc, c->xc_rho_min,
+                                                      c->xc_continuous);
         QSB_CUDA_TRY(cudaGetLastError());
         double d2[2], exc_int;
         {
@@ -828,18 +857,20 @@ qsb_status qsb_scf_run(qsb_scf* c, double* X, double* keep, int lobpcg_iters, in
         const auto t_now = std::chrono::steady_clock::now();
         c->step_s.push_back(std::chrono::duration<double>(t_now - t_prev).count());
         t_prev = t_now;
-        const double etol = polishing && c->polish_tol > 0.0 ? c->polish_tol : tol_per_atom;
-        bool done = step > 0 && std::fabs(etot - e_prev) / c->n_atoms < etol;
-        const double rho_tol = polishing ? c->polish_rho_tol : c->rho_tol;
-        if (done && rho_tol > 0.0) {
-            // and the density residual (CONVERGENCE_MODE::RHO_ETOT of the reference's loop)
+        // density residual int |rho_out - rho_in| dV / N_e, recorded every step
+        // (the RHO_ETOT convergence quantity of the reference's loop)
+        {
             l1_diff_partial_kernel<<<RBLOCKS, RB, 0, s>>>(N, c->rho_out, c->rho_in, c->partial);
             row_sum_kernel<<<1, 32, 0, s>>>(1, RBLOCKS, c->partial, c->sums);
             double l1 = 0.0;
             QSB_CUDA_TRY(cudaMemcpyAsync(&l1, c->sums, sizeof(double), cudaMemcpyDeviceToHost, s));
             QSB_CUDA_TRY(cudaStreamSynchronize(s));
-            done = l1 * c->dV / c->n_el < rho_tol;
+            c->step_res.push_back(l1 * c->dV / c->n_el);
         }
+        const double etol = polishing && c->polish_tol > 0.0 ? c->polish_tol : tol_per_atom;
+        bool done = step > 0 && std::fabs(etot - e_prev) / c->n_atoms < etol;
+        const double rho_tol = polishing ? c->polish_rho_tol : c->rho_tol;
+        if (done && rho_tol > 0.0) done = c->step_res.back() < rho_tol;
         e_prev = etot;
         if (polishing && c->last_polish_steps >= c->polish_max) done = true;
         if (done && !polishing && c->polish_es && step + 1 < max_steps) {

@@ -601,6 +601,10 @@ class SCF:
     def set_smearing(self, kbt):
         _check(lib.qsb_scf_set_smearing(self._h, _c_d(kbt)))
 
+    def set_xc(self, pz_variant=0, rho_min=1e-8):
+        """LDA form (qsb_scf_set_xc): 0 the reference's PZ, 1 PZ continuous at rs = 1; cut rho_min."""
+        _check(lib.qsb_scf_set_xc(self._h, int(pz_variant), _c_d(rho_min)))
+
     def set_polish(self, solver_fp64, max_steps=10, tol_per_atom=0.0, rho_tol=0.0):
         """FP64 polish of a mixed run (qsb_scf_set_polish); solver_fp64=None switches it off."""
         self._polish = solver_fp64
@@ -632,6 +636,13 @@ class SCF:
         f, f_p = _f64(np.zeros(3 * na))
         _check(lib.qsb_scf_local_forces(self._h, _dev_ptr(rho) if rho is not None else None, f_p))
         return f.reshape(na, 3)
+
+    def step_residuals(self):
+        """int |rho_out - rho_in| dV / N_e of each step of the last run."""
+        buf, buf_p = _f64(np.zeros(4096))
+        n = ctypes.c_int()
+        _check(lib.qsb_scf_step_residuals(self._h, buf_p, len(buf), ctypes.byref(n)))
+        return buf[:n.value].copy()
 
     def step_seconds(self):
         """Wall seconds of each step of the last run."""
