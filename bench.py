@@ -599,6 +599,9 @@ def main():
     ap.add_argument("--scf-polish-steps", type=int, default=12,
                     help="FP64 polish steps allowed after the mixed run's own stop (0: no polish)")
     ap.add_argument("--scf-max-steps", type=int, default=None, help="SCF step cap (default 120 for c2, 160 for c3)")
+    ap.add_argument("--only-hpsi", action="store_true",
+                    help="time the device-resident H.psi only (no e2e, FFT, Gram, LOBPCG, SCF or CPU sections); "
+                         "the profiler captures use it")
     ap.add_argument("--bands", type=int, default=NB,
                     help="bands per GPU (default 128, the benchmark workload; smaller only for profiler captures)")
     args = ap.parse_args()
@@ -667,6 +670,20 @@ def main():
         for _ in range(20):
             H.apply(psi, hpsi)
         torch.cuda.synchronize()
+
+    if args.only_hpsi:
+        clocks.stop()
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": whole_job_gbs(algorithmic_bytes(NB, N, n_pts, 4), world, ms),
+                              "unit": UNIT, "ms_per_step": ms, "bands_per_gpu": NB,
+                              "breakdown_ms": {"nonlocal_projection": proj_ms / max(applies, 1),
+                                               "stencil": sten_ms / max(applies, 1),
+                                               "nonlocal_expansion": exp_ms / max(applies, 1)},
+                              "note": "--only-hpsi: device-resident H.psi timing only"}))
+        H.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
 
     # ---- end to end through the public API with host buffers -------------------
     e2e_steps = max(3, min(args.steps, 10))

@@ -831,8 +831,18 @@ __device__ __forceinline__ WsItem ws_item(int w, int nx, int ny, int nz, int zch
 // One CTA per item (blockIdx.x).  A persistent form (one CTA per SM walking
 // the items, the ring running on across them) measured slower: 0.49 against
 // 0.42 ms at 96^3 x 128 bands.
-template <typename T, bool CPLX, int MODE, bool GRAD, bool ISO, int RY, int S>
-__global__ void __launch_bounds__(WNT, 1)
+// Register budget, given to the compiler as a cap (__maxnreg__) rather than
+// through __launch_bounds__: 9 warps (8 compute + the producer) take the
+// register file of 12 (the allocation rounds a CTA's warps up to a multiple of
+// four), 65536 / 384 = 170 -> 168 per thread at one CTA per SM.  With the cap
+// stated directly the compiler kept the 168-register form free of the spills
+// the launch-bounds form had (0.450 -> 0.417 ms at 96^3 x 128 bands, FP64).
+template <int RY, int MINB>
+struct WsRegs {
+    static constexpr int value = MINB == 1 ? 168 : 65536 / (MINB * 384) / 8 * 8;
+};
+template <typename T, bool CPLX, int MODE, bool GRAD, bool ISO, int RY, int S, int MINB>
+__global__ void __maxnreg__((WsRegs<RY, MINB>::value))
 fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, int ny, int nz, int zchunk, int tiles,
               int nzc, int items, KC<T> k, int* __restrict__ err) {
     using C = WsCfg<T, CPLX, MODE, RY, S>;
@@ -1204,6 +1214,7 @@ int stencil_variant() {
         v = 0;
         if (e && std::string(e) == "reg") v = 2;
         if (e && std::string(e) == "zacc") v = 3;
+
     }
     return v;
 }
@@ -1237,7 +1248,7 @@ int sm_count() {
 // boundary.
 bool ws_dim_ok(int n, int tile) { return n == tile || (n >= tile + HW && (n % tile == 0 || n % tile >= HW)); }
 
-template <typename T, bool CPLX, int MODE, int RY, int S>
+template <typename T, bool CPLX, int MODE, int RY, int S, int MINB = 1>
 bool launch_ws(const StencilLaunch& L, const FD8Coef& c, const KC<T>& k, cudaStream_t s) {
     using C = WsCfg<T, CPLX, MODE, RY, S>;
     if (!ws_dim_ok(L.nx, ZTX) || !ws_dim_ok(L.ny, C::TY) || L.nz < HW) return false;
@@ -1264,10 +1275,10 @@ bool launch_ws(const StencilLaunch& L, const FD8Coef& c, const KC<T>& k, cudaStr
     // equal x and y weights (hx == hy): the x and y pairs of each offset are summed first
     bool iso = true;
     for (int q = 0; q < 4; ++q) iso = iso && k.cx[q] == k.cy[q];
-    auto kern = CPLX && c.has_grad ? (iso ? fd8_ws_kernel<T, CPLX, MODE, CPLX, true, RY, S>
-                                          : fd8_ws_kernel<T, CPLX, MODE, CPLX, false, RY, S>)
-                                   : (iso ? fd8_ws_kernel<T, CPLX, MODE, false, true, RY, S>
-                                          : fd8_ws_kernel<T, CPLX, MODE, false, false, RY, S>);
+    auto kern = CPLX && c.has_grad ? (iso ? fd8_ws_kernel<T, CPLX, MODE, CPLX, true, RY, S, MINB>
+                                          : fd8_ws_kernel<T, CPLX, MODE, CPLX, false, RY, S, MINB>)
+                                   : (iso ? fd8_ws_kernel<T, CPLX, MODE, false, true, RY, S, MINB>
+                                          : fd8_ws_kernel<T, CPLX, MODE, false, false, RY, S, MINB>);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
     kern<<<grid, block, C::SMEM, s>>>(m, (T*)L.out, L.nx, L.ny, L.nz, zchunk, tiles, nzc, (int)items, k,
                                       device_error_word());
@@ -1334,11 +1345,16 @@ void launch_t(const StencilLaunch& L, const FD8Coef& c, cudaStream_t s) {
     // (centre + (x + y neighbours + z neighbours), each completed first)
     if constexpr (sizeof(T) == 8) {
         if (aligned && pairs_ok && L.tma_ok && variant == 0) {
-            // rows per thread: 2 (complex: 1, within the register file at one CTA per SM)
+            // rows per thread: 2 (complex: 1, within the register file at one CTA per SM).
+            // Measured alternatives (real, 96^3 x 128 bands, FP64): 1 row per thread
+            // at two CTAs per SM 0.474-0.502 ms (more shared loads per point); 3 rows
+            // need 224 registers, which 9 warps cannot have (launch out of
+            // resources); ring depth 4 / 5 / 6 / 8 stages: 0.473 / 0.428 / 0.419 / 0.463 ms.
             constexpr int WRY = CPLX ? 1 : 2;
             constexpr int WS = CPLX ? 8 : 6;
             if (launch_ws<T, CPLX, MODE, WRY, WS>(L, c, k, s)) return;
         }
+
         if (aligned && pairs_ok && L.tma_ok && (variant == 0 || variant == 3)) {
             // real 2 rows / 1 CTA per SM (212 registers), complex 1 row
             const bool done = CPLX ? launch_zacc<T, CPLX, MODE, 16, 1, 8, 1>(L, c, k, s)
