@@ -332,6 +332,16 @@ QSB_API qsb_status qsb_lobpcg_z(qsb_eigensolver* es, double dVol, int n, int ite
 QSB_API qsb_status qsb_lobpcg_d(qsb_eigensolver* es, double dVol, int n, int iter_max, double* eigen_values,
                                 double* X, double* keep, int is_first_time, void* stream);
 
+/* dV-weighted orthonormalisation of nb bands in place (X: device, real bundle
+ * nb x N or complex SoA bundle), the starting states of an SCF.  Replaces
+ * GramSchmidt_ddm (source/GramSchmidt_mpi.h:56-96: classical Gram-Schmidt band
+ * after band) by Cholesky QR applied twice (G = dV X^H X, G = U^H U, X <- X U^-1):
+ * the same Q factor with a positive-diagonal R, so the same states to rounding
+ * for bands that are not near-dependent.  QSB_ERR_NUMERIC when the bands are
+ * linearly dependent.  Allocates its scratch (2N nb doubles for complex bands)
+ * and BLAS handles for the call; synchronizes the stream. */
+QSB_API qsb_status qsb_orthonormalize(int64_t N, int nb, int is_complex, double* X, double dV, void* stream);
+
 /* Gram product T = U^T V on the tcgen05 tensor cores as split-BF16x3
  * compensated products (u = u_hi + u_lo in bfloat16, three products
  * hi.hi + hi.lo + lo.hi) with FP32 accumulation per CTA and FP64 summation of

@@ -466,6 +466,15 @@ def ref_lobpcg_d(grid, V, cube, X, keep, n, iter_max, eigen_values, is_first_tim
                        _d(eigen_values), _d(X), _d(keep), _d(work), int(is_first_time))
 
 
+def ref_gram_schmidt(grid, X, nb, is_complex=False):
+    """GramSchmidt_ddm of the reference (GramSchmidt_mpi.h:56-96), on a copy of X."""
+    lib = ref_lib()
+    nx, ny, nz, dx, dy, dz = grid
+    out = np.ascontiguousarray(X, np.float64).copy()
+    lib.qsref_gram_schmidt(nx, ny, nz, nb, int(is_complex), _d(out), ctypes.c_double(dx * dy * dz))
+    return out
+
+
 def dense_eigenvalues(grid, V, tables, k, is_complex=False, g=(0.0, 0.0, 0.0), fft=False):
     """Lowest k eigenvalues of H built column by column with the C restatement
     (fft: with the FFT kinetic of hamiltonian_fft; small grids only)."""

@@ -68,6 +68,7 @@ inline int lapack_DSYGVX(double* A, double* B, double* w, double* Z, double* /*t
 #include "lobpcg_z_multi_mpi.h"
 #include "Vxc.h"
 #include "SetOccupancy.h"
+#include "GramSchmidt_mpi.h"
 #endif
 #include "cube_reader3.h"
 #include "cube_writer.h"
@@ -463,6 +464,22 @@ void qsref_lobpcg_z(int nx, int ny, int nz, double dx, double dy, double dz, con
                               [&](SoAComplex* Ax, SoAComplex* x, int nb) { apply_h_complex(H, Ax, x, nb); }, watch);
 }
 #endif
+
+/* GramSchmidt_ddm (GramSchmidt_mpi.h:56-96) on a real bundle (nb x N) or a
+ * complex SoA bundle (2 nb x N), in place, dV-weighted. */
+void qsref_gram_schmidt(int nx, int ny, int nz, int nb, int is_complex, double* X, double dVol) {
+    GridRangeMPI grid = make_grid(nx, ny, nz);
+    const size_t N = (size_t)nx * ny * nz;
+    if (is_complex) {
+        std::vector<SoAComplex> xs(nb);
+        for (int k = 0; k < nb; ++k) xs[k] = SoAComplex{X + 2 * k * N, X + (2 * k + 1) * N};
+        GramSchmidt_ddm(grid, nb, xs.data(), dVol);
+    } else {
+        std::vector<double*> xs(nb);
+        for (int k = 0; k < nb; ++k) xs[k] = X + k * N;
+        GramSchmidt_ddm(grid, nb, xs.data(), dVol);
+    }
+}
 
 /* exc[i] = rho eps_xc (exchange + correlation energy density), vxc[i] = V_x + V_c. */
 void qsref_lda_pz(int n, const double* rho, double* exc, double* vxc) {

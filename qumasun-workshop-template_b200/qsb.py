@@ -115,6 +115,16 @@ def laplacian_kpoint8th(out, src, coef, dx, dy, dz, g, shape):
     return out
 
 
+def orthonormalize(X, N, dV, is_complex=False):
+    """dV-weighted orthonormalisation of a band bundle in place (qsb_orthonormalize,
+    the role of GramSchmidt_ddm); X: [nb, N] real or [nb, 2, N] complex SoA, fp64 CUDA."""
+    if X.dtype != _torch().float64:
+        raise TypeError("orthonormalize needs float64 bands")
+    nb = X.numel() // ((2 if is_complex else 1) * N)
+    _check(lib.qsb_orthonormalize(ctypes.c_int64(N), nb, int(is_complex), _dev_ptr(X), _c_d(dV), _stream_ptr(X)))
+    return X
+
+
 def _i32(a):
     a = np.ascontiguousarray(a, np.int32)
     return a, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
