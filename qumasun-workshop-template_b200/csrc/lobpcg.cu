@@ -913,6 +913,17 @@ qsb_status lobpcg_z_mixed(qsb_eigensolver* es, double dVol, int n, int iter_max,
     const int head0 = num_fix;
     // X32 = sqrt(dV) X (:1851), all bands: the fixed ones orthogonalize the active ones
     QSB_TRY(seg_convert_by(es, n, X64, es->X32, nullptr, std::sqrt(dVol), s));
+    // the active bands normalised (the reference takes them as passed in, which a
+    // normalised input makes the same; FP32 rounding of the conversion aside)
+    QSB_TRY(seg_dot(es, num_active, b32(es->X32, head0), b32(es->X32, head0), 1.0, nrm_d + head0, s));
+    QSB_CUDA_TRY(cudaMemcpyAsync(nx.data(), nrm_d + head0, sizeof(double) * num_active, cudaMemcpyDeviceToHost, s));
+    QSB_CUDA_TRY(cudaStreamSynchronize(s));
+    for (int k = 0; k < num_active; ++k) {
+        if (!(nx[k] > 0.0) || !std::isfinite(nx[k])) return fail(QSB_ERR_NUMERIC, "lobpcg_z: zero or non-finite band");
+        scl[k] = 1.0 / std::sqrt(nx[k]);
+    }
+    QSB_CUDA_TRY(cudaMemcpyAsync(scl_d, scl.data(), sizeof(double) * num_active, cudaMemcpyHostToDevice, s));
+    QSB_TRY(seg_scale_by(es, num_active, b32(es->X32, head0), scl_d, 0.0, s));
     QSB_TRY(apply_op32(es, num_active, b32(es->X32, head0), b32(es->AX32, head0), s));
     QSB_TRY(seg_dot(es, num_active, b32(es->X32, head0), b32(es->AX32, head0), 1.0, eps_d + head0, s));
     QSB_TRY(seg_residual(es, num_active, b32(es->R32, head0), b32(es->AX32, head0), b32(es->X32, head0), eps_d + head0,
@@ -985,6 +996,14 @@ qsb_status lobpcg_z_mixed(qsb_eigensolver* es, double dVol, int n, int iter_max,
         if (maxdiff > 1.0e-3) {   // rollback (:2611-2666): keep X, P <- R
             es->last_rollback = 1;
             QSB_TRY(copy32(Pa, Ra, L * N_, s));
+            // The reference rescales the kept X with the norms of the rejected X'
+            // (:2651), harmless when they are 1 +- 1e-3.  Here the rollback can
+            // come from coefficients spoilt by an ill-conditioned basis, with
+            // norms far from 1: the kept X is normalised with its own norms, or
+            // the next call would start from mis-scaled bands.
+            QSB_TRY(seg_dot(es, N_, Xa, Xa, 1.0, nrm_d, s));
+            QSB_CUDA_TRY(cudaMemcpyAsync(nx.data(), nrm_d, sizeof(double) * N_, cudaMemcpyDeviceToHost, s));
+            QSB_CUDA_TRY(cudaStreamSynchronize(s));
             QSB_TRY(write_back_x());
             ++iter;
             break;

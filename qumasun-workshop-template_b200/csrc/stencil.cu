@@ -359,11 +359,29 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// bounded wait; false after WAIT_LIMIT polls
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (unsigned it = 0; it < WAIT_LIMIT; ++it)
+// bounded wait; false after WAIT_LIMIT (or `limit`) polls
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned limit = WAIT_LIMIT) {
+    for (unsigned it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
+}
+
+// Test setting of the box-fed stencil's wait limits: the environment variable
+// QSB_STENCIL_COMPUTE_POLLS (read once per process) makes the compute warps wait
+// that many polls on a barrier that nothing arrives at, and the producer's
+// stage-release waits give up after as many polls: the waits run out, the
+// kernel sets bit 0 of the device error word and returns (the producer first
+// waits, with the full limit, for its copies in flight).  Unset: WAIT_LIMIT.
+unsigned compute_poll_limit() {
+    static unsigned v = 0;
+    if (v == 0) {
+        v = WAIT_LIMIT;
+        if (const char* e = std::getenv("QSB_STENCIL_COMPUTE_POLLS")) {
+            const long n = std::strtol(e, nullptr, 10);
+            if (n >= 1 && n < (long)WAIT_LIMIT) v = (unsigned)n;
+        }
+    }
+    return v;
 }
 
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
@@ -782,7 +800,7 @@ struct WsCfg {
     static constexpr int OFF_SIDE = NC * MAIN;              // side[c][L|R]
     static constexpr int OFF_E = OFF_SIDE + NC * 2 * SIDE;
     static constexpr int STAGE = OFF_E + NE * EBOX;
-    static constexpr size_t SMEM = (size_t)S * STAGE * sizeof(T) + 2 * S * sizeof(uint64_t) + 128;
+    static constexpr size_t SMEM = (size_t)S * STAGE * sizeof(T) + (2 * S + 1) * sizeof(uint64_t) + 128;
     static constexpr uint32_t MAIN_BYTES = (uint32_t)(MAIN * sizeof(T));
     static constexpr uint32_t SIDE_BYTES = (uint32_t)(SIDE * sizeof(T));
     static constexpr uint32_t E_BYTES = (uint32_t)(EBOX * sizeof(T));
@@ -844,7 +862,7 @@ struct WsRegs {
 template <typename T, bool CPLX, int MODE, bool GRAD, bool ISO, int RY, int S, int MINB>
 __global__ void __maxnreg__((WsRegs<RY, MINB>::value))
 fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, int ny, int nz, int zchunk, int tiles,
-              int nzc, int items, KC<T> k, int* __restrict__ err) {
+              int nzc, int items, KC<T> k, int* __restrict__ err, unsigned cpolls) {
     using C = WsCfg<T, CPLX, MODE, RY, S>;
     using P2 = typename Pair<T>::type;
     constexpr int NC = C::NC, NE = C::NE, TY = C::TY, SW = C::SW;
@@ -853,16 +871,23 @@ fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, 
     T* ring = reinterpret_cast<T*>(smraw);
     uint64_t* full = reinterpret_cast<uint64_t*>(smraw + (size_t)S * C::STAGE * sizeof(T));
     uint64_t* empty = full + S;
+    uint64_t* never = empty + S;   // no thread ever arrives here (the wait-limit test)
     const size_t nxy = (size_t)nx * ny;
     const size_t N = nxy * nz;
     const int t = threadIdx.y * ZX + threadIdx.x;
     const int warp = t >> 5, lane = t & 31;
+    // cpolls < WAIT_LIMIT: the test setting of the wait limits (compute_poll_limit):
+    // the compute warps first wait, with that limit, on a barrier nothing
+    // arrives at, and the producer's stage-release waits use it too; the
+    // producer's drain of its own copies keeps the full limit
+    const bool wait_test = cpolls < WAIT_LIMIT;
 
     if (t == 0) {
         for (int st = 0; st < S; ++st) {
             mbar_init(&full[st], 1);
             mbar_init(&empty[st], WCW);
         }
+        mbar_init(never, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -879,7 +904,7 @@ fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, 
         for (int j = 0; j < nplanes; ++j) {
             const int st = j % S;
             // stage st last held plane j - S: wait until every compute warp released it
-            if (j >= S && !mbar_wait(&empty[st], (uint32_t)(((j / S) - 1) & 1))) {
+            if (j >= S && !mbar_wait(&empty[st], (uint32_t)(((j / S) - 1) & 1), wait_test ? cpolls : WAIT_LIMIT)) {
                 failed = true;
                 break;
             }
@@ -937,7 +962,7 @@ fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, 
     const int tx = threadIdx.x, ty = threadIdx.y;
     const uint32_t soff = ((ty * RY + HW) * SW + 2 * tx + HW) * TB;    // centre pair (main box)
     const uint32_t eoff = (C::OFF_E + ty * RY * ZTX + 2 * tx) * TB;    // V / old output pair
-    bool failed = false;
+    bool failed = wait_test && __any_sync(0xffffffffu, !mbar_wait(never, 0, cpolls));
     {
     const WsItem it = ws_item<TY>(blockIdx.x, nx, ny, nz, zchunk, tiles, nzc);
     const int x0 = it.x0, y0 = it.y0, z0 = it.z0, nsteps = it.nsteps, band = it.band;
@@ -991,7 +1016,7 @@ fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, 
             const int j = jb + u;
             if (j < nplanes && !failed) {
                 const int st = j % S;
-                const bool ok = mbar_wait(&full[st], (uint32_t)((j / S) & 1));
+                const bool ok = mbar_wait(&full[st], (uint32_t)((j / S) & 1), cpolls);
                 if (__any_sync(0xffffffffu, !ok)) {
                     failed = true;
                     continue;
@@ -1281,7 +1306,7 @@ bool launch_ws(const StencilLaunch& L, const FD8Coef& c, const KC<T>& k, cudaStr
                                           : fd8_ws_kernel<T, CPLX, MODE, false, false, RY, S, MINB>);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
     kern<<<grid, block, C::SMEM, s>>>(m, (T*)L.out, L.nx, L.ny, L.nz, zchunk, tiles, nzc, (int)items, k,
-                                      device_error_word());
+                                      device_error_word(), compute_poll_limit());
     return true;
 }
 

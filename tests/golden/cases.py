@@ -171,3 +171,60 @@ def scf_inputs():
     sp = [dict(O.GTH_BCC)] * len(pos)
     X = O.orthonormal_psi(SCF_C0["seed"], SCF_C0["nb"], n ** 3, h ** 3)
     return dict(grid=grid, pos=pos, sp=sp, X=X, checked=[X, pos])
+
+
+# ---------------------------------------------------------------------------
+# Shapes of the larger configurations, pinned to the reference's own solvers:
+#   C4K: one k-point of config 4's k part -- the config-0 cell (a = 6 bohr) on a
+#        48^3 grid (h = 0.125), 24 complex bands, k = (1, 2, 3) / 4 of the
+#        reciprocal vectors (a point of the 4 x 4 x 4 Gamma-centred mesh);
+#   C0D: config 0's real shape -- 32^3 grid, 16 bands.
+# Potentials are the seeded V of the other LOBPCG cases (0.3 U[-1, 1]), atoms
+# off-grid, GTH s + p projectors (cutoff 6 r_l).
+# ---------------------------------------------------------------------------
+C4K_GRID = (48, 48, 48, 0.125, 0.125, 0.125)
+C4K_NB = 24
+C4K_G = tuple(2 * math.pi / A_BCC * f for f in (0.25, 0.5, 0.75))
+C0D_GRID = (32, 32, 32, 0.1875, 0.1875, 0.1875)
+C0D_NB = 16
+
+
+def big_eig_inputs(grid, nb, seed, cplx):
+    nx, ny, nz, dx, dy, dz = grid
+    N = nx * ny * nz
+    dV = dx * dy * dz
+    pos = O.bcc_positions(A_BCC, 1) + np.array([0.11, -0.07, 0.05])
+    sp = [O.GTH_BCC] * len(pos)
+    V = 0.3 * O.seeded_potential(seed, N)
+    X = O.orthonormal_psi(seed, nb, N, dV, cplx)
+    return dict(grid=grid, pos=pos, sp=sp, V=V, X=X, dV=dV, nb=nb, checked=[V, X])
+
+
+def big_eig_ref(inp, cplx, calls=3, iter_max=4, g=(0.0, 0.0, 0.0)):
+    """Reference solver calls (SCF steps 0..calls-1): eigenvalues (and num_fix) after each."""
+    nx, ny, nz, dx, dy, dz = inp["grid"]
+    nb = inp["nb"]
+    cube = O.gth_cube_tables(inp["pos"], inp["sp"], nx, ny, nz, dx, dy, dz)
+    X = inp["X"].copy()
+    keep = np.zeros_like(X)
+    ev = np.zeros(nb)
+    out, nf = [], 0
+    for step in range(calls):
+        if cplx:
+            nf = O.ref_lobpcg_z(inp["grid"], inp["V"], cube, X, keep, nb, iter_max, ev, nf, 1e-4, step, g)
+            out.append(np.concatenate([ev, [nf]]))
+        else:
+            O.ref_lobpcg_d(inp["grid"], inp["V"], cube, X, keep, nb, iter_max, ev, step == 0)
+            out.append(ev.copy())
+    return np.array(out)
+
+
+CASES.update({
+    "lobpcg_z_c4k": dict(inputs=lambda: big_eig_inputs(C4K_GRID, C4K_NB, 4, True),
+                         reference=lambda i: big_eig_ref(i, True, g=C4K_G), oracle=None),
+    "lobpcg_d_c0": dict(inputs=lambda: big_eig_inputs(C0D_GRID, C0D_NB, 0, False),
+                        reference=lambda i: big_eig_ref(i, False), oracle=None),
+    "ham_cplx_c4k": dict(inputs=lambda: _ham_inputs(C4K_GRID, 6, 1, True),
+                         reference=lambda i: _ham_ref(i, True, C4K_G),
+                         oracle=lambda i: _ham_oracle(i, True, C4K_G)),
+})

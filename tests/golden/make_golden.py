@@ -21,14 +21,19 @@ from cases import CASES, SCF_C0, scf_inputs  # noqa: E402
 import scf_oracle as S  # noqa: E402
 
 
-def main():
+def main(only=None):
+    """All fixtures, or only the named cases (python make_golden.py NAME ...)."""
     assert O.ref_available(), "build oracle/_ref first: make -C oracle ref"
     for name, case in CASES.items():
+        if only and name not in only:
+            continue
         inp = case["inputs"]()
         out = case["reference"](inp)
         np.savez_compressed(os.path.join(HERE, name + ".npz"), out=out,
                             checksum=np.array([float(np.sum(v)) for v in inp["checked"]]))
         print(name, out.shape, float(np.linalg.norm(out)))
+    if only and "scf_c0" not in only:
+        return
     # SCF of config 0: the oracle loop (reference LOBPCG + restated SCF pieces)
     inp = scf_inputs()
     r = S.scf(inp["grid"], inp["pos"], inp["sp"], SCF_C0["nb"], SCF_C0["n_el"], inp["X"], **SCF_C0["params"])
@@ -39,4 +44,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)
