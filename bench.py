@@ -170,6 +170,42 @@ def _ref_worker(args):
     return times
 
 
+def _ref_solver_c0(cores):
+    """Runs in a spawned process: the reference's own EigenLOBPCG_d_multi per
+    iteration, and a whole config-0 SCF to 1e-6 Ha / atom with it as the
+    eigensolver (oracle/scf_oracle.py: the loop and its density, Hartree, LDA,
+    occupations and Kerker-DIIS pieces restated in numpy, every LOBPCG call the
+    reference's), on `cores` BLAS threads."""
+    sys.path.insert(0, ORACLE)
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    import oracle as O
+    import scf_oracle as S
+    from cases import SCF_C0, scf_inputs
+    if not O.ref_available():
+        return None
+    O.ref_set_threads(cores)
+    inp = scf_inputs()
+    nx, ny, nz, dx, dy, dz = inp["grid"]
+    N = nx * ny * nz
+    cube = O.gth_cube_tables(inp["pos"], inp["sp"], nx, ny, nz, dx, dy, dz)
+    V = S.gth_local_potential(inp["grid"], inp["pos"], inp["sp"])
+    X = inp["X"].copy()
+    keep = np.zeros_like(X)
+    ev = np.zeros(SCF_C0["nb"])
+    import contextlib
+    import io
+    with contextlib.redirect_stdout(io.StringIO()):
+        O.ref_lobpcg_d(inp["grid"], V, cube, X, keep, SCF_C0["nb"], 2, ev, True)       # warm
+        t0 = time.perf_counter()
+        O.ref_lobpcg_d(inp["grid"], V, cube, X, keep, SCF_C0["nb"], 8, ev, False)
+        t_iter = (time.perf_counter() - t0) / 8
+    t0 = time.perf_counter()
+    r = S.scf(inp["grid"], inp["pos"], inp["sp"], SCF_C0["nb"], SCF_C0["n_el"], inp["X"], **SCF_C0["params"])
+    t_scf = time.perf_counter() - t0
+    return {"lobpcg_ms_per_iteration": t_iter * 1e3, "scf_seconds": t_scf, "scf_steps": int(r["steps"]),
+            "scf_final_energy_ha": float(r["energies"][-1]), "cores": cores}
+
+
 def cpu_kind():
     sys.path.insert(0, ORACLE)
     import oracle as O
@@ -207,6 +243,15 @@ def run_reference(args):
                                    f"(state decomposition), 1 BLAS thread each; wall {wall:.1f} s"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    # the SCF-wall-time half of the metric on the host: config 0 (2-atom bcc,
+    # 32^3, 16 bands, LDA, Kerker-DIIS, |dE| < 1e-6 Ha / atom)
+    with ctx.Pool(1) as pool:
+        sc = pool.map(_ref_solver_c0, [cores])[0]
+    if sc is not None:
+        line["scf_c0_cpu"] = dict(sc, kind="reference",
+                                  sample="config 0 whole SCF; every eigensolver call the reference's "
+                                         "EigenLOBPCG_d_multi (OpenBLAS on the host cores), the loop's "
+                                         "other pieces the numpy restatement (oracle/scf_oracle.py)")
     print(json.dumps(line))
     return 0
 
@@ -508,6 +553,45 @@ WATER_O = dict(zion=6.0, rloc=0.247, c1=-16.58, c2=2.40, r=0.222, h=18.27)
 WATER_H = dict(zion=1.0, rloc=0.2, c1=-4.18, c2=0.725)
 
 
+def scf_c0_section():
+    """Config 0 (2-atom bcc, 32^3, 16 bands) SCF to |dE| < 1e-6 Ha / atom on the
+    device, FP64 and mixed, from the same seeded orthonormal start as the
+    reference arm's host run (psi U[-0.5, 0.5] from PCG64(0), orthonormalised): wall seconds."""
+    import torch
+    import qsb
+    n, nb, n_el = 32, 16, 12.0
+    h = A_CELL / n
+    N = n ** 3
+    pos = np.array([[0.0, 0.0, 0.0], [0.5 * A_CELL] * 3])
+    # psi ~ U[-0.5, 0.5] from numpy PCG64(0) (the host run's start), then
+    # dV-orthonormalised on the device (qsb_orthonormalize)
+    psi0 = np.random.default_rng(0).uniform(-0.5, 0.5, size=(nb, N))
+    out = {"config": "c0", "atoms": 2, "grid": [n, n, n], "bands": nb, "tolerance_ha_per_atom": 1e-6}
+    for prec in ("fp64", "mixed"):
+        H = qsb.Hamiltonian(n, n, n, h, h, h)
+        H.set_gth_projectors(pos, [0, 0], [GTH["nl"]], [GTH["r"]], [GTH["h"]], RCUT)
+        H.set_potential(np.zeros(N))
+        es = qsb.EigenSolver(N, nb, False, prec)
+        scf = qsb.SCF(H, es, nb, n_el)
+        scf.set_gth_local(pos, [0, 0], [GTH_LOCAL["zion"]], [GTH_LOCAL["rloc"]], [GTH_LOCAL["c1"]],
+                          [GTH_LOCAL["c2"]])
+        scf.set_mixing(0.5, 0.8, 6)
+        scf.set_smearing(0.01)
+        for rep in range(2):                     # the first run sizes the workspaces
+            X = qsb.orthonormalize(torch.from_numpy(psi0).cuda(), N, h ** 3)
+            keep = torch.zeros_like(X)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            e, ev, occ = scf.run(X, keep, 4, 60, 1e-6)
+            torch.cuda.synchronize()
+            t = time.perf_counter() - t0
+        out[prec] = {"seconds": t, "steps": len(e), "final_energy_ha": float(e[-1])}
+        scf.close()
+        es.close()
+        H.close()
+    return out
+
+
 def relax_section(fmax=1e-4):
     """Wall time of the LBFGS relaxation of config 1 (qsb_relax_lbfgs: SCF warm
     from the previous geometry's states, local + nonlocal + Ewald forces) from
@@ -715,6 +799,7 @@ def main():
         scf = scf_section(args.scf_config, args.scf_tol_ref, args.scf_max_steps, args.scf_rho_tol,
                           args.scf_polish_steps)
     relax = relax_section() if args.relax and world == 1 else None
+    scf_c0 = scf_c0_section() if not args.no_scf and world == 1 else None
     clk = clocks.stop()
 
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist, "cuda")
@@ -755,6 +840,7 @@ def main():
         "relax": relax,
         "lobpcg": lob,
         "scf": scf,
+        "scf_c0": scf_c0,
         "gram": gram,
         "clocks": clk,
     }
