@@ -518,6 +518,44 @@ QSB_API qsb_status qsb_relax_lbfgs(qsb_scf* scf, int n_atoms, double* pos, const
                                    const int* fixed, double* X, double* keep, int lobpcg_iters, int scf_max_steps,
                                    double scf_tol, int max_iter, double fmax, double max_step, int history,
                                    double* energies, int* iters, double* forces, void* stream);
+/* k-point SCF (complex Bloch bands): the loop of QUMASUN_KPOINT::Execute over
+ * its k groups (source/qumasun_kpoint.scfloop.h:61-258, the solver calls of
+ * qumasun_kpoint.lobpcg.h:78-106) with the density summed over k
+ * (mSetDensityByPsi, source/qumasun_base1.density.h:19-105) and the Fermi level
+ * found over all (k, band) levels with the k weights.  Needs a complex solver
+ * context (either precision) given to qsb_scf_create.
+ *   qsb_scf_set_kpoints: kvec 3 n_k Bloch vectors (bohr^-1), weights n_k (> 0,
+ *     summing to 1), owned (may be NULL: all) marks the k-points this context
+ *     computes; with several contexts (one per GPU, or per rank) sharing a k
+ *     list, each owns a part and qsb_scf_set_reduce joins them.
+ *   qsb_scf_set_reduce: fn(user, buf, count) must replace the host buffer buf
+ *     of count doubles by its sum over all contexts sharing the k-points (an
+ *     allreduce) and return 0; called with the same sizes in the same order on
+ *     every context, twice per step (the levels, n_k nb; the density, N) and
+ *     once before the first (the starting density).  NULL: one context.
+ *   qsb_scf_run_kpoints: X[k], keep[k] device complex SoA bundles of nb bands
+ *     (owned k only; others may be NULL), updated in place; per step every owned
+ *     k-point gets lobpcg_iters solver iterations at its Bloch vector (no soft
+ *     locking), FP64 Rayleigh quotients of its bands, the occupations f_nk in
+ *     [0, 2] from the weighted Fermi level (sum_k w_k sum_n f_nk = N_e), the
+ *     output density sum_k w_k sum_n f_nk |psi_nk|^2, the energy as in qsb_scf_run
+ *     with the band energy sum_k w_k sum_n f_nk e_nk; stop and mixing as there
+ *     (the FP64 polish does not apply).  eigen_values, occupations: host, n_k x nb
+ *     (k-major, may be NULL), all k-points after the reduction. */
+typedef int (*qsb_reduce_fn)(void* user, double* buf, int64_t count);
+QSB_API qsb_status qsb_scf_set_kpoints(qsb_scf* scf, int n_k, const double* kvec, const double* weights,
+                                       const int* owned);
+QSB_API qsb_status qsb_scf_set_reduce(qsb_scf* scf, qsb_reduce_fn fn, void* user);
+QSB_API qsb_status qsb_scf_run_kpoints(qsb_scf* scf, double* const* X, double* const* keep, int lobpcg_iters,
+                                       int max_steps, double tol_per_atom, double* energies, int* steps,
+                                       double* eigen_values, double* occupations, void* stream);
+/* Fermi-Dirac occupations of n levels (host code): occ_i = 2 / (exp((e_i - mu) / kbt) + 1)
+ * with mu such that sum_i w_i occ_i = n_el (weights NULL: all 1) -- the bisection
+ * of mSetOccupancyTemperature (source/qumasun_base1.occupancy.h:76-170) with
+ * SetOccupancy's formula (source/SetOccupancy.h:7-18), refined by Newton steps to
+ * the exact count.  mu may be NULL. */
+QSB_API qsb_status qsb_fermi_occupations(int n, const double* eig, const double* weights, double n_el, double kbt,
+                                         double* occ, double* mu);
 /* Wall seconds of each step of the last qsb_scf_run (host clock; a step ends
  * when its energy is on the host): up to max values, *n = steps recorded. */
 QSB_API qsb_status qsb_scf_step_seconds(qsb_scf* scf, double* seconds, int max, int* n);

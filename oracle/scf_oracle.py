@@ -408,3 +408,100 @@ def ewald(pos, charge, cell, alpha=None, tol=1e-16):
                 F += (4 * pi / omega * w * Z * np.imag(np.conj(S) * np.exp(1j * ph)))[:, None] * G[None, :]
     E += -alpha / sqrt(pi) * float(np.sum(Z * Z)) - pi / (2 * omega * alpha * alpha) * float(np.sum(Z)) ** 2
     return E, F
+
+
+# --------------------------------------------------------------------------
+# k-point SCF (complex Bloch bands): the loop of QUMASUN_KPOINT::Execute over k
+# groups with the reference's own Eigen_z_multi_mpi (oracle/_ref) per k-point
+# --------------------------------------------------------------------------
+def fermi_occupancy_kpoints(eig, kweights, n_el, kbt):
+    """mSetOccupancyTemperature over k groups (source/qumasun_base1.occupancy.h:76-170):
+    occupancy_nk = SetOccupancy(2 w_k, ...) with one mu for all k, bisection on
+    sum_nk occupancy_nk = N_e between the lowest and highest level, then Newton
+    steps to the exact count (the device driver's refinement).  eig [n_k, nb];
+    returns (occupancy [n_k, nb] including the weight, mu)."""
+    eig = np.asarray(eig, np.float64)
+    w = np.asarray(kweights, np.float64)[:, None] * np.ones_like(eig)
+
+    def count(mu):
+        occ = np.stack([_occupancy(eig[k], mu, kbt, 2.0 * w[k, 0]) for k in range(eig.shape[0])])
+        return occ, float(occ.sum())
+    mu_min, mu_max = float(eig.min()), float(eig.max())
+    mu = 0.5 * (mu_min + mu_max)
+    go = abs(mu_max - mu_min) > 1.0e-9
+    mu_last = mu
+    while go:
+        occ, ne = count(mu)
+        mu_last = mu
+        if ne < n_el:
+            mu_min = mu
+        elif ne > n_el:
+            mu_max = mu
+        else:
+            break
+        mu = 0.5 * (mu_min + mu_max)
+        go = abs(mu_max - mu_min) > 1.0e-9
+    mu = mu_last
+    for _ in range(8):
+        occ, ne = count(mu)
+        f = occ / w
+        dn = float(np.sum(w * f * (1.0 - 0.5 * f))) / kbt
+        r = ne - n_el
+        if abs(r) <= 1e-14 * n_el or not dn > 1e-300:
+            break
+        mu -= r / dn
+    return count(mu)[0], mu
+
+
+def scf_kpoints(grid, pos, species_params, nb, n_el, X0s, kvecs, kweights, kbt=0.01, lobpcg_iters=4, max_steps=60,
+                tol_per_atom=1e-6, amplitude=0.5, q0=0.8, depth=6, rcut_factor=O.RCUT_FACTOR):
+    """The oracle k-point SCF: per step and k-point the reference's
+    Eigen_z_multi_mpi (no soft locking), FP64 Rayleigh quotients of the complex
+    bands with the restated H, occupations over all k (fermi_occupancy_kpoints),
+    rho_out = sum_nk occupancy |psi|^2, the energy and the Kerker-DIIS mixing of
+    the Gamma-point oracle."""
+    nx, ny, nz, dx, dy, dz = grid
+    N = nx * ny * nz
+    dV = dx * dy * dz
+    n_atoms = len(pos)
+    nk = len(kweights)
+    tables = O.gth_tables(pos, species_params, dx, dy, dz, rcut_factor=rcut_factor)
+    cube = O.gth_cube_tables(pos, species_params, nx, ny, nz, dx, dy, dz, rcut_factor=rcut_factor)
+    vloc = gth_local_potential(grid, pos, species_params)
+    Xs = [np.array(x, np.float64).reshape(2 * nb, N).copy() for x in X0s]
+    keeps = [np.zeros_like(x) for x in Xs]
+    evs = [np.zeros(nb) for _ in range(nk)]
+    f0 = zero_temperature_occupations(nb, n_el)
+
+    def dens(Xk, occk):
+        re, im = Xk[0::2], Xk[1::2]
+        return np.einsum("n,ni->i", occk, re * re + im * im)
+
+    rho_in = sum(dens(Xs[k], kweights[k] * f0) for k in range(nk))
+    mixer = KerkerDIIS(grid, amplitude, q0, depth)
+    energies, e_prev = [], None
+    rq = np.zeros((nk, nb))
+    occ = np.zeros((nk, nb))
+    for step in range(max_steps):
+        vh, _ = hartree(rho_in, grid)
+        _, vxc = lda_pz(rho_in)
+        veff = vloc + vh + vxc
+        for k in range(nk):
+            with _quiet_stdout():
+                O.ref_lobpcg_z(grid, veff, cube, Xs[k], keeps[k], nb, lobpcg_iters, evs[k], 0, 0.0, step,
+                               tuple(kvecs[k]))
+            HX = O.hamiltonian(grid, veff, tables, Xs[k], nb, True, tuple(kvecs[k])).reshape(2 * nb, N)
+            num = np.einsum("ni,ni->n", Xs[k], HX)
+            den = np.einsum("ni,ni->n", Xs[k], Xs[k])
+            rq[k] = (num[0::2] + num[1::2]) / (den[0::2] + den[1::2])
+        occ, mu = fermi_occupancy_kpoints(rq, kweights, n_el, kbt)
+        rho_out = sum(dens(Xs[k], occ[k]) for k in range(nk))
+        vh_out, eh = hartree(rho_out, grid)
+        exc_out, _ = lda_pz(rho_out)
+        etot = float(np.sum(occ * rq)) - float(np.dot(vh + vxc, rho_out)) * dV + eh + float(np.sum(exc_out)) * dV
+        energies.append(etot)
+        if e_prev is not None and abs(etot - e_prev) / n_atoms < tol_per_atom:
+            break
+        e_prev = etot
+        rho_in = mixer.next(rho_in, rho_out)
+    return dict(energies=np.array(energies), rq=rq, occ=occ, rho=rho_out, steps=len(energies))

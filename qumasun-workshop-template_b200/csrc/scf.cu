@@ -369,6 +369,16 @@ struct qsb_scf {
     std::vector<double> B;        // depth x depth residual inner products (by slot)
     std::vector<double> step_s;   // wall seconds of each step of the last run
     std::vector<double> step_res; // int |rho_out - rho_in| dV / N_e of each step of the last run
+    // k-point runs (qsb_scf_set_kpoints / qsb_scf_run_kpoints)
+    int n_k = 0;
+    std::vector<double> kvec, kw; // 3 n_k Bloch vectors (bohr^-1), n_k weights (sum 1)
+    std::vector<int> kown;        // k-points this context computes
+    std::vector<int> knfix;       // soft-locking count of each k-point's solver calls
+    double* hxc = nullptr;        // H X of one k-point's complex bundle (2 nb N)
+    double* occ2 = nullptr;       // per-plane weights w_k f_nk of a complex bundle (2 nb)
+    qsb_reduce_fn reduce = nullptr;   // sum over the ranks sharing the k-points (host buffers)
+    void* reduce_user = nullptr;
+    std::vector<double> hbuf;     // host staging of the density for the reduction
 };
 
 namespace qsb {
@@ -419,15 +429,20 @@ qsb_status potentials(qsb_scf* c, cudaStream_t s) {
 
 // Fermi-Dirac occupations (SetOccupancy, source/SetOccupancy.h:7-18) at the mu of
 // the bisection of mSetOccupancyTemperature (source/qumasun_base1.occupancy.h:76-170),
-// refined by Newton steps to the exact electron count
-void fermi(const std::vector<double>& eig, double n_el, double kbt, std::vector<double>& occ) {
+// refined by Newton steps to the exact electron count.  w (may be empty: all 1):
+// the weight of each level's k-point, so that sum_i w_i occ_i = n_el with
+// occ_i in [0, 2] (spin-paired); returns mu.
+double fermi_weighted(const std::vector<double>& eig, const std::vector<double>& w, double n_el, double kbt,
+                      std::vector<double>& occ) {
     const int n = (int)eig.size();
+    occ.resize(n);
+    auto wt = [&](int k) { return w.empty() ? 1.0 : w[k]; };
     auto fill = [&](double mu) {
         double sum = 0.0;
         for (int k = 0; k < n; ++k) {
             const double p = std::min((eig[k] - mu) / kbt, 80.0);
             occ[k] = 2.0 / (std::exp(p) + 1.0);
-            sum += occ[k];
+            sum += wt(k) * occ[k];
         }
         return sum;
     };
@@ -452,12 +467,17 @@ void fermi(const std::vector<double>& eig, double n_el, double kbt, std::vector<
     for (int it = 0; it < 8; ++it) {
         const double ne = fill(mu);
         double dn = 0.0;
-        for (int k = 0; k < n; ++k) dn += occ[k] * (1.0 - 0.5 * occ[k]) / kbt;
+        for (int k = 0; k < n; ++k) dn += wt(k) * occ[k] * (1.0 - 0.5 * occ[k]) / kbt;
         const double r = ne - n_el;
         if (std::fabs(r) <= 1e-14 * n_el || !(dn > 1e-300)) break;
         mu -= r / dn;
     }
     fill(mu);
+    return mu;
+}
+
+void fermi(const std::vector<double>& eig, double n_el, double kbt, std::vector<double>& occ) {
+    fermi_weighted(eig, std::vector<double>(), n_el, kbt, occ);
 }
 
 // Gaussian elimination with partial pivoting of the bordered DIIS system
@@ -618,6 +638,8 @@ qsb_status qsb_scf_destroy(qsb_scf* c) {
     for (double* f : fields)
         if (f) cudaFree(f);
     if (c->ptrs) cudaFree((void*)c->ptrs);
+    if (c->hxc) cudaFree(c->hxc);
+    if (c->occ2) cudaFree(c->occ2);
     if (c->fk) cudaFree(c->fk);
     if (c->atoms) cudaFree(c->atoms);
     if (c->have_plans) {
@@ -874,11 +896,245 @@ qsb_status qsb_scf_run(qsb_scf* c, double* X, double* keep, int lobpcg_iters, in
         e_prev = etot;
         if (polishing && c->last_polish_steps >= c->polish_max) done = true;
         if (done && !polishing && c->polish_es && step + 1 < max_steps) {
-            // the mixed run has met its stop: go on in FP64 from its states and density
+            // the mixed run has met its stop: go on in FP64 from its states and
+            // density, with a fresh mixing history (the kept residuals carry the
+            // FP32 states' noise, which would stay in the DIIS extrapolation)
             polishing = true;
             c->last_polish_first = step + 1;
+            c->slots.clear();
+            std::fill(c->B.begin(), c->B.end(), 0.0);
             done = false;
         }
+        if (done) break;
+        QSB_TRY(mix(c, s));
+    }
+    if (eigen_values) std::copy(rq.begin(), rq.end(), eigen_values);
+    if (occupations) std::copy(occ.begin(), occ.end(), occupations);
+    return QSB_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// k-point SCF: the loop of QUMASUN_KPOINT::Execute over (k) groups
+// (source/qumasun_kpoint.scfloop.h:61-258, qumasun_kpoint.lobpcg.h:78-106), the
+// density summed over k (qumasun_base1.density.h:19-105, mReduceFieldInSamePlace)
+// and the Fermi level over all (k, band) levels with the k weights.
+// ---------------------------------------------------------------------------
+namespace qsb {
+namespace {
+
+// host-staged sum of n doubles over the ranks sharing the k-points (device buffer)
+qsb_status reduce_device(qsb_scf* c, double* dev, size_t n, cudaStream_t s) {
+    if (!c->reduce) return QSB_OK;
+    c->hbuf.resize(n);
+    QSB_CUDA_TRY(cudaMemcpyAsync(c->hbuf.data(), dev, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    QSB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (c->reduce(c->reduce_user, c->hbuf.data(), (int64_t)n) != 0)
+        return fail(QSB_ERR_STATE, "scf_run_kpoints: the reduction callback failed");
+    QSB_CUDA_TRY(cudaMemcpyAsync(dev, c->hbuf.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+    return QSB_OK;
+}
+
+qsb_status reduce_host(qsb_scf* c, double* h, size_t n) {
+    if (!c->reduce) return QSB_OK;
+    if (c->reduce(c->reduce_user, h, (int64_t)n) != 0)
+        return fail(QSB_ERR_STATE, "scf_run_kpoints: the reduction callback failed");
+    return QSB_OK;
+}
+
+// rho (+)= sum_n occ2[2n] re_n^2 + occ2[2n+1] im_n^2 over a complex SoA bundle
+qsb_status density_complex(qsb_scf* c, int nb, const double* X, const std::vector<double>& wocc, double* rho,
+                           bool accumulate, cudaStream_t s) {
+    std::vector<double> o2(2 * (size_t)nb);
+    for (int n = 0; n < nb; ++n) o2[2 * n] = o2[2 * n + 1] = wocc[n];
+    QSB_CUDA_TRY(cudaMemcpyAsync(c->occ2, o2.data(), o2.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    double* dst = accumulate ? c->tmp : rho;
+    density_kernel<<<pw_blocks(c->N), 256, 0, s>>>(c->N, 2 * nb, X, c->occ2, dst);
+    if (accumulate) add_kernel<<<pw_blocks(c->N), 256, 0, s>>>(c->N, c->tmp, rho);
+    QSB_CUDA_TRY(cudaGetLastError());
+    // the host copy of o2 must outlive the copy: synchronize before it goes
+    QSB_CUDA_TRY(cudaStreamSynchronize(s));
+    return QSB_OK;
+}
+
+}  // namespace
+}  // namespace qsb
+
+extern "C" {
+
+qsb_status qsb_fermi_occupations(int n, const double* eig, const double* weights, double n_el, double kbt,
+                                 double* occ, double* mu) {
+    if (n <= 0 || !eig || !occ || !(kbt > 0.0) || !(n_el > 0.0))
+        return fail(QSB_ERR_INVALID, "fermi_occupations: bad argument");
+    std::vector<double> e(eig, eig + n), w, o;
+    if (weights) w.assign(weights, weights + n);
+    double cap = 0.0;
+    for (int k = 0; k < n; ++k) {
+        if (!std::isfinite(e[k]) || (weights && !(w[k] >= 0.0))) return fail(QSB_ERR_INVALID, "fermi_occupations: bad value");
+        cap += 2.0 * (weights ? w[k] : 1.0);
+    }
+    if (n_el > cap) return fail(QSB_ERR_INVALID, "fermi_occupations: more electrons than the levels hold");
+    const double m = fermi_weighted(e, w, n_el, kbt, o);
+    std::copy(o.begin(), o.end(), occ);
+    if (mu) *mu = m;
+    return QSB_OK;
+}
+
+qsb_status qsb_scf_set_kpoints(qsb_scf* c, int n_k, const double* kvec, const double* weights, const int* owned) {
+    if (!c || n_k < 1 || !kvec || !weights) return fail(QSB_ERR_INVALID, "scf_set_kpoints: bad argument");
+    int64_t N = 0;
+    int nmax = 0, cplx = 0, mixed = 0;
+    eigensolver_shape(c->es, &N, &nmax, &cplx, &mixed);
+    if (!cplx) return fail(QSB_ERR_INVALID, "scf_set_kpoints: needs a complex eigensolver context");
+    double wsum = 0.0;
+    for (int k = 0; k < n_k; ++k) {
+        if (!(weights[k] > 0.0)) return fail(QSB_ERR_INVALID, "scf_set_kpoints: weights must be > 0");
+        wsum += weights[k];
+    }
+    if (std::fabs(wsum - 1.0) > 1e-12) return fail(QSB_ERR_INVALID, "scf_set_kpoints: weights must sum to 1");
+    const size_t fb = c->N * sizeof(double);
+    if (!c->hxc && cudaMalloc((void**)&c->hxc, 2 * (size_t)c->nb * fb) != cudaSuccess)
+        return fail(QSB_ERR_NOMEM, "scf_set_kpoints: device allocation");
+    if (!c->occ2 && cudaMalloc((void**)&c->occ2, 2 * (size_t)c->nb * sizeof(double)) != cudaSuccess)
+        return fail(QSB_ERR_NOMEM, "scf_set_kpoints: device allocation");
+    c->n_k = n_k;
+    c->kvec.assign(kvec, kvec + 3 * (size_t)n_k);
+    c->kw.assign(weights, weights + n_k);
+    c->kown.assign(n_k, 1);
+    if (owned)
+        for (int k = 0; k < n_k; ++k) c->kown[k] = owned[k] != 0;
+    c->knfix.assign(n_k, 0);
+    return QSB_OK;
+}
+
+qsb_status qsb_scf_set_reduce(qsb_scf* c, qsb_reduce_fn fn, void* user) {
+    if (!c) return fail(QSB_ERR_INVALID, "scf_set_reduce: null context");
+    c->reduce = fn;
+    c->reduce_user = user;
+    return QSB_OK;
+}
+
+qsb_status qsb_scf_run_kpoints(qsb_scf* c, double* const* X, double* const* keep, int lobpcg_iters, int max_steps,
+                               double tol_per_atom, double* energies, int* steps, double* eigen_values,
+                               double* occupations, void* stream) {
+    if (!c || !X || !keep || lobpcg_iters <= 0 || max_steps <= 0 || !(tol_per_atom > 0.0) || !energies || !steps)
+        return fail(QSB_ERR_INVALID, "scf_run_kpoints: bad argument");
+    if (c->n_k < 1) return fail(QSB_ERR_STATE, "scf_run_kpoints: no k-points (qsb_scf_set_kpoints)");
+    if (c->n_atoms <= 0) return fail(QSB_ERR_STATE, "scf_run_kpoints: no local potential (qsb_scf_set_gth_local)");
+    for (int k = 0; k < c->n_k; ++k) {
+        if (c->kown[k] && (!X[k] || !keep[k])) return fail(QSB_ERR_INVALID, "scf_run_kpoints: null bundle of an owned k-point");
+        if (!c->kown[k] && !c->reduce)
+            return fail(QSB_ERR_STATE, "scf_run_kpoints: k-points owned elsewhere need a reduction (qsb_scf_set_reduce)");
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nb = c->nb, nk = c->n_k;
+    const size_t N = c->N;
+    std::vector<double> rq((size_t)nk * nb, 0.0), occ((size_t)nk * nb, 0.0), wl((size_t)nk * nb), wocc(nb);
+    for (int k = 0; k < nk; ++k)
+        for (int n = 0; n < nb; ++n) wl[(size_t)k * nb + n] = c->kw[k];
+    std::vector<double> ev(nb), sums(2 * (size_t)nb);
+    auto own_first = [&]() {
+        for (int k = 0; k < nk; ++k)
+            if (c->kown[k]) return k;
+        return -1;
+    };
+    // initial density: the input states of every k-point with the lowest bands
+    // doubly filled (mSetOccupancyZero), weighted by w_k, summed over the ranks
+    {
+        double left = c->n_el;
+        std::vector<double> f0(nb);
+        for (int n = 0; n < nb; ++n) {
+            f0[n] = std::min(2.0, std::max(left, 0.0));
+            left -= f0[n];
+        }
+        const int k0 = own_first();
+        if (k0 < 0) QSB_CUDA_TRY(cudaMemsetAsync(c->rho_in, 0, N * sizeof(double), s));
+        for (int k = 0; k < nk; ++k) {
+            if (!c->kown[k]) continue;
+            for (int n = 0; n < nb; ++n) wocc[n] = c->kw[k] * f0[n];
+            QSB_TRY(density_complex(c, nb, X[k], wocc, c->rho_in, k != k0, s));
+        }
+        QSB_TRY(reduce_device(c, c->rho_in, N, s));
+    }
+    c->slots.clear();
+    std::fill(c->B.begin(), c->B.end(), 0.0);
+    std::fill(c->knfix.begin(), c->knfix.end(), 0);
+    double e_prev = 0.0;
+    *steps = 0;
+    c->step_s.clear();
+    c->step_res.clear();
+    c->last_polish_first = -1;
+    c->last_polish_steps = 0;
+    QSB_CUDA_TRY(cudaStreamSynchronize(s));
+    auto t_prev = std::chrono::steady_clock::now();
+    for (int step = 0; step < max_steps; ++step) {
+        QSB_TRY(potentials(c, s));
+        std::fill(rq.begin(), rq.end(), 0.0);
+        for (int k = 0; k < nk; ++k) {
+            if (!c->kown[k]) continue;
+            const double* g = &c->kvec[3 * (size_t)k];
+            QSB_TRY(qsb_eigensolver_set_hamiltonian(c->es, c->ham, g[0], g[1], g[2]));
+            QSB_TRY(qsb_lobpcg_z(c->es, c->dV, nb, lobpcg_iters, ev.data(), X[k], keep[k], &c->knfix[k], 0.0, step,
+                                 stream));
+            // FP64 Rayleigh quotients <x|Hx> / <x|x> of the complex bands (re and im
+            // planes of a band are contiguous: one 2N-long dot per band)
+            QSB_TRY(qsb_ham_apply(c->ham, QSB_F64, 1, nb, X[k], c->hxc, g[0], g[1], g[2], stream));
+            band_dot_kernel<<<dim3(RBLOCKS / 4, nb), RB, 0, s>>>(2 * N, X[k], c->hxc, c->partial,
+                                                                 c->partial + (size_t)nb * (RBLOCKS / 4));
+            row_sum_kernel<<<2 * nb, 32, 0, s>>>(2 * nb, RBLOCKS / 4, c->partial, c->sums);
+            QSB_CUDA_TRY(cudaGetLastError());
+            QSB_CUDA_TRY(cudaMemcpyAsync(sums.data(), c->sums, 2 * nb * sizeof(double), cudaMemcpyDeviceToHost, s));
+            QSB_CUDA_TRY(cudaStreamSynchronize(s));
+            for (int n = 0; n < nb; ++n) {
+                if (!(sums[nb + n] > 0.0) || !std::isfinite(sums[n]))
+                    return fail(QSB_ERR_NUMERIC, "scf_run_kpoints: bad band norm");
+                rq[(size_t)k * nb + n] = sums[n] / sums[nb + n];
+            }
+        }
+        // every rank needs every level for the Fermi level: the levels of the
+        // k-points a rank does not own are zero there, so a sum gathers them
+        QSB_TRY(reduce_host(c, rq.data(), rq.size()));
+        fermi_weighted(rq, wl, c->n_el, c->kbt, occ);
+        const int k0 = own_first();
+        if (k0 < 0) QSB_CUDA_TRY(cudaMemsetAsync(c->rho_out, 0, N * sizeof(double), s));
+        for (int k = 0; k < nk; ++k) {
+            if (!c->kown[k]) continue;
+            for (int n = 0; n < nb; ++n) wocc[n] = c->kw[k] * occ[(size_t)k * nb + n];
+            QSB_TRY(density_complex(c, nb, X[k], wocc, c->rho_out, k != k0, s));
+        }
+        QSB_TRY(reduce_device(c, c->rho_out, N, s));
+        // energy of the output density, as the Gamma-point loop
+        sub_kernel<<<pw_blocks(N), 256, 0, s>>>(N, c->veff, c->vloc, c->tmp);
+        QSB_TRY(kspace(c, KOp::hartree, c->rho_out, c->vh, s));
+        lda_kernel<<<pw_blocks(N), 256, 0, s>>>(N, c->rho_out, c->exc, c->vxc, c->xc_rho_min, c->xc_continuous);
+        QSB_CUDA_TRY(cudaGetLastError());
+        double d2[2], exc_int;
+        {
+            const double* a[2] = {c->tmp, c->vh};
+            QSB_TRY(dots(c, 2, a, c->rho_out, d2, s));
+            const double* e[1] = {c->exc};
+            QSB_TRY(dots(c, 1, e, nullptr, &exc_int, s));
+        }
+        double eband = 0.0;
+        for (size_t i = 0; i < rq.size(); ++i) eband += wl[i] * occ[i] * rq[i];
+        const double etot = eband - d2[0] + 0.5 * d2[1] + exc_int;
+        energies[step] = etot;
+        *steps = step + 1;
+        const auto t_now = std::chrono::steady_clock::now();
+        c->step_s.push_back(std::chrono::duration<double>(t_now - t_prev).count());
+        t_prev = t_now;
+        {
+            l1_diff_partial_kernel<<<RBLOCKS, RB, 0, s>>>(N, c->rho_out, c->rho_in, c->partial);
+            row_sum_kernel<<<1, 32, 0, s>>>(1, RBLOCKS, c->partial, c->sums);
+            double l1 = 0.0;
+            QSB_CUDA_TRY(cudaMemcpyAsync(&l1, c->sums, sizeof(double), cudaMemcpyDeviceToHost, s));
+            QSB_CUDA_TRY(cudaStreamSynchronize(s));
+            c->step_res.push_back(l1 * c->dV / c->n_el);
+        }
+        bool done = step > 0 && std::fabs(etot - e_prev) / c->n_atoms < tol_per_atom;
+        if (done && c->rho_tol > 0.0) done = c->step_res.back() < c->rho_tol;
+        e_prev = etot;
         if (done) break;
         QSB_TRY(mix(c, s));
     }

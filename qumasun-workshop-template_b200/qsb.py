@@ -115,6 +115,16 @@ def laplacian_kpoint8th(out, src, coef, dx, dy, dz, g, shape):
     return out
 
 
+def fermi_occupations(eig, n_el, kbt, weights=None):
+    """(occupations in [0, 2], mu) of the levels eig with k weights (qsb_fermi_occupations; host)."""
+    e, e_p = _f64(np.asarray(eig, np.float64).ravel())
+    occ, occ_p = _f64(np.zeros(len(e)))
+    w, w_p = _f64(np.asarray(weights, np.float64).ravel()) if weights is not None else (None, None)
+    mu = ctypes.c_double()
+    _check(lib.qsb_fermi_occupations(len(e), e_p, w_p, _c_d(n_el), _c_d(kbt), occ_p, ctypes.byref(mu)))
+    return occ, mu.value
+
+
 def orthonormalize(X, N, dV, is_complex=False):
     """dV-weighted orthonormalisation of a band bundle in place (qsb_orthonormalize,
     the role of GramSchmidt_ddm); X: [nb, N] real or [nb, 2, N] complex SoA, fp64 CUDA."""
@@ -638,6 +648,54 @@ class SCF:
         _check(lib.qsb_scf_run(self._h, _dev_ptr(X), _dev_ptr(keep), lobpcg_iters, max_steps, _c_d(tol_per_atom),
                                e_p, ctypes.byref(steps), ev_p, occ_p, _stream_ptr(X)))
         return e[:steps.value].copy(), ev, occ
+
+    _REDUCE = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int64)
+
+    def set_kpoints(self, kvec, weights, owned=None):
+        """k-points of a complex-band SCF (qsb_scf_set_kpoints): kvec [n_k, 3] bohr^-1,
+        weights [n_k] summing to 1, owned [n_k] flags of the k-points this context computes."""
+        kv, kv_p = _f64(np.asarray(kvec, np.float64).reshape(-1, 3))
+        w, w_p = _f64(np.asarray(weights, np.float64).ravel())
+        self.n_k = len(w)
+        if owned is not None:
+            ow, ow_p = _i32(np.asarray(owned, np.int32).ravel())
+        else:
+            ow, ow_p = None, None
+        self._owned = [True] * self.n_k if owned is None else [bool(o) for o in np.asarray(owned).ravel()]
+        _check(lib.qsb_scf_set_kpoints(self._h, self.n_k, kv_p, w_p, ow_p))
+
+    def set_reduce(self, fn):
+        """fn(array) must replace the float64 numpy array (host) by its sum over the
+        contexts sharing the k-points (an allreduce); None: a single context."""
+        if fn is None:
+            self._reduce_cb = None
+            _check(lib.qsb_scf_set_reduce(self._h, None, None))
+            return
+
+        def cb(user, buf, count):
+            try:
+                fn(np.ctypeslib.as_array(buf, shape=(count,)))
+                return 0
+            except Exception:
+                return 1
+        self._reduce_cb = self._REDUCE(cb)         # kept alive with the context
+        _check(lib.qsb_scf_set_reduce(self._h, self._reduce_cb, None))
+
+    def run_kpoints(self, Xs, keeps, lobpcg_iters=4, max_steps=60, tol_per_atom=1e-6):
+        """k-point SCF (qsb_scf_run_kpoints); Xs, keeps: per k-point [nb, 2, N] fp64 CUDA
+        bundles (None for k-points owned elsewhere), updated in place.  Returns
+        (energies per step, levels [n_k, nb], occupations [n_k, nb])."""
+        nk = self.n_k
+        ptrs = (ctypes.c_void_p * nk)(*[_dev_ptr(x).value if x is not None else None for x in Xs])
+        kptrs = (ctypes.c_void_p * nk)(*[_dev_ptr(x).value if x is not None else None for x in keeps])
+        e, e_p = _f64(np.zeros(max_steps))
+        ev, ev_p = _f64(np.zeros(nk * self.nb))
+        occ, occ_p = _f64(np.zeros(nk * self.nb))
+        steps = ctypes.c_int()
+        ref = next(x for x in Xs if x is not None)
+        _check(lib.qsb_scf_run_kpoints(self._h, ptrs, kptrs, lobpcg_iters, max_steps, _c_d(tol_per_atom), e_p,
+                                       ctypes.byref(steps), ev_p, occ_p, _stream_ptr(ref)))
+        return e[:steps.value].copy(), ev.reshape(nk, self.nb), occ.reshape(nk, self.nb)
 
     def local_forces(self, rho=None, n_atoms=None):
         """Forces of the GTH local parts, [n_atoms, 3], from the last output

@@ -228,3 +228,25 @@ CASES.update({
                          reference=lambda i: _ham_ref(i, True, C4K_G),
                          oracle=lambda i: _ham_oracle(i, True, C4K_G)),
 })
+
+
+# k-point SCF: the config-0 cell (2-atom bcc, a = 6 bohr) on a 20^3 grid, the
+# 2 x 2 x 2 Gamma-centred k mesh (8 points, weight 1/8 each, no symmetry
+# reduction), 10 complex bands per k-point, 12 electrons, GTH as config 0, LDA,
+# Fermi 0.01 Ha, 4 LOBPCG iterations per step, Kerker-DIIS, |dE| < 1e-6 Ha / atom.
+SCF_KPT = dict(n=20, a=A_BCC, nb=10, n_el=12.0,
+               params=dict(kbt=0.01, lobpcg_iters=4, max_steps=60, tol_per_atom=1e-6, amplitude=0.5, q0=0.8,
+                           depth=6))
+
+
+def scf_kpt_inputs():
+    n, a = SCF_KPT["n"], SCF_KPT["a"]
+    h = a / n
+    grid = (n, n, n, h, h, h)
+    pos = O.bcc_positions(a, 1) + np.array([0.05, -0.03, 0.02])
+    sp = [dict(O.GTH_BCC)] * len(pos)
+    b = 2 * math.pi / a
+    kvecs = np.array([[i * b / 2, j * b / 2, k * b / 2] for i in range(2) for j in range(2) for k in range(2)])
+    weights = np.full(len(kvecs), 1.0 / len(kvecs))
+    Xs = [O.orthonormal_psi(10 + k, SCF_KPT["nb"], n ** 3, h ** 3, True) for k in range(len(kvecs))]
+    return dict(grid=grid, pos=pos, sp=sp, kvecs=kvecs, weights=weights, Xs=Xs, checked=Xs + [pos, kvecs])

@@ -32,6 +32,15 @@ def main(only=None):
         np.savez_compressed(os.path.join(HERE, name + ".npz"), out=out,
                             checksum=np.array([float(np.sum(v)) for v in inp["checked"]]))
         print(name, out.shape, float(np.linalg.norm(out)))
+    if not only or "scf_kpt" in only:
+        # k-point SCF: the oracle loop with the reference's Eigen_z_multi_mpi per k-point
+        from cases import SCF_KPT, scf_kpt_inputs
+        inp = scf_kpt_inputs()
+        r = S.scf_kpoints(inp["grid"], inp["pos"], inp["sp"], SCF_KPT["nb"], SCF_KPT["n_el"], inp["Xs"], inp["kvecs"],
+                          inp["weights"], **SCF_KPT["params"])
+        np.savez_compressed(os.path.join(HERE, "scf_kpt.npz"), energies=r["energies"], rq=r["rq"], occ=r["occ"],
+                            rho=r["rho"], checksum=np.array([float(np.sum(v)) for v in inp["checked"]]))
+        print("scf_kpt", r["steps"], r["energies"][-1])
     if only and "scf_c0" not in only:
         return
     # SCF of config 0: the oracle loop (reference LOBPCG + restated SCF pieces)
