@@ -160,6 +160,34 @@ QSB_API qsb_status qsb_ham_apply_host(qsb_ham* ham, qsb_dtype dtype, int is_comp
                                       const void* psi_host, void* hpsi_host,
                                       double gx, double gy, double gz, int chunk_bands, void* stream);
 
+/* H psi of n_sys independent systems at once (real bands, Gamma point, FD8
+ * kinetic): hpsi[i] = H_i psi[i] for nb[i] bands of system i (each its own
+ * qsb_ham: grid, spacing, potential, projectors).  The FD8 + V part of all
+ * systems runs in ONE persistent launch over a work list of (system, 32 x 8
+ * column tile, z chunk, band) items, largest systems first; each system's
+ * nonlocal projection and expansion keep their own launches.  The reference
+ * applies H system by system (mHamiltonianMatrix_ddm, source/qumasun_base1.matrix.h:263-291);
+ * for many small, uneven cells a launch per system leaves most SMs idle.
+ * Results equal qsb_ham_apply's to rounding (a different stencil kernel).
+ * With qsb_set_autotune on, the first call for a set of shapes times this
+ * form against the systems' own qsb_ham_apply and keeps the faster. */
+QSB_API qsb_status qsb_ham_apply_batch(qsb_dtype dtype, int n_sys, qsb_ham* const* hams, const int* nb,
+                                       const void* const* psi, void* const* hpsi, void* stream);
+
+/* Autotuner.  On (enable != 0), the first launch of each stencil shape in the
+ * H psi form (FP64; grid, bands rounded up to a power of two, real / complex)
+ * times the stencil kernels that apply to it (the TMA-box kernel with a
+ * producer warp, the TMA-plane kernel, the register-prefetch kernel) on the
+ * caller's stream and keeps the fastest for that shape; qsb_ham_apply_batch
+ * likewise chooses between its batched and per-system forms.  Tuning runs on
+ * the caller's buffers (the outputs are rewritten, the last run is the chosen
+ * kernel's), so make tuned first calls outside stream capture.  Off (the
+ * default): the fixed choice (the TMA-box kernel where it applies).
+ * qsb_autotune_report copies the decision log (one line per decision, with
+ * the times) into buf (len bytes, NUL-terminated); *needed = its size + 1. */
+QSB_API qsb_status qsb_set_autotune(int enable);
+QSB_API qsb_status qsb_autotune_report(char* buf, int len, int* needed);
+
 /* hpsi += V_NL psi.  Replaces PseudoPotNonlocal_SvF2_kpoint::ProjectionPP_bundle
  * (source/PseudoPotNonlocal_SvF2_kpoint.h:4239-4247, CPU :3911-4046, GPU :4053-4236). */
 QSB_API qsb_status qsb_ham_nonlocal_apply(qsb_ham* ham, qsb_dtype dtype, int is_complex, int nb,

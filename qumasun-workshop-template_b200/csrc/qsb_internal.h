@@ -39,6 +39,40 @@ struct FD8Coef {
 };
 FD8Coef make_fd8_coef(double coef, double dx, double dy, double dz, double gx, double gy, double gz);
 
+// Coefficients in the kernel's type.  In fp32 the centre weight is a pair
+// c0 + c0lo equal (to ~2^-48) to -2 * (sum of the ROUNDED fp32 neighbour
+// weights) - coef |g|^2, so the fp32 stencil still annihilates constants:
+// rounding c0 on its own would shift every eigenvalue of the fp32 operator by
+// ~|c0| 2^-24 (~1e-6 Ha at h = 0.5 bohr).  In fp64 c0lo is zero and unused.
+template <typename T>
+struct KC {
+    T c0, c0lo;
+    T cx[4], cy[4], cz[4];
+    T ax[4], ay[4], az[4];
+};
+
+template <typename T>
+KC<T> to_kc(const FD8Coef& c) {
+    KC<T> k;
+    double sum_exact = 0.0, sum_rounded = 0.0;
+    for (int m = 0; m < 4; ++m) {
+        k.cx[m] = (T)c.cx[m]; k.cy[m] = (T)c.cy[m]; k.cz[m] = (T)c.cz[m];
+        k.ax[m] = (T)c.ax[m]; k.ay[m] = (T)c.ay[m]; k.az[m] = (T)c.az[m];
+        sum_exact += c.cx[m] + c.cy[m] + c.cz[m];
+        sum_rounded += (double)k.cx[m] + (double)k.cy[m] + (double)k.cz[m];
+    }
+    if (sizeof(T) == sizeof(double)) {
+        k.c0 = (T)c.c0;
+        k.c0lo = T(0);
+    } else {
+        // c.c0 = -2 * sum_exact - coef |g|^2 (14350 = 2 * (8064 - 1008 + 128 - 9))
+        const double target = (c.c0 + 2.0 * sum_exact) - 2.0 * sum_rounded;
+        k.c0 = (T)target;
+        k.c0lo = (T)(target - (double)k.c0);
+    }
+    return k;
+}
+
 // Launch configuration of the stencil kernels.
 struct StencilLaunch {
     int nx, ny, nz;
@@ -56,6 +90,10 @@ struct StencilLaunch {
 int* device_error_word();
 
 qsb_status launch_stencil(qsb_dtype dt, const StencilLaunch& L, const FD8Coef& c, cudaStream_t s);
+// Autotuner state (stencil.cu): whether qsb_set_autotune is on, and a line for
+// the decision log qsb_autotune_report returns.
+bool autotune_enabled();
+void autotune_log(const std::string& line);
 
 // Argument checks shared by the apply entry points (context, dtype, band count
 // and the two bundle pointers).

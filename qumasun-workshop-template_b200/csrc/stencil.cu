@@ -18,6 +18,10 @@
 #include <cmath>
 #include <cstdlib>
 #include <cuda.h>
+#include <array>
+#include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 
 namespace qsb {
@@ -54,40 +58,6 @@ constexpr int TX = 32;        // tile width (one warp)
 constexpr int BY = 8;         // warps per CTA, stacked in y
 constexpr int NT = TX * BY;   // threads per CTA
 constexpr int HW = 4;         // halo width of the 8th-order stencil
-
-// Coefficients in the kernel's type.  In fp32 the centre weight is a pair
-// c0 + c0lo equal (to ~2^-48) to -2 * (sum of the ROUNDED fp32 neighbour
-// weights) - coef |g|^2, so the fp32 stencil still annihilates constants:
-// rounding c0 on its own would shift every eigenvalue of the fp32 operator by
-// ~|c0| 2^-24 (~1e-6 Ha at h = 0.5 bohr).  In fp64 c0lo is zero and unused.
-template <typename T>
-struct KC {
-    T c0, c0lo;
-    T cx[4], cy[4], cz[4];
-    T ax[4], ay[4], az[4];
-};
-
-template <typename T>
-KC<T> to_kc(const FD8Coef& c) {
-    KC<T> k;
-    double sum_exact = 0.0, sum_rounded = 0.0;
-    for (int m = 0; m < 4; ++m) {
-        k.cx[m] = (T)c.cx[m]; k.cy[m] = (T)c.cy[m]; k.cz[m] = (T)c.cz[m];
-        k.ax[m] = (T)c.ax[m]; k.ay[m] = (T)c.ay[m]; k.az[m] = (T)c.az[m];
-        sum_exact += c.cx[m] + c.cy[m] + c.cz[m];
-        sum_rounded += (double)k.cx[m] + (double)k.cy[m] + (double)k.cz[m];
-    }
-    if (sizeof(T) == sizeof(double)) {
-        k.c0 = (T)c.c0;
-        k.c0lo = T(0);
-    } else {
-        // c.c0 = -2 * sum_exact - coef |g|^2 (14350 = 2 * (8064 - 1008 + 128 - 9))
-        const double target = (c.c0 + 2.0 * sum_exact) - 2.0 * sum_rounded;
-        k.c0 = (T)target;
-        k.c0lo = (T)(target - (double)k.c0);
-    }
-    return k;
-}
 
 __device__ __forceinline__ int wrapi(int v, int n) {
     int m = v % n;
@@ -1343,7 +1313,7 @@ bool launch_zacc(const StencilLaunch& L, const FD8Coef& c, const KC<T>& k, cudaS
 }
 
 template <typename T, bool CPLX, int MODE>
-void launch_t(const StencilLaunch& L, const FD8Coef& c, cudaStream_t s) {
+void launch_t(const StencilLaunch& L, const FD8Coef& c, cudaStream_t s, int variant) {
     // rows per thread: as many as fit 128 registers without spilling
     constexpr int RY = (CPLX || sizeof(T) == 8) ? 2 : 4;
     constexpr int TY = BY * RY;
@@ -1361,7 +1331,6 @@ void launch_t(const StencilLaunch& L, const FD8Coef& c, cudaStream_t s) {
     // TMA path: the tensor map needs 16-byte aligned base and row pitch
     const int vec = 16 / (int)sizeof(T);
     const bool aligned = (L.nx % vec == 0) && (((uintptr_t)L.in) % 16 == 0);
-    const int variant = stencil_variant();
     // the pending-output kernel also moves out / V / old values in 16-byte pairs
     const bool pairs_ok = ((uintptr_t)L.out % 16 == 0) && (L.V == nullptr || (uintptr_t)L.V % 16 == 0);
     // FP64 only: the pending-output z sums round at 2^-24 of the ~|c0| partial
@@ -1396,24 +1365,132 @@ void launch_t(const StencilLaunch& L, const FD8Coef& c, cudaStream_t s) {
 }
 
 template <typename T>
-qsb_status launch_dtype(const StencilLaunch& L, const FD8Coef& c, cudaStream_t s) {
+qsb_status launch_dtype(const StencilLaunch& L, const FD8Coef& c, cudaStream_t s, int variant) {
     if (L.mode == 0) {
-        if (L.is_complex) launch_t<T, true, 0>(L, c, s);
-        else launch_t<T, false, 0>(L, c, s);
+        if (L.is_complex) launch_t<T, true, 0>(L, c, s, variant);
+        else launch_t<T, false, 0>(L, c, s, variant);
     } else {
-        if (L.is_complex) launch_t<T, true, 1>(L, c, s);
-        else launch_t<T, false, 1>(L, c, s);
+        if (L.is_complex) launch_t<T, true, 1>(L, c, s, variant);
+        else launch_t<T, false, 1>(L, c, s, variant);
     }
     QSB_CUDA_TRY(cudaGetLastError());
     return QSB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner (qsb_set_autotune): for the H psi form of the stencil (MODE 1, whose
+// output is overwritten, so a candidate can run on the caller's buffers) in
+// FP64, the first launch of each shape (grid, band count rounded up to a power
+// of two, real / complex, k-point terms) times the kernels that apply -- the
+// TMA-box kernel with its producer warp, the TMA-plane kernel with pending
+// outputs, the register-prefetch kernel -- two runs each after a warm one, on
+// the caller's stream with CUDA events, keeps the fastest for that shape, and
+// runs it once more so the output is its own.  Decisions are logged
+// (qsb_autotune_report).  FP32 keeps the register-prefetch kernel (its summation
+// order), MODE 0 ("+=") the default order of kernels.
+struct TuneState {
+    std::mutex mu;
+    bool on = false;
+    std::map<std::array<int, 8>, int> choice;
+    std::string log;
+};
+TuneState& tune_state() {
+    static TuneState t;
+    return t;
+}
+
+const char* variant_name(int v) { return v == 0 ? "tma-box (fd8_ws)" : v == 3 ? "tma-plane (fd8_zacc)" : "register (fd8)"; }
+
+qsb_status tune_and_launch(qsb_dtype dt, const StencilLaunch& L, const FD8Coef& c, cudaStream_t s) {
+    TuneState& ts = tune_state();
+    int nbb = 1;
+    while (nbb < L.nb) nbb *= 2;
+    const std::array<int, 8> key{L.nx, L.ny, L.nz, nbb, L.is_complex, c.has_grad ? 1 : 0, (int)dt, L.mode};
+    {
+        std::lock_guard<std::mutex> g(ts.mu);
+        auto it = ts.choice.find(key);
+        if (it != ts.choice.end()) return launch_dtype<double>(L, c, s, it->second);
+    }
+    const int cand[3] = {0, 3, 2};
+    float best = 1e30f;
+    int pick = 0;
+    std::string line = "stencil " + std::to_string(L.nx) + "x" + std::to_string(L.ny) + "x" + std::to_string(L.nz) +
+                       (L.is_complex ? " complex" : " real") + " x" + std::to_string(L.nb) + " bands:";
+    cudaEvent_t e0, e1;
+    QSB_CUDA_TRY(cudaEventCreate(&e0));
+    QSB_CUDA_TRY(cudaEventCreate(&e1));
+    for (int v : cand) {
+        qsb_status st = launch_dtype<double>(L, c, s, v);   // warm
+        float ms = 0.f;
+        if (st == QSB_OK) {
+            cudaEventRecord(e0, s);
+            for (int r = 0; r < 2; ++r) st = st == QSB_OK ? launch_dtype<double>(L, c, s, v) : st;
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms *= 0.5f;
+        }
+        if (st != QSB_OK) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return st;
+        }
+        line += std::string(" ") + variant_name(v) + " " + std::to_string(ms) + " ms;";
+        if (ms < best) {
+            best = ms;
+            pick = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    line += std::string(" -> ") + variant_name(pick) + "\n";
+    {
+        std::lock_guard<std::mutex> g(ts.mu);
+        ts.choice[key] = pick;
+        ts.log += line;
+    }
+    return launch_dtype<double>(L, c, s, pick);
 }
 
 }  // namespace
 
 qsb_status launch_stencil(qsb_dtype dt, const StencilLaunch& L, const FD8Coef& c, cudaStream_t s) {
     if (L.nb > 65535) return fail(QSB_ERR_INVALID, "stencil: nb > 65535");
-    if (dt == QSB_F64) return launch_dtype<double>(L, c, s);
-    return launch_dtype<float>(L, c, s);
+    const int forced = stencil_variant();   // QSB_STENCIL overrides the choice
+    if (dt == QSB_F64 && L.mode == 1 && forced == 0 && tune_state().on) return tune_and_launch(dt, L, c, s);
+    if (dt == QSB_F64) return launch_dtype<double>(L, c, s, forced);
+    return launch_dtype<float>(L, c, s, forced);
 }
+
+bool autotune_enabled() { return tune_state().on; }
+
+void autotune_log(const std::string& line) {
+    TuneState& ts = tune_state();
+    std::lock_guard<std::mutex> g(ts.mu);
+    ts.log += line;
+}
+
+}  // namespace qsb
+
+extern "C" qsb_status qsb_set_autotune(int enable) {
+    qsb::TuneState& ts = qsb::tune_state();
+    std::lock_guard<std::mutex> g(ts.mu);
+    ts.on = enable != 0;
+    return QSB_OK;
+}
+
+extern "C" qsb_status qsb_autotune_report(char* buf, int len, int* needed) {
+    qsb::TuneState& ts = qsb::tune_state();
+    std::lock_guard<std::mutex> g(ts.mu);
+    if (needed) *needed = (int)ts.log.size() + 1;
+    if (buf && len > 0) {
+        const size_t n = std::min<size_t>((size_t)len - 1, ts.log.size());
+        std::memcpy(buf, ts.log.data(), n);
+        buf[n] = '\0';
+    }
+    return QSB_OK;
+}
+
+namespace qsb {
 
 }  // namespace qsb

@@ -115,6 +115,34 @@ def laplacian_kpoint8th(out, src, coef, dx, dy, dz, g, shape):
     return out
 
 
+def apply_batch(hams, psis, hpsis):
+    """H psi of several independent systems (qsb_ham_apply_batch): hams a list of
+    Hamiltonian, psis / hpsis lists of [nb_i, N_i] real CUDA tensors of one dtype."""
+    n = len(hams)
+    dt = _dtype_code(psis[0])
+    nb = np.array([p.numel() // h.N for h, p in zip(hams, psis)], np.int32)
+    harr = (ctypes.c_void_p * n)(*[h._h.value for h in hams])
+    parr = (ctypes.c_void_p * n)(*[_dev_ptr(p).value for p in psis])
+    oarr = (ctypes.c_void_p * n)(*[_dev_ptr(p).value for p in hpsis])
+    _check(lib.qsb_ham_apply_batch(dt, n, harr, nb.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), parr, oarr,
+                                   _stream_ptr(psis[0])))
+    return hpsis
+
+
+def set_autotune(enable):
+    """qsb_set_autotune: time the stencil kernels (and batched vs per-system) on first use of a shape."""
+    _check(lib.qsb_set_autotune(int(bool(enable))))
+
+
+def autotune_report():
+    """The autotuner's decision log (qsb_autotune_report)."""
+    need = ctypes.c_int()
+    _check(lib.qsb_autotune_report(None, 0, ctypes.byref(need)))
+    buf = ctypes.create_string_buffer(max(1, need.value))
+    _check(lib.qsb_autotune_report(buf, len(buf), None))
+    return buf.value.decode()
+
+
 def fermi_occupations(eig, n_el, kbt, weights=None):
     """(occupations in [0, 2], mu) of the levels eig with k weights (qsb_fermi_occupations; host)."""
     e, e_p = _f64(np.asarray(eig, np.float64).ravel())
