@@ -592,6 +592,104 @@ def scf_c0_section():
     return out
 
 
+def config4_section(scf_steps=3):
+    """Config 4's two parts on one GPU.
+    Independent systems: 32 cubic cells with edges from {32, 40, 48, 56, 64}
+    (h = 0.25 bohr), 8-64 real bands and 1-4 GTH atoms at seeded positions
+    (seed 4); one H.psi of all of them through qsb_ham_apply_batch (the FD8 + V
+    part in one persistent launch) against the systems' own qsb_ham_apply one
+    after another, and with the autotuner on.
+    k-points: config 0's cell on a 48^3 grid (h = 0.125) with the 4 x 4 x 4
+    Gamma-centred mesh (64 k-points, weight 1/64, no symmetry reduction), 24
+    complex bands per k (12 electrons), k-point SCF steps (qsb_scf_run_kpoints),
+    FP64 and mixed (complex64 bundles): wall seconds per step over `scf_steps`
+    steps from seeded orthonormal starts."""
+    import torch
+    import qsb
+    rng = np.random.default_rng(4)
+    hams, psis, outs, nbs = [], [], [], []
+    alg = 0
+    for i in range(32):
+        n = int(rng.choice([32, 40, 48, 56, 64]))
+        nb = int(rng.integers(8, 65))
+        na = int(rng.integers(1, 5))
+        hh = 0.25
+        pos = rng.uniform(0, n * hh, (na, 3))
+        H = qsb.Hamiltonian(n, n, n, hh, hh, hh)
+        H.set_potential(rng.uniform(-1, 1, n ** 3))
+        H.set_gth_projectors(pos, [0] * na, [GTH["nl"]], [GTH["r"]], [GTH["h"]], RCUT)
+        hams.append(H)
+        psis.append(torch.rand(nb, n ** 3, dtype=torch.float64, device="cuda") - 0.5)
+        outs.append(torch.empty_like(psis[-1]))
+        nbs.append(nb)
+        alg += nb * n ** 3 * 16 + n ** 3 * 8
+    out = {"systems": {"count": 32, "bands_total": int(sum(nbs)),
+                       "grid_points_total": int(sum(h.N for h in hams)), "algorithmic_bytes": alg}}
+
+    def timed(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def per_system():
+        for H, p, o in zip(hams, psis, outs):
+            H.apply(p, o)
+    t_b = timed(lambda: qsb.apply_batch(hams, psis, outs))
+    t_p = timed(per_system)
+    qsb.set_autotune(True)
+    t_t = timed(lambda: qsb.apply_batch(hams, psis, outs))
+    qsb.set_autotune(False)
+    out["systems"].update({"batched_ms": t_b, "per_system_ms": t_p, "autotuned_ms": t_t,
+                           "batched_gbs": alg / t_b / 1e6, "per_system_gbs": alg / t_p / 1e6,
+                           "autotune_log": qsb.autotune_report().strip().splitlines()[-1:]})
+    for H in hams:
+        H.close()
+    del psis, outs
+    torch.cuda.empty_cache()
+    # k-point part
+    n, nb, n_el = 48, 24, 12.0
+    hh = A_CELL / n
+    N = n ** 3
+    b = 2 * math.pi / A_CELL
+    kvec = np.array([[i * b / 4, j * b / 4, k * b / 4] for i in range(4) for j in range(4) for k in range(4)])
+    w = np.full(64, 1.0 / 64)
+    pos = np.array([[0.0, 0.0, 0.0], [0.5 * A_CELL] * 3])
+    kp = {"kpoints": 64, "grid": [n, n, n], "bands_per_k": nb, "electrons": n_el, "steps_timed": scf_steps}
+    for prec in ("fp64", "mixed"):
+        H = qsb.Hamiltonian(n, n, n, hh, hh, hh)
+        H.set_gth_projectors(pos, [0, 0], [GTH["nl"]], [GTH["r"]], [GTH["h"]], RCUT)
+        H.set_potential(np.zeros(N))
+        es = qsb.EigenSolver(N, nb, True, prec)
+        scf = qsb.SCF(H, es, nb, n_el)
+        scf.set_gth_local(pos, [0, 0], [GTH_LOCAL["zion"]], [GTH_LOCAL["rloc"]], [GTH_LOCAL["c1"]], [GTH_LOCAL["c2"]])
+        scf.set_kpoints(kvec, w)
+        gen = torch.Generator(device="cuda").manual_seed(4)
+        Xs = []
+        for k in range(64):
+            x = torch.rand(nb, 2, N, dtype=torch.float64, device="cuda", generator=gen) - 0.5
+            Xs.append(qsb.orthonormalize(x, N, hh ** 3, True))
+        keeps = [torch.zeros_like(x) for x in Xs]
+        scf.run_kpoints(Xs, keeps, 4, 1, 1e-6)            # sizes the workspaces
+        torch.cuda.synchronize()
+        e, ev, occ = scf.run_kpoints(Xs, keeps, 4, scf_steps, 1e-12)
+        t = scf.step_seconds()
+        kp[prec] = {"seconds_per_step": float(np.mean(t)), "steps": len(e), "last_energy_ha": float(e[-1])}
+        scf.close()
+        es.close()
+        H.close()
+        del Xs, keeps
+        torch.cuda.empty_cache()
+    kp["speedup_per_step_mixed_vs_fp64"] = kp["fp64"]["seconds_per_step"] / kp["mixed"]["seconds_per_step"]
+    out["kpoints"] = kp
+    return out
+
+
 def relax_section(fmax=1e-4):
     """Wall time of the LBFGS relaxation of config 1 (qsb_relax_lbfgs: SCF warm
     from the previous geometry's states, local + nonlocal + Ewald forces) from
@@ -683,6 +781,9 @@ def main():
     ap.add_argument("--scf-polish-steps", type=int, default=12,
                     help="FP64 polish steps allowed after the mixed run's own stop (0: no polish)")
     ap.add_argument("--scf-max-steps", type=int, default=None, help="SCF step cap (default 120 for c2, 160 for c3)")
+    ap.add_argument("--config4", action="store_true",
+                    help="also run config 4: 32 uneven independent systems through the batched H.psi, and "
+                         "k-point SCF steps at 64 k x 48^3 x 24 complex bands (FP64 and mixed)")
     ap.add_argument("--only-hpsi", action="store_true",
                     help="time the device-resident H.psi only (no e2e, FFT, Gram, LOBPCG, SCF or CPU sections); "
                          "the profiler captures use it")
@@ -800,6 +901,7 @@ def main():
                           args.scf_polish_steps)
     relax = relax_section() if args.relax and world == 1 else None
     scf_c0 = scf_c0_section() if not args.no_scf and world == 1 else None
+    config4 = config4_section() if args.config4 and world == 1 else None
     clk = clocks.stop()
 
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist, "cuda")
@@ -841,6 +943,7 @@ def main():
         "lobpcg": lob,
         "scf": scf,
         "scf_c0": scf_c0,
+        "config4": config4,
         "gram": gram,
         "clocks": clk,
     }

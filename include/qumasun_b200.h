@@ -163,8 +163,10 @@ QSB_API qsb_status qsb_ham_apply_host(qsb_ham* ham, qsb_dtype dtype, int is_comp
 /* H psi of n_sys independent systems at once (real bands, Gamma point, FD8
  * kinetic): hpsi[i] = H_i psi[i] for nb[i] bands of system i (each its own
  * qsb_ham: grid, spacing, potential, projectors).  The FD8 + V part of all
- * systems runs in ONE persistent launch over a work list of (system, 32 x 8
- * column tile, z chunk, band) items, largest systems first; each system's
+ * systems runs in ONE persistent launch over a work list of (system, tile of
+ * 32 x 16 points (FP32: 32 x 32), 32-plane z chunk, band) items, largest
+ * systems first, each item the tile work of the register-prefetch stencil
+ * (results equal the per-system FP32 stencil's bit for bit); each system's
  * nonlocal projection and expansion keep their own launches.  The reference
  * applies H system by system (mHamiltonianMatrix_ddm, source/qumasun_base1.matrix.h:263-291);
  * for many small, uneven cells a launch per system leaves most SMs idle.

@@ -13,11 +13,11 @@
 // projections run before the batched stencil and the expansions after it, as
 // in qsb_ham_apply.
 //
-// Each thread owns one grid column of its tile and marches z with the 9-deep
-// column in registers; x and y neighbours come through the read-only data path
-// (L1), so a tile reads its psi once from HBM plus its 4-wide halo.  Sums in the
-// order of the per-system stencils (d = c0 p; d += x terms; d += y terms;
-// d += z terms; out = V p + d), so FP32 keeps their rounding behaviour.
+// A persistent CTA runs, item after item, the tile work of the register-prefetch
+// stencil (fd8_tile in stencil.cu: the tile plane with its 4-wide halo in a
+// double-buffered shared tile, the z column of each thread's rows in
+// registers, every global load issued planes ahead), so its arithmetic and
+// summation order are those of the per-system FP32 stencil.
 #include "qsb_internal.h"
 
 #include <algorithm>
@@ -27,129 +27,6 @@
 #include <vector>
 
 namespace {
-
-constexpr int BTX = 32, BTY = 8, BNT = BTX * BTY;   // item tile and threads per CTA
-constexpr int BZ = 32;                              // planes per item (z chunk)
-
-template <typename T>
-struct BSys {
-    const T* in;
-    T* out;
-    const T* V;
-    int nx, ny, nz;
-    qsb::KC<T> k;
-};
-
-struct BItem {
-    int sys, x0, y0, z0, band;
-};
-
-__device__ __forceinline__ int bwrap(int v, int n) {
-    const int m = v % n;
-    return m < 0 ? m + n : m;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(BNT) fd8_batch_kernel(const BSys<T>* __restrict__ sys, const BItem* __restrict__ items,
-                                                         int n_items) {
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
-        const BItem w = items[it];
-        const BSys<T> S = sys[w.sys];
-        const int x = w.x0 + tx, y = w.y0 + ty;
-        if (x >= S.nx || y >= S.ny) continue;
-        const size_t nxy = (size_t)S.nx * S.ny;
-        const size_t N = nxy * S.nz;
-        const T* src = S.in + (size_t)w.band * N;
-        T* dst = S.out + (size_t)w.band * N;
-        const int z1 = min(S.nz, w.z0 + BZ);
-        int xo[8], yo[8];
-#pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            xo[m] = bwrap(x - 4 + m, S.nx);
-            xo[7 - m] = bwrap(x + 4 - m, S.nx);
-            yo[m] = bwrap(y - 4 + m, S.ny) * S.nx;
-            yo[7 - m] = bwrap(y + 4 - m, S.ny) * S.nx;
-        }
-        const size_t col = (size_t)y * S.nx + x;
-        T q[9];   // z - 4 .. z + 4 of this column
-#pragma unroll
-        for (int m = 0; m < 8; ++m) q[m] = __ldg(src + (size_t)bwrap(w.z0 - 4 + m, S.nz) * nxy + col);
-        for (int z = w.z0; z < z1; ++z) {
-            q[8] = __ldg(src + (size_t)bwrap(z + 4, S.nz) * nxy + col);
-            const T* pl = src + (size_t)z * nxy;
-            const size_t row = (size_t)y * S.nx;
-            const T xm4 = __ldg(pl + row + xo[0]), xm3 = __ldg(pl + row + xo[1]);
-            const T xm2 = __ldg(pl + row + xo[2]), xm1 = __ldg(pl + row + xo[3]);
-            const T xp4 = __ldg(pl + row + xo[7]), xp3 = __ldg(pl + row + xo[6]);
-            const T xp2 = __ldg(pl + row + xo[5]), xp1 = __ldg(pl + row + xo[4]);
-            const T ym4 = __ldg(pl + yo[0] + x), ym3 = __ldg(pl + yo[1] + x);
-            const T ym2 = __ldg(pl + yo[2] + x), ym1 = __ldg(pl + yo[3] + x);
-            const T yp4 = __ldg(pl + yo[7] + x), yp3 = __ldg(pl + yo[6] + x);
-            const T yp2 = __ldg(pl + yo[5] + x), yp1 = __ldg(pl + yo[4] + x);
-            const T p = q[4];
-            const qsb::KC<T>& k = S.k;
-            T d = k.c0 * p;
-            d += k.cx[3] * (xp4 + xm4) + k.cx[2] * (xp3 + xm3) + k.cx[1] * (xp2 + xm2) + k.cx[0] * (xp1 + xm1);
-            d += k.cy[3] * (yp4 + ym4) + k.cy[2] * (yp3 + ym3) + k.cy[1] * (yp2 + ym2) + k.cy[0] * (yp1 + ym1);
-            d += k.cz[3] * (q[8] + q[0]) + k.cz[2] * (q[7] + q[1]) + k.cz[1] * (q[6] + q[2]) + k.cz[0] * (q[5] + q[3]);
-            if constexpr (sizeof(T) == 4) d = fmaf(k.c0lo, p, d);
-            dst[(size_t)z * nxy + col] = __ldg(S.V + (size_t)z * nxy + col) * p + d;
-#pragma unroll
-            for (int m = 0; m < 8; ++m) q[m] = q[m + 1];
-        }
-    }
-}
-
-template <typename T>
-qsb_status launch_batch(int n, qsb_ham* const* hams, const int* nb, const void* const* psi, void* const* hpsi,
-                        cudaStream_t s, int* launches) {
-    std::vector<BSys<T>> hs(n);
-    std::vector<BItem> items;
-    std::vector<std::pair<long long, int>> order;   // (work, system): largest first
-    for (int i = 0; i < n; ++i) {
-        const qsb_ham* h = hams[i];
-        hs[i] = BSys<T>{(const T*)psi[i], (T*)hpsi[i],
-                        sizeof(T) == 8 ? (const T*)(const void*)h->V64 : (const T*)(const void*)h->V32, h->nx, h->ny,
-                        h->nz, qsb::to_kc<T>(qsb::make_fd8_coef(-0.5, h->dx, h->dy, h->dz, 0, 0, 0))};
-        order.push_back({(long long)h->N * nb[i], i});
-    }
-    std::sort(order.begin(), order.end(), [](const std::pair<long long, int>& a, const std::pair<long long, int>& b) {
-        return a.first != b.first ? a.first > b.first : a.second < b.second;
-    });
-    for (const auto& o : order) {
-        const int i = o.second;
-        const qsb_ham* h = hams[i];
-        for (int b = 0; b < nb[i]; ++b)
-            for (int z0 = 0; z0 < h->nz; z0 += BZ)
-                for (int y0 = 0; y0 < h->ny; y0 += BTY)
-                    for (int x0 = 0; x0 < h->nx; x0 += BTX) items.push_back(BItem{i, x0, y0, z0, b});
-    }
-    if (items.empty()) return QSB_OK;
-    if (items.size() > (size_t)0x7fffffff) return qsb::fail(QSB_ERR_INVALID, "ham_apply_batch: too many work items");
-    // descriptors and the work list in one device block, freed once the launch is done
-    const size_t sys_bytes = hs.size() * sizeof(BSys<T>);
-    const size_t off_items = (sys_bytes + 255) / 256 * 256;
-    const size_t bytes = off_items + items.size() * sizeof(BItem);
-    void* dmem = nullptr;
-    QSB_CUDA_TRY(cudaMallocAsync(&dmem, bytes, s));
-    QSB_CUDA_TRY(cudaMemcpyAsync(dmem, hs.data(), sys_bytes, cudaMemcpyHostToDevice, s));
-    QSB_CUDA_TRY(cudaMemcpyAsync((char*)dmem + off_items, items.data(), items.size() * sizeof(BItem),
-                                 cudaMemcpyHostToDevice, s));
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int grid = (int)std::min<size_t>(items.size(), (size_t)sms * 8);
-    fd8_batch_kernel<T><<<grid, dim3(BTX, BTY), 0, s>>>((const BSys<T>*)dmem, (const BItem*)((char*)dmem + off_items),
-                                                        (int)items.size());
-    const cudaError_t e = cudaGetLastError();
-    cudaFreeAsync(dmem, s);
-    if (e != cudaSuccess) return qsb::cuda_fail(e, "fd8_batch_kernel");
-    ++*launches;
-    // the host copies above are pageable: wait until they have been read
-    QSB_CUDA_TRY(cudaStreamSynchronize(s));
-    return QSB_OK;
-}
 
 // batched-or-not decisions of the autotuner, by the set's shape
 std::mutex g_batch_mu;
@@ -247,8 +124,14 @@ qsb_status apply_batched(qsb_dtype dtype, int n_sys, qsb_ham* const* hams, const
         launches += 2;
     }
     // 2) V psi - 1/2 FD8 psi of all systems in one persistent launch
-    if (dtype == QSB_F64) QSB_TRY(launch_batch<double>(n_sys, hams, nb, psi, hpsi, s, &launches));
-    else QSB_TRY(launch_batch<float>(n_sys, hams, nb, psi, hpsi, s, &launches));
+    std::vector<qsb::BatchSysDesc> d(n_sys);
+    for (int i = 0; i < n_sys; ++i) {
+        const qsb_ham* h = hams[i];
+        d[i] = qsb::BatchSysDesc{psi[i], hpsi[i], dtype == QSB_F64 ? (const void*)h->V64 : (const void*)h->V32,
+                                 h->nx, h->ny, h->nz, nb[i], qsb::make_fd8_coef(-0.5, h->dx, h->dy, h->dz, 0, 0, 0)};
+    }
+    QSB_TRY(qsb::launch_stencil_batch(dtype, n_sys, d.data(), s));
+    ++launches;
     // 3) + the nonlocal expansion of every system
     for (int i = 0; i < n_sys; ++i) {
         if (!coef[i]) continue;

@@ -90,6 +90,16 @@ struct StencilLaunch {
 int* device_error_word();
 
 qsb_status launch_stencil(qsb_dtype dt, const StencilLaunch& L, const FD8Coef& c, cudaStream_t s);
+// One system of the batched stencil (stencil.cu): real bundle of nb bands,
+// out = V in + FD8 coefficients applied to in (the H psi local part).
+struct BatchSysDesc {
+    const void* in;
+    void* out;
+    const void* V;
+    int nx, ny, nz, nb;
+    FD8Coef coef;
+};
+qsb_status launch_stencil_batch(qsb_dtype dt, int n, const BatchSysDesc* d, cudaStream_t s);
 // Autotuner state (stencil.cu): whether qsb_set_autotune is on, and a line for
 // the decision log qsb_autotune_report returns.
 bool autotune_enabled();

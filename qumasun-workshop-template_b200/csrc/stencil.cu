@@ -23,6 +23,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <vector>
 
 namespace qsb {
 
@@ -76,24 +77,21 @@ __device__ __forceinline__ int wrapi(int v, int n) {
 //
 // MODE 0: out += L(psi)      (Laplacian8th / LaplacianKpoint8th "+=")
 // MODE 1: out = V psi + L(psi)   (the local part of mHamiltonianMatrix_ddm)
+//
+// The work of one CTA (tile x0, y0 of band `band`, planes [z0, z1)) is the
+// device function fd8_tile, shared by fd8_kernel (one item per CTA) and
+// fd8_batch_kernel (a persistent CTA walking a list of items of many systems).
 template <typename T, bool CPLX, int MODE, bool GRAD, int RY>
-__global__ void __launch_bounds__(NT, (CPLX && sizeof(T) == 8) ? 1 : 2)
-fd8_kernel(const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ V,
-           int nx, int ny, int nz, int zchunk, KC<T> k) {
+__device__ __forceinline__ void fd8_tile(const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ V,
+                                         int nx, int ny, int nz, int x0, int y0, int z0, int z1, int band,
+                                         const KC<T>& k, T* smraw) {
     constexpr int NC = CPLX ? 2 : 1;
     constexpr int TY = BY * RY;
     constexpr int SW = TX + 2 * HW;
     constexpr int SH = TY + 2 * HW;
-    __shared__ T sm[2][NC][SH][SW];
-
-    const int ntx = (nx + TX - 1) / TX;
-    const int x0 = (blockIdx.x % ntx) * TX;
-    const int y0 = (blockIdx.x / ntx) * TY;
+    T(*sm)[NC][SH][SW] = reinterpret_cast<T(*)[NC][SH][SW]>(smraw);
     const int wx = min(TX, nx - x0);
     const int wy = min(TY, ny - y0);
-    const int z0 = blockIdx.y * zchunk;
-    const int z1 = min(nz, z0 + zchunk);
-    const int band = blockIdx.z;
     const size_t nxy = (size_t)nx * ny;
     const size_t N = nxy * nz;
 
@@ -276,6 +274,49 @@ fd8_kernel(const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ 
                 }
             }
         }
+    }
+}
+
+template <typename T, bool CPLX, int MODE, bool GRAD, int RY>
+__global__ void __launch_bounds__(NT, (CPLX && sizeof(T) == 8) ? 1 : 2)
+fd8_kernel(const T* __restrict__ in, T* __restrict__ out, const T* __restrict__ V,
+           int nx, int ny, int nz, int zchunk, KC<T> k) {
+    constexpr int NC = CPLX ? 2 : 1;
+    constexpr int TY = BY * RY;
+    __shared__ T sm[2 * NC * (TY + 2 * HW) * (TX + 2 * HW)];
+    const int ntx = (nx + TX - 1) / TX;
+    const int z0 = blockIdx.y * zchunk;
+    fd8_tile<T, CPLX, MODE, GRAD, RY>(in, out, V, nx, ny, nz, (blockIdx.x % ntx) * TX, (blockIdx.x / ntx) * TY, z0,
+                                      min(nz, z0 + zchunk), blockIdx.z, k, sm);
+}
+
+// Batched form (qsb_ham_apply_batch): real bands, MODE 1 (out = V psi + L psi),
+// a persistent grid walking (system, tile, z chunk, band) items of many grids.
+template <typename T>
+struct BatchSys {
+    const T* in;
+    T* out;
+    const T* V;
+    int nx, ny, nz;
+    KC<T> k;
+};
+struct BatchItem {
+    int sys, x0, y0, z0, z1, band;
+};
+template <typename T>
+constexpr int batch_ry() { return sizeof(T) == 8 ? 2 : 4; }
+
+template <typename T>
+__global__ void __launch_bounds__(NT, 2)
+fd8_batch_kernel(const BatchSys<T>* __restrict__ sys, const BatchItem* __restrict__ items, int n_items) {
+    constexpr int RY = batch_ry<T>();
+    constexpr int TY = BY * RY;
+    __shared__ T sm[2 * (TY + 2 * HW) * (TX + 2 * HW)];
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const BatchItem w = items[it];
+        const BatchSys<T>& S = sys[w.sys];
+        fd8_tile<T, false, 1, false, RY>(S.in, S.out, S.V, S.nx, S.ny, S.nz, w.x0, w.y0, w.z0, w.z1, w.band, S.k, sm);
+        __syncthreads();   // the next item reuses the shared tiles
     }
 }
 
@@ -825,12 +866,10 @@ __device__ __forceinline__ WsItem ws_item(int w, int nx, int ny, int nz, int zch
 // four), 65536 / 384 = 170 -> 168 per thread at one CTA per SM.  With the cap
 // stated directly the compiler kept the 168-register form free of the spills
 // the launch-bounds form had (0.450 -> 0.417 ms at 96^3 x 128 bands, FP64).
-template <int RY, int MINB>
-struct WsRegs {
-    static constexpr int value = MINB == 1 ? 168 : 65536 / (MINB * 384) / 8 * 8;
-};
-template <typename T, bool CPLX, int MODE, bool GRAD, bool ISO, int RY, int S, int MINB>
-__global__ void __maxnreg__((WsRegs<RY, MINB>::value))
+// WT: the wait-limit test form (compute_poll_limit set); a separate
+// instantiation, so that the production kernel carries none of it.
+template <typename T, bool CPLX, int MODE, bool GRAD, bool ISO, int RY, int S, bool WT>
+__global__ void __maxnreg__(168)
 fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, int ny, int nz, int zchunk, int tiles,
               int nzc, int items, KC<T> k, int* __restrict__ err, unsigned cpolls) {
     using C = WsCfg<T, CPLX, MODE, RY, S>;
@@ -850,14 +889,14 @@ fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, 
     // the compute warps first wait, with that limit, on a barrier nothing
     // arrives at, and the producer's stage-release waits use it too; the
     // producer's drain of its own copies keeps the full limit
-    const bool wait_test = cpolls < WAIT_LIMIT;
+    constexpr bool wait_test = WT;
 
     if (t == 0) {
         for (int st = 0; st < S; ++st) {
             mbar_init(&full[st], 1);
             mbar_init(&empty[st], WCW);
         }
-        mbar_init(never, 1);
+        if constexpr (WT) mbar_init(never, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -874,7 +913,7 @@ fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, 
         for (int j = 0; j < nplanes; ++j) {
             const int st = j % S;
             // stage st last held plane j - S: wait until every compute warp released it
-            if (j >= S && !mbar_wait(&empty[st], (uint32_t)(((j / S) - 1) & 1), wait_test ? cpolls : WAIT_LIMIT)) {
+            if (j >= S && !mbar_wait(&empty[st], (uint32_t)(((j / S) - 1) & 1), WT ? cpolls : WAIT_LIMIT)) {
                 failed = true;
                 break;
             }
@@ -932,7 +971,8 @@ fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, 
     const int tx = threadIdx.x, ty = threadIdx.y;
     const uint32_t soff = ((ty * RY + HW) * SW + 2 * tx + HW) * TB;    // centre pair (main box)
     const uint32_t eoff = (C::OFF_E + ty * RY * ZTX + 2 * tx) * TB;    // V / old output pair
-    bool failed = wait_test && __any_sync(0xffffffffu, !mbar_wait(never, 0, cpolls));
+    bool failed = false;
+    if constexpr (WT) failed = __any_sync(0xffffffffu, !mbar_wait(never, 0, cpolls));
     {
     const WsItem it = ws_item<TY>(blockIdx.x, nx, ny, nz, zchunk, tiles, nzc);
     const int x0 = it.x0, y0 = it.y0, z0 = it.z0, nsteps = it.nsteps, band = it.band;
@@ -986,7 +1026,7 @@ fd8_ws_kernel(const __grid_constant__ WsMaps maps, T* __restrict__ out, int nx, 
             const int j = jb + u;
             if (j < nplanes && !failed) {
                 const int st = j % S;
-                const bool ok = mbar_wait(&full[st], (uint32_t)((j / S) & 1), cpolls);
+                const bool ok = mbar_wait(&full[st], (uint32_t)((j / S) & 1), WT ? cpolls : WAIT_LIMIT);
                 if (__any_sync(0xffffffffu, !ok)) {
                     failed = true;
                     continue;
@@ -1270,10 +1310,16 @@ bool launch_ws(const StencilLaunch& L, const FD8Coef& c, const KC<T>& k, cudaStr
     // equal x and y weights (hx == hy): the x and y pairs of each offset are summed first
     bool iso = true;
     for (int q = 0; q < 4; ++q) iso = iso && k.cx[q] == k.cy[q];
-    auto kern = CPLX && c.has_grad ? (iso ? fd8_ws_kernel<T, CPLX, MODE, CPLX, true, RY, S, MINB>
-                                          : fd8_ws_kernel<T, CPLX, MODE, CPLX, false, RY, S, MINB>)
-                                   : (iso ? fd8_ws_kernel<T, CPLX, MODE, false, true, RY, S, MINB>
-                                          : fd8_ws_kernel<T, CPLX, MODE, false, false, RY, S, MINB>);
+    const bool wt = compute_poll_limit() < WAIT_LIMIT;
+    auto kern = CPLX && c.has_grad ? (iso ? fd8_ws_kernel<T, CPLX, MODE, CPLX, true, RY, S, false>
+                                          : fd8_ws_kernel<T, CPLX, MODE, CPLX, false, RY, S, false>)
+                                   : (iso ? fd8_ws_kernel<T, CPLX, MODE, false, true, RY, S, false>
+                                          : fd8_ws_kernel<T, CPLX, MODE, false, false, RY, S, false>);
+    if (wt)
+        kern = CPLX && c.has_grad ? (iso ? fd8_ws_kernel<T, CPLX, MODE, CPLX, true, RY, S, true>
+                                         : fd8_ws_kernel<T, CPLX, MODE, CPLX, false, RY, S, true>)
+                                  : (iso ? fd8_ws_kernel<T, CPLX, MODE, false, true, RY, S, true>
+                                         : fd8_ws_kernel<T, CPLX, MODE, false, false, RY, S, true>);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
     kern<<<grid, block, C::SMEM, s>>>(m, (T*)L.out, L.nx, L.ny, L.nz, zchunk, tiles, nzc, (int)items, k,
                                       device_error_word(), compute_poll_limit());
@@ -1460,6 +1506,52 @@ qsb_status launch_stencil(qsb_dtype dt, const StencilLaunch& L, const FD8Coef& c
     if (dt == QSB_F64 && L.mode == 1 && forced == 0 && tune_state().on) return tune_and_launch(dt, L, c, s);
     if (dt == QSB_F64) return launch_dtype<double>(L, c, s, forced);
     return launch_dtype<float>(L, c, s, forced);
+}
+
+template <typename T>
+qsb_status stencil_batch_t(int n, const BatchSysDesc* d, cudaStream_t s) {
+    constexpr int TY = BY * batch_ry<T>();
+    constexpr int ZC = 32;   // planes per item
+    std::vector<BatchSys<T>> hs(n);
+    std::vector<BatchItem> items;
+    std::vector<std::pair<long long, int>> order;
+    for (int i = 0; i < n; ++i) {
+        hs[i] = BatchSys<T>{(const T*)d[i].in, (T*)d[i].out, (const T*)d[i].V, d[i].nx, d[i].ny, d[i].nz,
+                            to_kc<T>(d[i].coef)};
+        order.push_back({(long long)d[i].nx * d[i].ny * d[i].nz * d[i].nb, i});
+    }
+    // largest systems first, so the smallest fill the tail
+    std::sort(order.begin(), order.end(), [](const std::pair<long long, int>& a, const std::pair<long long, int>& b) {
+        return a.first != b.first ? a.first > b.first : a.second < b.second;
+    });
+    for (const auto& o : order) {
+        const BatchSysDesc& q = d[o.second];
+        for (int b = 0; b < q.nb; ++b)
+            for (int z0 = 0; z0 < q.nz; z0 += ZC)
+                for (int y0 = 0; y0 < q.ny; y0 += TY)
+                    for (int x0 = 0; x0 < q.nx; x0 += TX)
+                        items.push_back(BatchItem{o.second, x0, y0, z0, std::min(q.nz, z0 + ZC), b});
+    }
+    if (items.empty()) return QSB_OK;
+    if (items.size() > (size_t)0x7fffffff) return fail(QSB_ERR_INVALID, "stencil batch: too many work items");
+    const size_t sys_bytes = hs.size() * sizeof(BatchSys<T>);
+    const size_t off = (sys_bytes + 255) / 256 * 256;
+    void* dmem = nullptr;
+    QSB_CUDA_TRY(cudaMallocAsync(&dmem, off + items.size() * sizeof(BatchItem), s));
+    QSB_CUDA_TRY(cudaMemcpyAsync(dmem, hs.data(), sys_bytes, cudaMemcpyHostToDevice, s));
+    QSB_CUDA_TRY(cudaMemcpyAsync((char*)dmem + off, items.data(), items.size() * sizeof(BatchItem),
+                                 cudaMemcpyHostToDevice, s));
+    const int grid = (int)std::min<size_t>(items.size(), (size_t)sm_count() * 2);
+    fd8_batch_kernel<T><<<grid, dim3(TX, BY), 0, s>>>((const BatchSys<T>*)dmem, (const BatchItem*)((char*)dmem + off),
+                                                      (int)items.size());
+    const cudaError_t e = cudaGetLastError();
+    cudaFreeAsync(dmem, s);
+    if (e != cudaSuccess) return cuda_fail(e, "fd8_batch_kernel");
+    return QSB_OK;
+}
+
+qsb_status launch_stencil_batch(qsb_dtype dt, int n, const BatchSysDesc* d, cudaStream_t s) {
+    return dt == QSB_F64 ? stencil_batch_t<double>(n, d, s) : stencil_batch_t<float>(n, d, s);
 }
 
 bool autotune_enabled() { return tune_state().on; }
