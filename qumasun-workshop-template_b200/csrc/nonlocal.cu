@@ -64,14 +64,18 @@ inline int fold(int v, int n) {
 // ---------------------------------------------------------------------------
 template <typename T, bool CPLX, int WM, int CB, int UP, int MINB>
 __global__ void __launch_bounds__(PROJ_THREADS, MINB)
-nl_proj_kernel(const int* __restrict__ chunk_begin, const int* __restrict__ chunk_end,
-               const int* __restrict__ pt_idx, const int* __restrict__ pt_xyz, const T* __restrict__ pt_beta,
-               int wmax, const T* __restrict__ psi, size_t N, int nb, double gx_dx, double gy_dy, double gz_dz,
-               double* __restrict__ partial, int ncol) {
+nl_proj_kernel(const int* __restrict__ chunk_order, const int* __restrict__ chunk_begin,
+               const int* __restrict__ chunk_end, const int* __restrict__ pt_idx, const int* __restrict__ pt_xyz,
+               const T* __restrict__ pt_beta, int wmax, const T* __restrict__ psi, size_t N, int nb, double gx_dx,
+               double gy_dy, double gz_dz, double* __restrict__ partial, int ncol) {
     constexpr int NCB = CPLX ? 2 * CB : CB;
     constexpr int NV = WM * NCB;
-    const int chunk = blockIdx.x;
-    const int band0 = blockIdx.y * CB;
+    // launch order: chunks of all atoms by their position along the grid, so
+    // that the CTAs in flight together gather from the same region of psi and
+    // the overlapping spheres of neighbouring atoms meet in L2; each CTA writes
+    // the partials of its own chunk, so the sums do not depend on the order
+    const int chunk = chunk_order[blockIdx.y];
+    const int band0 = blockIdx.x * CB;
     const int nbl = min(CB, nb - band0);
     const int p0 = chunk_begin[chunk], p1 = chunk_end[chunk];
 
@@ -444,8 +448,9 @@ void launch_proj(const NLDevice& d, int table, int nb, const void* psi, size_t N
     constexpr int CB = CPLX ? 4 : 8;
     constexpr int UP = (WM <= 4 && !CPLX) ? 2 : 1;
     constexpr int MINB = WM <= 4 ? 2 : 1;
-    dim3 grid(d.n_chunks, (nb + CB - 1) / CB);
-    nl_proj_kernel<T, CPLX, WM, CB, UP, MINB><<<grid, PROJ_THREADS, 0, s>>>(d.chunk_begin, d.chunk_end, d.pt_idx, d.pt_xyz,
+    dim3 grid((nb + CB - 1) / CB, d.n_chunks);
+    nl_proj_kernel<T, CPLX, WM, CB, UP, MINB><<<grid, PROJ_THREADS, 0, s>>>(d.chunk_order, d.chunk_begin, d.chunk_end,
+                                                                        d.pt_idx, d.pt_xyz,
                                                                         beta, d.wmax, (const T*)psi, N, nb, gx_dx,
                                                                         gy_dy, gz_dz, partial, ncol);
 }
@@ -502,7 +507,7 @@ __global__ void nl_energy_force_kernel(const double* __restrict__ c, const doubl
 void nl_free(NLDevice& d) {
     dfree(d.pt_idx); dfree(d.pt_xyz); dfree(d.pt_beta64); dfree(d.pt_beta32);
     dfree(d.atom_width); dfree(d.atom_proj_off); dfree(d.atom_E);
-    dfree(d.chunk_atom); dfree(d.chunk_begin); dfree(d.chunk_end);
+    dfree(d.chunk_atom); dfree(d.chunk_begin); dfree(d.chunk_end); dfree(d.chunk_order);
     dfree(d.atom_chunk_begin); dfree(d.atom_chunk_end);
     dfree(d.grid_ptr); dfree(d.cov_grid); dfree(d.ent_atom); dfree(d.ent_xyz);
     dfree(d.ent_beta64); dfree(d.ent_beta32);
@@ -585,6 +590,14 @@ qsb_status nl_upload(NLDevice& d, int nx, int ny, int nz, int n_atoms, const int
         }
     }
     d.n_chunks = (int)chunk_b.size();
+    // launch order of the projection: by the grid index of each chunk's middle point
+    std::vector<int> corder(d.n_chunks);
+    std::iota(corder.begin(), corder.end(), 0);
+    {
+        std::vector<int> mid(d.n_chunks);
+        for (int c = 0; c < d.n_chunks; ++c) mid[c] = idx[(chunk_b[c] + chunk_e[c] - 1) / 2];
+        std::stable_sort(corder.begin(), corder.end(), [&](int u, int v) { return mid[u] < mid[v]; });
+    }
 
     // grid-ordered CSR (counting sort by folded index, stable in atom-major order)
     std::vector<int> gptr(N + 1, 0);
@@ -613,6 +626,7 @@ qsb_status nl_upload(NLDevice& d, int nx, int ny, int nz, int n_atoms, const int
     QSB_TRY(dupload(d.atom_proj_off, d.h_atom_proj_off.data(), (size_t)n_atoms));
     QSB_TRY(dupload(d.atom_E, E.data(), E.size()));
     QSB_TRY(dupload(d.chunk_atom, chunk_atom.data(), chunk_atom.size()));
+    QSB_TRY(dupload(d.chunk_order, corder.data(), corder.size()));
     QSB_TRY(dupload(d.chunk_begin, chunk_b.data(), chunk_b.size()));
     QSB_TRY(dupload(d.chunk_end, chunk_e.data(), chunk_e.size()));
     QSB_TRY(dupload(d.atom_chunk_begin, acb.data(), acb.size()));

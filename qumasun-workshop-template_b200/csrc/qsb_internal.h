@@ -127,6 +127,7 @@ struct NLDevice {
     // projection chunks: each chunk is a run of points of one atom
     int n_chunks = 0;
     int* chunk_atom = nullptr;
+    int* chunk_order = nullptr;    // launch order of the projection's chunks (by grid position)
     int* chunk_begin = nullptr;
     int* chunk_end = nullptr;
     int* atom_chunk_begin = nullptr;  // [n_atoms]
