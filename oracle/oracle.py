@@ -25,6 +25,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REFERENCE_ROOT = os.environ.get("QSB_REFERENCE_ROOT", "/root/reference")
 LIB_ORACLE = os.path.join(HERE, "_build", "libqsoracle.so")
 LIB_REF = os.path.join(HERE, "_ref", "libqsref.so")
+LIB_REF_FFT = os.path.join(HERE, "_ref", "libqsref_fft.so")
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -63,6 +64,52 @@ def ref_lib():
     if _ref is None:
         _ref = ctypes.CDLL(LIB_REF)
     return _ref
+
+
+_ref_fft = None
+
+
+def ref_fft_available():
+    return os.path.exists(LIB_REF_FFT)
+
+
+def ref_hamiltonian_fft(grid, V, psi, nb, is_complex=False, ksample=(1, 1, 1), kidx=(0, 0, 0)):
+    """-1/2 (grad + i k)^2 psi + V psi by the reference's own FFT-kinetic
+    Hamiltonian (QUMASUN_BASE1::mHamiltonianMatrix_ddm_bundle, algorithm 1,
+    source/qumasun_base1.matrix.h:142-228, run on a reference object without
+    nuclei: oracle/ref_fft.cpp, oracle/_ref/libqsref_fft.so), FFTW replaced by
+    the DFT restated in oracle/ref_shim/fftw_dft.cpp.  k_d = kidx_d * 2 pi /
+    (n_d h_d ksample_d), the reference's k-point indexing.  Real bands run as
+    complex bands with zero imaginary part; the real part is returned."""
+    global _ref_fft
+    if _ref_fft is None:
+        _ref_fft = ctypes.CDLL(LIB_REF_FFT)
+        _ref_fft.qsref_ham_fft.restype = ctypes.c_int
+    nx, ny, nz, dx, dy, dz = grid
+    N = nx * ny * nz
+    psi = np.asarray(psi, np.float64)
+    if is_complex:
+        z = np.ascontiguousarray(psi)
+    else:
+        z = np.zeros((nb, 2, N))
+        z[:, 0] = psi.reshape(nb, N)
+    out = np.zeros_like(z)
+    ks = np.ascontiguousarray(ksample, np.int32)
+    ki = np.ascontiguousarray(kidx, np.int32)
+    V = np.ascontiguousarray(V, np.float64)
+    rc = _ref_fft.qsref_ham_fft(nx, ny, nz, ctypes.c_double(nx * dx), ctypes.c_double(ny * dy),
+                                ctypes.c_double(nz * dz), _i(ks), _i(ki), _d(V), nb, _d(z), _d(out))
+    assert rc == 0, "qsref_ham_fft failed"
+    if is_complex:
+        return out.reshape(psi.shape)
+    return np.ascontiguousarray(out.reshape(nb, 2, N)[:, 0]).reshape(psi.shape)
+
+
+def kpoint_vector(grid, ksample, kidx):
+    """The reference's k vector of k-point index kidx on a ksample grid:
+    k_d = kidx_d * 2 pi / (L_d ksample_d) (qumasun_base1.constructor.h:34-36)."""
+    nx, ny, nz, dx, dy, dz = grid
+    return tuple(k * 2.0 * math.pi / (n * h * s) for k, n, h, s in zip(kidx, (nx, ny, nz), (dx, dy, dz), ksample))
 
 
 # --------------------------------------------------------------------------

@@ -10,6 +10,7 @@ lapack_int LAPACKE_dsygvd(int, lapack_int, char, char, lapack_int, double*, lapa
 lapack_int LAPACKE_zhegvd(int, lapack_int, char, char, lapack_int, lapack_complex_double*, lapack_int,
                           lapack_complex_double*, lapack_int, double*);
 lapack_int LAPACKE_zheevd(int, char, char, lapack_int, lapack_complex_double*, lapack_int, double*);
+lapack_int LAPACKE_dsyevd(int, char, char, lapack_int, double*, lapack_int, double*);
 lapack_int LAPACKE_dpotrf(int, char, lapack_int, double*, lapack_int);
 lapack_int LAPACKE_zpotrf(int, char, lapack_int, lapack_complex_double*, lapack_int);
 lapack_int LAPACKE_dtrtrs(int, char, char, char, lapack_int, lapack_int, const double*, lapack_int, double*, lapack_int);

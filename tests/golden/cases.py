@@ -65,6 +65,31 @@ def _ham_oracle(inp, cplx, g):
     return O.hamiltonian(inp["grid"], inp["V"], tab, inp["psi"], inp["nb"], cplx, g)
 
 
+def _fft_inputs(grid, seed, nb, cplx):
+    N = grid[0] * grid[1] * grid[2]
+    psi = O.seeded_psi(seed, nb, N, cplx)
+    V = O.seeded_potential(seed, N)
+    return dict(grid=grid, psi=psi, V=V, nb=nb, checked=[psi, V])
+
+
+def _fft_ref(inp, cplx, ks, ki):
+    return O.ref_hamiltonian_fft(inp["grid"], inp["V"], inp["psi"], inp["nb"], cplx, ks, ki)
+
+
+def _fft_oracle(inp, cplx, ks, ki):
+    g = O.kpoint_vector(inp["grid"], ks, ki)
+    nb, N = inp["nb"], inp["V"].size
+    vpsi = (inp["psi"].reshape(-1, N) * inp["V"][None, :]).reshape(inp["psi"].shape)
+    return O.kinetic_fft(inp["grid"], inp["psi"], nb, cplx, g) + vpsi
+
+
+# the FFT-kinetic cases: k-point sampling and index of each (the reference's k)
+FFT_GRID_EVEN = (24, 20, 16, 0.25, 0.3, 0.375)
+FFT_GRID_ODD = (15, 12, 9, 0.4, 0.5, 0.6)
+FFT_KPT = {"ham_fft_real_c0": ((1, 1, 1), (0, 0, 0)),
+           "ham_fft_kpt_even": ((2, 4, 2), (1, -1, 1)),
+           "ham_fft_kpt_odd": ((4, 3, 2), (1, 2, 1))}
+
 G_KP = (0.3, 0.0, -0.2)
 G_SMALL = (1.0e-9, 0.4, 0.1)    # |gx| below the 1e-8 dispatch threshold
 G_C0 = (2 * math.pi / A_BCC * 0.25, 2 * math.pi / A_BCC * 0.5, 0.0)
@@ -91,6 +116,16 @@ CASES = {
     "ham_cplx_c0": dict(inputs=lambda: _ham_inputs(C0_20, 5, 2, True),
                         reference=lambda i: _ham_ref(i, True, G_C0),
                         oracle=lambda i: _ham_oracle(i, True, G_C0)),
+    # FFT kinetic + V (the reference's default operator, run by its own code)
+    "ham_fft_real_c0": dict(inputs=lambda: _fft_inputs(C0_24, 7, 3, False),
+                            reference=lambda i: _fft_ref(i, False, *FFT_KPT["ham_fft_real_c0"]),
+                            oracle=lambda i: _fft_oracle(i, False, *FFT_KPT["ham_fft_real_c0"])),
+    "ham_fft_kpt_even": dict(inputs=lambda: _fft_inputs(FFT_GRID_EVEN, 8, 3, True),
+                             reference=lambda i: _fft_ref(i, True, *FFT_KPT["ham_fft_kpt_even"]),
+                             oracle=lambda i: _fft_oracle(i, True, *FFT_KPT["ham_fft_kpt_even"])),
+    "ham_fft_kpt_odd": dict(inputs=lambda: _fft_inputs(FFT_GRID_ODD, 9, 2, True),
+                            reference=lambda i: _fft_ref(i, True, *FFT_KPT["ham_fft_kpt_odd"]),
+                            oracle=lambda i: _fft_oracle(i, True, *FFT_KPT["ham_fft_kpt_odd"])),
 }
 
 

@@ -1,11 +1,14 @@
 """GPU parity of the FFT-kinetic Hamiltonian (qsb_ham_set_kinetic(ham, 1): the
 reference's default operator, mHamiltonianMatrix_ddm_bundle algorithm 1,
 source/qumasun_base1.matrix.h:171-228) against the oracle's restatement
-(oracle.hamiltonian_fft), called through the C ABI.
+(oracle.hamiltonian_fft) and against fixtures made by the reference's own
+FFT-kinetic code (tests/golden/ham_fft_*.npz), called through the C ABI.
 
 Tolerances: FP64 1e-12 relative L2 (the H.psi bar); FP32 2e-5 relative L2
 against the FP64 oracle; LOBPCG on the FFT operator reaches the dense
 eigenvalues of the oracle's FFT Hamiltonian to 1e-8 Ha."""
+import os
+
 import numpy as np
 import pytest
 
@@ -14,6 +17,7 @@ import oracle as O
 pytestmark = pytest.mark.gpu
 TOL64 = 1e-12
 TOL32 = 2e-5
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def rel(a, b):
@@ -88,3 +92,31 @@ def test_lobpcg_on_the_fft_operator_reaches_dense_eigenvalues(qsb):
         es.lobpcg_d(h ** 3, nb, 4, ev, X, keep, step == 0)
     np.testing.assert_allclose(np.sort(ev)[:6], exact, rtol=0, atol=1e-8)
     assert qsb.device_status() == 0
+
+
+@pytest.mark.parametrize("name", ["ham_fft_real_c0", "ham_fft_kpt_even", "ham_fft_kpt_odd"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_fft_hamiltonian_vs_reference_fixture(qsb, name, prec):
+    """-1/2 (grad + ik)^2 psi + V psi of the FFT-kinetic context against the
+    output of the reference's own mHamiltonianMatrix_ddm_bundle (algorithm 1),
+    stored in tests/golden/<name>.npz (tests/golden/make_golden.py): even and
+    odd extents, Gamma and k-points on the reference's k index grid."""
+    import torch
+    from cases import CASES, FFT_KPT
+    case = CASES[name]
+    inp = case["inputs"]()
+    gold = np.load(os.path.join(GOLD, name + ".npz"))
+    np.testing.assert_array_equal(gold["checksum"], np.array([float(np.sum(v)) for v in inp["checked"]]))
+    grid, nb = inp["grid"], inp["nb"]
+    cplx = name != "ham_fft_real_c0"
+    g = O.kpoint_vector(grid, *FFT_KPT[name])
+    H = qsb.Hamiltonian(*grid)
+    H.set_potential(inp["V"])
+    H.set_kinetic(1)
+    p = torch.from_numpy(np.ascontiguousarray(inp["psi"])).cuda()
+    if prec == "f32":
+        p = p.float()
+    hp = torch.full_like(p, float("nan"))
+    H.apply(p, hp, cplx, g)
+    torch.cuda.synchronize()
+    assert rel(hp.double().cpu().numpy(), gold["out"]) < (TOL64 if prec == "f64" else TOL32)

@@ -2,10 +2,12 @@
 hamiltonian_fft) of the reference's default Hamiltonian
 (mHamiltonianMatrix_ddm_bundle, algorithm 1, source/qumasun_base1.matrix.h:171-228).
 
-The reference's FFT path needs FFTW or cuFFT, neither of which its CPU build
-finds here, so the restatement is pinned by the operator's own definition:
-plane waves exp(i G.r) are eigenfunctions with eigenvalue |G + k|^2 / 2, the G
-of an even grid's Nyquist index taken as +n/2 (the fold of
+The restatement is pinned to the reference's own FFT-kinetic code by the
+ham_fft_* golden cases (tests/test_oracle.py: the reference object built in
+oracle/_ref/libqsref_fft.so with FFTW's documented DFT restated in
+oracle/ref_shim/fftw_dft.cpp, 1e-14), and here by the operator's own
+definition: plane waves exp(i G.r) are eigenfunctions with eigenvalue
+|G + k|^2 / 2, the G of an even grid's Nyquist index taken as +n/2 (the fold of
 OperateKineticInKspace_bundle, :96-123) -- 1e-12 relative; the operator is
 Hermitian (1e-12); on a smooth periodic field it agrees with the reference's
 own FD8 Laplacian (oracle/_ref) converges to it at eighth order."""
