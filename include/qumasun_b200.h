@@ -338,6 +338,20 @@ QSB_API qsb_status qsb_eigensolver_solve_stats(const qsb_eigensolver* es, int* c
  * tolerance in force. */
 QSB_API qsb_status qsb_eigensolver_overlap_stats(const qsb_eigensolver* es, int* max_dropped, double* min_kept_ratio,
                                                  double* drop_tolerance);
+/* FP64 complex solver: how the Rayleigh-Ritz pencil is formed between full
+ * recomputes.  mode 1 (the default) is the reference's steady-state update
+ * (NextMatrix_z, source/lobpcg_z_multi_mpi.h:579-794, used at :2782, and
+ * MakeMatrix_z_blas's skips at :2091-2101): in iterations that are not a
+ * multiple of 6 (S_MAT_REST_LIMIT, :1808) only X^H A R, R^H A R, R^H A P and
+ * R^H R are formed from the bundles; the X/P blocks come from the previous
+ * pencil and its eigenvectors, and X^H R, R^H P from R = AX - X E.  mode 0
+ * forms every block from the bundles in every iteration.  The keep_S_matrix
+ * reuse across calls (:1811) is not taken: the first iteration of each call
+ * forms the whole pencil. */
+QSB_API qsb_status qsb_eigensolver_set_pencil_update(qsb_eigensolver* es, int mode);
+/* Of the last FP64 complex call: pencils formed in full from the bundles, and
+ * pencils formed by the steady-state update. */
+QSB_API qsb_status qsb_eigensolver_pencil_stats(const qsb_eigensolver* es, int* full, int* steady);
 
 /* Complex block LOBPCG.  Replaces LOBPCG::Eigen_z_multi_mpi(l_grid, dVol,
  * num_solution, iter_max, eigen_values, eigen_vectors, keep, work, temporary,

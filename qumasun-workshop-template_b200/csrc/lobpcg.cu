@@ -187,6 +187,30 @@ __global__ void pack_orth(double* __restrict__ T, int nf, int na) {
     T[(2 * j + 1) + (size_t)ld * (2 * k)] = -im;
 }
 
+// One n x n block (I0, J0) of the full Hermitian pencil M (ld m) from the dense
+// complex matrix B (ld n): value = B, minus Bs[a,b] E[b] (mode 1) or E[a] Bs[a,b]
+// (mode 2).  On a diagonal block only a <= b is read and the diagonal's imaginary
+// part is dropped; the mirrored position gets the conjugate.
+__global__ void put_pencil_block(const double2* __restrict__ B, const double2* __restrict__ Bs,
+                                 const double* __restrict__ E, int mode, int n, double2* __restrict__ M, int m, int I0,
+                                 int J0, int diag) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y;
+    if (a >= n || b >= n) return;
+    if (diag && a > b) return;
+    double2 v = B[a + (size_t)n * b];
+    if (mode != 0) {
+        const double2 w = Bs[a + (size_t)n * b];
+        const double e = mode == 1 ? E[b] : E[a];
+        v.x -= w.x * e;
+        v.y -= w.y * e;
+    }
+    if (diag && a == b) v.y = 0.0;
+    const int r = I0 + a, c = J0 + b;
+    M[r + (size_t)m * c] = v;
+    M[c + (size_t)m * r] = make_double2(v.x, -v.y);
+}
+
 const char* cublas_name(cublasStatus_t s) {
     switch (s) {
     case CUBLAS_STATUS_SUCCESS: return "CUBLAS_STATUS_SUCCESS";
@@ -266,6 +290,13 @@ struct qsb_eigensolver {
     double last_min_kept = 1.0;   // smallest kept overlap eigenvalue / max in the last call
     qsb_apply_f32_fn op32 = nullptr;
     void* user32 = nullptr;
+    // steady-state pencil update of the FP64 complex solver (NextMatrix_z): the
+    // previous pencil (S0a, S0b, m x m each), the X'/P' blocks it gives (6 x n x n)
+    // and two m x n products, complex
+    double* nxt = nullptr;
+    int pencil_update = 1;   // 1: X/P blocks from the previous pencil between full recomputes; 0: all from the grid
+    int last_full = 0;       // pencils of the last call formed from the grid in full ...
+    int last_steady = 0;     // ... and with only the R blocks from the grid
 };
 
 namespace qsb {
@@ -439,6 +470,71 @@ qsb_status make_coefficients(qsb_eigensolver* es, int na, int m, int nblk, cudaS
             copy_real_block<<<grid, 128, 0, s>>>(es->Sa, m, b * na, na, na, es->rc + (size_t)b * na * na);
         }
     }
+    QSB_CUDA_TRY(cudaGetLastError());
+    return QSB_OK;
+}
+
+// The steady-state pencil update of LOBPCG::Eigen_z_multi_mpi (NextMatrix_z,
+// source/lobpcg_z_multi_mpi.h:579-794, with DIRECT_S_MATRIX_XR_RP, :58): with
+// X' = X Cx + P', P' = R Cr + P Cp and C = [Cx; Cr; Cp] the lowest n generalized
+// eigenvectors of the pencil S0 (first n columns of Sa, ld m), the X'/P' blocks of
+// the next pencil follow from S0 alone:
+//   W = S0[:, n:m] C[n:m],  U = S0[:, 0:n] C[0:n] + W   (= S0 C),
+//   X'^H S X' = C^H U,  X'^H S P' = C^H W,  P'^H S P' = C[n:m]^H W[n:m]
+// for S = the overlap and for S = the Hamiltonian (small complex GEMMs).
+// Layout of es->nxt (complex): S0a, S0b (m x m), then XX, XP, PP, HXX, HXP, HPP
+// (n x n), then W, U (m x n).
+qsb_status next_pencil_blocks(qsb_eigensolver* es, int n, int m, cudaStream_t s) {
+    const int mmax = 3 * es->nmax;
+    double2* base = (double2*)es->nxt;
+    const double2* S0[2] = {base, base + (size_t)mmax * mmax};      // Hamiltonian, overlap
+    double2* blk = base + (size_t)2 * mmax * mmax;
+    const size_t nn = (size_t)es->nmax * es->nmax;
+    double2* Wk = blk + 6 * nn;
+    double2* Uk = Wk + (size_t)mmax * es->nmax;
+    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+    const cuDoubleComplex* C = (const cuDoubleComplex*)es->Sa;
+    for (int h = 0; h < 2; ++h) {
+        const cuDoubleComplex* S = (const cuDoubleComplex*)S0[h];
+        cuDoubleComplex* XX = (cuDoubleComplex*)(blk + (size_t)(h == 0 ? 3 : 0) * nn);
+        cuDoubleComplex* XP = XX + nn;
+        cuDoubleComplex* PP = XP + nn;
+        QSB_BLAS_TRY(cublasZgemm(es->blas, CUBLAS_OP_N, CUBLAS_OP_N, m, n, m - n, &one, S + (size_t)n * m, m, C + n, m,
+                                 &zero, (cuDoubleComplex*)Wk, m));
+        QSB_CUDA_TRY(cudaMemcpyAsync(Uk, Wk, sizeof(double2) * (size_t)m * n, cudaMemcpyDeviceToDevice, s));
+        QSB_BLAS_TRY(cublasZgemm(es->blas, CUBLAS_OP_N, CUBLAS_OP_N, m, n, n, &one, S, m, C, m, &one,
+                                 (cuDoubleComplex*)Uk, m));
+        QSB_BLAS_TRY(cublasZgemm(es->blas, CUBLAS_OP_C, CUBLAS_OP_N, n, n, m, &one, C, m, (cuDoubleComplex*)Uk, m, &zero,
+                                 XX, n));
+        QSB_BLAS_TRY(cublasZgemm(es->blas, CUBLAS_OP_C, CUBLAS_OP_N, n, n, m, &one, C, m, (cuDoubleComplex*)Wk, m, &zero,
+                                 XP, n));
+        QSB_BLAS_TRY(cublasZgemm(es->blas, CUBLAS_OP_C, CUBLAS_OP_N, n, n, m - n, &one, C + n, m,
+                                 (cuDoubleComplex*)Wk + n, m, &zero, PP, n));
+    }
+    return QSB_OK;
+}
+
+// The X/P blocks of the 3n pencil from next_pencil_blocks, and the two overlap
+// blocks of R that follow from them with R = AX - X E (E the Ritz values the
+// residual was formed with, es->W): X^H R = X^H A X - X^H X E,
+// R^H P = X^H A P - E X^H P.
+qsb_status put_next_blocks(qsb_eigensolver* es, int n, int m, cudaStream_t s) {
+    const int mmax = 3 * es->nmax;
+    const size_t nn = (size_t)es->nmax * es->nmax;
+    const double2* blk = (const double2*)es->nxt + (size_t)2 * mmax * mmax;
+    const double2 *XX = blk, *XP = blk + nn, *PP = blk + 2 * nn;
+    const double2 *HXX = blk + 3 * nn, *HXP = blk + 4 * nn, *HPP = blk + 5 * nn;
+    double2* Sa = (double2*)es->Sa;
+    double2* Sb = (double2*)es->Sb;
+    const dim3 g((n + 127) / 128, n);
+    put_pencil_block<<<g, 128, 0, s>>>(HXX, nullptr, nullptr, 0, n, Sa, m, 0, 0, 1);
+    put_pencil_block<<<g, 128, 0, s>>>(HXP, nullptr, nullptr, 0, n, Sa, m, 0, 2 * n, 0);
+    put_pencil_block<<<g, 128, 0, s>>>(HPP, nullptr, nullptr, 0, n, Sa, m, 2 * n, 2 * n, 1);
+    put_pencil_block<<<g, 128, 0, s>>>(XX, nullptr, nullptr, 0, n, Sb, m, 0, 0, 1);
+    put_pencil_block<<<g, 128, 0, s>>>(XP, nullptr, nullptr, 0, n, Sb, m, 0, 2 * n, 0);
+    put_pencil_block<<<g, 128, 0, s>>>(PP, nullptr, nullptr, 0, n, Sb, m, 2 * n, 2 * n, 1);
+    put_pencil_block<<<g, 128, 0, s>>>(HXX, XX, es->W, 1, n, Sb, m, 0, n, 0);
+    put_pencil_block<<<g, 128, 0, s>>>(HXP, XP, es->W, 2, n, Sb, m, n, 2 * n, 0);
     QSB_CUDA_TRY(cudaGetLastError());
     return QSB_OK;
 }
@@ -1117,6 +1213,12 @@ qsb_status qsb_eigensolver_create_ex(qsb_eigensolver** out, int64_t N, int n, in
         cudaSuccess)
         return cleanup(fail(QSB_ERR_NOMEM, "eigensolver: pencil workspace allocation"));
     if (!es->mixed) es->drop_tol = 1e-12;
+    if (!es->mixed && is_complex) {
+        const size_t mx = (size_t)3 * n;
+        if (cudaMalloc((void**)&es->nxt, sizeof(double2) * (2 * mx * mx + (size_t)6 * n * n + 2 * mx * n)) !=
+            cudaSuccess)
+            return cleanup(fail(QSB_ERR_NOMEM, "eigensolver: pencil update allocation"));
+    }
     const int m = 3 * n;
     const size_t cm = (size_t)m * m * (is_complex ? 2 : 1);
     const size_t tsz = (size_t)(2 * n) * (2 * n);
@@ -1146,7 +1248,7 @@ qsb_status qsb_eigensolver_destroy(qsb_eigensolver* es) {
     float* b32[7] = {es->X32, es->R32, es->P32, es->AX32, es->AR32, es->AP32, es->TMP32};
     for (float* p : b32)
         if (p) cudaFree(p);
-    void* mw[8] = {es->su, es->sau, es->gpart, es->T2, es->rc32, es->svq, es->rotw, es->rotc};
+    void* mw[9] = {es->su, es->sau, es->gpart, es->T2, es->rc32, es->svq, es->rotw, es->rotc, es->nxt};
     for (void* p : mw)
         if (p) cudaFree(p);
     if (es->T) cudaFree(es->T);
@@ -1205,6 +1307,19 @@ qsb_status qsb_eigensolver_set_gram_kind(qsb_eigensolver* es, qsb_gram_kind kind
     return QSB_OK;
 }
 
+qsb_status qsb_eigensolver_set_pencil_update(qsb_eigensolver* es, int mode) {
+    if (!es || (mode != 0 && mode != 1)) return fail(QSB_ERR_INVALID, "eigensolver_set_pencil_update: bad arguments");
+    es->pencil_update = mode;
+    return QSB_OK;
+}
+
+qsb_status qsb_eigensolver_pencil_stats(const qsb_eigensolver* es, int* full, int* steady) {
+    if (!es || !full || !steady) return fail(QSB_ERR_INVALID, "eigensolver_pencil_stats: bad arguments");
+    *full = es->last_full;
+    *steady = es->last_steady;
+    return QSB_OK;
+}
+
 qsb_status qsb_eigensolver_solve_stats(const qsb_eigensolver* es, int* cholesky_solves, int* overlap_basis_solves) {
     if (!es) return fail(QSB_ERR_INVALID, "solve_stats: null solver");
     if (cholesky_solves) *cholesky_solves = es->last_chol;
@@ -1248,6 +1363,8 @@ qsb_status qsb_lobpcg_z(qsb_eigensolver* es, double dVol, int n, int iter_max, d
     es->last_chol = 0;
     es->last_svqb = 0;
     es->last_min_kept = 1.0;
+    es->last_full = 0;
+    es->last_steady = 0;
     if (es->mixed)
         return lobpcg_z_mixed(es, dVol, n, iter_max, eigen_values, X, keep, p_num_fix, residual_threshold, scf_step, s);
     const size_t L = es->L;
@@ -1308,6 +1425,7 @@ qsb_status qsb_lobpcg_z(qsb_eigensolver* es, double dVol, int n, int iter_max, d
         // the Rayleigh quotients of the active bands drive the loop
         int iter;
         bool large_difference = false;
+        bool have_next = false;   // X'/P' pencil blocks of this iteration were formed by the update
         for (iter = 0; iter < iter_max; ++iter) {
             // orthogonalize R to X_fix (:2080)
             if (num_fix > 0) {
@@ -1321,12 +1439,35 @@ qsb_status qsb_lobpcg_z(qsb_eigensolver* es, double dVol, int n, int iter_max, d
             const int m = nblk * N_;
             const double* U[3] = {band(X, head), band(es->R, head), band(keep, head)};
             const double* AU[3] = {band(es->AX, head), band(es->AR, head), band(es->AP, head)};
-            // Hermitian pencil (MakeMatrix_z_blas, :300-558): upper blocks, lower = conj
-            for (int I = 0; I < nblk; ++I)
-                for (int J = I; J < nblk; ++J) {
-                    QSB_TRY(gram_block(es, U[I], AU[J], N_, es->Sa, m, I, J, 1.0, s));
-                    QSB_TRY(gram_block(es, U[I], U[J], N_, es->Sb, m, I, J, 1.0, s));
-                }
+            // Hermitian pencil (MakeMatrix_z_blas, :300-558): upper blocks, lower = conj.
+            // Between full recomputes (every S_MAT_REST_LIMIT = 6 iterations, :1808,
+            // :2091-2101) only X^H A R, R^H A R, R^H A P and R^H R come from the grid;
+            // the X and P blocks are the previous iteration's update (:2782).
+            if (have_next && use_p) {
+                QSB_TRY(gram_block(es, U[0], AU[1], N_, es->Sa, m, 0, 1, 1.0, s));
+                QSB_TRY(gram_block(es, U[1], AU[1], N_, es->Sa, m, 1, 1, 1.0, s));
+                QSB_TRY(gram_block(es, U[1], AU[2], N_, es->Sa, m, 1, 2, 1.0, s));
+                QSB_TRY(gram_block(es, U[1], U[1], N_, es->Sb, m, 1, 1, 1.0, s));
+                QSB_TRY(put_next_blocks(es, N_, m, s));
+                ++es->last_steady;
+            } else {
+                for (int I = 0; I < nblk; ++I)
+                    for (int J = I; J < nblk; ++J) {
+                        QSB_TRY(gram_block(es, U[I], AU[J], N_, es->Sa, m, I, J, 1.0, s));
+                        QSB_TRY(gram_block(es, U[I], U[J], N_, es->Sb, m, I, J, 1.0, s));
+                    }
+                ++es->last_full;
+            }
+            have_next = false;
+            // the next iteration updates its X/P blocks from this pencil unless it
+            // is the last one or a full recompute
+            const bool update_next = es->pencil_update && iter + 1 < iter_max && (iter + 1) % 6 != 0;
+            if (update_next) {
+                const size_t mmax = (size_t)3 * es->nmax;
+                QSB_CUDA_TRY(cudaMemcpyAsync(es->nxt, es->Sa, sizeof(double2) * (size_t)m * m, cudaMemcpyDeviceToDevice, s));
+                QSB_CUDA_TRY(cudaMemcpyAsync((double2*)es->nxt + mmax * mmax, es->Sb, sizeof(double2) * (size_t)m * m,
+                                             cudaMemcpyDeviceToDevice, s));
+            }
             QSB_TRY(solve_pencil_fp64(es, m, N_, s));   // ZHEGVD (:2254-2263 / :2492-2511)
             QSB_TRY(make_coefficients(es, N_, m, nblk, s));
             // P' = R Cr + P Cp (into TMP), P = TMP; TMP += X Cx  (NextVector_z2)
@@ -1375,6 +1516,11 @@ qsb_status qsb_lobpcg_z(qsb_eigensolver* es, double dVol, int n, int iter_max, d
                 // R = AX - eps X (:2750)
                 QSB_CUDA_TRY(cudaMemcpyAsync(eps_d, w.data(), sizeof(double) * N_, cudaMemcpyHostToDevice, s));
                 QSB_TRY(seg_residual(es, N_, band(es->R, head), band(es->AX, head), band(X, head), eps_d, nullptr, 1.0, s));
+                if (update_next) {
+                    // NextMatrix_z (:2782): the next pencil's X'/P' blocks (S0 saved before the solve)
+                    QSB_TRY(next_pencil_blocks(es, N_, m, s));
+                    have_next = true;
+                }
             } else {
                 // undo the scaling: fixed bands by 1/sqrt(dV), active by 1/sqrt(|x|^2 dV) (:2792-2803)
                 if (num_fix > 0) QSB_TRY(seg_scale_by(es, num_fix, X, nullptr, 1.0 / std::sqrt(dVol), s));

@@ -382,6 +382,19 @@ class EigenSolver:
         _check(lib.qsb_eigensolver_solve_stats(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
+    def set_pencil_update(self, mode):
+        """FP64 complex solver: 1 (default) the reference's steady-state pencil
+        update between full recomputes every 6 iterations; 0 every block from
+        the bundles in every iteration."""
+        _check(lib.qsb_eigensolver_set_pencil_update(self._h, int(mode)))
+
+    def pencil_stats(self):
+        """(pencils formed in full, pencils formed by the steady-state update) of
+        the last FP64 complex call."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        _check(lib.qsb_eigensolver_pencil_stats(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def overlap_stats(self):
         """(most directions dropped in one iteration, smallest kept overlap
         eigenvalue / largest, drop tolerance) of the last call (mixed precision)."""
