@@ -787,6 +787,8 @@ def main():
     ap.add_argument("--only-hpsi", action="store_true",
                     help="time the device-resident H.psi only (no e2e, FFT, Gram, LOBPCG, SCF or CPU sections); "
                          "the profiler captures use it")
+    ap.add_argument("--only-fft", action="store_true",
+                    help="time the device-resident FFT-kinetic H.psi only (the profiler captures use it)")
     ap.add_argument("--bands", type=int, default=NB,
                     help="bands per GPU (default 128, the benchmark workload; smaller only for profiler captures)")
     args = ap.parse_args()
@@ -855,6 +857,17 @@ def main():
         for _ in range(20):
             H.apply(psi, hpsi)
         torch.cuda.synchronize()
+
+    if args.only_fft:
+        clocks.stop()
+        fft = fft_kinetic_section(H, psi, hpsi, stream, algorithmic_bytes(NB, N, n_pts, 4), steps=args.steps)
+        if rank == 0:
+            print(json.dumps({"metric": "FFT-kinetic H.psi", "bands_per_gpu": NB, "fft_kinetic": fft,
+                              "note": "--only-fft: device-resident FFT-kinetic H.psi timing only"}))
+        H.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
 
     if args.only_hpsi:
         clocks.stop()
