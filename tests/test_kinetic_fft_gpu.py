@@ -40,7 +40,9 @@ def _setup(qsb, grid, nb, cplx, seed, reps=1):
 @pytest.mark.parametrize("grid,nb,cplx,g", [
     ((32, 32, 32, 0.1875, 0.1875, 0.1875), 16, False, (0.0, 0.0, 0.0)),   # config 0 shape
     ((32, 32, 32, 0.1875, 0.1875, 0.1875), 40, False, (0.0, 0.0, 0.0)),   # two band chunks, ragged
-    ((33, 17, 9, 0.2, 0.3, 0.25), 3, False, (0.0, 0.0, 0.0)),             # odd extents
+    ((33, 17, 9, 0.2, 0.3, 0.25), 3, False, (0.0, 0.0, 0.0)),             # odd extents, a half pair
+    ((20, 18, 16, 0.3, 0.3, 0.3), 1, False, (0.0, 0.0, 0.0)),             # one real band: R2C / C2R
+    ((20, 18, 16, 0.3, 0.3, 0.3), 35, False, (0.0, 0.0, 0.0)),            # pairs over two chunks, odd tail
     ((24, 20, 16, 0.25, 0.3, 0.375), 3, True, (0.3, -0.2, 0.7)),          # Bloch vector
     ((24, 20, 16, 0.25, 0.3, 0.375), 35, True, (0.26, 0.52, 0.0)),        # two chunks, complex
     ((15, 12, 10, 0.3, 0.3, 0.3), 2, True, (0.0, 0.0, 0.0))])
