@@ -485,6 +485,22 @@ QSB_API qsb_status qsb_scf_destroy(qsb_scf* scf);
 QSB_API qsb_status qsb_scf_set_gth_local(qsb_scf* scf, int n_atoms, const double* pos, const int* species,
                                          int n_species, const double* zion, const double* rloc, const double* c1,
                                          const double* c2);
+/* Local parts from radial tables instead of the analytic GTH form (replaces a
+ * qsb_scf_set_gth_local; the last call of the two decides): per species k the
+ * table v_k(G) of qsb_radial_local_table (n_g values on |G| = j dg, computed
+ * with charge z[k] and Gaussian width sigma[k] -- for a UPF, its radius,
+ * v_local and z_valence), V_loc(G) = (1/Omega) sum_a v_{species[a]}(|G|)
+ * exp(-i G.R_a).  The smooth part v + 4 pi z exp(-G^2 sigma^2 / 2) / G^2 is
+ * interpolated (cubic, four nearest samples) and the Gaussian charge's term is
+ * added back exactly, so the 1/G^2 tail is not interpolated.  The table must
+ * reach |G| = sqrt(sum_d (pi / h_d)^2) with three samples to spare.
+ * qsb_scf_local_forces then returns the force of these local parts.  The
+ * reference builds its local potential from core charges by a Poisson solve
+ * on a finer grid (source/qumasun_base1.core.h:54,139, upf_oncv_loader.h:337);
+ * this is the G-space route of the same potential. */
+QSB_API qsb_status qsb_scf_set_radial_local(qsb_scf* scf, int n_atoms, const double* pos, const int* species,
+                                            int n_species, const double* z, const double* sigma, int n_g, double dg,
+                                            const double* table);
 QSB_API qsb_status qsb_scf_set_mixing(qsb_scf* scf, double amplitude, double q0, int depth);
 QSB_API qsb_status qsb_scf_set_smearing(qsb_scf* scf, double kbt);
 /* The SCF's LDA.  pz_variant 0 (default): Perdew-Zunger with the published
@@ -524,7 +540,7 @@ QSB_API qsb_status qsb_scf_run(qsb_scf* scf, double* X, double* keep, int lobpcg
                                double tol_per_atom, double* energies, int* steps, double* eigen_values,
                                double* occupations, void* stream);
 QSB_API qsb_status qsb_scf_get_field(qsb_scf* scf, int which, double* out);
-/* Force of the GTH local parts on every atom, -d/dR_a int rho V_loc, from the
+/* Force of the local parts (GTH, or radial tables) on every atom, -d/dR_a int rho V_loc, from the
  * last output density (rho_dev = NULL) or a given device density: forces
  * (host, 3 x n_atoms) accumulate ("+="), so the nonlocal part
  * (qsb_ham_nonlocal_energy_force) adds on.  Exact derivative of the grid sum

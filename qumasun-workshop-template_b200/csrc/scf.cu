@@ -331,6 +331,102 @@ __global__ void __launch_bounds__(RB) local_force_kernel(KGrid g, size_t M, doub
     }
 }
 
+// Radial-table local parts (qsb_scf_set_radial_local).  Per species the table
+// holds the smooth part s(G) = v(G) + 4 pi z exp(-G^2 sigma^2 / 2) / G^2 on
+// |G| = j dg (s(0) = v(0) + 2 pi z sigma^2); v(G) is s(|G|), by cubic Lagrange
+// interpolation through the four nearest samples (s is even in G: index -1 is
+// index 1), minus the Gaussian charge's 4 pi z exp(-G^2 sigma^2 / 2) / G^2, and
+// s(0) - 2 pi z sigma^2 at G = 0 -- the finite-part convention of the GTH path.
+struct TabAtom {
+    double x, y, z;
+    int sp;
+};
+struct TabSpecies {
+    double z, sigma;
+};
+__device__ __forceinline__ double table_v(const double* __restrict__ tab, int n_g, double dg, double z, double sigma,
+                                          double g2) {
+    const double g = sqrt(g2);
+    const double u = g / dg;
+    const int j = (int)u;
+    const double t = u - (double)j;
+    const int im = j == 0 ? 1 : j - 1;
+    const int i1 = min(j + 1, n_g - 1), i2 = min(j + 2, n_g - 1);
+    const double wm = -t * (t - 1.0) * (t - 2.0) / 6.0, w0 = (t + 1.0) * (t - 1.0) * (t - 2.0) / 2.0;
+    const double w1 = -(t + 1.0) * t * (t - 2.0) / 2.0, w2 = (t + 1.0) * t * (t - 1.0) / 6.0;
+    const double sg = wm * tab[im] + w0 * tab[min(j, n_g - 1)] + w1 * tab[i1] + w2 * tab[i2];
+    if (g2 > 0.0) return sg - 4.0 * M_PI * z * exp(-0.5 * g2 * sigma * sigma) / g2;
+    return sg - 2.0 * M_PI * z * sigma * sigma;
+}
+
+__global__ void vloc_table_kernel(KGrid g, size_t M, double inv_omega, int na, const TabAtom* __restrict__ atoms,
+                                  const TabSpecies* __restrict__ sp, const double* __restrict__ tab, int n_g,
+                                  double dg, cufftDoubleComplex* __restrict__ f) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < M; i += (size_t)gridDim.x * blockDim.x) {
+        double gx, gy, gz;
+        kvec(g, i, gx, gy, gz);
+        const double g2 = gx * gx + gy * gy + gz * gz;
+        if (on_nyquist(g, i)) {
+            f[i].x = 0.0;
+            f[i].y = 0.0;
+            continue;
+        }
+        double re = 0.0, im = 0.0;
+        int last = -1;
+        double v = 0.0;
+        for (int a = 0; a < na; ++a) {
+            const TabAtom at = atoms[a];
+            if (at.sp != last) {
+                v = table_v(tab + (size_t)at.sp * n_g, n_g, dg, sp[at.sp].z, sp[at.sp].sigma, g2);
+                last = at.sp;
+            }
+            double sn, cs;
+            sincos(gx * at.x + gy * at.y + gz * at.z, &sn, &cs);
+            re += v * cs;
+            im -= v * sn;
+        }
+        f[i].x = re * inv_omega;
+        f[i].y = im * inv_omega;
+    }
+}
+
+// the force of the table local parts, as local_force_kernel for the GTH ones
+__global__ void __launch_bounds__(RB) local_force_table_kernel(KGrid g, size_t M, double inv_n, int na,
+                                                               const TabAtom* __restrict__ atoms,
+                                                               const TabSpecies* __restrict__ sp,
+                                                               const double* __restrict__ tab, int n_g, double dg,
+                                                               const cufftDoubleComplex* __restrict__ f,
+                                                               double* __restrict__ partial) {
+    __shared__ double sh[RB / 32];
+    for (int a = 0; a < na; ++a) {
+        const TabAtom at = atoms[a];
+        const double* ts = tab + (size_t)at.sp * n_g;
+        const double z = sp[at.sp].z, sigma = sp[at.sp].sigma;
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        for (size_t i = blockIdx.x * (size_t)RB + threadIdx.x; i < M; i += (size_t)gridDim.x * RB) {
+            double gx, gy, gz;
+            kvec(g, i, gx, gy, gz);
+            const double g2 = gx * gx + gy * gy + gz * gz;
+            if (g2 == 0.0 || on_nyquist(g, i)) continue;
+            const int kx = (int)(i % g.nxh);
+            const double w = kx == 0 ? 1.0 : 2.0;
+            const double v = table_v(ts, n_g, dg, z, sigma, g2);
+            double sn, cs;
+            sincos(gx * at.x + gy * at.y + gz * at.z, &sn, &cs);
+            const double t = w * v * (sn * f[i].x + cs * f[i].y) * inv_n;
+            fx += gx * t;
+            fy += gy * t;
+            fz += gz * t;
+        }
+        const double sx = block_sum(fx, sh), sy = block_sum(fy, sh), sz = block_sum(fz, sh);
+        if (threadIdx.x == 0) {
+            partial[(size_t)(a * 3 + 0) * gridDim.x + blockIdx.x] = sx;
+            partial[(size_t)(a * 3 + 1) * gridDim.x + blockIdx.x] = sy;
+            partial[(size_t)(a * 3 + 2) * gridDim.x + blockIdx.x] = sz;
+        }
+    }
+}
+
 inline int pw_blocks(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
 
 }  // namespace
@@ -362,6 +458,12 @@ struct qsb_scf {
     const double** ptrs = nullptr;
     cufftDoubleComplex* fk = nullptr;
     qsb::GthAtom* atoms = nullptr;     // GTH local parts (device), set_gth_local
+    // radial-table local parts (device), set_radial_local; used when tab_atoms is set
+    qsb::TabAtom* tab_atoms = nullptr;
+    qsb::TabSpecies* tab_species = nullptr;
+    double* tab = nullptr;
+    int tab_ng = 0;
+    double tab_dg = 0.0;
     cufftHandle plan_f = 0, plan_b = 0;
     bool have_plans = false;
     // host
@@ -641,7 +743,9 @@ qsb_status qsb_scf_destroy(qsb_scf* c) {
     if (c->hxc) cudaFree(c->hxc);
     if (c->occ2) cudaFree(c->occ2);
     if (c->fk) cudaFree(c->fk);
-    if (c->atoms) cudaFree(c->atoms);
+    void* loc[4] = {c->atoms, c->tab_atoms, c->tab_species, c->tab};
+    for (void* q : loc)
+        if (q) cudaFree(q);
     if (c->have_plans) {
         cufftDestroy(c->plan_f);
         cufftDestroy(c->plan_b);
@@ -717,6 +821,19 @@ qsb_status qsb_scf_set_smearing(qsb_scf* c, double kbt) {
     return QSB_OK;
 }
 
+namespace {
+void free_local_parts(qsb_scf* c) {
+    void* p[4] = {c->atoms, c->tab_atoms, c->tab_species, c->tab};
+    for (void* q : p)
+        if (q) cudaFree(q);
+    c->atoms = nullptr;
+    c->tab_atoms = nullptr;
+    c->tab_species = nullptr;
+    c->tab = nullptr;
+    c->n_atoms = 0;
+}
+}  // namespace
+
 qsb_status qsb_scf_set_gth_local(qsb_scf* c, int n_atoms, const double* pos, const int* species, int n_species,
                                  const double* zion, const double* rloc, const double* c1, const double* c2) {
     if (!c || n_atoms <= 0 || !pos || !species || n_species <= 0 || !zion || !rloc || !c1 || !c2)
@@ -727,9 +844,7 @@ qsb_status qsb_scf_set_gth_local(qsb_scf* c, int n_atoms, const double* pos, con
         if (sp < 0 || sp >= n_species || !(rloc[sp] > 0.0)) return fail(QSB_ERR_INVALID, "scf_set_gth_local: bad species");
         at[a] = GthAtom{pos[3 * a], pos[3 * a + 1], pos[3 * a + 2], zion[sp], rloc[sp], c1[sp], c2[sp]};
     }
-    if (c->atoms) cudaFree(c->atoms);
-    c->atoms = nullptr;
-    c->n_atoms = 0;
+    free_local_parts(c);
     GthAtom* d = nullptr;
     QSB_CUDA_TRY(cudaMalloc((void**)&d, n_atoms * sizeof(GthAtom)));
     QSB_CUDA_TRY(cudaMemcpy(d, at.data(), n_atoms * sizeof(GthAtom), cudaMemcpyHostToDevice));
@@ -744,6 +859,59 @@ qsb_status qsb_scf_set_gth_local(qsb_scf* c, int n_atoms, const double* pos, con
         return cuda_fail(e, "vloc_k_kernel");
     }
     c->atoms = d;
+    c->n_atoms = n_atoms;
+    return QSB_OK;
+}
+
+qsb_status qsb_scf_set_radial_local(qsb_scf* c, int n_atoms, const double* pos, const int* species, int n_species,
+                                    const double* z, const double* sigma, int n_g, double dg, const double* table) {
+    if (!c || n_atoms <= 0 || !pos || !species || n_species <= 0 || !z || !sigma || n_g < 4 || !(dg > 0.0) || !table)
+        return fail(QSB_ERR_INVALID, "scf_set_radial_local: bad argument");
+    // the table must reach past the largest |G| of the grid by the interpolation stencil
+    const double gmax = std::sqrt(std::pow(M_PI / c->dx, 2) + std::pow(M_PI / c->dy, 2) + std::pow(M_PI / c->dz, 2));
+    if ((double)(n_g - 3) * dg < gmax)
+        return fail(QSB_ERR_INVALID, "scf_set_radial_local: table ends at |G| = " + std::to_string((n_g - 3) * dg) +
+                                         " below the grid's " + std::to_string(gmax) + " (+ 3 samples)");
+    std::vector<TabAtom> at(n_atoms);
+    for (int a = 0; a < n_atoms; ++a) {
+        const int sp = species[a];
+        if (sp < 0 || sp >= n_species) return fail(QSB_ERR_INVALID, "scf_set_radial_local: bad species");
+        at[a] = TabAtom{pos[3 * a], pos[3 * a + 1], pos[3 * a + 2], sp};
+    }
+    std::vector<TabSpecies> spc(n_species);
+    std::vector<double> smooth((size_t)n_species * n_g);
+    for (int k = 0; k < n_species; ++k) {
+        if (!(sigma[k] > 0.0)) return fail(QSB_ERR_INVALID, "scf_set_radial_local: sigma must be > 0");
+        spc[k] = TabSpecies{z[k], sigma[k]};
+        for (int j = 0; j < n_g; ++j) {
+            const double v = table[(size_t)k * n_g + j];
+            if (!std::isfinite(v)) return fail(QSB_ERR_INVALID, "scf_set_radial_local: non-finite table value");
+            const double g = j * dg;
+            smooth[(size_t)k * n_g + j] =
+                j == 0 ? v + 2.0 * M_PI * z[k] * sigma[k] * sigma[k]
+                       : v + 4.0 * M_PI * z[k] * std::exp(-0.5 * g * g * sigma[k] * sigma[k]) / (g * g);
+        }
+    }
+    free_local_parts(c);
+    QSB_CUDA_TRY(cudaMalloc((void**)&c->tab_atoms, n_atoms * sizeof(TabAtom)));
+    QSB_CUDA_TRY(cudaMalloc((void**)&c->tab_species, n_species * sizeof(TabSpecies)));
+    QSB_CUDA_TRY(cudaMalloc((void**)&c->tab, smooth.size() * sizeof(double)));
+    QSB_CUDA_TRY(cudaMemcpy(c->tab_atoms, at.data(), n_atoms * sizeof(TabAtom), cudaMemcpyHostToDevice));
+    QSB_CUDA_TRY(cudaMemcpy(c->tab_species, spc.data(), n_species * sizeof(TabSpecies), cudaMemcpyHostToDevice));
+    QSB_CUDA_TRY(cudaMemcpy(c->tab, smooth.data(), smooth.size() * sizeof(double), cudaMemcpyHostToDevice));
+    c->tab_ng = n_g;
+    c->tab_dg = dg;
+    const double omega = (double)c->N * c->dV;
+    vloc_table_kernel<<<pw_blocks(c->M), 256>>>(kgrid(c), c->M, 1.0 / omega, n_atoms, c->tab_atoms, c->tab_species,
+                                                c->tab, n_g, dg, c->fk);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        free_local_parts(c);
+        return cuda_fail(e, "vloc_table_kernel");
+    }
+    QSB_CUFFT_TRY(cufftSetStream(c->plan_b, 0));
+    QSB_CUFFT_TRY(cufftExecZ2D(c->plan_b, c->fk, c->vloc));
+    QSB_CUDA_TRY(cudaDeviceSynchronize());
     c->n_atoms = n_atoms;
     return QSB_OK;
 }
@@ -763,7 +931,11 @@ qsb_status qsb_scf_local_forces(qsb_scf* c, const double* rho_dev, double* force
         cudaFree(part);
         return fail(QSB_ERR_NOMEM, "scf_local_forces: device allocation");
     }
-    local_force_kernel<<<blocks, RB>>>(kgrid(c), c->M, 1.0 / (double)c->N, c->n_atoms, c->atoms, c->fk, part);
+    if (c->tab_atoms)
+        local_force_table_kernel<<<blocks, RB>>>(kgrid(c), c->M, 1.0 / (double)c->N, c->n_atoms, c->tab_atoms,
+                                                 c->tab_species, c->tab, c->tab_ng, c->tab_dg, c->fk, part);
+    else
+        local_force_kernel<<<blocks, RB>>>(kgrid(c), c->M, 1.0 / (double)c->N, c->n_atoms, c->atoms, c->fk, part);
     row_sum_kernel<<<rows, 32>>>(rows, blocks, part, sums);
     std::vector<double> h(rows);
     const cudaError_t e = cudaMemcpy(h.data(), sums, rows * sizeof(double), cudaMemcpyDeviceToHost);

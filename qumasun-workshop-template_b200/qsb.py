@@ -653,6 +653,19 @@ class SCF:
         _check(lib.qsb_scf_set_gth_local(self._h, len(pos), pos_p, sp_p, len(arrs[0][0]),
                                          *[p for _, p in arrs]))
 
+    def set_radial_local(self, pos, species, z, sigma, dg, tables):
+        """Local parts from radial tables (qsb_scf_set_radial_local): tables
+        [n_species, n_g] of radial_local_table(radius, v, z[k], n_g, dg, sigma[k])."""
+        pos, pos_p = _f64(np.asarray(pos, np.float64).reshape(-1, 3))
+        self._n_atoms = len(pos)
+        sp, sp_p = _i32(species)
+        zz, z_p = _f64(np.asarray(z, np.float64).ravel())
+        ss, s_p = _f64(np.asarray(sigma, np.float64).ravel())
+        tab = np.ascontiguousarray(np.asarray(tables, np.float64).reshape(len(zz), -1))
+        t, t_p = _f64(tab.ravel())
+        _check(lib.qsb_scf_set_radial_local(self._h, len(pos), pos_p, sp_p, len(zz), z_p, s_p, tab.shape[1],
+                                            _c_d(dg), t_p))
+
     def set_mixing(self, amplitude=0.5, q0=0.8, depth=6):
         _check(lib.qsb_scf_set_mixing(self._h, _c_d(amplitude), _c_d(q0), depth))
 
