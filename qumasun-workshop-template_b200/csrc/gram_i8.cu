@@ -423,7 +423,7 @@ rot_i8_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ C
               const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mA3,
               const __grid_constant__ CUtensorMap mB0, const __grid_constant__ CUtensorMap mB1,
               const __grid_constant__ CUtensorMap mB2, const __grid_constant__ CUtensorMap mB3, int kstages,
-              int64_t N, int q, const double* __restrict__ fscale, ColumnSet out, int* __restrict__ err) {
+              int64_t N, int q, int ntn, const double* __restrict__ fscale, ColumnSet out, int* __restrict__ err) {
     extern __shared__ unsigned char rt_raw[];
     unsigned char* base = (unsigned char*)(((uintptr_t)rt_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* full = reinterpret_cast<uint64_t*>(base + (size_t)RT_STAGES * RT_STAGE_BYTES);
@@ -433,7 +433,9 @@ rot_i8_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ C
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int mt = blockIdx.x, nt = blockIdx.y;
+    // the column tiles of one row tile are neighbours in launch order, so the
+    // row tile's slices of U come from DRAM once and from L2 for the others
+    const int mt = (int)(blockIdx.x / (unsigned)ntn), nt = (int)(blockIdx.x % (unsigned)ntn);
     const int nk = kstages;
 
     if (threadIdx.x == 0) {
@@ -731,9 +733,12 @@ qsb_status ozaki_rotate(int64_t N, const void* Usplit, int K, const double* C, i
             !make_kmajor_map(&m[4 + k], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, cs + k * cstride, kpad, q, RT_K, RT_N))
             return fail(QSB_ERR_CUDA, "ozaki_rotate: tensor map encoding failed");
     QSB_CUDA_TRY(cudaFuncSetAttribute(rot_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RT_SMEM));
-    const dim3 grid((unsigned)((N + OZ_M - 1) / OZ_M), (unsigned)((q + RT_N - 1) / RT_N));
-    rot_i8_kernel<<<grid, OZ_THREADS, RT_SMEM, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7], kpad / RT_K, N, q,
-                                                    fscale, out, device_error_word());
+    const int ntn = (q + RT_N - 1) / RT_N;
+    const long long ctas = (long long)((N + OZ_M - 1) / OZ_M) * ntn;
+    if (ctas > 0x7fffffffLL) return fail(QSB_ERR_INVALID, "ozaki_rotate: grid too large");
+    rot_i8_kernel<<<(unsigned)ctas, OZ_THREADS, RT_SMEM, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7],
+                                                              kpad / RT_K, N, q, ntn, fscale, out,
+                                                              device_error_word());
     QSB_CUDA_TRY(cudaGetLastError());
     return QSB_OK;
 }
