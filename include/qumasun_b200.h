@@ -512,8 +512,22 @@ QSB_API qsb_status qsb_scf_set_smearing(qsb_scf* scf, double kbt);
  * and slope continuity at rs = 1 (C = 0.0020191519, D = -0.0116320664; A, B
  * and the low-density branch unchanged), which leaves the energy a smooth
  * function of the positions.  rho_min (default 1e-8, Calc_XC_LDA's cut,
- * >= 1e-30): exc = vxc = 0 below it. */
+ * >= 1e-30): exc = vxc = 0 below it.  pz_variant 2: GGA-PBE instead
+ * (spin-unpolarised, as qsb_gga_pbe; rho_min not used). */
 QSB_API qsb_status qsb_scf_set_xc(qsb_scf* scf, int pz_variant, double rho_min);
+/* GGA-PBE exchange-correlation of a spin-unpolarised density on an
+ * nx x ny x nz periodic grid (device arrays of N doubles; exc may be NULL):
+ * exc = the energy density (E_xc = dV sum exc), vxc = the potential
+ * v_x + v_c - 2 div(P_x grad rho_s) - 2 div(P_c grad rho), gradients and
+ * divergences by the eighth-order central difference.  Replaces the GGA branch
+ * of QUMASUN_BASE1::mSetPotentialVxc (source/qumasun_base1.potential.h:383-470,
+ * 585-640, XC_IMPLE_VER2) with GGA_PBE::Potential_X_test3 and
+ * EnergyDensityPotential_C_test3 (source/xc_gga_pbe.h:326-356, 525-594):
+ * exchange per spin channel on rho / 2, correlation on rho, PW92 local part,
+ * densities below 1e-8 contributing nothing.  Allocates 3 N doubles of
+ * scratch per call and synchronizes the stream. */
+QSB_API qsb_status qsb_gga_pbe(int nx, int ny, int nz, double dx, double dy, double dz, const double* rho,
+                               double* exc, double* vxc, void* stream);
 /* Also require int |rho_out - rho_in| dV / N_e < rho_tol to stop (the
  * reference's RHO_ETOT convergence mode, source/qumasun_kpoint.scfloop.h:182-213);
  * 0 (default) stops on the energy alone. */

@@ -1,7 +1,9 @@
 /*
- * oracle/ref_fft.cpp -- extern "C" entry around the REFERENCE's own FFT-kinetic
- * Hamiltonian, compiled in place from the reference's source/ directory (never
- * copied) into oracle/_ref/libqsref_fft.so.  Test infrastructure only.
+ * oracle/ref_fft.cpp -- extern "C" entries around the REFERENCE's own
+ * QUMASUN_BASE1 object (its FFT-kinetic Hamiltonian and its GGA-PBE
+ * exchange-correlation), compiled in place from the reference's source/
+ * directory (never copied) into oracle/_ref/libqsref_fft.so.  Test
+ * infrastructure only.
  *
  * What runs is QUMASUN_BASE1::mHamiltonianMatrix_ddm_bundle, algorithm 1
  * (source/qumasun_base1.matrix.h:142-228): the SoA bands gathered into
@@ -33,6 +35,20 @@ namespace {
 class RefFFTHamiltonian : public QUMASUN_BASE1 {
 public:
     RefFFTHamiltonian(const Input& input, const int ddm[4]) : QUMASUN_BASE1(input, MPI_COMM_WORLD, ddm) {}
+
+    // the reference's spin-unpolarised GGA branch of mSetPotentialVxc on a given density
+    void GgaPbe(const double* rho, double* vxc, double* e_x, double* e_c) {
+        const size_t N = (size_t)m_size_3d;
+        mInitializeWorkBuffer(16 * N + 64);
+        for (size_t i = 0; i < N; ++i) {
+            ml_rho[i] = rho[i];
+            ml_pcc_rho[i] = 0.0;
+        }
+        mSetPotentialVxc();
+        for (size_t i = 0; i < N; ++i) vxc[i] = ml_Vx[i] + ml_Vc[i];
+        *e_x = m_E_x;
+        *e_c = m_E_c;
+    }
 
     // H psi of nb SoA bands (band b: re at 2bN, im at (2b+1)N)
     void Apply(const double* V, int nb, const double* psi, double* hpsi, int kx, int ky, int kz) {
@@ -77,6 +93,33 @@ int qsref_ham_fft(int nx, int ny, int nz, double lx, double ly, double lz, const
     const int ddm[4] = {1, 1, 1, 1};
     RefFFTHamiltonian H(in, ddm);
     H.Apply(V, nb, psi, hpsi, kidx ? kidx[0] : 0, kidx ? kidx[1] : 0, kidx ? kidx[2] : 0);
+    return 0;
+}
+
+/* The reference's GGA-PBE exchange-correlation (XC_TYPE::GGA, spin off) of a
+ * density rho on an nx x ny x nz periodic box of sides (lx, ly, lz):
+ * vxc = V_x + V_c (N doubles), e_xc[0] = E_x, e_xc[1] = E_c (QUMASUN_BASE1::
+ * mSetPotentialVxc, source/qumasun_base1.potential.h:376-640). */
+int qsref_gga_pbe(int nx, int ny, int nz, double lx, double ly, double lz, const double* rho, double* vxc,
+                  double* e_xc) {
+    if (nx < 1 || ny < 1 || nz < 1 || !rho || !vxc || !e_xc) return 1;
+    QUMASUN::Input in{};
+    in.hamiltonian_type = QUMASUN::HAMILTONIAN::KohnSham_PP;
+    in.xc_type = QUMASUN::XC_TYPE::GGA;
+    in.grid_size[0] = nx;
+    in.grid_size[1] = ny;
+    in.grid_size[2] = nz;
+    std::memset(in.box_axis, 0, sizeof(in.box_axis));
+    in.box_axis[0] = lx;
+    in.box_axis[4] = ly;
+    in.box_axis[8] = lz;
+    in.num_solutions = 1;
+    in.num_nuclei = 0;
+    in.HR_ratio = 1;
+    in.test_algorithm_Laplacian = 1;
+    const int ddm[4] = {1, 1, 1, 1};
+    RefFFTHamiltonian H(in, ddm);
+    H.GgaPbe(rho, vxc, &e_xc[0], &e_xc[1]);
     return 0;
 }
 

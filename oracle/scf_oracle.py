@@ -21,6 +21,7 @@ grid, source/qumasun_base1.core.h), and the device SCF is checked against
 this oracle.
 """
 import contextlib
+import math
 import ctypes
 import os
 import sys
@@ -58,6 +59,106 @@ def lda_pz(rho):
     exc[m] = r * ex + r * ec
     vxc[m] = (ex + ex / 3.0) + (ec + ndec)
     return exc, vxc
+
+
+def _fd8_d1(f, axis, h):
+    """Eighth-order central first derivative along a numpy axis (periodic),
+    GridGradient8th.h:23-26,65: c4 (f+4 - f-4) + c3 (..) + c2 (..) + c1 (..)."""
+    c = {4: -3.0 / (840.0 * h), 3: 32.0 / (840.0 * h), 2: -168.0 / (840.0 * h), 1: 672.0 / (840.0 * h)}
+    out = None
+    for m in (4, 3, 2, 1):
+        t = c[m] * (np.roll(f, -m, axis=axis) - np.roll(f, m, axis=axis))
+        out = t if out is None else out + t
+    return out
+
+
+def gga_pbe(grid, rho):
+    """Spin-unpolarised GGA-PBE as the reference's mSetPotentialVxc forms it
+    (source/qumasun_base1.potential.h:383-470, 585-640, XC_IMPLE_VER2):
+    exchange on rho_s = rho / 2 per spin channel (GGA_PBE::Potential_X_test3,
+    source/xc_gga_pbe.h:326-356), correlation on rho (EnergyDensityPotential_C_test3
+    :525-594 with LDA_PW92 :7-76 at zeta = 0), FD8 gradients and divergences.
+    Returns (exc energy density, vxc, E_x, E_c); grid = (nx, ny, nz, dx, dy, dz),
+    rho with x fastest."""
+    nx, ny, nz, dx, dy, dz = grid
+    r = np.asarray(rho, np.float64).reshape(nz, ny, nx)
+    rs_ = r / 2.0
+    hs = (dz, dy, dx)
+    g = [_fd8_d1(rs_, ax, hs[ax]) for ax in (2, 1, 0)]          # d/dx, d/dy, d/dz
+    kappa, mu, beta, gamma = 0.804, 0.21951, 0.066725, 0.031091
+    cut = 1.0e-8
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        # exchange
+        s2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2]
+        r13 = np.cbrt(rs_)
+        r43 = r13 * rs_
+        c6 = np.cbrt(6.0 / math.pi)
+        c62 = (6.0 * math.pi) / c6
+        qm = 4.0 * c62 * r43 * r43
+        q = s2 / qm
+        den = 1.0 + q * mu / kappa
+        F = 1.0 + kappa - kappa / den
+        dF = mu / (den * den)
+        dq = -(8.0 / 3.0) * q / rs_
+        okx = rs_ >= cut
+        ex = np.where(okx, -(3.0 / 4.0) * c6 * r43 * F, 0.0)
+        vx = np.where(okx, -c6 * (r13 * F + (3.0 / 4.0) * r43 * dF * dq), 0.0)
+        px = np.where(okx, -(3.0 / 4.0) * c6 * r43 * dF * (1.0 / qm), 0.0)
+        # correlation
+        G = [2.0 * gi for gi in g]
+        s2c = G[0] * G[0] + G[1] * G[1] + G[2] * G[2]
+        A, al, b1, b2, b3, b4 = 0.031091, 0.21370, 7.5957, 3.5876, 1.6382, 0.49294
+        rsw = np.cbrt(3.0 / (4.0 * math.pi * r))
+        sq = np.sqrt(rsw)
+        mother = 2.0 * A * (b1 * sq + b2 * rsw + b3 * rsw * sq + b4 * rsw * rsw)
+        lnt = np.log(1.0 + 1.0 / mother)
+        el = -2.0 * A * (1.0 + al * rsw) * lnt
+        dmo = 2.0 * A * (b1 / (2.0 * sq) + b2 + (3.0 / 2.0) * b3 * sq + 2.0 * b4 * rsw)
+        dln = -dmo / ((mother + 1.0) * mother)
+        de = -2.0 * A * (al * lnt + (1.0 + al * rsw) * dln)
+        vl = el - (1.0 / 3.0) * rsw * de
+        ee = np.exp(-el / gamma)
+        alpha = ee - 1.0
+        C = (beta / gamma) * np.cbrt(math.pi / 3.0) / 16.0
+        cr = np.cbrt(r)
+        Y = C * s2c
+        r73 = r * r * cr
+        B = alpha * r73
+        BeY = np.maximum(B + ee * Y, 1e-30)
+        BY = np.maximum(B + Y, 1e-30)
+        lg = np.log(BeY / BY)
+        H = gamma * lg
+        dexp = np.where(0.5 * r < cut, 0.0, -(ee / gamma) * (vl - el) / r)
+        dB = (7.0 / 3.0) * alpha * cr * r + r73 * dexp
+        vH = H + r * gamma * ((-alpha * Y / (BeY * BY)) * dB + Y / BeY * dexp)
+        okc = r >= cut
+        ec = np.where(okc, el + H, 0.0)
+        vc = np.where(okc, vl + vH, 0.0)
+        pc = np.where(okc, r * gamma * (alpha * B / (BeY * BY)) * C, 0.0)
+    dV = dx * dy * dz
+    E_x = 2.0 * float(np.sum(ex)) * dV
+    E_c = float(np.sum(r * ec)) * dV
+    vxc = vx + vc
+    for ax, gi in zip((2, 1, 0), g):
+        vxc = vxc - _fd8_d1((2.0 * px + 4.0 * pc) * gi, ax, hs[ax])
+    exc = 2.0 * ex + r * ec
+    return exc.ravel(), vxc.ravel(), E_x, E_c
+
+
+def ref_gga_pbe(grid, rho):
+    """The reference's own GGA branch of mSetPotentialVxc on its QUMASUN_BASE1
+    object (oracle/_ref/libqsref_fft.so): (vxc, E_x, E_c)."""
+    nx, ny, nz, dx, dy, dz = grid
+    lib = ctypes.CDLL(O.LIB_REF_FFT)
+    rho = np.ascontiguousarray(rho, np.float64)
+    vxc = np.zeros_like(rho)
+    e = np.zeros(2)
+    dp = ctypes.POINTER(ctypes.c_double)
+    with contextlib.redirect_stdout(None):
+        rc = lib.qsref_gga_pbe(nx, ny, nz, ctypes.c_double(nx * dx), ctypes.c_double(ny * dy), ctypes.c_double(nz * dz),
+                               rho.ctypes.data_as(dp), vxc.ctypes.data_as(dp), e.ctypes.data_as(dp))
+    assert rc == 0
+    return vxc, float(e[0]), float(e[1])
 
 
 def ref_lda_pz(rho):
@@ -315,10 +416,19 @@ def density(X, occ, N):
     return np.einsum("n,ni->i", np.asarray(occ, np.float64), X * X)
 
 
+def xc_of(grid, rho, xc):
+    """(energy density, v_xc) of the LDA-PZ (xc "lda") or the GGA-PBE ("pbe")."""
+    if xc == "pbe":
+        exc, vxc, _, _ = gga_pbe(grid, rho)
+        return exc, vxc
+    return lda_pz(rho)
+
+
 def scf(grid, pos, species_params, nb, n_el, X0, kbt=0.01, lobpcg_iters=4, max_steps=60, tol_per_atom=1e-6,
-        amplitude=0.5, q0=0.8, depth=6, rcut_factor=O.RCUT_FACTOR):
+        amplitude=0.5, q0=0.8, depth=6, rcut_factor=O.RCUT_FACTOR, xc="lda"):
     """The oracle SCF.  Returns a dict with the per-step total energies,
-    final Rayleigh quotients, occupations, density and wavefunctions."""
+    final Rayleigh quotients, occupations, density and wavefunctions.
+    xc: "lda" (PZ) or "pbe" (GGA-PBE, gga_pbe)."""
     nx, ny, nz, dx, dy, dz = grid
     N = nx * ny * nz
     dV = dx * dy * dz
@@ -334,7 +444,7 @@ def scf(grid, pos, species_params, nb, n_el, X0, kbt=0.01, lobpcg_iters=4, max_s
     energies, e_prev = [], None
     for step in range(max_steps):
         vh, _ = hartree(rho_in, grid)
-        _, vxc = lda_pz(rho_in)
+        _, vxc = xc_of(grid, rho_in, xc)
         veff = vloc + vh + vxc
         with _quiet_stdout():
             O.ref_lobpcg_d(grid, veff, cube, X, keep, nb, lobpcg_iters, ev, step == 0)
@@ -343,7 +453,7 @@ def scf(grid, pos, species_params, nb, n_el, X0, kbt=0.01, lobpcg_iters=4, max_s
         occ, mu = fermi_occupations_exact(rq, n_el, kbt)
         rho_out = density(X, occ, N)
         vh_out, eh = hartree(rho_out, grid)
-        exc_out, _ = lda_pz(rho_out)
+        exc_out, _ = xc_of(grid, rho_out, xc)
         etot = float(np.dot(occ, rq)) - float(np.dot(vh + vxc, rho_out)) * dV + eh + float(np.sum(exc_out)) * dV
         energies.append(etot)
         done = e_prev is not None and abs(etot - e_prev) / n_atoms < tol_per_atom

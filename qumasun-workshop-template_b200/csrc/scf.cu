@@ -93,6 +93,132 @@ __global__ void lda_kernel(size_t N, const double* __restrict__ rho, double* __r
     }
 }
 
+// ---------------------------------------------------------------------------
+// GGA-PBE, spin-unpolarised, as the reference's mSetPotentialVxc takes it
+// (source/qumasun_base1.potential.h:383-470, 585-640 with XC_IMPLE_VER2):
+// exchange per spin channel on rho_s = rho / 2 (GGA_PBE::Potential_X_test3,
+// source/xc_gga_pbe.h:326-356; E_x = 2 E_x[rho_s]), correlation on rho with
+// |grad rho|^2 (EnergyDensityPotential_C_test3, :525-594, PW92 local part
+// LDA_PW92, :7-76, at zeta = 0), gradients and divergences by the eighth-order
+// central first derivative (GridGradient8th.h:23-26), V_xc = v_x + v_c
+// - 2 div(P_x grad rho_s) - 2 div(P_c grad rho).  The published PBE (Perdew,
+// Burke, Ernzerhof, PRL 77, 3865) and PW92 (Perdew, Wang, PRB 45, 13244)
+// parameters as the reference rounds them.
+// ---------------------------------------------------------------------------
+struct Grid3 {
+    int nx, ny, nz;
+    double dx, dy, dz;
+};
+
+// first derivative along axis `axis` of f at point (x, y, z), periodic, FD8
+__device__ __forceinline__ double fd8_d1(const double* __restrict__ f, const Grid3& g, int x, int y, int z, int axis,
+                                         double scale) {
+    const double h = axis == 0 ? g.dx : axis == 1 ? g.dy : g.dz;
+    const double c4 = -3.0 / (840.0 * h), c3 = 32.0 / (840.0 * h), c2 = -168.0 / (840.0 * h), c1 = 672.0 / (840.0 * h);
+    auto at = [&](int m) -> double {
+        int xx = x, yy = y, zz = z;
+        if (axis == 0) xx = (x + m + 4 * g.nx) % g.nx;
+        else if (axis == 1) yy = (y + m + 4 * g.ny) % g.ny;
+        else zz = (z + m + 4 * g.nz) % g.nz;
+        return scale * f[(size_t)xx + (size_t)g.nx * (yy + (size_t)g.ny * zz)];
+    };
+    return c4 * (at(4) - at(-4)) + c3 * (at(3) - at(-3)) + c2 * (at(2) - at(-2)) + c1 * (at(1) - at(-1));
+}
+
+// grad rho_s (rho_s = rho / 2) into g[0..3N)
+__global__ void gga_grad_kernel(Grid3 g, const double* __restrict__ rho, double* __restrict__ grad) {
+    const size_t N = (size_t)g.nx * g.ny * g.nz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / ((size_t)g.nx * g.ny));
+        grad[i] = fd8_d1(rho, g, x, y, z, 0, 0.5);
+        grad[N + i] = fd8_d1(rho, g, x, y, z, 1, 0.5);
+        grad[2 * N + i] = fd8_d1(rho, g, x, y, z, 2, 0.5);
+    }
+}
+
+// Per point: exc = 2 rho_s eps_x(rho_s, s_s) + rho (eps_c^PW92 + H), vxc = v_x + v_c
+// (the local parts), and grad (in) -> the flux 2 P_x grad rho_s + 2 P_c grad rho (out).
+__global__ void gga_pbe_point_kernel(size_t N, const double* __restrict__ rho, double* __restrict__ grad,
+                                     double* __restrict__ exc, double* __restrict__ vxc) {
+    const double kappa = 0.804, mu = 0.21951, beta = 0.066725, gamma = 0.031091;
+    const double cut = 1.0e-8;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+        const double gx = grad[i], gy = grad[N + i], gz = grad[2 * N + i];
+        const double rs_ = 0.5 * rho[i];
+        // exchange, one spin channel
+        double ex = 0.0, vx = 0.0, px = 0.0;
+        if (rs_ >= cut) {
+            const double s2 = gx * gx + gy * gy + gz * gz;
+            const double r13 = cbrt(rs_);
+            const double r43 = r13 * rs_;
+            const double c6 = cbrt(6.0 / M_PI);
+            const double c62 = (6.0 * M_PI) / c6;
+            const double qm = 4.0 * c62 * r43 * r43;
+            const double q = s2 / qm;
+            const double den = 1.0 + q * mu / kappa;
+            const double F = 1.0 + kappa - kappa / den;
+            const double dF = mu / (den * den);
+            const double dq_dr = -(8.0 / 3.0) * q / rs_;
+            ex = -(3.0 / 4.0) * c6 * r43 * F;
+            vx = -c6 * (r13 * F + (3.0 / 4.0) * r43 * dF * dq_dr);
+            px = -(3.0 / 4.0) * c6 * r43 * dF * (1.0 / qm);
+        }
+        // correlation on rho = 2 rho_s with grad rho = 2 grad rho_s
+        const double r = 2.0 * rs_;
+        double ec = 0.0, vc = 0.0, pc = 0.0;
+        if (r >= cut) {
+            const double Gx = 2.0 * gx, Gy = 2.0 * gy, Gz = 2.0 * gz;
+            const double s2 = Gx * Gx + Gy * Gy + Gz * Gz;
+            // PW92, zeta = 0
+            const double A = 0.031091, al = 0.21370, b1 = 7.5957, b2 = 3.5876, b3 = 1.6382, b4 = 0.49294;
+            const double rsw = cbrt(3.0 / (4.0 * M_PI * r));
+            const double sq = sqrt(rsw);
+            const double mother = 2.0 * A * (b1 * sq + b2 * rsw + b3 * rsw * sq + b4 * rsw * rsw);
+            const double lnt = log(1.0 + 1.0 / mother);
+            const double el = -2.0 * A * (1.0 + al * rsw) * lnt;
+            const double dmo = 2.0 * A * (b1 / (2.0 * sq) + b2 + (3.0 / 2.0) * b3 * sq + 2.0 * b4 * rsw);
+            const double dln = -dmo / ((mother + 1.0) * mother);
+            const double de = -2.0 * A * (al * lnt + (1.0 + al * rsw) * dln);
+            const double vl = el - (1.0 / 3.0) * rsw * de;
+            // PBE gradient correction H, phi = 1 at zeta = 0
+            const double ee = exp(-el / gamma);
+            const double alpha = ee - 1.0;
+            const double C = (beta / gamma) * cbrt(M_PI / 3.0) / 16.0;
+            const double cr = cbrt(r);
+            const double Y = C * s2;
+            const double r73 = r * r * cr;
+            const double B = alpha * r73;
+            const double BeY = fmax(B + ee * Y, 1e-30);
+            const double BY = fmax(B + Y, 1e-30);
+            const double lg = log(BeY / BY);
+            const double H = gamma * lg;
+            const double dexp = (0.5 * r < cut) ? 0.0 : -(ee / gamma) * (vl - el) / r;
+            const double dB = (7.0 / 3.0) * alpha * cr * r + r73 * dexp;
+            const double vH = H + r * gamma * ((-alpha * Y / (BeY * BY)) * dB + Y / BeY * dexp);
+            ec = el + H;
+            vc = vl + vH;
+            pc = r * gamma * (alpha * B / (BeY * BY)) * C;
+        }
+        if (exc) exc[i] = 2.0 * ex + r * ec;
+        vxc[i] = vx + vc;
+        const double f = 2.0 * px + 4.0 * pc;
+        grad[i] = f * gx;
+        grad[N + i] = f * gy;
+        grad[2 * N + i] = f * gz;
+    }
+}
+
+// vxc -= div(flux)
+__global__ void gga_div_kernel(Grid3 g, const double* __restrict__ flux, double* __restrict__ vxc) {
+    const size_t N = (size_t)g.nx * g.ny * g.nz;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / ((size_t)g.nx * g.ny));
+        const double d = fd8_d1(flux, g, x, y, z, 0, 1.0) + fd8_d1(flux + N, g, x, y, z, 1, 1.0) +
+                         fd8_d1(flux + 2 * N, g, x, y, z, 2, 1.0);
+        vxc[i] -= d;
+    }
+}
+
 // out = a + b + c
 __global__ void sum3_kernel(size_t N, const double* __restrict__ a, const double* __restrict__ b,
                             const double* __restrict__ c, double* __restrict__ out) {
@@ -443,6 +569,8 @@ struct qsb_scf {
     double rho_tol = 0.0;         // int |rho_out - rho_in| / N_e bound of the stop (0: off)
     double xc_rho_min = 1.0e-8;   // LDA: exc = vxc = 0 below this density (Calc_XC_LDA's cut)
     bool xc_continuous = false;   // PZ correlation made continuous at rs = 1 (qsb_scf_set_xc)
+    int xc_kind = 0;              // 0 LDA-PZ, 2 GGA-PBE (qsb_scf_set_xc)
+    double* gga = nullptr;        // GGA: grad rho_s, then the flux (3 N)
     // FP64 polish of a mixed-precision run (qsb_scf_set_polish)
     qsb_eigensolver* polish_es = nullptr;
     int polish_max = 0;
@@ -519,11 +647,24 @@ qsb_status kspace(qsb_scf* c, KOp op, const double* in, double* out, cudaStream_
     return QSB_OK;
 }
 
+// vxc = V_xc[rho], exc = its energy density (may be null): LDA-PZ or GGA-PBE
+qsb_status xc_eval(qsb_scf* c, const double* rho, double* exc, double* vxc, cudaStream_t s) {
+    if (c->xc_kind == 2) {
+        const Grid3 g{c->nx, c->ny, c->nz, c->dx, c->dy, c->dz};
+        gga_grad_kernel<<<pw_blocks(c->N), 256, 0, s>>>(g, rho, c->gga);
+        gga_pbe_point_kernel<<<pw_blocks(c->N), 256, 0, s>>>(c->N, rho, c->gga, exc, vxc);
+        gga_div_kernel<<<pw_blocks(c->N), 256, 0, s>>>(g, c->gga, vxc);
+    } else {
+        lda_kernel<<<pw_blocks(c->N), 256, 0, s>>>(c->N, rho, exc, vxc, c->xc_rho_min, c->xc_continuous);
+    }
+    QSB_CUDA_TRY(cudaGetLastError());
+    return QSB_OK;
+}
+
 // veff = vloc + V_H[rho_in] + V_xc[rho_in]
 qsb_status potentials(qsb_scf* c, cudaStream_t s) {
     QSB_TRY(kspace(c, KOp::hartree, c->rho_in, c->vh, s));
-    lda_kernel<<<pw_blocks(c->N), 256, 0, s>>>(c->N, c->rho_in, nullptr, c->vxc, c->xc_rho_min,
-                                                c->xc_continuous);
+    QSB_TRY(xc_eval(c, c->rho_in, nullptr, c->vxc, s));
     sum3_kernel<<<pw_blocks(c->N), 256, 0, s>>>(c->N, c->vloc, c->vh, c->vxc, c->veff);
     QSB_CUDA_TRY(cudaGetLastError());
     return qsb_ham_set_potential(c->ham, c->veff, 1);
@@ -743,7 +884,7 @@ qsb_status qsb_scf_destroy(qsb_scf* c) {
     if (c->hxc) cudaFree(c->hxc);
     if (c->occ2) cudaFree(c->occ2);
     if (c->fk) cudaFree(c->fk);
-    void* loc[4] = {c->atoms, c->tab_atoms, c->tab_species, c->tab};
+    void* loc[5] = {c->atoms, c->tab_atoms, c->tab_species, c->tab, c->gga};
     for (void* q : loc)
         if (q) cudaFree(q);
     if (c->have_plans) {
@@ -808,10 +949,32 @@ qsb_status qsb_scf_polish_stats(const qsb_scf* c, int* first_step, int* steps) {
 }
 
 qsb_status qsb_scf_set_xc(qsb_scf* c, int pz_variant, double rho_min) {
-    if (!c || (pz_variant != 0 && pz_variant != 1) || !(rho_min >= 1e-30))
-        return fail(QSB_ERR_INVALID, "scf_set_xc: need pz_variant 0 or 1 and rho_min >= 1e-30");
+    if (!c || pz_variant < 0 || pz_variant > 2 || !(rho_min >= 1e-30))
+        return fail(QSB_ERR_INVALID, "scf_set_xc: need variant 0, 1 (LDA-PZ) or 2 (GGA-PBE) and rho_min >= 1e-30");
+    if (pz_variant == 2 && !c->gga) QSB_CUDA_TRY(cudaMalloc((void**)&c->gga, 3 * c->N * sizeof(double)));
+    c->xc_kind = pz_variant == 2 ? 2 : 0;
     c->xc_continuous = pz_variant == 1;
     c->xc_rho_min = rho_min;
+    return QSB_OK;
+}
+
+qsb_status qsb_gga_pbe(int nx, int ny, int nz, double dx, double dy, double dz, const double* rho, double* exc,
+                       double* vxc, void* stream) {
+    if (nx < 1 || ny < 1 || nz < 1 || !(dx > 0.0) || !(dy > 0.0) || !(dz > 0.0) || !rho || !vxc)
+        return fail(QSB_ERR_INVALID, "gga_pbe: bad argument");
+    const size_t N = (size_t)nx * ny * nz;
+    cudaStream_t s = (cudaStream_t)stream;
+    double* work = nullptr;
+    QSB_CUDA_TRY(cudaMalloc((void**)&work, 3 * N * sizeof(double)));
+    const Grid3 g{nx, ny, nz, dx, dy, dz};
+    gga_grad_kernel<<<pw_blocks(N), 256, 0, s>>>(g, rho, work);
+    gga_pbe_point_kernel<<<pw_blocks(N), 256, 0, s>>>(N, rho, work, exc, vxc);
+    gga_div_kernel<<<pw_blocks(N), 256, 0, s>>>(g, work, vxc);
+    const cudaError_t e = cudaGetLastError();
+    const cudaError_t e2 = cudaStreamSynchronize(s);
+    cudaFree(work);
+    if (e != cudaSuccess) return cuda_fail(e, "gga_pbe");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "gga_pbe");
     return QSB_OK;
 }
 
@@ -1032,8 +1195,7 @@ qsb_status qsb_scf_run(qsb_scf* c, double* X, double* keep, int lobpcg_iters, in
         // energy of the output density: sum occ rq - int (V_H + V_xc)[rho_in] rho_out + E_H + E_xc [rho_out]
         sub_kernel<<<pw_blocks(N), 256, 0, s>>>(N, c->veff, c->vloc, c->tmp);
         QSB_TRY(kspace(c, KOp::hartree, c->rho_out, c->vh, s));
-        lda_kernel<<<pw_blocks(N), 256, 0, s>>>(N, c->rho_out, c->exc, c->vxc, c->xc_rho_min,
-                                                      c->xc_continuous);
+        QSB_TRY(xc_eval(c, c->rho_out, c->exc, c->vxc, s));
         QSB_CUDA_TRY(cudaGetLastError());
         double d2[2], exc_int;
         {
@@ -1279,7 +1441,7 @@ qsb_status qsb_scf_run_kpoints(qsb_scf* c, double* const* X, double* const* keep
         // energy of the output density, as the Gamma-point loop
         sub_kernel<<<pw_blocks(N), 256, 0, s>>>(N, c->veff, c->vloc, c->tmp);
         QSB_TRY(kspace(c, KOp::hartree, c->rho_out, c->vh, s));
-        lda_kernel<<<pw_blocks(N), 256, 0, s>>>(N, c->rho_out, c->exc, c->vxc, c->xc_rho_min, c->xc_continuous);
+        QSB_TRY(xc_eval(c, c->rho_out, c->exc, c->vxc, s));
         QSB_CUDA_TRY(cudaGetLastError());
         double d2[2], exc_int;
         {

@@ -615,6 +615,18 @@ def ewald(pos, charge, cell):
     return e.value, f.reshape(len(p), 3)
 
 
+def gga_pbe(rho, grid):
+    """(energy density, v_xc) of spin-unpolarised GGA-PBE on a periodic grid
+    (qsb_gga_pbe ~ the GGA branch of mSetPotentialVxc); grid = (nx, ny, nz, dx, dy, dz)."""
+    torch = _torch()
+    nx, ny, nz, dx, dy, dz = grid
+    assert rho.numel() == nx * ny * nz
+    exc, vxc = torch.empty_like(rho), torch.empty_like(rho)
+    _check(lib.qsb_gga_pbe(int(nx), int(ny), int(nz), _c_d(dx), _c_d(dy), _c_d(dz), _dev_ptr(rho), _dev_ptr(exc),
+                           _dev_ptr(vxc), _stream_ptr(rho)))
+    return exc, vxc
+
+
 def lda_pz(rho):
     """(rho eps_xc, v_xc) of the Perdew-Zunger LDA (qsb_lda_pz ~ Calc_XC_LDA)."""
     torch = _torch()
@@ -676,7 +688,8 @@ class SCF:
         _check(lib.qsb_scf_set_smearing(self._h, _c_d(kbt)))
 
     def set_xc(self, pz_variant=0, rho_min=1e-8):
-        """LDA form (qsb_scf_set_xc): 0 the reference's PZ, 1 PZ continuous at rs = 1; cut rho_min."""
+        """XC form (qsb_scf_set_xc): 0 the reference's LDA-PZ, 1 PZ continuous at
+        rs = 1 (cut rho_min), 2 GGA-PBE."""
         _check(lib.qsb_scf_set_xc(self._h, int(pz_variant), _c_d(rho_min)))
 
     def set_polish(self, solver_fp64, max_steps=10, tol_per_atom=0.0, rho_tol=0.0):

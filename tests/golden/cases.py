@@ -83,6 +83,37 @@ def _fft_oracle(inp, cplx, ks, ki):
     return O.kinetic_fft(inp["grid"], inp["psi"], nb, cplx, g) + vpsi
 
 
+GGA_GRID = (20, 18, 16, 0.3, 0.33, 0.375)
+
+
+def gga_density(grid=GGA_GRID):
+    """A smooth positive periodic density with three points below the GGA cut."""
+    nx, ny, nz, dx, dy, dz = grid
+    x, y, z = np.arange(nx) * dx, np.arange(ny) * dy, np.arange(nz) * dz
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    L = (nx * dx, ny * dy, nz * dz)
+    rho = 0.02 + 0.3 * np.exp(np.cos(2 * np.pi * X / L[0]) + np.sin(2 * np.pi * Y / L[1]) * np.cos(4 * np.pi * Z / L[2]))
+    rho[0, 0, :3] = 1e-9
+    return rho.ravel()
+
+
+def _gga_inputs():
+    rho = gga_density()
+    return dict(grid=GGA_GRID, rho=rho, checked=[rho])
+
+
+def _gga_ref(inp):
+    import scf_oracle as S
+    v, ex, ec = S.ref_gga_pbe(inp["grid"], inp["rho"])
+    return np.concatenate([v, [ex, ec]])
+
+
+def _gga_oracle(inp):
+    import scf_oracle as S
+    _, v, ex, ec = S.gga_pbe(inp["grid"], inp["rho"])
+    return np.concatenate([v, [ex, ec]])
+
+
 # the FFT-kinetic cases: k-point sampling and index of each (the reference's k)
 FFT_GRID_EVEN = (24, 20, 16, 0.25, 0.3, 0.375)
 FFT_GRID_ODD = (15, 12, 9, 0.4, 0.5, 0.6)
@@ -123,6 +154,8 @@ CASES = {
     "ham_fft_kpt_even": dict(inputs=lambda: _fft_inputs(FFT_GRID_EVEN, 8, 3, True),
                              reference=lambda i: _fft_ref(i, True, *FFT_KPT["ham_fft_kpt_even"]),
                              oracle=lambda i: _fft_oracle(i, True, *FFT_KPT["ham_fft_kpt_even"])),
+    # GGA-PBE exchange-correlation: V_xc on the grid, then E_x, E_c (the reference's own mSetPotentialVxc)
+    "gga_pbe": dict(inputs=_gga_inputs, reference=_gga_ref, oracle=_gga_oracle),
     "ham_fft_kpt_odd": dict(inputs=lambda: _fft_inputs(FFT_GRID_ODD, 9, 2, True),
                             reference=lambda i: _fft_ref(i, True, *FFT_KPT["ham_fft_kpt_odd"]),
                             oracle=lambda i: _fft_oracle(i, True, *FFT_KPT["ham_fft_kpt_odd"])),

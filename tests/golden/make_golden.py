@@ -41,6 +41,16 @@ def main(only=None):
         np.savez_compressed(os.path.join(HERE, "scf_kpt.npz"), energies=r["energies"], rq=r["rq"], occ=r["occ"],
                             rho=r["rho"], checksum=np.array([float(np.sum(v)) for v in inp["checked"]]))
         print("scf_kpt", r["steps"], r["energies"][-1])
+    if not only or "scf_c0_pbe" in only:
+        # the same SCF with the GGA-PBE (restated, pinned to the reference's
+        # mSetPotentialVxc by the gga_pbe case)
+        inp = scf_inputs()
+        r = S.scf(inp["grid"], inp["pos"], inp["sp"], SCF_C0["nb"], SCF_C0["n_el"], inp["X"], xc="pbe",
+                  **SCF_C0["params"])
+        np.savez_compressed(os.path.join(HERE, "scf_c0_pbe.npz"), energies=r["energies"], rq=r["rq"], occ=r["occ"],
+                            rho=r["rho"], converged=np.array(r["converged"]),
+                            checksum=np.array([float(np.sum(v)) for v in inp["checked"]]))
+        print("scf_c0_pbe", r["steps"], r["energies"][-1])
     if only and "scf_c0" not in only:
         return
     # SCF of config 0: the oracle loop (reference LOBPCG + restated SCF pieces)
