@@ -787,6 +787,9 @@ def main():
     ap.add_argument("--only-hpsi", action="store_true",
                     help="time the device-resident H.psi only (no e2e, FFT, Gram, LOBPCG, SCF or CPU sections); "
                          "the profiler captures use it")
+    ap.add_argument("--only-lobpcg-mixed", action="store_true",
+                    help="time two steady mixed-precision LOBPCG iterations only, after one first-time and one "
+                         "steady call (the profiler captures use it)")
     ap.add_argument("--only-fft", action="store_true",
                     help="time the device-resident FFT-kinetic H.psi only (the profiler captures use it)")
     ap.add_argument("--bands", type=int, default=NB,
@@ -857,6 +860,32 @@ def main():
         for _ in range(20):
             H.apply(psi, hpsi)
         torch.cuda.synchronize()
+
+    if args.only_lobpcg_mixed:
+        clocks.stop()
+        dV = H_GRID ** 3
+        X = torch.linalg.qr(psi.t())[0].t().contiguous() / math.sqrt(dV)
+        es = qsb.EigenSolver(N, NB, False, "mixed")
+        es.set_hamiltonian(H)
+        keep = torch.zeros_like(X)
+        ev = np.zeros(NB)
+        es.lobpcg_d(dV, NB, 1, ev, X, keep, True)
+        es.lobpcg_d(dV, NB, 1, ev, X, keep, False)
+        torch.cuda.synchronize()
+        l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0.record(stream)
+        es.lobpcg_d(dV, NB, 2, ev, X, keep, False)
+        l1.record(stream)
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"metric": "mixed LOBPCG iteration", "bands_per_gpu": NB,
+                              "ms_per_iteration": l0.elapsed_time(l1) / 2,
+                              "note": "--only-lobpcg-mixed: two steady iterations"}))
+        es.close()
+        H.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
 
     if args.only_fft:
         clocks.stop()
