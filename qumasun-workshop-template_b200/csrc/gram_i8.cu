@@ -347,10 +347,8 @@ constexpr int RT_K = 128;   // K per stage (rows of the MN-major A tile, bytes o
 constexpr int RT_N = 64;    // output columns per CTA (UMMA N)
 constexpr int RT_TILE_B = RT_N * RT_K;          // 8 KB per slice of C'
 constexpr int RT_STAGE_BYTES = 4 * OZ_TILE + 4 * RT_TILE_B;   // four slices of U, four of C'
-// One stage per CTA so that two CTAs share an SM (2 x 256 TMEM columns): each
-// CTA's tile is short (K <= a few hundred), so the overlap that matters is one
-// CTA's loads under the other's MMAs and epilogue.
-constexpr int RT_STAGES = 1;
+// Two stages of the ring of the persistent kernel (one CTA per SM).
+constexpr int RT_STAGES = 2;
 constexpr size_t RT_SMEM = (size_t)RT_STAGES * RT_STAGE_BYTES + 1024 + 256;
 static_assert(RT_SMEM <= 232448, "rotation stages must fit the 227 KB of shared memory per CTA");
 
@@ -417,39 +415,56 @@ __global__ void rot_coef_split_kernel(const double* __restrict__ C, int ldc, int
     }
 }
 
-// One CTA: rows [mt*128, +128) of OUT, columns [nt*64, +64), all of K.
-__global__ void __launch_bounds__(OZ_THREADS, 1)
+// Persistent rotation kernel: one CTA per SM walks the output tiles (rows
+// [mt*128, +128) of OUT x columns [nt*64, +64), tile t = mt * ntn + nt, CTAs
+// take t = blockIdx.x, blockIdx.x + gridDim.x, ...), all of K per tile.
+// Warp 0 lane 0 streams the K stages of every tile into a 2-stage shared
+// ring, warp 1 lane 0 issues the ten MMAs per 32-K step into one of two TMEM
+// accumulator sets (4 x 64 columns each, 512 columns in all), and warps 2-9
+// (two per TMEM lane quarter, 32 output columns each) read a finished set,
+// store it and hand it back -- so the loads of the next
+// stages, the MMAs of the next tile and the epilogue of the last one overlap.
+// Every wait is bounded: one that runs out sets the device error word and the
+// abort flag; all roles then stop, in-flight copies are drained and TMEM is
+// freed.
+constexpr int RT_THREADS = 320;   // producer warp, MMA warp, eight epilogue warps
+
+__global__ void __launch_bounds__(RT_THREADS, 1)
 rot_i8_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ CUtensorMap mA1,
               const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mA3,
               const __grid_constant__ CUtensorMap mB0, const __grid_constant__ CUtensorMap mB1,
               const __grid_constant__ CUtensorMap mB2, const __grid_constant__ CUtensorMap mB3, int kstages,
-              int64_t N, int q, int ntn, const double* __restrict__ fscale, ColumnSet out, int* __restrict__ err) {
+              int64_t N, int q, int ntn, int ntiles, const double* __restrict__ fscale, ColumnSet out,
+              int* __restrict__ err) {
     extern __shared__ unsigned char rt_raw[];
     unsigned char* base = (unsigned char*)(((uintptr_t)rt_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* full = reinterpret_cast<uint64_t*>(base + (size_t)RT_STAGES * RT_STAGE_BYTES);
     uint64_t* empty = full + RT_STAGES;
-    uint64_t* done = empty + RT_STAGES;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    uint64_t* tfull = empty + RT_STAGES;      // accumulator set ready for the epilogue
+    uint64_t* tempty = tfull + 2;             // accumulator set read out
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tempty + 2);
     int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // the column tiles of one row tile are neighbours in launch order, so the
-    // row tile's slices of U come from DRAM once and from L2 for the others
-    const int mt = (int)(blockIdx.x / (unsigned)ntn), nt = (int)(blockIdx.x % (unsigned)ntn);
     const int nk = kstages;
+    // tiles of this CTA: t_j = blockIdx.x + j * gridDim.x, j < my_tiles
+    const int my_tiles = blockIdx.x < (unsigned)ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < RT_STAGES; ++s) {
-            bar_init(&full[s], 1);
-            bar_init(&empty[s], 1);
+        for (int st = 0; st < RT_STAGES; ++st) {
+            bar_init(&full[st], 1);
+            bar_init(&empty[st], 1);
         }
-        bar_init(done, 1);
+        for (int b = 0; b < 2; ++b) {
+            bar_init(&tfull[b], 1);
+            bar_init(&tempty[b], 8);
+        }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tmem_slot)),
-                     "r"(256)
+                     "r"(512)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -458,123 +473,164 @@ rot_i8_kernel(const __grid_constant__ CUtensorMap mA0, const __grid_constant__ C
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
-    int issued = 0;
+    int issued = 0;   // stages the producer issued (for the drain)
     if (warp == 0 && lane == 0) {
+        // ---------------- producer ----------------
         const CUtensorMap* amaps[4] = {&mA0, &mA1, &mA2, &mA3};
         const CUtensorMap* bmaps[4] = {&mB0, &mB1, &mB2, &mB3};
-        for (int it = 0; it < nk; ++it) {
-            const int s = it % RT_STAGES;
-            if (it >= RT_STAGES && !bar_wait(&empty[s], (uint32_t)(((it / RT_STAGES) - 1) & 1), OZ_WAIT_LIMIT)) {
-                atomicOr(err, ERR_GEMM_TIMEOUT);
-                atomicExch(abort_flag, 1);
-                break;
+        int g = 0;
+        for (int j = 0; j < my_tiles && !*(volatile int*)abort_flag; ++j) {
+            const int t = (int)blockIdx.x + j * (int)gridDim.x;
+            const int mt = t / ntn, nt = t - mt * ntn;
+            for (int it = 0; it < nk; ++it, ++g) {
+                const int st = g % RT_STAGES;
+                if (g >= RT_STAGES && !bar_wait(&empty[st], (uint32_t)(((g / RT_STAGES) - 1) & 1), OZ_WAIT_LIMIT)) {
+                    atomicOr(err, ERR_GEMM_TIMEOUT);
+                    atomicExch(abort_flag, 1);
+                    break;
+                }
+                if (*(volatile int*)abort_flag) break;
+                unsigned char* sp = base + (size_t)st * RT_STAGE_BYTES;
+                bar_expect_tx(&full[st], RT_STAGE_BYTES);
+                // A: box (128 grid points, 128 columns of U) at (mt*128, it*128); B: box (128 K, 64 columns of C')
+#pragma unroll
+                for (int k = 0; k < 4; ++k) tma_2d(sp + k * OZ_TILE, amaps[k], mt * OZ_M, it * RT_K, &full[st]);
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    tma_2d(sp + 4 * OZ_TILE + k * RT_TILE_B, bmaps[k], it * RT_K, nt * RT_N, &full[st]);
+                issued = g + 1;
             }
-            if (*(volatile int*)abort_flag) break;
-            unsigned char* st = base + (size_t)s * RT_STAGE_BYTES;
-            bar_expect_tx(&full[s], RT_STAGE_BYTES);
-            // A: box (128 grid points, 128 columns of U) at (mt*128, it*128); B: box (128 K, 64 columns of C')
-#pragma unroll
-            for (int k = 0; k < 4; ++k) tma_2d(st + k * OZ_TILE, amaps[k], mt * OZ_M, it * RT_K, &full[s]);
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                tma_2d(st + 4 * OZ_TILE + k * RT_TILE_B, bmaps[k], it * RT_K, nt * RT_N, &full[s]);
-            issued = it + 1;
         }
     } else if (warp == 1 && lane == 0) {
-        const uint32_t d0 = tmem, d1 = tmem + RT_N, d2 = tmem + 2 * RT_N, d3 = tmem + 3 * RT_N;
-        for (int it = 0; it < nk; ++it) {
-            const int s = it % RT_STAGES;
-            if (!bar_wait(&full[s], (uint32_t)((it / RT_STAGES) & 1), OZ_WAIT_LIMIT)) {
+        // ---------------- MMA issuer ----------------
+        int g = 0;
+        for (int j = 0; j < my_tiles && !*(volatile int*)abort_flag; ++j) {
+            const int ab = j & 1;
+            // the epilogue must have read this accumulator set (two tiles ago)
+            if (j >= 2 && !bar_wait(&tempty[ab], (uint32_t)(((j >> 1) - 1) & 1), OZ_WAIT_LIMIT)) {
                 atomicOr(err, ERR_GEMM_TIMEOUT);
                 atomicExch(abort_flag, 1);
                 break;
             }
-            if (*(volatile int*)abort_flag) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t st = su32(base + (size_t)s * RT_STAGE_BYTES);
-            uint32_t a[4], b[4];
+            const uint32_t d0 = tmem + (uint32_t)(ab * 4 * RT_N), d1 = d0 + RT_N, d2 = d0 + 2 * RT_N,
+                           d3 = d0 + 3 * RT_N;
+            bool ok = true;
+            for (int it = 0; it < nk; ++it, ++g) {
+                const int st = g % RT_STAGES;
+                if (!bar_wait(&full[st], (uint32_t)((g / RT_STAGES) & 1), OZ_WAIT_LIMIT)) {
+                    atomicOr(err, ERR_GEMM_TIMEOUT);
+                    atomicExch(abort_flag, 1);
+                    ok = false;
+                    break;
+                }
+                if (*(volatile int*)abort_flag) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t sa = su32(base + (size_t)st * RT_STAGE_BYTES);
+                uint32_t a[4], b[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                a[k] = st + k * OZ_TILE;
-                b[k] = st + 4 * OZ_TILE + k * RT_TILE_B;
-            }
+                for (int k = 0; k < 4; ++k) {
+                    a[k] = sa + k * OZ_TILE;
+                    b[k] = sa + 4 * OZ_TILE + k * RT_TILE_B;
+                }
 #pragma unroll
-            for (int kk = 0; kk < RT_K / 32; ++kk) {
-                const uint32_t ao = kk * 4096;   // 32 K rows of 128 bytes (four 8-row atoms)
-                const uint32_t bo = kk * 32;     // 32 int8 along the K-major row
-                const uint32_t acc = (it > 0 || kk > 0) ? 1u : 0u;
+                for (int kk = 0; kk < RT_K / 32; ++kk) {
+                    const uint32_t ao = kk * 4096;   // 32 K rows of 128 bytes (four 8-row atoms)
+                    const uint32_t bo = kk * 32;     // 32 int8 along the K-major row
+                    const uint32_t acc = (it > 0 || kk > 0) ? 1u : 0u;
 #define RT_MMA(D, I, J, ACC) umma_i8_mn(D, sw128_mnmajor_desc(a[I] + ao), sw128_kmajor_desc(b[J] + bo), ACC)
-                RT_MMA(d0, 0, 0, acc);
-                RT_MMA(d1, 0, 1, acc);
-                RT_MMA(d1, 1, 0, 1u);
-                RT_MMA(d2, 0, 2, acc);
-                RT_MMA(d2, 1, 1, 1u);
-                RT_MMA(d2, 2, 0, 1u);
-                RT_MMA(d3, 0, 3, acc);
-                RT_MMA(d3, 1, 2, 1u);
-                RT_MMA(d3, 2, 1, 1u);
-                RT_MMA(d3, 3, 0, 1u);
+                    RT_MMA(d0, 0, 0, acc);
+                    RT_MMA(d1, 0, 1, acc);
+                    RT_MMA(d1, 1, 0, 1u);
+                    RT_MMA(d2, 0, 2, acc);
+                    RT_MMA(d2, 1, 1, 1u);
+                    RT_MMA(d2, 2, 0, 1u);
+                    RT_MMA(d3, 0, 3, acc);
+                    RT_MMA(d3, 1, 2, 1u);
+                    RT_MMA(d3, 2, 1, 1u);
+                    RT_MMA(d3, 3, 0, 1u);
 #undef RT_MMA
+                }
+                umma_commit(&empty[st]);
             }
-            umma_commit(&empty[s]);
+            if (!ok) break;
+            umma_commit(&tfull[ab]);
         }
-        umma_commit(done);
+    } else if (warp >= 2) {
+        // ---------------- epilogue (warps 2-9: TMEM lanes 32 (warp % 4) ..., column half (warp - 2) / 4) ----------------
+        const int quarter = warp & 3;
+        const int chalf = (warp - 2) >> 2;
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        for (int j = 0; j < my_tiles; ++j) {
+            const int ab = j & 1;
+            const bool ok = bar_wait(&tfull[ab], (uint32_t)((j >> 1) & 1), OZ_WAIT_LIMIT);
+            if (!ok) {
+                atomicOr(err, ERR_GEMM_TIMEOUT);
+                atomicExch(abort_flag, 1);
+            }
+            // the TMEM loads below are warp-collective: stop as one warp
+            if (__any_sync(0xffffffffu, !ok || *(volatile int*)abort_flag)) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int t = (int)blockIdx.x + j * (int)gridDim.x;
+            const int mt = t / ntn, nt = t - mt * ntn;
+            const int64_t gp = (int64_t)mt * OZ_M + quarter * 32 + lane;   // grid point of this TMEM lane
+            const uint32_t dset = tmem + lane_base + (uint32_t)(ab * 4 * RT_N);
+            {
+                const int c0 = chalf * 32;
+                uint32_t r0[32], r1[32], r2[32], r3[32];
+                tmem_ld32(dset + (uint32_t)c0, r0);
+                tmem_ld32(dset + (uint32_t)(RT_N + c0), r1);
+                tmem_ld32(dset + (uint32_t)(2 * RT_N + c0), r2);
+                tmem_ld32(dset + (uint32_t)(3 * RT_N + c0), r3);
+                if (gp < N && nk > 0) {
+                    const int j0 = nt * RT_N + c0;
+                    // one destination lookup for the chunk when its 32 columns lie in one array
+                    const void* bp;
+                    const int local0 = column_of(out, j0, &bp);
+                    const void* bl;
+                    const int local31 = j0 + 31 < q ? column_of(out, j0 + 31, &bl) : -1;
+                    const bool one = local31 == local0 + 31 && bl == bp;
+                    float* dst0 = (float*)bp + (size_t)local0 * N + gp;
+#pragma unroll
+                    for (int jj = 0; jj < 32; ++jj) {
+                        const int col = j0 + jj;
+                        if (col >= q) continue;
+                        float* dst;
+                        if (one) {
+                            dst = dst0 + (size_t)jj * N;
+                        } else {
+                            const void* bj;
+                            const int lj = column_of(out, col, &bj);
+                            dst = (float*)bj + (size_t)lj * N + gp;
+                        }
+                        // D0 + D1 2^-7 + D2 2^-14 + D3 2^-21 summed exactly as an integer in units of
+                        // 2^-21, one rounding to FP32, then the column's power-of-two scale (exact)
+                        const long long iv = (long long)(int)r0[jj] * 2097152LL + (long long)(int)r1[jj] * 16384LL +
+                                             (long long)(int)r2[jj] * 128LL + (long long)(int)r3[jj];
+                        *dst = (float)iv * (float)(__ldg(fscale + col) * 0x1p-21);
+                    }
+                }
+            }
+            // this warp is done with the set: hand it back to the MMA issuer
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(&tempty[ab])) : "memory");
+        }
     }
     __syncwarp();
-
-    bool ok = bar_wait(done, 0, OZ_WAIT_LIMIT);
-    if (!ok) {
-        atomicOr(err, ERR_GEMM_TIMEOUT);
-        atomicExch(abort_flag, 1);
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const int64_t g = (int64_t)mt * OZ_M + warp * 32 + lane;   // grid point of this TMEM lane
-    const bool have = ok && nk > 0 && !*(volatile int*)abort_flag;
-    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-#pragma unroll 1
-    for (int c0 = 0; c0 < RT_N; c0 += 32) {
-        uint32_t r0[32], r1[32], r2[32], r3[32];
-        tmem_ld32(tmem + lane_base + (uint32_t)c0, r0);
-        tmem_ld32(tmem + lane_base + (uint32_t)(RT_N + c0), r1);
-        tmem_ld32(tmem + lane_base + (uint32_t)(2 * RT_N + c0), r2);
-        tmem_ld32(tmem + lane_base + (uint32_t)(3 * RT_N + c0), r3);
-        if (have && g < N) {
-            const int j0 = nt * RT_N + c0;
-            // one destination lookup for the chunk when its 32 columns lie in one array
-            const void* bp;
-            const int local0 = column_of(out, j0, &bp);
-            const void* bl;
-            const int local31 = j0 + 31 < q ? column_of(out, j0 + 31, &bl) : -1;
-            const bool one = local31 == local0 + 31 && bl == bp;
-            float* dst0 = (float*)bp + (size_t)local0 * N + g;
-#pragma unroll
-            for (int jj = 0; jj < 32; ++jj) {
-                const int j = j0 + jj;
-                if (j >= q) continue;
-                float* dst;
-                if (one) {
-                    dst = dst0 + (size_t)jj * N;
-                } else {
-                    const void* bj;
-                    const int lj = column_of(out, j, &bj);
-                    dst = (float*)bj + (size_t)lj * N + g;
-                }
-                const double v = (double)(int)r0[jj] + (double)(int)r1[jj] * 0x1p-7 +
-                                 (double)(int)r2[jj] * 0x1p-14 + (double)(int)r3[jj] * 0x1p-21;
-                *dst = (float)(v * __ldg(fscale + j));
-            }
-        }
-    }
-
     __syncthreads();
     if (threadIdx.x == 0 && *(volatile int*)abort_flag) {
-        for (int it = max(0, issued - RT_STAGES); it < issued; ++it)
-            (void)bar_wait(&full[it % RT_STAGES], (uint32_t)((it / RT_STAGES) & 1), OZ_DRAIN_LIMIT);
+        // copies in flight must land before the CTA may exit
+        for (int g = max(0, issued - RT_STAGES); g < issued; ++g)
+            (void)bar_wait(&full[g % RT_STAGES], (uint32_t)((g / RT_STAGES) & 1), OZ_DRAIN_LIMIT);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
     }
 }
 
@@ -734,11 +790,14 @@ qsb_status ozaki_rotate(int64_t N, const void* Usplit, int K, const double* C, i
             return fail(QSB_ERR_CUDA, "ozaki_rotate: tensor map encoding failed");
     QSB_CUDA_TRY(cudaFuncSetAttribute(rot_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RT_SMEM));
     const int ntn = (q + RT_N - 1) / RT_N;
-    const long long ctas = (long long)((N + OZ_M - 1) / OZ_M) * ntn;
-    if (ctas > 0x7fffffffLL) return fail(QSB_ERR_INVALID, "ozaki_rotate: grid too large");
-    rot_i8_kernel<<<(unsigned)ctas, OZ_THREADS, RT_SMEM, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7],
-                                                              kpad / RT_K, N, q, ntn, fscale, out,
-                                                              device_error_word());
+    const long long tiles = (long long)((N + OZ_M - 1) / OZ_M) * ntn;
+    if (tiles > 0x7fffffffLL) return fail(QSB_ERR_INVALID, "ozaki_rotate: too many tiles");
+    int dev = 0, sms = 148;
+    QSB_CUDA_TRY(cudaGetDevice(&dev));
+    QSB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int ctas = (int)std::min<long long>(tiles, (long long)sms);
+    rot_i8_kernel<<<ctas, RT_THREADS, RT_SMEM, s>>>(m[0], m[1], m[2], m[3], m[4], m[5], m[6], m[7], kpad / RT_K, N, q,
+                                                    ntn, (int)tiles, fscale, out, device_error_word());
     QSB_CUDA_TRY(cudaGetLastError());
     return QSB_OK;
 }
