@@ -1,7 +1,7 @@
 /*
  * oracle/ref_fft.cpp -- extern "C" entries around the REFERENCE's own
- * QUMASUN_BASE1 object (its FFT-kinetic Hamiltonian and its GGA-PBE
- * exchange-correlation), compiled in place from the reference's source/
+ * QUMASUN_BASE1 object (its FFT-kinetic Hamiltonian, its GGA-PBE
+ * exchange-correlation and its Hartree potential), compiled in place from the reference's source/
  * directory (never copied) into oracle/_ref/libqsref_fft.so.  Test
  * infrastructure only.
  *
@@ -48,6 +48,16 @@ public:
         for (size_t i = 0; i < N; ++i) vxc[i] = ml_Vx[i] + ml_Vc[i];
         *e_x = m_E_x;
         *e_c = m_E_c;
+    }
+
+    // the reference's Hartree potential of a density (mSetPotentialVhart)
+    void Hartree(const double* rho, double* vh) {
+        const size_t N = (size_t)m_size_3d;
+        const size_t hr = (size_t)m_HR_ratio_x * m_HR_ratio_y * m_HR_ratio_z;
+        mInitializeWorkBuffer(16 * N * hr + 64);
+        for (size_t i = 0; i < N; ++i) ml_rho[i] = rho[i];
+        mSetPotentialVhart();
+        for (size_t i = 0; i < N; ++i) vh[i] = ml_Vhart[i];
     }
 
     // H psi of nb SoA bands (band b: re at 2bN, im at (2b+1)N)
@@ -120,6 +130,31 @@ int qsref_gga_pbe(int nx, int ny, int nz, double lx, double ly, double lz, const
     const int ddm[4] = {1, 1, 1, 1};
     RefFFTHamiltonian H(in, ddm);
     H.GgaPbe(rho, vxc, &e_xc[0], &e_xc[1]);
+    return 0;
+}
+
+/* The reference's Hartree potential V_H of rho (QUMASUN_BASE1::mSetPotentialVhart,
+ * source/qumasun_base1.potential.h:32-100: the Poisson solve of
+ * mPoissonDDMFFT_Upconvert on the high-resolution grid, then DownConvert_Realspace),
+ * on an nx x ny x nz box of sides (lx, ly, lz) with the high-resolution ratio hr. */
+int qsref_hartree(int nx, int ny, int nz, double lx, double ly, double lz, int hr, const double* rho, double* vh) {
+    if (nx < 1 || ny < 1 || nz < 1 || hr < 1 || !rho || !vh) return 1;
+    QUMASUN::Input in{};
+    in.hamiltonian_type = QUMASUN::HAMILTONIAN::KohnSham_PP;
+    in.grid_size[0] = nx;
+    in.grid_size[1] = ny;
+    in.grid_size[2] = nz;
+    std::memset(in.box_axis, 0, sizeof(in.box_axis));
+    in.box_axis[0] = lx;
+    in.box_axis[4] = ly;
+    in.box_axis[8] = lz;
+    in.num_solutions = 1;
+    in.num_nuclei = 0;
+    in.HR_ratio = hr;
+    in.test_algorithm_Laplacian = 1;
+    const int ddm[4] = {1, 1, 1, 1};
+    RefFFTHamiltonian H(in, ddm);
+    H.Hartree(rho, vh);
     return 0;
 }
 

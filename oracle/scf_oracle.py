@@ -161,6 +161,21 @@ def ref_gga_pbe(grid, rho):
     return vxc, float(e[0]), float(e[1])
 
 
+def ref_hartree(grid, rho, hr=2):
+    """The reference's own Hartree potential (QUMASUN_BASE1::mSetPotentialVhart on its
+    object in oracle/_ref/libqsref_fft.so; high-resolution ratio hr, the
+    reference's default 2)."""
+    nx, ny, nz, dx, dy, dz = grid
+    lib = ctypes.CDLL(O.LIB_REF_FFT)
+    rho = np.ascontiguousarray(rho, np.float64)
+    vh = np.zeros_like(rho)
+    dp = ctypes.POINTER(ctypes.c_double)
+    rc = lib.qsref_hartree(nx, ny, nz, ctypes.c_double(nx * dx), ctypes.c_double(ny * dy), ctypes.c_double(nz * dz),
+                           int(hr), rho.ctypes.data_as(dp), vh.ctypes.data_as(dp))
+    assert rc == 0
+    return vh
+
+
 def ref_lda_pz(rho):
     """The reference's Calc_XC_LDA, compiled from its sources."""
     lib = O.ref_lib()

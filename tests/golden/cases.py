@@ -114,6 +114,25 @@ def _gga_oracle(inp):
     return np.concatenate([v, [ex, ec]])
 
 
+HARTREE_ODD = (15, 12, 9, 0.4, 0.5, 0.6)
+
+
+def _hartree_inputs(grid, seed):
+    nx, ny, nz = grid[:3]
+    rho = gga_density(grid) if seed is None else np.random.default_rng(seed).uniform(0.0, 1.0, nx * ny * nz)
+    return dict(grid=grid, rho=rho, checked=[rho])
+
+
+def _hartree_ref(inp):
+    import scf_oracle as S
+    return S.ref_hartree(inp["grid"], inp["rho"], 2)
+
+
+def _hartree_oracle(inp):
+    import scf_oracle as S
+    return S.hartree(inp["rho"], inp["grid"])[0]
+
+
 # the FFT-kinetic cases: k-point sampling and index of each (the reference's k)
 FFT_GRID_EVEN = (24, 20, 16, 0.25, 0.3, 0.375)
 FFT_GRID_ODD = (15, 12, 9, 0.4, 0.5, 0.6)
@@ -156,6 +175,11 @@ CASES = {
                              oracle=lambda i: _fft_oracle(i, True, *FFT_KPT["ham_fft_kpt_even"])),
     # GGA-PBE exchange-correlation: V_xc on the grid, then E_x, E_c (the reference's own mSetPotentialVxc)
     "gga_pbe": dict(inputs=_gga_inputs, reference=_gga_ref, oracle=_gga_oracle),
+    # Hartree potential: the reference's mSetPotentialVhart (Poisson on its 2x high-resolution grid)
+    "hartree_even": dict(inputs=lambda: _hartree_inputs(GGA_GRID, None), reference=_hartree_ref,
+                         oracle=_hartree_oracle),
+    "hartree_odd": dict(inputs=lambda: _hartree_inputs(HARTREE_ODD, 13), reference=_hartree_ref,
+                        oracle=_hartree_oracle),
     "ham_fft_kpt_odd": dict(inputs=lambda: _fft_inputs(FFT_GRID_ODD, 9, 2, True),
                             reference=lambda i: _fft_ref(i, True, *FFT_KPT["ham_fft_kpt_odd"]),
                             oracle=lambda i: _fft_oracle(i, True, *FFT_KPT["ham_fft_kpt_odd"])),
