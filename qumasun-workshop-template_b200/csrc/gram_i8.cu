@@ -109,6 +109,8 @@ __global__ void column_absmax_kernel(ColumnSet src, int64_t N, unsigned long lon
     const bool vec = ((uintptr_t)s % 16) == 0;
     double m = 0.0;
     const int64_t n4 = (N + 3) / 4;
+    // unrolled so that several 16-byte loads per thread are in flight
+#pragma unroll 4
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += (int64_t)gridDim.x * blockDim.x) {
         double v[4];
         load4<T>(s, 4 * q, N, vec, v);
@@ -147,6 +149,7 @@ __global__ void slice_kernel(ColumnSet src, int64_t N, int64_t ldk, const unsign
     int8_t* o2 = o0 + 2 * slice_stride;
     int8_t* o3 = o0 + 3 * slice_stride;
     const int64_t n4 = ldk / 4;
+#pragma unroll 4
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = 4 * q;
         double v[4];
